@@ -1,0 +1,428 @@
+#!/usr/bin/env python
+"""Benchmark of the tomocupy_b200 reconstruction hot path.
+
+Workload (production configuration): 2048 rows x 1500 angles over [0, pi) x
+2048 columns of uint16 projections from a seeded synthetic ellipsoid phantom
+(Poisson noise, 10 darks, 10 flats; the reference's APS datasets are not
+available), dark/flat -> -log -> Shepp filter -> fourierrec, producing a
+2048^3 float32 volume in device memory.  One step = the whole volume.
+
+  value : GUPS (voxel*angle updates per second, n^2 * nz * nproj / t) with
+          the frames already resident in HBM (12.6 GB input, larger than L2,
+          so no flush is needed between steps).
+  e2e   : the same metric through the public driver GPURec.recon_all with
+          pinned HOST input and output (H2D of the frames and D2H of the
+          volume inside the timed region).
+  roofline : the dominant native kernel, timed with CUDA events recorded by
+          the library around each launch on its stream.
+  cpu_baseline : the NumPy port of the same steps on this host's cores,
+          on a bounded sample (one slice pair), scaled to GUPS.
+
+``--impl reference`` times the reference's own CUDA operators (built from the
+reference sources into oracle/_ref) behind a torch restatement of its glue,
+on the same workload and metric (a bounded slab per step).
+
+N > 1 (torchrun): every rank reconstructs its own full volume (independent
+datasets, no collective on the data path): weak scaling; NCCL is used only
+for the barrier and the max-over-ranks of the step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# algorithmic bytes per launch of each native stage (compulsory HBM traffic)
+def stage_bytes(stage, n, nproj, ncz):
+    ne = 4 * n
+    pairs = ncz // 2
+    table = {
+        "prep_rows": ncz * nproj * n * (2 + 4),
+        "filter_mulw": ncz * nproj * (ne // 2 + 1) * 16,
+        "fr_pack": ncz * nproj * n * 4 + pairs * nproj * n * 8,
+        "fr_gather": pairs * (nproj * n * 8 + (2 * n) ** 2 * 8),
+        "fr_deapod": pairs * (n * n * 8 + 2 * n * n * 4),
+        "linerec": ncz * (nproj * n * 4 + n * n * 8),
+    }
+    return table.get(stage)
+
+
+def setup_dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier_max(t_ms, ws):
+    import torch
+    if ws == 1:
+        return t_ms
+    import torch.distributed as dist
+    x = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def barrier(ws):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def make_data(a, device):
+    from tomocupy_b200 import synthetic
+    return synthetic.make_dataset(a.nproj, a.nz, a.n, seed=a.seed, device=device,
+                                  block=32)
+
+
+def cpu_baseline(a, data_cpu, dark, flat, theta):
+    """NumPy port on the host cores: one slice pair through prep + filter + fourierrec."""
+    from oracle import np_tomo
+    z0 = a.nz // 2
+    d = data_cpu[:, z0:z0 + 2]
+    t0 = time.perf_counter()
+    sino = np_tomo.minus_log(np_tomo.darkflat(d, dark[:, z0:z0 + 2], flat[:, z0:z0 + 2]))
+    sino = np.ascontiguousarray(sino.transpose(1, 0, 2))
+    wf = np_tomo.calc_filter(4 * a.n, a.filter)
+    t1 = time.perf_counter()  # filter spectrum construction is setup, not timed
+    filt = np_tomo.fbp_filter_center(sino, wf, a.n / 2, 0.0)
+    np_tomo.fourierrec(filt, theta)
+    t2 = time.perf_counter()
+    secs = (t1 - t0) + (t2 - t1)
+    gups = a.n * a.n * 2 * a.nproj / secs / 1e9
+    return {"value": gups, "unit": "GUPS", "cores": np_tomo.WORKERS, "kind": "port",
+            "sample": f"1 slice pair of the {a.n}x{a.nproj} geometry (prep+filter+fourierrec, "
+                      f"NumPy/scipy.fft float32, workers={np_tomo.WORKERS}), {secs:.1f} s",
+            "seconds": secs}
+
+
+def run_ours(a, ws, rank, local):
+    import torch
+    from tomocupy_b200 import _lib, global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.processing.proc_functions import darkflat_stats
+    from tomocupy_b200.rec import GPURec
+
+    dev = torch.device("cuda", local)
+    t_gen = time.perf_counter()
+    data, dark, flat, theta, _ = make_data(a, dev)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] generated {tuple(data.shape)} in {time.perf_counter() - t_gen:.1f} s")
+    global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
+                      nsino_per_chunk=a.ncz)
+    reader = ArrayReader(data, dark, flat, theta=theta)
+    writer = ArrayWriter(device=dev)
+    rec = GPURec(reader, writer, device=dev)
+    dark0, flat0, _ = darkflat_stats(dark, flat)
+    out = torch.empty((params.nz, params.n, params.n), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    for _ in range(a.warmup):
+        rec.recon_device(data, dark0, flat0, out)
+    barrier(ws)
+    _lib.profile_enable(True)
+    l0 = _lib.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(ws)
+        ev0.record(stream)
+        for _ in range(a.steps):
+            rec.recon_device(data, dark0, flat0, out)
+        ev1.record(stream)
+        barrier(ws)
+    launches = _lib.launch_count() - l0
+    stages = _lib.profile_report()
+    _lib.profile_enable(False)
+    ms_total = barrier_max(ev0.elapsed_time(ev1), ws)
+    ms_step = ms_total / a.steps
+    vox = float(a.n) ** 2 * a.nz * a.nproj
+    value = ws * vox / (ms_step / 1e3) / 1e9
+    slices_s = ws * a.nz / (ms_step / 1e3)
+
+    # dominant native stage and its roofline
+    peaks, peaks_kind = load_peaks()
+    own = {k: v for k, v in stages.items() if stage_bytes(k, a.n, a.nproj, a.ncz) is not None}
+    dom = max(own, key=lambda k: own[k]["ms"]) if own else None
+    roofline = None
+    if dom:
+        per_launch_ms = own[dom]["ms"] / own[dom]["count"]
+        algo = stage_bytes(dom, a.n, a.nproj, a.ncz)
+        achieved = algo / (per_launch_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                    "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": round(achieved / peaks["hbm_gbs"], 4),
+                    "traffic": None, "algorithmic_bytes_per_launch": algo,
+                    "ms_per_launch": round(per_launch_ms, 4),
+                    "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                    if peaks_kind == "measured" else "fallback 6.65 TB/s"}
+    clocks = clk.summary()
+
+    # ---------------- e2e through the public driver with host buffers
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, data, dark, flat, theta, dev, ws, rank)
+
+    base = None
+    if rank == 0 and ws == 1 and not a.no_cpu:
+        dcpu, dkc, flc = data.cpu().numpy(), dark.cpu().numpy(), flat.cpu().numpy()
+        base = cpu_baseline(a, dcpu, dkc, flc, theta)
+
+    if rank == 0:
+        line = {
+            "metric": f"GUPS @{a.n}^2x{a.nproj} ({a.algorithm} fp32 pipeline, 1 GPU rate)",
+            "value": round(value, 2), "unit": "GUPS", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{a.nz} rows x {a.nproj} angles x {a.n} cols uint16 -> "
+                                   f"{a.nz}x{a.n}^2 f32 volume; dark/flat, -log, {a.filter} "
+                                   f"filter, {a.algorithm}; ring removal off",
+                       "n": a.n, "nproj": a.nproj, "nz": a.nz, "ncz": a.ncz,
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "inputs (12.6 GB frames) larger than L2; no flush"},
+            "slices_per_s": round(slices_s, 1),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": base,
+            "clocks": clocks, "gpu_launches": launches,
+            "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in stages.items()},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(a, data, dark, flat, theta, dev, ws, rank):
+    import torch
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    avail = 0
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                avail = int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    full_bytes = data.numel() * 2 + a.nz * a.n * a.n * 4
+    nz_e2e = a.nz if (avail > 3 * full_bytes * ws) else min(a.nz, a.e2e_slab)
+    nz_e2e -= nz_e2e % a.ncz
+    d_host = data[:, :nz_e2e].cpu().pin_memory()
+    dk_host = dark[:, :nz_e2e].cpu().pin_memory()
+    fl_host = flat[:, :nz_e2e].cpu().pin_memory()
+    global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
+                      nsino_per_chunk=a.ncz)
+    reader = ArrayReader(d_host, dk_host, fl_host, theta=theta)
+    writer = ArrayWriter(device="cpu", pin=True)
+    rec = GPURec(reader, writer, device=dev)
+    for _ in range(max(1, min(a.warmup, 2))):
+        rec.recon_all()
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(a.steps):
+        rec.recon_all()  # ends with a device synchronize
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / a.steps
+    ms = barrier_max(ev0.elapsed_time(ev1) / a.steps, ws)
+    vox = float(a.n) ** 2 * nz_e2e * a.nproj
+    h2d = d_host.numel() * 2 + dk_host.numel() * 2 + fl_host.numel() * 2
+    d2h = nz_e2e * a.n * a.n * 4
+    return {"value": round(ws * vox / (ms / 1e3) / 1e9, 2), "unit": "GUPS",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "rows": nz_e2e, "ms_per_step": round(ms, 2), "wall_ms_per_step": round(wall * 1e3, 2),
+            "api": "GPURec.recon_all (pinned host frames -> pinned host volume)"}
+
+
+def run_reference(a, ws, rank, local):
+    """The reference's CUDA operators (oracle/_ref) behind its restated glue."""
+    import torch
+    if rank != 0:
+        return
+    from oracle import np_tomo, refglue
+    if not refglue.available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return
+    dev = torch.device("cuda", local)
+    rows = min(a.nz, a.ref_rows)
+    aa = argparse.Namespace(**vars(a))
+    aa.nz = rows
+    data, dark, flat, theta, _ = make_data(aa, dev)
+    n, P, ncz = a.n, a.nproj, 8  # the reference default nsino_per_chunk
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, a.filter), device=dev)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=dev)
+    th = torch.as_tensor(theta, device=dev)
+    filt = refglue.RefFilter(ne, P, ncz)
+    if a.algorithm == "fourierrec":
+        op = refglue.RefFourierRec(n, P, ncz, th)
+    else:
+        op = refglue.RefLineRec(th, P, P, ncz, ncz, n)
+    out = torch.zeros((rows, n, n), dtype=torch.float32, device=dev)
+
+    def step():
+        for z0 in range(0, rows, ncz):
+            d = refglue.ref_darkflat_minus_log(data[:, z0:z0 + ncz], dark[:, z0:z0 + ncz],
+                                               flat[:, z0:z0 + ncz])
+            d = d.permute(1, 0, 2).contiguous()
+            d = refglue.ref_fbp_filter_center(filt, d, wf, t, n / 2, 0.0, n, ne)
+            op.backprojection(out[z0:z0 + ncz], d)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(a.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / a.steps
+    value = float(n) ** 2 * rows * P / (ms / 1e3) / 1e9
+    line = {"impl": "reference",
+            "metric": f"GUPS @{a.n}^2x{a.nproj} ({a.algorithm} fp32 pipeline, 1 GPU rate)",
+            "value": round(value, 2), "unit": "GUPS", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{rows}-row slab of the {a.nz} rows x {a.nproj} angles x "
+                                   f"{a.n} cols workload; dark/flat, -log, {a.filter}, "
+                                   f"{a.algorithm}", "n": n, "nproj": P, "rows_per_step": rows,
+                       "ncz": ncz},
+            "cpu_baseline": {"value": round(value, 2), "unit": "GUPS", "cores": 1,
+                             "kind": "reference",
+                             "sample": f"reference CUDA build (sources compiled for sm_100a) "
+                                       f"on the B200, {rows} rows per step, driven by 1 host "
+                                       f"thread; the reference has no CPU implementation"},
+            "e2e": {"value": round(value, 2), "unit": "GUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--nproj", type=int, default=1500)
+    ap.add_argument("--nz", type=int, default=2048)
+    ap.add_argument("--ncz", type=int, default=32)
+    ap.add_argument("--algorithm", default="fourierrec", choices=["fourierrec", "linerec"])
+    ap.add_argument("--filter", default="shepp")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--e2e-slab", type=int, default=512)
+    ap.add_argument("--ref-rows", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        log("note: warmup < 3 requested; using 3")
+        a.warmup = 3
+    ws, rank, local = setup_dist()
+    try:
+        if a.impl == "reference":
+            run_reference(a, ws, rank, local)
+        else:
+            run_ours(a, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

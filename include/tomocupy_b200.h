@@ -1,0 +1,165 @@
+/*
+ * tomocupy_b200 — C ABI of the B200-native tomographic reconstruction kernels.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*; NULL means the legacy default stream), enqueues its work
+ * asynchronously on that stream, and returns a tcb_status.  On a non-zero
+ * status tcb_last_error() returns a message for the calling thread.
+ *
+ * Operators mirror the reference's SWIG classes (src/cuda/*.i): an opaque
+ * handle replaces the C++ object, *_create replaces the constructor,
+ * *_destroy replaces free()/the destructor, and one function exists per
+ * method.  A precision argument (TCB_FLOAT32 / TCB_FLOAT16) replaces the
+ * reference's split into cfunc_X and cfunc_Xfp16 modules: FLOAT16 means fp16
+ * storage of the caller's buffers with fp32 arithmetic inside the kernels.
+ *
+ * Handles are not re-entrant across concurrently running streams (they own
+ * scratch memory), exactly like the reference objects.
+ */
+#ifndef TOMOCUPY_B200_H
+#define TOMOCUPY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TCB_OK = 0,
+  TCB_ERR_INVALID_ARGUMENT = 1,
+  TCB_ERR_CUDA = 2,
+  TCB_ERR_CUFFT = 3,
+  TCB_ERR_OUT_OF_MEMORY = 4,
+  TCB_ERR_NOT_SUPPORTED = 5,
+  TCB_ERR_FREED = 6
+} tcb_status;
+
+typedef enum { TCB_FLOAT32 = 0, TCB_FLOAT16 = 1 } tcb_precision;
+
+/* Element type of raw detector frames. */
+typedef enum { TCB_U8 = 0, TCB_U16 = 1, TCB_F32 = 2 } tcb_dtype;
+
+/* Message describing the last failure on this thread ("" if none). */
+const char *tcb_last_error(void);
+/* Library ABI version (major*100 + minor). */
+int tcb_version(void);
+
+/* Instrumentation (no counterpart in the reference, which has no profiling
+ * hooks).  tcb_profile_enable(1) clears and starts recording a CUDA event
+ * pair around every native stage launch (on the stream it is launched on);
+ * tcb_profile_report synchronises the recorded events and writes JSON
+ * {"stage": {"count": c, "ms": total}, ...} into buf.  tcb_launch_count
+ * returns the number of native kernel launches since process start (cuFFT
+ * launches are not counted). */
+int tcb_profile_enable(int on);
+int tcb_profile_report(char *buf, size_t len);
+int tcb_launch_count(uint64_t *out);
+
+/* Asynchronous 2D copy (host<->device or device<->device, direction inferred
+ * from the pointers): height rows of width_bytes, with row pitches in bytes.
+ * The chunk conveyor uses it to move [nproj, ncz, n] slabs of a
+ * [nproj, nz, n] stack without a host-side repack; it replaces the pinned
+ * staging copies of GPURec.recon_all (src/tomocupy/rec.py:184-195). */
+int tcb_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch,
+               size_t width_bytes, size_t height, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Pre-processing: dark/flat normalisation and -log.
+ * ------------------------------------------------------------------------ */
+
+/* Flat/dark reductions for one chunk of rows.
+ * Replaces the mean part of ProcFunctions.darkflat_correction
+ * (src/tomocupy/processing/proc_functions.py:55-74).
+ *   dark  [ndark, nz, n], flat [nflat, nz, n] of type in_dtype
+ *   dark0 [nz, n] fp32 = mean_k dark[k]
+ *   flat_linear == 0: flat0 [nz, n] fp32 = mean_k(flat[k]/bright_ratio)*(1+1e-5) - dark0
+ *   flat_linear != 0: flat0 = mean of flat[:nflat/2]/bright_ratio,
+ *                     flat1 = mean of flat[nflat/2+1:]/bright_ratio (unscaled;
+ *                     the per-angle blend happens in tcb_prep_rows). */
+int tcb_darkflat_stats(void *dark0, void *flat0, void *flat1, const void *dark,
+                       const void *flat, size_t ndark, size_t nflat, size_t nz,
+                       size_t n, int in_dtype, float bright_ratio, int flat_linear,
+                       void *stream);
+
+/* Prep flags. */
+#define TCB_PREP_DARKFLAT 1u   /* apply (x - dark0)/flat0                        */
+#define TCB_PREP_MINUS_LOG 2u  /* where(x<=0,1,x) -> -log -> nan_to_num(6,0,0)   */
+#define TCB_PREP_FLAT_LINEAR 4u /* flat0/flat1 are the two half-means            */
+#define TCB_PREP_EDGE_PAD 8u   /* replicate first/last column into the padding   */
+
+/* One fused pass over rows: reads input row (p, z) of a [nproj, nz, n]
+ * frame stack (in_dtype; TCB_F32 when the input is already normalised) and
+ * writes output row (z, p) in sinogram order:
+ *   out[z*out_zstride + (p+out_poff)*out_pstride + out_xoff + x]
+ * with the columns [0, out_xoff) and [out_xoff+n, out_width) filled with the
+ * edge values when TCB_PREP_EDGE_PAD is set.  in_zstride/in_pstride describe
+ * the input layout in elements.  Replaces darkflat_correction + minus_log +
+ * the swapaxes copy (rec.py:174) + the edge padding of fbp_filter_center
+ * (reconstruction/backproj_functions.py:93-109). */
+int tcb_prep_rows(float *out, const void *in, const float *dark0, const float *flat0,
+                  const float *flat1, size_t nproj, size_t nz, size_t n,
+                  size_t in_pstride, size_t in_zstride, int in_dtype,
+                  size_t out_zstride, size_t out_pstride, size_t out_poff,
+                  size_t out_xoff, size_t out_width, unsigned flags, void *stream);
+
+/* ------------------------------------------------------------------------
+ * FBP filter.  Replaces cfunc_filter (src/include/cfunc_filter.cuh:9-23,
+ * src/cuda/cfunc_filter.i:9-21): g real [nz, nproj, n] filtered in place
+ * with w complex [nz, n/2+1] (one spectrum per slice).
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_filter tcb_filter;
+int tcb_filter_create(tcb_filter **out, size_t nproj, size_t nz, size_t n,
+                      int precision);
+int tcb_filter_apply(tcb_filter *h, void *g, const void *w, void *stream);
+int tcb_filter_destroy(tcb_filter *h);
+
+/* ------------------------------------------------------------------------
+ * Fourier-gridding backprojector.  Replaces cfunc_fourierrec
+ * (src/include/cfunc_fourierrec.cuh:10-36, src/cuda/cfunc_fourierrec.i:9-21).
+ *   theta: device fp32 [nproj] (read during create only, as in the reference)
+ *   nz:    number of complex slice pairs
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_fourierrec tcb_fourierrec;
+int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t nz, size_t n,
+                          const float *theta, int precision);
+/* cfunc_fourierrec::backprojection: g complex [nz, nproj, n] (overwritten,
+ * as in the reference), f complex [nz, n, n]. */
+int tcb_fourierrec_backprojection(tcb_fourierrec *h, void *f, void *g, void *stream);
+/* Same reconstruction with the real/imaginary unpacking of
+ * FourierRec.backprojection (reconstruction/fourierrec.py:61-68) fused in:
+ * f real [2*nz, n, n] (slice k = real part of pair k, slice nz+k = imaginary). */
+int tcb_fourierrec_backprojection_slices(tcb_fourierrec *h, void *f, void *g,
+                                         void *stream);
+/* Pack 2*nz filtered real sinograms into nz complex pairs, cropping columns
+ * [xoff, xoff+n) from rows of length row_stride:
+ *   g[k, p, x] = src[k, p, xoff+x] + i*src[k+nz, p, xoff+x]
+ * (reconstruction/fourierrec.py:63-64 plus the crop of
+ * backproj_functions.py:107). */
+int tcb_fourierrec_pack(tcb_fourierrec *h, void *g, const void *src,
+                        size_t row_stride, size_t xoff, void *stream);
+int tcb_fourierrec_destroy(tcb_fourierrec *h);
+
+/* ------------------------------------------------------------------------
+ * Line backprojector.  Replaces cfunc_linerec
+ * (src/include/cfunc_linerec.cuh:9-23, src/cuda/cfunc_linerec.i:9-25).
+ * All methods accumulate into f [ncz, n, n]; g is [nz, ncproj, n].
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_linerec tcb_linerec;
+int tcb_linerec_create(tcb_linerec **out, size_t nproj, size_t nz, size_t n,
+                       size_t ncproj, size_t ncz, int precision);
+int tcb_linerec_backprojection(tcb_linerec *h, void *f, const void *g,
+                               const float *theta, float phi, int sz, void *stream);
+int tcb_linerec_backprojection_try(tcb_linerec *h, void *f, const void *g,
+                                   const float *theta, const float *sh, float phi,
+                                   int sz, void *stream);
+int tcb_linerec_backprojection_try_lamino(tcb_linerec *h, void *f, const void *g,
+                                          const float *theta, const float *phi,
+                                          int sz, void *stream);
+int tcb_linerec_destroy(tcb_linerec *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOMOCUPY_B200_H */

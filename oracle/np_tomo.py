@@ -1,0 +1,292 @@
+"""NumPy restatement of the reference reconstruction path (test oracle / CPU baseline).
+
+Every function cites the reference code it restates.  ``dtype`` selects the
+working precision: float32 reproduces the reference's arithmetic (with
+NumPy's cos/sin/exp standing in for CUDA intrinsics), float64 is the
+"accurate" oracle with the same algorithm and constants.  FFTs use
+scipy.fft (multi-threaded via ``workers``); cuFFT's unnormalised inverse is
+matched with ``norm="forward"``.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+import scipy.fft as sfft
+
+WORKERS = os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------
+# pre-processing (src/tomocupy/processing/proc_functions.py:55-83)
+# --------------------------------------------------------------------------
+def darkflat(data, dark, flat, bright_ratio=1.0):
+    """(data - mean(dark)) / (mean(flat/bright_ratio)*f32(1+1e-5) - mean(dark)), float32."""
+    dark0 = dark.astype(np.float32)
+    flat0 = flat.astype(np.float32)
+    flat0 = flat0 / np.float32(bright_ratio)
+    flat0 = np.mean(flat0, axis=0, dtype=np.float32)
+    dark0 = np.mean(dark0, axis=0, dtype=np.float32)
+    flat0 = flat0 * np.float32(1 + 1e-5)
+    flat0 = flat0 - dark0
+    return (data.astype(np.float32) - dark0) / flat0
+
+
+def darkflat_linear(data, dark, flat, bright_ratio=1.0):
+    """flat_linear variant (proc_functions.py:62-66): float64 blend across angles."""
+    nproj = data.shape[0]
+    flat0 = flat.astype(np.float32) / np.float32(bright_ratio)
+    p0 = np.mean(flat0[:flat0.shape[0] // 2], axis=0, dtype=np.float32)
+    p1 = np.mean(flat0[flat0.shape[0] // 2 + 1:], axis=0, dtype=np.float32)
+    v = np.linspace(0, 1, nproj)[..., np.newaxis, np.newaxis]
+    f = (1 - v) * p0 + v * p1
+    dark0 = np.mean(dark.astype(np.float32), axis=0, dtype=np.float32)
+    f = f * np.float64(np.float32(1 + 1e-5))
+    f = f - dark0
+    return ((data.astype(np.float32) - dark0) / f).astype(np.float32)
+
+
+def minus_log(x):
+    """where(x<=0 -> 1), -log, nan_to_num(nan=6, posinf=0, neginf=0)."""
+    x = np.where(x <= 0, np.float32(1.0), x).astype(np.float32)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r = -np.log(x)
+    return np.nan_to_num(r, nan=6.0, posinf=0.0, neginf=0.0).astype(np.float32)
+
+
+# --------------------------------------------------------------------------
+# filter (reconstruction/fbp_filter.py:60-118, backproj_functions.py:93-109)
+# --------------------------------------------------------------------------
+def wint(n, t):
+    N = len(t)
+    s = np.linspace(1e-40, 1, n)
+    iv = np.linalg.inv(np.exp(np.outer(np.arange(n), np.log(s))))
+    k = np.arange(1, n + 2)
+    u = np.diff(np.exp(np.outer(k, np.log(s))) * np.tile(1.0 / k[..., None], [1, n]))
+    W1 = iv @ u[1:n + 1, :]
+    W2 = iv @ u[0:n, :]
+    p = 1 / np.concatenate((np.arange(1, n), (n - 1) * np.ones(N - 2 * (n - 1) - 1),
+                            np.arange(n - 1, 0, -1)))
+    w = np.zeros(N)
+    for j in range(N - n + 1):
+        W = ((t[j + n - 1] - t[j]) ** 2) * W1 + (t[j + n - 1] - t[j]) * t[j] * W2
+        for kk in range(n - 1):
+            w[j:j + n] = w[j:j + n] + p[j + kk] * W[:, kk]
+    w[-40:] = (w[-40]) / (N - 40) * np.arange(N - 40, N)
+    return w
+
+
+def calc_filter(ne, name):
+    d = 0.5
+    t = np.arange(0, ne / 2 + 1) / ne
+    windows = {
+        "ramp": lambda: 1.0,
+        "shepp": lambda: np.sinc(t / (2 * d)) * (t / d <= 2),
+        "cosine": lambda: np.cos(np.pi * t / (2 * d)) * (t / d <= 1),
+        "cosine2": lambda: (np.cos(np.pi * t / (2 * d))) ** 2 * (t / d <= 1),
+        "hamming": lambda: (.54 + .46 * np.cos(np.pi * t / d)) * (t / d <= 1),
+        "hann": lambda: (1 + np.cos(np.pi * t / d)) / 2.0 * (t / d <= 1),
+        "parzen": lambda: pow(1 - t / d, 3) * (t / d <= 1),
+    }
+    if name == "none":
+        wfa = ne * 0.5 + t * 0
+        wfa[0] *= 2
+    else:
+        wfa = ne * 0.5 * wint(12, t) * windows[name]()
+    wfa = 2 * wfa * (wfa >= 0)
+    wfa[0] *= 2
+    return wfa.astype("float32") / ne
+
+
+def rfftfreq32(ne):
+    return (np.arange(0, ne // 2 + 1, dtype=np.float64) / ne).astype(np.float32)
+
+
+def phase_weights(wfilter, t, center, sht, n):
+    """complex64 [nz, ne/2+1] in the reference's float32 operation order."""
+    a = (np.float32(-center) + np.asarray(sht, np.float32)) + np.float32(n / 2)
+    ci = np.float32(-2.0) * np.float32(math.pi)
+    phase = (a * ci)[:, None] * t[None, :]
+    return (wfilter * np.cos(phase) + 1j * (wfilter * np.sin(phase))).astype(np.complex64)
+
+
+def filter_rows(rows, w, dtype=np.float32):
+    """cfunc_filter::filter: R2C (len ne) -> * w[z] -> C2R (unnormalised)."""
+    ne = rows.shape[-1]
+    cdt = np.complex64 if dtype == np.float32 else np.complex128
+    spec = sfft.rfft(rows.astype(dtype), axis=-1, workers=WORKERS).astype(cdt)
+    spec *= w.astype(cdt)[:, None, :]
+    return sfft.irfft(spec, n=ne, axis=-1, norm="forward", workers=WORKERS).astype(dtype)
+
+
+def fbp_filter_center(data, wfilter, center, sht, dtype=np.float32):
+    """Edge pad [nz, P, n] rows to ne, filter with the centred spectra, crop back."""
+    nz, nproj, n = data.shape
+    ne = (len(wfilter) - 1) * 2
+    pad = ne // 2 - n // 2
+    rows = np.empty((nz, nproj, ne), dtype=dtype)
+    rows[:, :, pad:pad + n] = data
+    rows[:, :, :pad] = data[:, :, :1]
+    rows[:, :, pad + n:] = data[:, :, -1:]
+    w = phase_weights(wfilter, rfftfreq32(ne), center, np.broadcast_to(sht, (nz,)), n)
+    if dtype == np.float64:
+        w = _phase_weights64(wfilter, ne, center, np.broadcast_to(sht, (nz,)), n)
+    out = filter_rows(rows, w, dtype)
+    return np.ascontiguousarray(out[:, :, pad:pad + n])
+
+
+def _phase_weights64(wfilter, ne, center, sht, n):
+    t = np.arange(0, ne // 2 + 1, dtype=np.float64) / ne
+    a = -center + np.asarray(sht, np.float64) + n / 2
+    return wfilter.astype(np.float64) * np.exp(-2j * np.pi * a[:, None] * t[None, :])
+
+
+# --------------------------------------------------------------------------
+# fourierrec (src/include/kernels_fourierrec.cuh, src/cuda/cfunc_fourierrec.cu)
+# --------------------------------------------------------------------------
+def fourierrec_constants(n):
+    eps = np.float32(1e-3)
+    mu = np.float32(-np.log(eps)) / np.float32(2 * n * n)
+    m = int(np.ceil(2 * n * 1 / np.float32(3.1415926535) *
+                    np.sqrt(-mu * np.log(eps) + (mu * n) * (mu * n) / 4)))
+    return mu, m
+
+
+def fourierrec_pairs(gc, theta, n, dtype=np.float32):
+    """cfunc_fourierrec::backprojection on complex pairs gc [nz, P, n] -> [nz, n, n]."""
+    cdt = np.complex64 if dtype == np.float32 else np.complex128
+    nz, nproj, _ = gc.shape
+    mu, m = fourierrec_constants(n)
+    mu = dtype(mu)
+    pi = dtype(3.1415926535) if dtype == np.float32 else np.pi
+    # takexy (kernels_fourierrec.cuh:23-36)
+    th = np.asarray(theta, dtype=dtype)
+    r = ((np.arange(n) - n // 2) / dtype(n)).astype(dtype)
+    x = (r[None, :] * np.cos(th)[:, None]).astype(dtype)
+    y = (-(r[None, :] * np.sin(th)[:, None])).astype(dtype)
+    x[x >= 0.5] = dtype(0.5 - 1e-5)
+    y[y >= 0.5] = dtype(0.5 - 1e-5)
+    # ifftshiftc -> FFT(n) -> ifftshiftc
+    sgn = (1 - 2 * ((np.arange(n) + 1) % 2)).astype(dtype)
+    g = gc.astype(cdt) * sgn
+    g = sfft.fft(g, axis=-1, workers=WORKERS).astype(cdt) * sgn
+    # gather (kernels_fourierrec.cuh:60-119) with bincount accumulation
+    N2 = 2 * n + 2 * m
+    coeff0 = pi / (mu * dtype(4 * n * n))
+    coeff1 = -pi * pi / mu
+    b0 = np.floor(dtype(2 * n) * x).astype(np.int64) - m
+    b1 = np.floor(dtype(2 * n) * y).astype(np.int64) - m
+    k0 = [np.exp(coeff1 * ((b0 + i).astype(dtype) / dtype(2 * n) - x) ** 2).astype(dtype)
+          for i in range(2 * m + 1)]
+    k1 = [np.exp(coeff1 * ((b1 + i).astype(dtype) / dtype(2 * n) - y) ** 2).astype(dtype)
+          for i in range(2 * m + 1)]
+    fde = np.zeros((nz, N2 * N2), dtype=cdt)
+    for z in range(nz):
+        g0 = (g[z] * dtype(4.0 / n)).astype(cdt)
+        acc_r = np.zeros(N2 * N2, dtype=np.float64)
+        acc_i = np.zeros(N2 * N2, dtype=np.float64)
+        for i1 in range(2 * m + 1):
+            row = (n + m + b1 + i1) * N2
+            for i0 in range(2 * m + 1):
+                w = coeff0 * (k0[i0] * k1[i1])
+                idx = (row + n + m + b0 + i0).ravel()
+                acc_r += np.bincount(idx, weights=(w * g0.real).ravel(), minlength=N2 * N2)
+                acc_i += np.bincount(idx, weights=(w * g0.imag).ravel(), minlength=N2 * N2)
+        fde[z] = (acc_r + 1j * acc_i).astype(cdt)
+    fde = fde.reshape(nz, N2, N2)
+    # wrap (kernels_fourierrec.cuh:38-58): halo folded periodically
+    core = fde[:, m:2 * n + m, m:2 * n + m].copy()
+    tx = np.arange(N2)
+    halo = (tx < m) | (tx >= 2 * n + m)
+    dst = (tx - m + 2 * n) % (2 * n)
+    ys, xs = np.nonzero(halo[:, None] | halo[None, :])
+    for z in range(nz):
+        np.add.at(core[z], (dst[ys], dst[xs]), fde[z, ys, xs])
+    # fftshiftc over the (2n+2m)^2 buffer restricted to the interior, 2D inverse FFT
+    idx = np.arange(m, 2 * n + m)
+    s1 = (1 - 2 * ((idx + 1) % 2)).astype(dtype)
+    sgn2 = s1[:, None] * s1[None, :]
+    core = sfft.ifft2(core * sgn2, axes=(-2, -1), norm="forward", workers=WORKERS).astype(cdt)
+    core = core * sgn2
+    # divphi (kernels_fourierrec.cuh:4-21) + circ (:161-174)
+    t = np.arange(n)
+    dx = (t / dtype(n) - dtype(0.5)).astype(dtype)
+    phi = np.exp(mu * dtype(n * n) * (dx[None, :] ** 2 + dx[:, None] ** 2)) / dtype(nproj)
+    phi = phi * dtype(1 - n % 4)
+    ix = t + n // 2
+    iy = t + 1 + n // 2
+    f = core[:, iy][:, :, ix] * phi.astype(dtype)
+    xc = ((t - n // 2) / dtype(n)).astype(dtype)
+    lam = ((4 * xc[None, :] ** 2 + 4 * xc[:, None] ** 2) < 1).astype(dtype)
+    return (f * lam).astype(cdt)
+
+
+def fourierrec(data, theta, dtype=np.float32):
+    """FourierRec.backprojection (fourierrec.py:61-68): real [nz, P, n] -> [nz, n, n]."""
+    nz, nproj, n = data.shape
+    h = nz // 2
+    gc = data[:h].astype(dtype) + 1j * data[h:].astype(dtype)
+    f = fourierrec_pairs(gc, theta, n, dtype)
+    return np.concatenate((f.real, f.imag)).astype(dtype)
+
+
+# --------------------------------------------------------------------------
+# linerec (src/include/kernels_linerec.cuh:3-137)
+# --------------------------------------------------------------------------
+def linerec(data, theta, n, nz, ncz, phi=np.pi / 2, sz=0, nproj_scale=None, sh=None,
+            phis=None, dtype=np.float32):
+    """f[ncz, n, n] = sum over angles of bilinear samples of data [nz, P, n]."""
+    nproj = data.shape[1]
+    c = dtype(4.0) / dtype(nproj_scale or nproj)
+    tx = np.arange(n)
+    X = (tx - n // 2).astype(dtype)[None, :]
+    Y = (tx - n // 2).astype(dtype)[:, None]
+    out = np.zeros((ncz, n, n), dtype=dtype)
+    flat = data.astype(dtype).ravel()
+    for tz in range(ncz):
+        ph = dtype(phis[tz]) if phis is not None else dtype(phi)
+        cphi, sphi = dtype(np.cos(ph)), dtype(np.sin(ph))
+        zz = (tz + sz - nz // 2) if (sh is None and phis is None) else (sz - nz // 2)
+        acc = np.zeros((n, n), dtype=dtype)
+        for t in range(nproj):
+            ct, st = dtype(np.cos(dtype(theta[t]))), dtype(np.sin(dtype(theta[t])))
+            u = ct * X + st * Y + dtype(n // 2)
+            if sh is not None:
+                u = u - dtype(sh[tz])
+            v = (st * cphi) * X + (-ct * cphi) * Y + sphi * dtype(zz) + dtype(nz // 2)
+            u = np.broadcast_to(u, (n, n))
+            v = np.broadcast_to(v, (n, n))
+            ur = np.trunc(u - dtype(1e-5)).astype(np.int64)
+            vr = np.trunc(v - dtype(1e-5)).astype(np.int64)
+            ok = (ur >= 0) & (ur < n - 1) & (vr >= 0) & (vr < nz - 1)
+            uu = np.where(ok, u - ur, 0).astype(dtype)
+            vv = np.where(ok, v - vr, 0).astype(dtype)
+            urc = np.where(ok, ur, 0)
+            vrc = np.where(ok, vr, 0)
+            base = urc + t * n + vrc * n * nproj
+            val = (flat[base] * ((1 - uu) * (1 - vv)) + flat[base + 1] * (uu * (1 - vv)) +
+                   flat[base + n * nproj] * ((1 - uu) * vv) +
+                   flat[base + n * nproj + 1] * (uu * vv))
+            acc += np.where(ok, val, 0).astype(dtype)
+        out[tz] = (acc * c)[::-1]
+    return out
+
+
+def direct_fbp64(filtered, theta, n):
+    """Direct FP64 pixel-driven backprojection with linear interpolation (discretisation
+    truth for the filtered sinograms [nz, P, n]); same output orientation as fourierrec."""
+    nz, nproj, _ = filtered.shape
+    t = np.arange(n) - n / 2
+    X, Y = np.meshgrid(t, t)
+    out = np.zeros((nz, n, n))
+    for p in range(nproj):
+        s = X * np.cos(theta[p]) - Y * np.sin(theta[p]) + n / 2
+        i0 = np.floor(s).astype(np.int64)
+        fr = s - i0
+        ok = (i0 >= 0) & (i0 < n - 1)
+        i0c = np.clip(i0, 0, n - 2)
+        for z in range(nz):
+            row = filtered[z, p].astype(np.float64)
+            out[z] += np.where(ok, row[i0c] * (1 - fr) + row[i0c + 1] * fr, 0)
+    return out * np.pi / nproj

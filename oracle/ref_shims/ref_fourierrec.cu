@@ -1,0 +1,18 @@
+// Test-only shim: exposes the reference's own cfunc_fourierrec class (compiled
+// from the reference sources at build time, never copied) behind a tiny C ABI
+// so the test suite can run the reference CUDA build on the same inputs as the
+// new kernels. Built with -DHALF for the fp16 variant.
+//
+// Wraps src/include/cfunc_fourierrec.cuh:10-36 and src/cuda/cfunc_fourierrec.cu:4-94.
+#include "cfunc_fourierrec.cu"
+
+extern "C" {
+void *ref_create(size_t nproj, size_t nz, size_t n, size_t theta) {
+  return new cfunc_fourierrec(nproj, nz, n, theta);
+}
+void ref_backprojection(void *h, size_t f, size_t g, size_t stream) {
+  static_cast<cfunc_fourierrec *>(h)->backprojection(f, g, stream);
+}
+void ref_destroy(void *h) { delete static_cast<cfunc_fourierrec *>(h); }
+int ref_last_error(void) { return (int)cudaGetLastError(); }
+}

@@ -1,0 +1,186 @@
+"""Drive the reference's own CUDA operators (oracle/_ref/*.so) from torch.
+
+The shared libraries are built by ``oracle/Makefile`` from the reference's
+sources.  The classes below restate the reference's CuPy glue line by line
+with torch tensors (GPU only), e.g. ``RefFourierRec.backprojection`` is
+src/tomocupy/reconstruction/fourierrec.py:61-68.  Test infrastructure only.
+
+Index arithmetic of the reference kernels is int32: callers keep
+nz * (2n+2m)^2 (fourierrec) and nz * nproj * n below 2**31.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import torch
+
+REF_DIR = Path(__file__).resolve().parent / "_ref"
+_libs: dict = {}
+
+vp, sz, f32, i32 = C.c_void_p, C.c_size_t, C.c_float, C.c_int
+
+_SIGS = {
+    "fourierrec": {"ref_create": ([sz, sz, sz, sz], vp), "ref_backprojection": ([vp, sz, sz, sz], None)},
+    "filter": {"ref_create": ([sz, sz, sz], vp), "ref_filter": ([vp, sz, sz, sz], None)},
+    "linerec": {"ref_create": ([sz, sz, sz, sz, sz], vp),
+                "ref_backprojection": ([vp, sz, sz, sz, f32, i32, sz], None),
+                "ref_backprojection_try": ([vp, sz, sz, sz, sz, f32, i32, sz], None),
+                "ref_backprojection_try_lamino": ([vp, sz, sz, sz, sz, i32, sz], None)},
+    "lprec": {"ref_create": ([i32, i32, i32, i32, i32], vp),
+              "ref_setgrids": ([vp] + [sz] * 13, None),
+              "ref_backprojection": ([vp, sz, sz, sz], None)},
+    "usfft1d": {"ref_create": ([sz, sz, sz, sz], vp), "ref_fwd": ([vp, sz, sz, f32, sz], None),
+                "ref_adj": ([vp, sz, sz, f32, sz], None)},
+    "usfft2d": {"ref_create": ([sz] * 6, vp), "ref_fwd": ([vp, sz, sz, sz, f32, i32, i32, sz], None),
+                "ref_adj": ([vp, sz, sz, sz, f32, i32, i32, sz], None)},
+    "fft2d": {"ref_create": ([sz, sz, sz], vp), "ref_fwd": ([vp, sz, sz, sz], None)},
+}
+
+
+def available() -> bool:
+    return (REF_DIR / "libref_fourierrec.so").exists()
+
+
+def lib(op: str, fp16: bool = False):
+    key = (op, fp16)
+    if key not in _libs:
+        path = REF_DIR / f"libref_{op}{'_fp16' if fp16 else ''}.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
+        L = C.CDLL(str(path))
+        for name, (args, res) in _SIGS[op].items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        L.ref_destroy.argtypes = [vp]
+        L.ref_destroy.restype = None
+        L.ref_last_error.argtypes = []
+        L.ref_last_error.restype = C.c_int
+        _libs[key] = L
+    return _libs[key]
+
+
+def _s(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+class _Handle:
+    op = ""
+
+    def __init__(self, fp16, *args):
+        self.L = lib(self.op, fp16)
+        self.h = self.L.ref_create(*args)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.L.ref_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class RefFourierRec(_Handle):
+    """reconstruction/fourierrec.py:46-68 over the reference cfunc_fourierrec."""
+    op = "fourierrec"
+
+    def __init__(self, n, nproj, nz, theta, dtype="float32"):
+        self.theta = theta.to(torch.float32).contiguous()
+        self.nz, self.n, self.nproj = nz, n, nproj
+        self.dtype = torch.float16 if dtype == "float16" else torch.float32
+        super().__init__(dtype == "float16", nproj, nz // 2, n, self.theta.data_ptr())
+
+    def backprojection(self, obj, data, stream=None):
+        h = self.nz // 2
+        data = torch.cat((data[:h, :, :, None], data[h:, :, :, None]), dim=3).reshape(
+            data.shape).to(self.dtype).contiguous()
+        assert obj.is_contiguous() and obj.dtype == self.dtype
+        objc = obj.view(h, self.n, 2 * self.n)
+        self.L.ref_backprojection(self.h, obj.data_ptr(), data.data_ptr(), _s(stream))
+        obj[:] = torch.cat((objc[:, :, ::2], objc[:, :, 1::2]))
+        return obj
+
+
+class RefFilter(_Handle):
+    """reconstruction/fbp_filter.py:45-58 over the reference cfunc_filter."""
+    op = "filter"
+
+    def __init__(self, n, ntheta, nz, dtype="float32"):
+        self.dtype = torch.float16 if dtype == "float16" else torch.float32
+        super().__init__(dtype == "float16", ntheta, nz, n)
+
+    def filter(self, data, w, stream=None):
+        assert data.is_contiguous()
+        w = torch.view_as_real(w.contiguous()).to(self.dtype).contiguous()
+        self.L.ref_filter(self.h, data.data_ptr(), w.data_ptr(), _s(stream))
+        return data
+
+
+def ref_fbp_filter_center(filt: RefFilter, data, wfilter, t, center, sht, n, ne):
+    """backproj_functions.py:93-109 with torch standing in for CuPy."""
+    nz = data.shape[0]
+    pad = ne // 2 - n // 2
+    tmp = torch.empty((nz, data.shape[1], ne), dtype=data.dtype, device=data.device)
+    tmp[:, :, pad:pad + n] = data
+    tmp[:, :, :pad] = data[:, :, :1]
+    tmp[:, :, pad + n:] = data[:, :, -1:]
+    if not torch.is_tensor(sht):
+        sht = torch.full((nz,), float(sht), dtype=torch.float32, device=data.device)
+    a = (-center + sht.reshape(-1).to(torch.float32)) + n / 2
+    ci = float(torch.tensor(-2.0, dtype=torch.float32) * torch.tensor(math.pi, dtype=torch.float32))
+    phase = (a * ci)[:, None] * t[None, :]
+    w = torch.complex(wfilter * torch.cos(phase), wfilter * torch.sin(phase))
+    filt.filter(tmp, w)
+    data[:] = tmp[:, :, pad:pad + n]
+    return data
+
+
+class RefLineRec(_Handle):
+    """reconstruction/linerec.py:44-85 over the reference cfunc_linerec."""
+    op = "linerec"
+
+    def __init__(self, theta, nproj, ncproj, nz, ncz, n, dtype="float32"):
+        self.theta = theta.to(torch.float32).contiguous()
+        super().__init__(dtype == "float16", nproj, nz, n, ncproj, ncz)
+
+    def backprojection(self, f, data, stream=None, theta=None, lamino_angle=0.0, sz=0):
+        if theta is None:
+            theta = self.theta
+            f[:] = 0
+        phi = math.pi / 2 + lamino_angle / 180 * math.pi
+        self.L.ref_backprojection(self.h, f.data_ptr(), data.contiguous().data_ptr(),
+                                  theta.data_ptr(), phi, sz, _s(stream))
+
+    def backprojection_try(self, f, data, sh, stream=None, theta=None, lamino_angle=0.0, sz=0):
+        theta = self.theta if theta is None else theta
+        phi = math.pi / 2 + lamino_angle / 180 * math.pi
+        self.L.ref_backprojection_try(self.h, f.data_ptr(), data.contiguous().data_ptr(),
+                                      theta.data_ptr(), sh.contiguous().data_ptr(), phi, sz,
+                                      _s(stream))
+
+    def backprojection_try_lamino(self, f, data, sh, stream=None, theta=None, lamino_angle=0.0,
+                                  sz=0):
+        theta = self.theta if theta is None else theta
+        phi = (math.pi / 2 + (lamino_angle + sh.to(torch.float32)) / 180 * math.pi).contiguous()
+        self.L.ref_backprojection_try_lamino(self.h, f.data_ptr(), data.contiguous().data_ptr(),
+                                             theta.data_ptr(), phi.data_ptr(), sz, _s(stream))
+
+
+def ref_darkflat_minus_log(data, dark, flat, bright_ratio=1.0, minus_log=True):
+    """proc_functions.py:55-83 in torch, operation by operation (float32)."""
+    dark0 = dark.to(torch.float32)
+    flat0 = flat.to(torch.float32) / bright_ratio
+    flat0 = flat0.mean(dim=0)
+    dark0 = dark0.mean(dim=0)
+    flat0 = flat0 * torch.tensor(1 + 1e-5, dtype=torch.float32)
+    flat0 = flat0 - dark0
+    res = (data.to(torch.float32) - dark0) / flat0
+    if minus_log:
+        res = torch.where(res <= 0, torch.ones((), dtype=torch.float32, device=res.device), res)
+        res = -torch.log(res)
+        res = torch.nan_to_num(res, nan=6.0, posinf=0.0, neginf=0.0)
+    return res

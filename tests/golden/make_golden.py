@@ -1,0 +1,205 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py --cpu [--ref /root/reference]
+        Executes the reference's own Python sources with NumPy standing in
+        for CuPy (and stubs for h5py / the SWIG modules):
+          * FBPFilter.calc_filter for every filter at several widths
+            (src/tomocupy/reconstruction/fbp_filter.py:60-118)
+          * Reader.init_sizes / init_sizes_try / init_sizes_lamino for a set
+            of option combinations (src/tomocupy/dataio/reader.py:82-272)
+        -> filter_spectra.npz, sizes_cases.json
+
+    python tests/golden/make_golden.py --gpu --out DIR
+        Runs the reference's CUDA operators (oracle/_ref, built from the
+        reference sources) on small seeded inputs and stores their outputs
+        -> ref_gpu_small.npz (needs a GPU; the inputs are re-generated from
+        the stored seeds by the tests).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import sys
+import types
+from argparse import Namespace
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+FILTER_WIDTHS = (256, 1024, 2048, 4096)
+FILTER_NAMES = ("none", "ramp", "shepp", "cosine", "cosine2", "hamming", "hann", "parzen")
+
+
+def _numpy_as_cupy():
+    cp = types.ModuleType("cupy")
+    for name in dir(np):
+        if not name.startswith("__"):
+            setattr(cp, name, getattr(np, name))
+    cp.fft = np.fft
+    cp.linalg = np.linalg
+    cp.asnumpy = np.asarray
+    return cp
+
+
+def _install_stubs():
+    sys.modules["cupy"] = _numpy_as_cupy()
+    pkg = types.ModuleType("tomocupy")
+    pkg.__path__ = []
+    sys.modules["tomocupy"] = pkg
+    for sub in ("cfunc_filter", "cfunc_filterfp16", "utils"):
+        m = types.ModuleType(f"tomocupy.{sub}")
+        sys.modules[f"tomocupy.{sub}"] = m
+        setattr(pkg, sub, m)
+    import logging as _logging
+    lg = types.ModuleType("tomocupy.logging")
+    lg.getLogger = _logging.getLogger
+    sys.modules["tomocupy.logging"] = lg
+    pkg.logging = lg
+    gv = types.ModuleType("tomocupy.global_vars")
+    gv.args = Namespace()
+    gv.params = Namespace()
+    sys.modules["tomocupy.global_vars"] = gv
+    pkg.global_vars = gv
+    sys.modules["h5py"] = types.ModuleType("h5py")
+    return gv
+
+
+def _load(path: Path, name: str):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+SIZE_CASES = [
+    dict(sizes=dict(nproji=360, nzi=16, ni=512, nflat=10, ndark=10, dtype="uint16"), args={}),
+    dict(sizes=dict(nproji=1500, nzi=2048, ni=2048, nflat=10, ndark=10, dtype="uint16"),
+         args=dict(nsino_per_chunk=32)),
+    dict(sizes=dict(nproji=1500, nzi=2048, ni=2448, nflat=20, ndark=10, dtype="uint16"),
+         args=dict(dtype="float16")),
+    dict(sizes=dict(nproji=721, nzi=100, ni=1001, nflat=10, ndark=5, dtype="uint16"),
+         args=dict(start_column=3, end_column=-1, rotation_axis=480.5, nsino_per_chunk=1)),
+    dict(sizes=dict(nproji=3000, nzi=1, ni=4096, nflat=10, ndark=10, dtype="uint16"),
+         args=dict(reconstruction_type="try", rotation_axis=2048.0, center_search_width=48.0,
+                   center_search_step=0.375, nsino="0")),
+    dict(sizes=dict(nproji=1200, nzi=1024, ni=1024, nflat=10, ndark=10, dtype="uint16"),
+         args=dict(lamino_angle=30.0, lamino_start_row=0, lamino_end_row=512,
+                   reconstruction_type="full")),
+    dict(sizes=dict(nproji=400, nzi=64, ni=256, nflat=10, ndark=10, dtype="uint16"),
+         args=dict(reconstruction_type="try_lamino", lamino_angle=20.0,
+                   lamino_search_width=2.0, lamino_search_step=0.5, nsino="[0.2,0.7]")),
+    dict(sizes=dict(nproji=900, nzi=40, ni=640, nflat=10, ndark=10, dtype="uint16"),
+         args=dict(start_proj=10, end_proj=890, blocked_views="[0.5,0.9]")),
+]
+
+
+def gen_cpu(ref: Path):
+    gv = _install_stubs()
+    fbp = _load(ref / "src/tomocupy/reconstruction/fbp_filter.py", "ref_fbp_filter")
+    spectra = {}
+    for ne in FILTER_WIDTHS:
+        obj = fbp.FBPFilter.__new__(fbp.FBPFilter)
+        obj.n = ne
+        for name in FILTER_NAMES:
+            spectra[f"{name}_{ne}"] = np.asarray(obj.calc_filter(name), dtype=np.float32)
+    np.savez_compressed(HERE / "filter_spectra.npz", **spectra)
+
+    reader = _load(ref / "src/tomocupy/dataio/reader.py", "ref_reader")
+    from tomocupy_b200.config import DEFAULTS
+    out = []
+    for case in SIZE_CASES:
+        args = Namespace(**DEFAULTS)
+        for k, v in case["args"].items():
+            setattr(args, k, v)
+        gv.args.__dict__.clear()
+        gv.args.__dict__.update(vars(args))
+        gv.params.__dict__.clear()
+        reader.args, reader.params = gv.args, gv.params
+        r = reader.Reader.__new__(reader.Reader)
+        sizes = case["sizes"]
+        theta = np.linspace(0, np.pi, sizes["nproji"], dtype="float32")
+        r.read_sizes = lambda s=sizes: dict(s)
+        r.read_theta = lambda nproj, th=theta: th
+        r.init_sizes()
+        if gv.args.reconstruction_type[:3] == "try":
+            r.init_sizes_try()
+        if gv.args.lamino_angle != 0:
+            r.init_sizes_lamino()
+        p = {}
+        for k, v in vars(gv.params).items():
+            if isinstance(v, np.ndarray):
+                p[k] = {"array": v.tolist(), "dtype": str(v.dtype)}
+            elif isinstance(v, (np.integer,)):
+                p[k] = int(v)
+            elif isinstance(v, (np.floating,)):
+                p[k] = float(v)
+            elif isinstance(v, (list, tuple)):
+                p[k] = [x.item() if hasattr(x, "item") else x for x in v]
+            else:
+                p[k] = v
+        out.append({"case": case, "params": p,
+                    "args_after": {k: getattr(gv.args, k) for k in
+                                   ("end_row", "end_proj", "end_column")}})
+    (HERE / "sizes_cases.json").write_text(json.dumps(out, indent=1, default=str))
+    print("wrote filter_spectra.npz and sizes_cases.json")
+
+
+GPU_CASES = dict(n=128, nproj=90, nz=4, seed=7)
+
+
+def gpu_inputs():
+    """Seeded inputs of the GPU golden cases (re-generated identically by the tests)."""
+    import torch
+    from tomocupy_b200 import synthetic
+    c = GPU_CASES
+    data, dark, flat, theta, _ = synthetic.make_dataset(c["nproj"], c["nz"], c["n"],
+                                                        seed=c["seed"], device="cpu")
+    return data, dark, flat, theta
+
+
+def gen_gpu(out_dir: Path):
+    import torch
+    from oracle import refglue, np_tomo
+    data, dark, flat, theta = gpu_inputs()
+    c = GPU_CASES
+    n, nproj, nz = c["n"], c["nproj"], c["nz"]
+    dev = torch.device("cuda")
+    d = torch.as_tensor(np_tomo.minus_log(np_tomo.darkflat(data.numpy(), dark.numpy(),
+                                                           flat.numpy())))
+    sino = d.permute(1, 0, 2).contiguous().to(dev)  # [nz, P, n]
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, "parzen"), device=dev)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=dev)
+    filt = refglue.RefFilter(ne, nproj, nz)
+    filtered = refglue.ref_fbp_filter_center(filt, sino.clone(), wf, t, n / 2, 0.0, n, ne)
+    th = torch.as_tensor(theta, device=dev)
+    fr = refglue.RefFourierRec(n, nproj, nz, th)
+    rec_fr = torch.zeros((nz, n, n), dtype=torch.float32, device=dev)
+    fr.backprojection(rec_fr, filtered.clone())
+    lr = refglue.RefLineRec(th, nproj, nproj, nz, nz, n)
+    rec_lr = torch.zeros((nz, n, n), dtype=torch.float32, device=dev)
+    lr.backprojection(rec_lr, filtered.clone())
+    torch.cuda.synchronize()
+    out_dir.mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(out_dir / "ref_gpu_small.npz", filtered=filtered.cpu().numpy(),
+                        fourierrec=rec_fr.cpu().numpy(), linerec=rec_lr.cpu().numpy(),
+                        **{k: np.int64(v) for k, v in GPU_CASES.items()})
+    print("wrote", out_dir / "ref_gpu_small.npz")
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cpu", action="store_true")
+    ap.add_argument("--gpu", action="store_true")
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--out", default=str(HERE))
+    a = ap.parse_args()
+    if a.cpu:
+        gen_cpu(Path(a.ref))
+    if a.gpu:
+        gen_gpu(Path(a.out))

@@ -1,0 +1,58 @@
+"""Drop-in for the reference module ``tomocupy.cfunc_fourierrec``.
+
+Same class name, constructor argument order and method signature as the SWIG
+class (src/cuda/cfunc_fourierrec.i:9-21): pointers and streams are integer
+addresses.  ``nz`` counts complex slice pairs; ``g`` is overwritten during
+``backprojection`` exactly as in the reference.
+"""
+from __future__ import annotations
+
+from . import _lib
+
+
+class cfunc_fourierrec:
+    _precision = _lib.TCB_FLOAT32
+
+    def __init__(self, nproj, nz, n, theta_):
+        self._h = _lib.create("tcb_fourierrec_create", int(nproj), int(nz), int(n),
+                              _lib.ptr(theta_), self._precision)
+        self._n, self._nproj, self._nz = int(n), int(nproj), int(nz)
+
+    # read-only attributes, as %immutable in the SWIG interface
+    n = property(lambda self: self._n)
+    nproj = property(lambda self: self._nproj)
+    nz = property(lambda self: self._nz)
+
+    def backprojection(self, f, g, stream):
+        """f complex [nz, n, n] <- backprojection of g complex [nz, nproj, n]."""
+        self._check()
+        _lib.call("tcb_fourierrec_backprojection", self._h, _lib.ptr(f), _lib.ptr(g),
+                  _lib.stream_ptr(stream))
+
+    def backprojection_slices(self, f, g, stream):
+        """f real [2*nz, n, n] (pair k -> slices k and nz+k) from g complex [nz, nproj, n]."""
+        self._check()
+        _lib.call("tcb_fourierrec_backprojection_slices", self._h, _lib.ptr(f), _lib.ptr(g),
+                  _lib.stream_ptr(stream))
+
+    def pack(self, g, src, row_stride, xoff, stream):
+        """g[k] = src[k, :, xoff:xoff+n] + 1j*src[k+nz, :, xoff:xoff+n]."""
+        self._check()
+        _lib.call("tcb_fourierrec_pack", self._h, _lib.ptr(g), _lib.ptr(src), int(row_stride),
+                  int(xoff), _lib.stream_ptr(stream))
+
+    def _check(self):
+        if self._h is None:
+            raise _lib.TcbError(6, type(self).__name__, "object was freed")
+
+    def free(self):
+        """Release device memory; idempotent like the reference's is_free guard."""
+        if getattr(self, "_h", None) is not None:
+            _lib.call("tcb_fourierrec_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

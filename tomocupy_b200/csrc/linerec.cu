@@ -1,0 +1,184 @@
+// Line (pixel-driven) backprojector for tomography and laminography.
+//
+// Same geometry and bilinear weights as cfunc_linerec
+// (src/include/kernels_linerec.cuh:3-137): for voxel (tx, ty, tz) and angle t
+//   u = cos(t)(x) + sin(t)(y) + n/2
+//   v = sin(t)cos(phi)(x) - cos(t)cos(phi)(y) + sin(phi)(z) + nz/2
+// with x = tx - n/2, y = ty - n/2, truncation (int)(u - 1e-5), and the
+// output row flip f[tx + (n-1-ty) n + tz n^2] += 4/nproj * sum.
+//
+// B200 design: the per-angle rotation coefficients are computed once per CTA
+// into shared memory (with the reference's __cosf/__sinf, so u and v are
+// bit-identical) instead of by every thread for every angle; each thread
+// accumulates in fp32 registers (also in the FLOAT16 variant, whose caller
+// buffers are fp16); reads of the sinogram go through the read-only path.
+#include <cuda_fp16.h>
+
+#include "common.cuh"
+
+struct tcb_linerec {
+  size_t nproj, nz, n, ncproj, ncz;
+  int precision;
+  bool freed = false;
+};
+
+namespace tcb {
+namespace lr {
+
+constexpr int BX = 32, BY = 8;
+constexpr int ACHUNK = 256;  // angles staged in shared memory per pass
+
+enum Mode { FULL = 0, TRY = 1, TRY_LAMINO = 2 };
+
+template <typename T> __device__ __forceinline__ float ld(const T *p) { return (float)*p; }
+template <> __device__ __forceinline__ float ld<__half>(const __half *p) {
+  return __half2float(*p);
+}
+template <typename T> __device__ __forceinline__ T from_f32(float v) { return (T)v; }
+template <> __device__ __forceinline__ __half from_f32<__half>(float v) {
+  return __float2half_rn(v);
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(BX *BY)
+    backproject_kernel(T *__restrict__ f, const T *__restrict__ data,
+                       const float *__restrict__ theta, float phi_s,
+                       const float *__restrict__ phi_v, const float *__restrict__ sh,
+                       float c, int sz, int ncz, int n, int nz, int nproj) {
+  __shared__ float s_c[ACHUNK], s_s[ACHUNK];
+  const int tx = blockIdx.x * BX + threadIdx.x;
+  const int ty = blockIdx.y * BY + threadIdx.y;
+  const int tz = blockIdx.z;
+  const bool active = tx < n && ty < n && tz < ncz;
+  const float phi = (MODE == TRY_LAMINO) ? (active ? phi_v[tz] : 0.f) : phi_s;
+  const float cphi = __cosf(phi);
+  const float sphi = __sinf(phi);
+  const float shift = (MODE == TRY && active) ? sh[tz] : 0.f;
+  const int zz = (MODE == FULL) ? (tz + sz - nz / 2) : (sz - nz / 2);
+  float f0 = 0.f;
+  const int tid = threadIdx.y * BX + threadIdx.x;
+  for (int t0 = 0; t0 < nproj; t0 += ACHUNK) {
+    int cnt = min(ACHUNK, nproj - t0);
+    __syncthreads();
+    for (int k = tid; k < cnt; k += BX * BY) {
+      float th = theta[t0 + k];
+      s_c[k] = __cosf(th);
+      s_s[k] = __sinf(th);
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int k = 0; k < cnt; k++) {
+      const int t = t0 + k;
+      float ctheta = s_c[k];
+      float stheta = s_s[k];
+      float R0 = ctheta, R1 = stheta;
+      float R3 = stheta * cphi, R4 = -ctheta * cphi, R5 = sphi;
+      float u, v;
+      if (MODE == TRY)
+        u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2 - shift;
+      else
+        u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2;
+      v = R3 * (tx - n / 2) + R4 * (ty - n / 2) + R5 * zz + nz / 2;
+      int ur = (int)(u - 1e-5f);
+      int vr = (int)(v - 1e-5f);
+      if ((ur >= 0) & (ur < n - 1) & (vr >= 0) & (vr < nz - 1)) {
+        u = u - ur;
+        v = v - vr;
+        const T *d0 = data + ur + (size_t)t * n + (size_t)vr * n * nproj;
+        const T *d1 = d0 + (size_t)n * nproj;
+        f0 += ld(d0) * ((1 - u) * (1 - v)) + ld(d0 + 1) * ((0 + u) * (1 - v)) +
+              ld(d1) * ((1 - u) * (0 + v)) + ld(d1 + 1) * ((0 + u) * (0 + v));
+      }
+    }
+  }
+  if (!active) return;
+  T *o = f + tx + (size_t)(n - ty - 1) * n + (size_t)tz * n * n;
+  *o = from_f32<T>(ld(o) + f0 * c);
+}
+
+template <typename T>
+int launch(tcb_linerec *h, int mode, void *f, const void *g, const float *theta,
+           float phi, const float *phi_v, const float *sh, int sz, cudaStream_t s) {
+  dim3 blk(BX, BY), grd(ceil_div(h->n, BX), ceil_div(h->n, BY), (unsigned)h->ncz);
+  StageTimer st("linerec", s);
+  count_launch();
+  float c = 4.0f / h->nproj;
+  int n = (int)h->n, nz = (int)h->nz, ncz = (int)h->ncz, np = (int)h->ncproj;
+  switch (mode) {
+    case FULL:
+      backproject_kernel<T, FULL><<<grd, blk, 0, s>>>((T *)f, (const T *)g, theta, phi,
+                                                      nullptr, nullptr, c, sz, ncz, n, nz, np);
+      break;
+    case TRY:
+      backproject_kernel<T, TRY><<<grd, blk, 0, s>>>((T *)f, (const T *)g, theta, phi,
+                                                     nullptr, sh, c, sz, ncz, n, nz, np);
+      break;
+    default:
+      backproject_kernel<T, TRY_LAMINO><<<grd, blk, 0, s>>>(
+          (T *)f, (const T *)g, theta, 0.f, phi_v, nullptr, c, sz, ncz, n, nz, np);
+  }
+  TCB_LAUNCH_CHECK();
+  return TCB_OK;
+}
+
+int run(tcb_linerec *h, int mode, void *f, const void *g, const float *theta, float phi,
+        const float *phi_v, const float *sh, int sz, void *stream) {
+  TCB_CHECK_ARG(h, "linerec: null handle");
+  TCB_CHECK_ARG(!h->freed, "linerec: handle was freed");
+  TCB_CHECK_ARG(f && g && theta, "linerec: null pointer");
+  TCB_CHECK_ARG(mode != TRY || sh, "linerec: backprojection_try needs sh");
+  TCB_CHECK_ARG(mode != TRY_LAMINO || phi_v, "linerec: backprojection_try_lamino needs phi");
+  if (h->precision == TCB_FLOAT16)
+    return launch<__half>(h, mode, f, g, theta, phi, phi_v, sh, sz, (cudaStream_t)stream);
+  return launch<float>(h, mode, f, g, theta, phi, phi_v, sh, sz, (cudaStream_t)stream);
+}
+
+}  // namespace lr
+}  // namespace tcb
+
+using namespace tcb;
+
+extern "C" int tcb_linerec_create(tcb_linerec **out, size_t nproj, size_t nz, size_t n,
+                                  size_t ncproj, size_t ncz, int precision) {
+  TCB_CHECK_ARG(out, "tcb_linerec_create: null out");
+  *out = nullptr;
+  TCB_CHECK_ARG(nproj >= 1 && nz >= 1 && n >= 2 && ncproj >= 1 && ncz >= 1,
+                "tcb_linerec_create: bad sizes");
+  TCB_CHECK_ARG(n < 65536 && ncz < 65536, "tcb_linerec_create: sizes too large");
+  TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
+                "tcb_linerec_create: bad precision %d", precision);
+  tcb_linerec *h = new tcb_linerec();
+  h->nproj = nproj;
+  h->nz = nz;
+  h->n = n;
+  h->ncproj = ncproj;
+  h->ncz = ncz;
+  h->precision = precision;
+  *out = h;
+  return TCB_OK;
+}
+
+extern "C" int tcb_linerec_backprojection(tcb_linerec *h, void *f, const void *g,
+                                          const float *theta, float phi, int sz,
+                                          void *stream) {
+  return lr::run(h, lr::FULL, f, g, theta, phi, nullptr, nullptr, sz, stream);
+}
+
+extern "C" int tcb_linerec_backprojection_try(tcb_linerec *h, void *f, const void *g,
+                                              const float *theta, const float *sh,
+                                              float phi, int sz, void *stream) {
+  return lr::run(h, lr::TRY, f, g, theta, phi, nullptr, sh, sz, stream);
+}
+
+extern "C" int tcb_linerec_backprojection_try_lamino(tcb_linerec *h, void *f,
+                                                     const void *g, const float *theta,
+                                                     const float *phi, int sz,
+                                                     void *stream) {
+  return lr::run(h, lr::TRY_LAMINO, f, g, theta, 0.f, phi, nullptr, sz, stream);
+}
+
+extern "C" int tcb_linerec_destroy(tcb_linerec *h) {
+  if (!h) return TCB_OK;
+  delete h;
+  return TCB_OK;
+}

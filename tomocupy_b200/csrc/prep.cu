@@ -1,0 +1,239 @@
+// Pre-processing kernels: dark/flat reductions and one fused pass that turns
+// raw detector rows into (optionally -log'd, edge-padded) sinogram rows.
+//
+// Arithmetic follows ProcFunctions.darkflat_correction / minus_log
+// (src/tomocupy/processing/proc_functions.py:55-83) operation by operation.
+// Every CuPy elementwise step there is a separate kernel, so no multiply-add
+// is ever contracted; the explicit __f*_rn intrinsics below keep nvcc from
+// contracting either, which makes the fp32 results bit-identical.
+#include "common.cuh"
+
+namespace tcb {
+namespace {
+
+template <typename T> __device__ __forceinline__ float to_f32(T v) { return (float)v; }
+
+template <typename T>
+__global__ void darkflat_stats_kernel(float *__restrict__ dark0, float *__restrict__ flat0,
+                                      float *__restrict__ flat1,
+                                      const T *__restrict__ dark, const T *__restrict__ flat,
+                                      int ndark, int nflat, size_t plane, float bright_ratio,
+                                      int flat_linear) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= plane) return;
+  // dark0 = mean(dark, axis=0): float32 sum in frame order, then / count.
+  float sd = 0.f;
+  for (int k = 0; k < ndark; k++) sd = __fadd_rn(sd, to_f32(dark[(size_t)k * plane + i]));
+  float d0 = __fdiv_rn(sd, (float)ndark);
+  dark0[i] = d0;
+  if (!flat_linear) {
+    float sf = 0.f;
+    for (int k = 0; k < nflat; k++)
+      sf = __fadd_rn(sf, __fdiv_rn(to_f32(flat[(size_t)k * plane + i]), bright_ratio));
+    float f0 = __fdiv_rn(sf, (float)nflat);
+    f0 = __fmul_rn(f0, 1.00001f);  // cp.float32(1 + 1e-5)
+    flat0[i] = __fsub_rn(f0, d0);
+  } else {
+    // flat0_p0 = mean(flat0[:nflat//2]), flat0_p1 = mean(flat0[nflat//2+1:])
+    int h = nflat / 2;
+    float s0 = 0.f, s1 = 0.f;
+    for (int k = 0; k < h; k++)
+      s0 = __fadd_rn(s0, __fdiv_rn(to_f32(flat[(size_t)k * plane + i]), bright_ratio));
+    for (int k = h + 1; k < nflat; k++)
+      s1 = __fadd_rn(s1, __fdiv_rn(to_f32(flat[(size_t)k * plane + i]), bright_ratio));
+    flat0[i] = __fdiv_rn(s0, (float)h);
+    flat1[i] = __fdiv_rn(s1, (float)(nflat - h - 1));
+  }
+}
+
+struct PrepArgs {
+  float *out;
+  const void *in;
+  const float *dark0, *flat0, *flat1;
+  int nproj, nz, n;
+  size_t in_pstride, in_zstride;
+  size_t out_zstride, out_pstride, out_poff, out_xoff, out_width;
+  unsigned flags;
+};
+
+// -log with the reference's clean-up: where(x<=0 -> 1), log, negate,
+// nan_to_num(nan=6, posinf=0, neginf=0).
+__device__ __forceinline__ float minus_log(float x) {
+  if (x <= 0.f) x = 1.f;
+  float r = -logf(x);
+  if (isnan(r)) r = 6.f;
+  else if (isinf(r)) r = 0.f;
+  return r;
+}
+
+// Apply the normalisation chain to one raw value.  d0/f0/f1 are the
+// dark/flat statistics of this (z, x) position.
+__device__ __forceinline__ float prep_apply(unsigned flags, float v, float d0, float f0,
+                                            float f1, double vlin) {
+  if (flags & TCB_PREP_DARKFLAT) {
+    if (flags & TCB_PREP_FLAT_LINEAR) {
+      // float64 path of the reference: (1-v)*p0 + v*p1, *= f32(1+1e-5), -= dark0
+      double f = __dadd_rn(__dmul_rn(__dsub_rn(1.0, vlin), (double)f0),
+                           __dmul_rn(vlin, (double)f1));
+      f = __dmul_rn(f, (double)1.00001f);
+      f = __dsub_rn(f, (double)d0);
+      v = (float)__ddiv_rn((double)__fsub_rn(v, d0), f);
+    } else {
+      v = __fdiv_rn(__fsub_rn(v, d0), f0);
+    }
+  }
+  if (flags & TCB_PREP_MINUS_LOG) v = minus_log(v);
+  return v;
+}
+
+template <typename T> struct Vec4Of;
+template <> struct Vec4Of<uint16_t> { using type = ushort4; };
+template <> struct Vec4Of<uint8_t> { using type = uchar4; };
+template <> struct Vec4Of<float> { using type = float4; };
+
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+template <typename T>
+__device__ __forceinline__ float prep_scalar(const PrepArgs &a, const T *src, int z, int x,
+                                             double vlin) {
+  size_t i = (size_t)z * a.n + x;
+  float d0 = 0.f, f0 = 1.f, f1 = 0.f;
+  if (a.flags & TCB_PREP_DARKFLAT) {
+    d0 = a.dark0[i];
+    f0 = a.flat0[i];
+    if (a.flags & TCB_PREP_FLAT_LINEAR) f1 = a.flat1[i];
+  }
+  return prep_apply(a.flags, to_f32(src[x]), d0, f0, f1, vlin);
+}
+
+// One CTA per output row (z, p); rows are enumerated z-major so consecutive
+// CTAs write consecutive output rows.
+template <typename T>
+__global__ void __launch_bounds__(256) prep_rows_kernel(PrepArgs a) {
+  size_t row = blockIdx.x;
+  int z = (int)(row / a.nproj);
+  int p = (int)(row % a.nproj);
+  const T *src = (const T *)a.in + (size_t)p * a.in_pstride + (size_t)z * a.in_zstride;
+  float *dst = a.out + (size_t)z * a.out_zstride + (size_t)(p + a.out_poff) * a.out_pstride;
+  double vlin = 0.0;
+  if (a.flags & TCB_PREP_FLAT_LINEAR)
+    vlin = (p == a.nproj - 1) ? 1.0 : __dmul_rn((double)p, 1.0 / (double)(a.nproj - 1));
+  const int n = a.n;
+  float *row_out = dst + a.out_xoff;
+  const bool df = (a.flags & TCB_PREP_DARKFLAT) != 0;
+  const bool lin = (a.flags & TCB_PREP_FLAT_LINEAR) != 0;
+  // Vector path: 4 elements per thread per step when everything is aligned.
+  bool vec = (n % 4 == 0) && ((((uintptr_t)row_out) & 15) == 0) &&
+             ((((uintptr_t)src) & (sizeof(T) * 4 - 1)) == 0) &&
+             (!df || ((((uintptr_t)(a.dark0 + (size_t)z * n)) & 15) == 0 &&
+                      (((uintptr_t)(a.flat0 + (size_t)z * n)) & 15) == 0 &&
+                      (!lin || (((uintptr_t)(a.flat1 + (size_t)z * n)) & 15) == 0)));
+  if (vec) {
+    using V = typename Vec4Of<T>::type;
+    for (int x = threadIdx.x * 4; x < n; x += blockDim.x * 4) {
+      V raw = *reinterpret_cast<const V *>(src + x);
+      float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f), f0 = make_float4(1.f, 1.f, 1.f, 1.f),
+             f1 = d0;
+      if (df) {
+        size_t i = (size_t)z * n + x;
+        d0 = ld4(a.dark0 + i);
+        f0 = ld4(a.flat0 + i);
+        if (lin) f1 = ld4(a.flat1 + i);
+      }
+      float4 r;
+      r.x = prep_apply(a.flags, (float)raw.x, d0.x, f0.x, f1.x, vlin);
+      r.y = prep_apply(a.flags, (float)raw.y, d0.y, f0.y, f1.y, vlin);
+      r.z = prep_apply(a.flags, (float)raw.z, d0.z, f0.z, f1.z, vlin);
+      r.w = prep_apply(a.flags, (float)raw.w, d0.w, f0.w, f1.w, vlin);
+      *reinterpret_cast<float4 *>(row_out + x) = r;
+    }
+  } else {
+    for (int x = threadIdx.x; x < n; x += blockDim.x)
+      row_out[x] = prep_scalar<T>(a, src, z, x, vlin);
+  }
+  if (a.flags & TCB_PREP_EDGE_PAD) {
+    float left = prep_scalar<T>(a, src, z, 0, vlin);
+    float right = prep_scalar<T>(a, src, z, n - 1, vlin);
+    size_t xo = a.out_xoff, xe = a.out_xoff + n;
+    for (size_t x = threadIdx.x; x < xo; x += blockDim.x) dst[x] = left;
+    for (size_t x = xe + threadIdx.x; x < a.out_width; x += blockDim.x) dst[x] = right;
+  }
+}
+
+}  // namespace
+}  // namespace tcb
+
+using namespace tcb;
+
+extern "C" int tcb_darkflat_stats(void *dark0, void *flat0, void *flat1, const void *dark,
+                                  const void *flat, size_t ndark, size_t nflat, size_t nz,
+                                  size_t n, int in_dtype, float bright_ratio,
+                                  int flat_linear, void *stream) {
+  TCB_CHECK_ARG(dark0 && flat0 && dark && flat, "tcb_darkflat_stats: null pointer");
+  TCB_CHECK_ARG(ndark >= 1 && nflat >= 1, "tcb_darkflat_stats: need >=1 dark and flat");
+  TCB_CHECK_ARG(!flat_linear || (nflat >= 3 && flat1),
+                "tcb_darkflat_stats: flat_linear needs >=3 flats and flat1");
+  size_t plane = nz * n;
+  if (plane == 0) return TCB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned grid = ceil_div(plane, 256);
+  StageTimer st("darkflat_stats", s);
+  count_launch();
+  switch (in_dtype) {
+    case TCB_U16:
+      darkflat_stats_kernel<uint16_t><<<grid, 256, 0, s>>>(
+          (float *)dark0, (float *)flat0, (float *)flat1, (const uint16_t *)dark,
+          (const uint16_t *)flat, (int)ndark, (int)nflat, plane, bright_ratio, flat_linear);
+      break;
+    case TCB_U8:
+      darkflat_stats_kernel<uint8_t><<<grid, 256, 0, s>>>(
+          (float *)dark0, (float *)flat0, (float *)flat1, (const uint8_t *)dark,
+          (const uint8_t *)flat, (int)ndark, (int)nflat, plane, bright_ratio, flat_linear);
+      break;
+    case TCB_F32:
+      darkflat_stats_kernel<float><<<grid, 256, 0, s>>>(
+          (float *)dark0, (float *)flat0, (float *)flat1, (const float *)dark,
+          (const float *)flat, (int)ndark, (int)nflat, plane, bright_ratio, flat_linear);
+      break;
+    default:
+      set_error("tcb_darkflat_stats: unknown dtype %d", in_dtype);
+      return TCB_ERR_INVALID_ARGUMENT;
+  }
+  TCB_LAUNCH_CHECK();
+  return TCB_OK;
+}
+
+extern "C" int tcb_prep_rows(float *out, const void *in, const float *dark0,
+                             const float *flat0, const float *flat1, size_t nproj,
+                             size_t nz, size_t n, size_t in_pstride, size_t in_zstride,
+                             int in_dtype, size_t out_zstride, size_t out_pstride,
+                             size_t out_poff, size_t out_xoff, size_t out_width,
+                             unsigned flags, void *stream) {
+  TCB_CHECK_ARG(out && in, "tcb_prep_rows: null pointer");
+  TCB_CHECK_ARG(!(flags & TCB_PREP_DARKFLAT) || (dark0 && flat0),
+                "tcb_prep_rows: darkflat needs dark0/flat0");
+  TCB_CHECK_ARG(!(flags & TCB_PREP_FLAT_LINEAR) || (flat1 && nproj >= 2),
+                "tcb_prep_rows: flat_linear needs flat1 and nproj>=2");
+  TCB_CHECK_ARG(out_width >= out_xoff + n || !(flags & TCB_PREP_EDGE_PAD),
+                "tcb_prep_rows: out_width < out_xoff + n");
+  TCB_CHECK_ARG(nproj < (1u << 31) && nz < (1u << 31) && n < (1u << 31),
+                "tcb_prep_rows: size too large");
+  if (nproj == 0 || nz == 0 || n == 0) return TCB_OK;
+  size_t rows = nproj * nz;
+  TCB_CHECK_ARG(rows < (1ull << 31), "tcb_prep_rows: too many rows in one call");
+  PrepArgs a{out, in, dark0, flat0, flat1, (int)nproj, (int)nz, (int)n, in_pstride,
+             in_zstride, out_zstride, out_pstride, out_poff, out_xoff, out_width, flags};
+  cudaStream_t s = (cudaStream_t)stream;
+  StageTimer st("prep_rows", s);
+  count_launch();
+  switch (in_dtype) {
+    case TCB_U16: prep_rows_kernel<uint16_t><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_U8: prep_rows_kernel<uint8_t><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_F32: prep_rows_kernel<float><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    default:
+      set_error("tcb_prep_rows: unknown dtype %d", in_dtype);
+      return TCB_ERR_INVALID_ARGUMENT;
+  }
+  TCB_LAUNCH_CHECK();
+  return TCB_OK;
+}

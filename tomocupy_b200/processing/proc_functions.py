@@ -1,0 +1,127 @@
+"""Pre-processing of projection chunks.
+
+``ProcFunctions`` mirrors the reference class
+(src/tomocupy/processing/proc_functions.py:47-198) for the hot-path steps:
+``darkflat_correction`` and ``minus_log`` run as native kernels with the
+reference's float32 operation order (bit-identical results).  The other
+steps of that file (dezinger, phase retrieval, rotation, beam hardening,
+double-FOV padding) are outside this package's scope and raise
+``NotImplementedError`` when enabled, instead of silently doing nothing.
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _lib
+from ..global_vars import args, params
+
+_DT = {torch.uint16: _lib.TCB_U16, torch.uint8: _lib.TCB_U8, torch.float32: _lib.TCB_F32}
+
+
+def in_dtype_code(t: torch.Tensor) -> int:
+    try:
+        return _DT[t.dtype]
+    except KeyError:
+        raise TypeError(f"unsupported frame dtype {t.dtype}; expected uint16, uint8 or float32")
+
+
+def darkflat_stats(dark: torch.Tensor, flat: torch.Tensor, bright_ratio: float = 1.0,
+                   flat_linear: bool = False, stream=None):
+    """dark0 [nz, n], flat0 [nz, n] (and flat1 for flat_linear) from [k, nz, n] frames."""
+    nd, nz, n = dark.shape
+    nf = flat.shape[0]
+    assert flat.shape[1:] == (nz, n), "dark/flat shapes differ"
+    assert dark.dtype == flat.dtype
+    dark = dark.contiguous()
+    flat = flat.contiguous()
+    dev = dark.device
+    dark0 = torch.empty((nz, n), dtype=torch.float32, device=dev)
+    flat0 = torch.empty((nz, n), dtype=torch.float32, device=dev)
+    flat1 = torch.empty((nz, n), dtype=torch.float32, device=dev) if flat_linear else None
+    _lib.call("tcb_darkflat_stats", _lib.ptr(dark0), _lib.ptr(flat0), _lib.ptr(flat1),
+              _lib.ptr(dark), _lib.ptr(flat), nd, nf, nz, n, in_dtype_code(dark),
+              float(bright_ratio), int(flat_linear), _lib.stream_ptr(stream))
+    return dark0, flat0, flat1
+
+
+def prep_rows(out, data, dark0=None, flat0=None, flat1=None, *, darkflat=True, minus_log=True,
+              flat_linear=False, out_zstride, out_pstride, out_poff=0, out_xoff=0,
+              out_width=None, edge_pad=False, stream=None):
+    """Fused native pass over rows of a [nproj, nz, n] stack (see tcb_prep_rows)."""
+    nproj, nz, n = data.shape
+    assert data.stride(2) == 1
+    flags = 0
+    if darkflat:
+        flags |= _lib.PREP_DARKFLAT
+    if minus_log:
+        flags |= _lib.PREP_MINUS_LOG
+    if flat_linear:
+        flags |= _lib.PREP_FLAT_LINEAR
+    if edge_pad:
+        flags |= _lib.PREP_EDGE_PAD
+    _lib.call("tcb_prep_rows", _lib.ptr(out), _lib.ptr(data), _lib.ptr(dark0), _lib.ptr(flat0),
+              _lib.ptr(flat1), nproj, nz, n, data.stride(0), data.stride(1), in_dtype_code(data),
+              out_zstride, out_pstride, out_poff, out_xoff,
+              out_width if out_width is not None else out_xoff + n, flags,
+              _lib.stream_ptr(stream))
+    return out
+
+
+class ProcFunctions:
+    def __init__(self):
+        if args.beam_hardening_method != "none":
+            raise NotImplementedError("beam hardening is not part of tomocupy_b200")
+
+    def darkflat_correction(self, data, dark, flat):
+        """(data - mean(dark)) / (mean(flat/bright_ratio)*(1+1e-5) - mean(dark)), float32."""
+        flat_linear = args.flat_linear == "True" and data.shape[0] == params.nproj
+        dark0, flat0, flat1 = darkflat_stats(dark, flat, args.bright_ratio, flat_linear)
+        nproj, nz, n = data.shape
+        res = torch.empty((nproj, nz, n), dtype=torch.float32, device=data.device)
+        prep_rows(res, data, dark0, flat0, flat1, darkflat=True, minus_log=False,
+                  flat_linear=flat_linear, out_zstride=n, out_pstride=nz * n)
+        return res
+
+    def minus_log(self, data):
+        """In place: where(x<=0,1,x) -> -log -> nan_to_num(nan=6, posinf=0, neginf=0)."""
+        assert data.dtype == torch.float32 and data.is_contiguous()
+        nproj, nz, n = data.shape
+        prep_rows(data, data, darkflat=False, minus_log=True, out_zstride=n,
+                  out_pstride=nz * n)
+        return data
+
+    def remove_outliers(self, data):
+        if int(args.dezinger) > 0:
+            raise NotImplementedError("dezinger is not part of tomocupy_b200")
+        return data
+
+    def proc_sino(self, data, dark, flat, res=None):
+        """Processing of a sinogram chunk: dark/flat correction and ring removal."""
+        data = self.remove_outliers(data)
+        out = self.darkflat_correction(data, dark, flat)
+        if args.remove_stripe_method == "fw":
+            from . import remove_stripe
+            out = remove_stripe.remove_stripe_fw(out, args.fw_sigma, args.fw_filter,
+                                                 args.fw_level)
+        elif args.remove_stripe_method != "none":
+            raise NotImplementedError(
+                f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
+        if res is not None:
+            res[:] = out
+            return res
+        return out
+
+    def proc_proj(self, data, st=None, end=None, res=None):
+        """Processing of a projection chunk: -log (other steps are out of scope)."""
+        if args.retrieve_phase_method != "none":
+            raise NotImplementedError("phase retrieval is not part of tomocupy_b200")
+        if args.rotate_proj_angle != 0:
+            raise NotImplementedError("projection rotation is not part of tomocupy_b200")
+        if args.file_type == "double_fov":
+            raise NotImplementedError("double_fov padding is not part of tomocupy_b200")
+        if args.minus_log == "True":
+            data = self.minus_log(data.contiguous())
+        if res is not None:
+            res[:] = data
+            return res
+        return data

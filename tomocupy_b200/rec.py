@@ -1,0 +1,163 @@
+"""Chunked reconstruction drivers: ``GPURec.recon_all`` and ``GPURec.recon_try``.
+
+Mirrors ``GPURec`` (src/tomocupy/rec.py:62-275).  The reference's conveyor
+(read queue -> pinned staging -> H2D on stream1 -> compute on stream2 ->
+D2H on stream3, with a host ``synchronize()`` of every stream each
+iteration) becomes a device-side dependency graph: each chunk's H2D,
+compute and D2H are ordered by CUDA events only, buffers are double
+buffered, and the host blocks once at the end.  Slabs of the host stack are
+moved with one strided 2D copy each (no host repacking).  Dark/flat means
+are computed once for all rows and stay resident.
+
+``recon_device`` is the same reconstruction with the whole input already in
+device memory (no host traffic at all).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .global_vars import args, params
+from .pipeline import SinoPipeline, copy2d_rows
+from .processing.proc_functions import darkflat_stats
+
+
+def _supported():
+    if args.remove_stripe_method not in ("none",):
+        raise NotImplementedError(
+            f"remove_stripe_method={args.remove_stripe_method!r} in the fused driver")
+    if args.file_type != "standard" or args.binning != 0:
+        raise NotImplementedError("double_fov / binning are not part of tomocupy_b200")
+    if args.dtype != "float32":
+        raise NotImplementedError("the fused driver runs the float32 drop-in path")
+
+
+class GPURec:
+    """Tomographic reconstruction by sinogram chunks on one GPU."""
+
+    def __init__(self, cl_reader, cl_writer, device="cuda"):
+        _supported()
+        self.device = torch.device(device)
+        self.cl_reader = cl_reader
+        self.cl_writer = cl_writer
+        self.pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
+                                 params.center, args.fbp_filter, args.reconstruction_algorithm,
+                                 minus_log=args.minus_log == "True", device=self.device)
+        self.stream1 = torch.cuda.Stream(self.device)
+        self.stream2 = torch.cuda.Stream(self.device)
+        self.stream3 = torch.cuda.Stream(self.device)
+
+    # ------------------------------------------------------------------ helpers
+    def _stats(self, dark, flat, stream):
+        flat_linear = args.flat_linear == "True"
+        if flat_linear:
+            raise NotImplementedError("flat_linear in the fused driver")
+        return darkflat_stats(dark, flat, args.bright_ratio, False, stream)
+
+    # ------------------------------------------------------------------ full
+    def recon_all(self):
+        """Reconstruct every slice; results go to ``cl_writer`` (host or device)."""
+        data, dark, flat = self.cl_reader.frames()
+        ncz, n, nz, nproj = params.ncz, params.n, params.nz, params.nproj
+        dev = self.device
+        rec_out = self.cl_writer.allocate(nz, n)
+        s1, s2, s3 = self.stream1, self.stream2, self.stream3
+        cur = torch.cuda.current_stream(dev)
+        s1.wait_stream(cur)
+        s2.wait_stream(cur)
+        s3.wait_stream(cur)
+        # dark/flat: one upload, statistics for all rows, resident
+        with torch.cuda.stream(s1):
+            dark_d = dark.to(dev, non_blocking=True)
+            flat_d = flat.to(dev, non_blocking=True)
+        s2.wait_stream(s1)
+        with torch.cuda.stream(s2):
+            dark0, flat0, _ = self._stats(dark_d, flat_d, s2)
+        host_in = data.device.type == "cpu"
+        host_out = rec_out.device.type == "cpu"
+        dbuf = [torch.empty((nproj, ncz, n), dtype=data.dtype, device=dev) for _ in range(2)]
+        rbuf = [torch.empty((ncz, n, n), dtype=torch.float32, device=dev) for _ in range(2)]
+        h2d_done = [torch.cuda.Event() for _ in range(2)]
+        comp_done = [torch.cuda.Event() for _ in range(2)]
+        d2h_done = [torch.cuda.Event() for _ in range(2)]
+        nchunk = params.nzchunk
+        for k in range(nchunk):
+            b = k % 2
+            z0 = k * ncz
+            lz = int(params.lzchunk[k])
+            # H2D of the slab (waits until compute of chunk k-2 released dbuf[b])
+            if host_in:
+                with torch.cuda.stream(s1):
+                    if k >= 2:
+                        s1.wait_event(comp_done[b])
+                    copy2d_rows(dbuf[b][:, :lz], data[:, z0:z0 + lz], s1)
+                    h2d_done[b].record(s1)
+                src = dbuf[b][:, :lz]
+            else:
+                src = data[:, z0:z0 + lz]
+            with torch.cuda.stream(s2):
+                if host_in:
+                    s2.wait_event(h2d_done[b])
+                if k >= 2 and host_out:
+                    s2.wait_event(d2h_done[b])
+                out = rbuf[b] if (host_out or lz < ncz) else rec_out[z0:z0 + ncz]
+                self.pipe.reconstruct(out, src, dark0, flat0, z_lo=z0, stream=s2)
+                if not host_out and lz < ncz:
+                    rec_out[z0:z0 + lz].copy_(out[:lz])
+                comp_done[b].record(s2)
+            if host_out:
+                with torch.cuda.stream(s3):
+                    s3.wait_event(comp_done[b])
+                    rec_out[z0:z0 + lz].copy_(rbuf[b][:lz], non_blocking=True)
+                    d2h_done[b].record(s3)
+        cur.wait_stream(s1)
+        cur.wait_stream(s2)
+        cur.wait_stream(s3)
+        torch.cuda.synchronize(dev)
+        return rec_out
+
+    # ------------------------------------------------------------------ try
+    def recon_try(self):
+        """Reconstruct slice(s) ``params.id_slices`` for every centre in ``params.shift_array``."""
+        data, dark, flat = self.cl_reader.frames()
+        ncz, n, nproj = params.ncz, params.n, params.nproj
+        dev = self.device
+        out = torch.empty((ncz, n, n), dtype=torch.float32, device=dev)
+        for id_slice in params.id_slices:
+            z = int(id_slice)
+            row = data[:, z:z + 1].to(dev)
+            d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
+            # one prep pass into slice 0 of the padded rows, replicated to all slices
+            self.pipe.load_rows(row, d0, f0, 0)
+            self.pipe.rows[1:].copy_(self.pipe.rows[:1].expand(ncz - 1, -1, -1))
+            base = self.pipe.rows[0].clone()
+            for k in range(params.nschunk):
+                lk = int(params.lschunk[k])
+                sht = np.zeros(ncz, dtype=np.float32)
+                sht[:lk] = params.shift_array[k * ncz:k * ncz + lk]
+                if k > 0:
+                    self.pipe.rows.copy_(base.expand(ncz, -1, -1))
+                self.pipe.filter_and_backproject(out, sht)
+                for kk in range(lk):
+                    self.cl_writer.write_data_try(out[kk], params.save_centers[k * ncz + kk],
+                                                  id_slice)
+        torch.cuda.synchronize(dev)
+
+    # ------------------------------------------------------------------ device
+    def recon_device(self, data, dark0, flat0, out, stream=None):
+        """All-device reconstruction: data [nproj, nz, n] (any frame dtype, on device),
+        dark0/flat0 [nz, n] resident statistics, out [nz, n, n] float32."""
+        ncz, nz = params.ncz, params.nz
+        for k in range(params.nzchunk):
+            z0 = k * ncz
+            lz = int(params.lzchunk[k])
+            if lz == ncz:
+                self.pipe.reconstruct(out[z0:z0 + ncz], data[:, z0:z0 + ncz], dark0, flat0,
+                                      z_lo=z0, stream=stream)
+            else:
+                tmp = torch.empty((ncz, params.n, params.n), dtype=torch.float32,
+                                  device=out.device)
+                self.pipe.reconstruct(tmp, data[:, z0:z0 + lz], dark0, flat0, z_lo=z0,
+                                      stream=stream)
+                out[z0:z0 + lz].copy_(tmp[:lz])
+        return out
