@@ -159,6 +159,47 @@ int tcb_linerec_backprojection_try_lamino(tcb_linerec *h, void *f, const void *g
                                           int sz, void *stream);
 int tcb_linerec_destroy(tcb_linerec *h);
 
+/* ------------------------------------------------------------------------
+ * Laminography Fourier chain.
+ * ------------------------------------------------------------------------ */
+
+/* Replaces cfunc_fft2d (src/include/cfunc_fft2d.cuh:7-26, src/cuda/cfunc_fft2d.i:9-18).
+ * fwd: g complex [ntheta, deth, detw/2+1] <- f real [ntheta, deth, detw]
+ * (f is sign-flipped in place, as in the reference). */
+typedef struct tcb_fft2d tcb_fft2d;
+int tcb_fft2d_create(tcb_fft2d **out, size_t ntheta, size_t detw, size_t deth);
+int tcb_fft2d_fwd(tcb_fft2d *h, void *g, void *f, void *stream);
+int tcb_fft2d_destroy(tcb_fft2d *h);
+
+/* Replaces cfunc_usfft2d (src/include/cfunc_usfft2d.cuh:7-33,
+ * src/cuda/cfunc_usfft2d.i:9-18); constructor arguments in the reference's
+ * Python order (n0, n1, n2) = (slabs per call, grid y, grid x).
+ * adj: f complex [n1][n0][n2] (y, slab, x in the Python argument names)
+ *      <- g complex [2*ntheta, deth, detw/2+1]
+ * (the packed chunk of BackprojLamFourierParallel.usfft2d_chunks), theta
+ * device fp32 [ntheta], chunk index k, full detector height deth0. */
+typedef struct tcb_usfft2d tcb_usfft2d;
+int tcb_usfft2d_create(tcb_usfft2d **out, size_t n0, size_t n1, size_t n2, size_t ntheta,
+                       size_t detw, size_t deth);
+int tcb_usfft2d_adj(tcb_usfft2d *h, void *f, const void *g, const float *theta, float phi,
+                    int k, int deth0, void *stream);
+/* Fused form: rows [row0, row0+nrows) of the whole stage-1 spectrum
+ * S1 [ntheta, deth_full, detw/2+1] (conjugate mirror read in place) into
+ * S2 [n1, deth_full/2+1, n0] at frequency rows row0.. (replaces the packing
+ * of backproj_lamfourier_parallel.py:197-215 and the host copies). */
+int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1, const float *theta,
+                         float phi, int row0, int nrows, int deth_full, void *stream);
+int tcb_usfft2d_destroy(tcb_usfft2d *h);
+
+/* Replaces cfunc_usfft1d (src/include/cfunc_usfft1d.cuh:7-34,
+ * src/cuda/cfunc_usfft1d.i:9-18); constructor in the reference's Python
+ * order (n0, n1, n2, deth) = (height, rows per call, width, detector height).
+ * adj: f real [n1, n0(height), n2(width)] <- g complex [n1, deth/2+1, n2]. */
+typedef struct tcb_usfft1d tcb_usfft1d;
+int tcb_usfft1d_create(tcb_usfft1d **out, size_t n0, size_t n1, size_t n2, size_t deth);
+int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi, void *stream);
+int tcb_usfft1d_destroy(tcb_usfft1d *h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -184,3 +184,104 @@ def ref_darkflat_minus_log(data, dark, flat, bright_ratio=1.0, minus_log=True):
         res = -torch.log(res)
         res = torch.nan_to_num(res, nan=6.0, posinf=0.0, neginf=0.0)
     return res
+
+
+# --------------------------------------------------------------------------
+# laminography chain (reconstruction/lamfourierrec.py:46-73 and
+# reconstruction/backproj_lamfourier_parallel.py:57-304, device-resident)
+# --------------------------------------------------------------------------
+class RefFFT2D(_Handle):
+    op = "fft2d"
+
+    def __init__(self, ntheta, detw, deth):
+        super().__init__(False, ntheta, detw, deth)
+
+    def fwd(self, g, f, stream=None):
+        self.L.ref_fwd(self.h, g.data_ptr(), f.data_ptr(), _s(stream))
+
+
+class RefUSFFT2D(_Handle):
+    op = "usfft2d"
+
+    def __init__(self, n0, n1, n2, ntheta, detw, deth):
+        super().__init__(False, n0, n1, n2, ntheta, detw, deth)
+
+    def adj(self, f, g, theta, phi, k, deth0, stream=None):
+        self.L.ref_adj(self.h, f.data_ptr(), g.data_ptr(), theta.data_ptr(), phi, k, deth0,
+                       _s(stream))
+
+
+class RefUSFFT1D(_Handle):
+    op = "usfft1d"
+
+    def __init__(self, n0, n1, n2, deth):
+        super().__init__(False, n0, n1, n2, deth)
+
+    def adj(self, f, g, phi, stream=None):
+        self.L.ref_adj(self.h, f.data_ptr(), g.data_ptr(), phi, _s(stream))
+
+
+def ref_rec_lam(data, theta, center, lamino_angle, rh, wfilter, nthetac=8, dethc=8, n1c=8):
+    """BackprojLamFourierParallel.rec_lam with the reference operators; the
+    pinned host staging buffers become device tensors, the chunk packing and
+    copies are restated with torch.  data: [ntheta, deth, detw] float32."""
+    dev = data.device
+    ntheta, deth, detw = data.shape
+    n0, n1, n2 = rh, detw, detw
+    ne = 4 * detw
+    pad = ne // 2 - detw // 2
+    t = (torch.arange(0, ne // 2 + 1, dtype=torch.float64, device=dev) / ne).to(torch.float32)
+    phi = math.pi / 2 + lamino_angle / 180 * math.pi
+    filt = RefFilter(ne, deth, nthetac)
+    fft2 = RefFFT2D(nthetac, detw, deth)
+    us2 = RefUSFFT2D(dethc, n1, n2, ntheta, detw, dethc)
+    us1 = RefUSFFT1D(n0, n1c, n2, deth)
+    th = theta.to(torch.float32).contiguous()
+    # stage 1: filter rows of each projection, 2D FFT (fft2_chunks)
+    s1 = torch.empty((ntheta, deth, detw // 2 + 1), dtype=torch.complex64, device=dev)
+    ci = float(torch.tensor(-2.0, dtype=torch.float32) * torch.tensor(math.pi, dtype=torch.float32))
+    for st in range(0, ntheta, nthetac):
+        end = min(ntheta, st + nthetac)
+        d0 = torch.zeros((nthetac, deth, detw), dtype=torch.float32, device=dev)
+        d0[:end - st] = data[st:end]
+        tmp = torch.empty((nthetac, deth, ne), dtype=torch.float32, device=dev)
+        tmp[:, :, pad:pad + detw] = d0
+        tmp[:, :, :pad] = d0[:, :, :1]
+        tmp[:, :, pad + detw:] = d0[:, :, -1:]
+        sht = torch.zeros((nthetac, 1), dtype=torch.float32, device=dev)
+        a = -center + sht + n2 / 2                      # [nthetac, 1] float32
+        phase = (t * ci)[None, :] * a                   # (c*t)*a order of the lamino glue
+        w = torch.complex(wfilter * torch.cos(phase), wfilter * torch.sin(phase))
+        filt.filter(tmp, w)
+        d0 = tmp[:, :, pad:pad + detw].contiguous()
+        g = torch.empty((nthetac, deth, detw // 2 + 1), dtype=torch.complex64, device=dev)
+        fft2.fwd(g, d0)
+        s1[st:end] = g[:end - st]
+    # stage 2: usfft2d over chunks of frequency rows (usfft2d_chunks)
+    nrow = deth // 2 + 1
+    s2 = torch.empty((n1, nrow, n2), dtype=torch.complex64, device=dev)
+    inp = torch.zeros((2 * ntheta, dethc, detw // 2 + 1), dtype=torch.complex64, device=dev)
+    for k, st in enumerate(range(0, nrow, dethc)):
+        end = min(nrow, st + dethc)
+        s = end - st
+        inp[:ntheta, :s] = s1[:, st:end]
+        if k == 0:
+            inp[ntheta:, dethc - s:dethc - 1] = s1[:, deth - end + 1:deth - st + 1]
+            inp[ntheta:, dethc - 1] = s1[:, 0]
+        else:
+            inp[ntheta:, dethc - s:] = s1[:, deth - end + 1:deth - st + 1]
+        out = torch.empty((n1, dethc, n2), dtype=torch.complex64, device=dev)
+        us2.adj(out, inp, th, phi, k, deth)
+        s2[:, st:end] = out[:, :s]
+    # stage 3: usfft1d over chunks of rows (usfft1d_chunks)
+    s3 = torch.empty((n1, n0, n2), dtype=torch.float32, device=dev)
+    for st in range(0, n1, n1c):
+        end = min(n1, st + n1c)
+        gin = torch.zeros((n1c, nrow, n2), dtype=torch.complex64, device=dev)
+        gin[:end - st] = s2[st:end]
+        out = torch.empty((n1c, n0, n2), dtype=torch.float32, device=dev)
+        us1.adj(out, gin, phi)
+        s3[st:end] = out[:end - st]
+    torch.cuda.synchronize()
+    # stage 4: copyTransposed -> [rh, n1, n2]
+    return s3.permute(1, 0, 2).contiguous()

@@ -65,6 +65,16 @@ SIGNATURES: dict[str, list] = {
     "tcb_linerec_backprojection_try": [vp, vp, vp, vp, vp, f32, i32, vp],
     "tcb_linerec_backprojection_try_lamino": [vp, vp, vp, vp, vp, i32, vp],
     "tcb_linerec_destroy": [vp],
+    "tcb_fft2d_create": [C.POINTER(vp), sz, sz, sz],
+    "tcb_fft2d_fwd": [vp, vp, vp, vp],
+    "tcb_fft2d_destroy": [vp],
+    "tcb_usfft2d_create": [C.POINTER(vp), sz, sz, sz, sz, sz, sz],
+    "tcb_usfft2d_adj": [vp, vp, vp, vp, f32, i32, i32, vp],
+    "tcb_usfft2d_adj_rows": [vp, vp, vp, vp, f32, i32, i32, i32, vp],
+    "tcb_usfft2d_destroy": [vp],
+    "tcb_usfft1d_create": [C.POINTER(vp), sz, sz, sz, sz],
+    "tcb_usfft1d_adj": [vp, vp, vp, f32, vp],
+    "tcb_usfft1d_destroy": [vp],
 }
 
 _lib = None

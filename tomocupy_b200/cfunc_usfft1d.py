@@ -1,0 +1,23 @@
+"""Drop-in for ``tomocupy.cfunc_usfft1d`` (src/cuda/cfunc_usfft1d.i:9-18).
+
+Only the adjoint is used by the reconstruction path
+(LamFourierRec.usfft1d_adj); ``fwd`` raises NotImplementedError.
+"""
+from __future__ import annotations
+
+from . import _lib
+from ._handle import NativeHandle
+
+
+class cfunc_usfft1d(NativeHandle):
+    _destroy = "tcb_usfft1d_destroy"
+
+    def __init__(self, n0, n1, n2, deth):
+        self._set(_lib.create("tcb_usfft1d_create", int(n0), int(n1), int(n2), int(deth)))
+
+    def adj(self, f_, g_, phi, stream_):
+        _lib.call("tcb_usfft1d_adj", self._live(), _lib.ptr(f_), _lib.ptr(g_), float(phi),
+                  _lib.stream_ptr(stream_))
+
+    def fwd(self, *a, **k):
+        raise NotImplementedError("usfft1d forward is not on the reconstruction path")

@@ -1,0 +1,30 @@
+"""Drop-in for ``tomocupy.cfunc_usfft2d`` (src/cuda/cfunc_usfft2d.i:9-18).
+
+Only the adjoint is used by the reconstruction path
+(LamFourierRec.usfft2d_adj); ``fwd`` raises NotImplementedError.
+"""
+from __future__ import annotations
+
+from . import _lib
+from ._handle import NativeHandle
+
+
+class cfunc_usfft2d(NativeHandle):
+    _destroy = "tcb_usfft2d_destroy"
+
+    def __init__(self, n0, n1, n2, ntheta, detw, deth):
+        self._set(_lib.create("tcb_usfft2d_create", int(n0), int(n1), int(n2), int(ntheta),
+                              int(detw), int(deth)))
+
+    def adj(self, f_, g_, theta_, phi, k, deth0, stream_):
+        _lib.call("tcb_usfft2d_adj", self._live(), _lib.ptr(f_), _lib.ptr(g_), _lib.ptr(theta_),
+                  float(phi), int(k), int(deth0), _lib.stream_ptr(stream_))
+
+    def adj_rows(self, S2, S1, theta, phi, row0, nrows, deth_full, stream_):
+        """Fused adjoint on rows [row0, row0+nrows) of the whole stage-1 spectrum."""
+        _lib.call("tcb_usfft2d_adj_rows", self._live(), _lib.ptr(S2), _lib.ptr(S1),
+                  _lib.ptr(theta), float(phi), int(row0), int(nrows), int(deth_full),
+                  _lib.stream_ptr(stream_))
+
+    def fwd(self, *a, **k):
+        raise NotImplementedError("usfft2d forward is not on the reconstruction path")

@@ -111,8 +111,11 @@ __device__ __forceinline__ int block_exscan(int v, int *warp_tot, int &total) {
 }
 
 struct GatherSmem {
-  float accr[T][T];
-  float acci[T][T];
+  // rows padded to T+1 floats: lanes that walk a near-vertical line of
+  // samples hit rows two apart, which with a stride of T (a multiple of the 32
+  // banks) would all fall into one bank
+  float accr[T][T + 1];
+  float acci[T][T + 1];
   int seg_p[MAXSEG];     // angle | image << 20
   int seg_i0[MAXSEG];
   int seg_start[MAXSEG + 1];
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(NT) gather_tiles(const float2 *__restrict__ G,
   // centred cell coordinates of the tile: X = ix - n
   const int X0 = ix0 - n, Y0 = iy0 - n;
 
-  for (int k = threadIdx.x; k < T * T; k += NT) {
+  for (int k = threadIdx.x; k < T * (T + 1); k += NT) {
     (&sm.accr[0][0])[k] = 0.f;
     (&sm.acci[0][0])[k] = 0.f;
   }
