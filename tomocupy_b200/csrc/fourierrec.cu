@@ -5,17 +5,24 @@
 // gridding of the polar samples onto a 2x oversampled Cartesian grid
 // (eps = 1e-3, half-width m = 4), 2D inverse FFT, deapodization, circular mask.
 //
-// B200 design (this is not a transcription of the reference kernels):
+// B200 design (not a transcription of the reference kernels):
 //  * ifftshiftc before/after the 1D FFT becomes an index shift by n/2 plus a
 //    (-1)^k sign at read time, so g is transformed in a single cuFFT call.
-//  * The gridding kernel is tile-stationary: each CTA owns a T x T tile of the
-//    periodic (2n)^2 grid, finds the polar samples whose (2m+1)^2 footprint
-//    touches the tile (an analytic radial interval per angle), accumulates
-//    them in shared memory and writes the finished tile once.  No global
-//    atomics, no memset of the grid, the halo "wrap" pass disappears (the
-//    grid is periodic by construction) and the fftshift sign before the 2D
-//    FFT is applied in the store.  Tiles are dispatched centre-first because
-//    the polar sample density (and so the work per tile) peaks at the origin.
+//  * Gridding is output-stationary and atomic-free.  The periodic (2n)^2 grid
+//    is cut into 32x16-cell tiles; each warp of a tile's CTA owns one 8x4
+//    block of cells (one cell per lane) and keeps the accumulators of up to
+//    16 slice pairs in registers.  The polar samples whose (2m+1)^2 footprint
+//    reaches a tile, and for each 8x4 block the subset reaching it, depend on
+//    the angles only; they are listed once when the object is created (theta
+//    is fixed for the object's lifetime, as in the reference).  Per launch a
+//    CTA stages the spectrum values of its samples (all pairs, pair-innermost)
+//    in shared memory, and every lane adds w(cell, sample) * g[pair] for the
+//    samples of its block: two exp per lane per sample serve all pairs.
+//    There is no memset, no wrap pass (the grid is periodic by
+//    construction), no global atomics, the summation order is fixed (results
+//    are bit-reproducible) and the fftshift sign before the 2D FFT is
+//    applied in the store.  Tiles are dispatched centre-first because the
+//    polar sample density peaks at the origin.
 //  * The 2D FFT runs on a dense (2n)^2 grid; the fftshift after it, divphi,
 //    circ and (optionally) the real/imaginary unpacking of the slice pairs
 //    are one kernel.
@@ -35,11 +42,15 @@
 namespace tcb {
 namespace fr {
 
-constexpr int M = 4;          // gridding half-width for eps = 1e-3 (any n)
-constexpr int T = 64;         // grid tile edge
-constexpr int NT = 256;       // threads per gridding CTA
-constexpr int CHUNK = NT;     // angles enumerated per pass
-constexpr int MAXSEG = 4 * CHUNK;
+constexpr int M = 4;            // gridding half-width for eps = 1e-3 (any n)
+constexpr int TX = 32, TY = 16; // grid tile (cells)
+constexpr int RX = 8, RY = 4;   // cell block owned by one warp (one cell per lane)
+constexpr int NRX = TX / RX, NRY = TY / RY;
+constexpr int NREG = NRX * NRY; // 16 blocks = 16 warps per tile
+constexpr int NTH = NREG * 32;  // 512 threads
+constexpr int SC = 256;         // samples staged per chunk
+constexpr int ZMAX = 16;        // slice pairs per CTA
+constexpr int SETUP_NT = 256;
 // Margin of the ell/(2n) table: __cosf/__sinf may exceed 1 in magnitude by an
 // ulp, which moves floor(2n*x0) one cell below -n.
 constexpr int EPAD = 8;
@@ -47,7 +58,7 @@ constexpr int EPAD = 8;
 struct Geom {
   int n, nproj, nz;
   int twon;        // 2n (grid edge)
-  int ntx;         // tiles per grid edge
+  int ntx, nty;    // tiles per grid axis
   float mu, coeff0, coeff1, scale;
 };
 
@@ -64,6 +75,20 @@ __global__ void setup_tables(float2 *__restrict__ cs, float *__restrict__ rtab,
     int ell = t - n - M - EPAD;
     etab[t] = ell / (float)(2 * n);
   }
+}
+
+// Sample position exactly as takexy computes it, and the footprint origin.
+__device__ __forceinline__ void sample_pos(const float2 *__restrict__ cs,
+                                           const float *__restrict__ rtab, int p, int i,
+                                           float twonf, float &x0, float &y0, int &fx, int &fy) {
+  float2 c = cs[p];
+  float r = rtab[i];
+  x0 = r * c.x;
+  y0 = -(r * c.y);
+  if (x0 >= 0.5f) x0 = 0.5f - 1e-5;
+  if (y0 >= 0.5f) y0 = 0.5f - 1e-5;
+  fx = (int)floorf(twonf * x0);
+  fy = (int)floorf(twonf * y0);
 }
 
 // Interval of u with u*c in [a, b] (u unbounded when c ~ 0 and 0 in [a, b]).
@@ -83,7 +108,7 @@ __device__ __forceinline__ void u_interval(float c, float a, float b, float &lo,
   hi = fmaxf(u0, u1);
 }
 
-// Block-wide exclusive scan of one int per thread (NT threads).
+template <int NT>
 __device__ __forceinline__ int block_exscan(int v, int *warp_tot, int &total) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int x = v;
@@ -101,7 +126,7 @@ __device__ __forceinline__ int block_exscan(int v, int *warp_tot, int &total) {
       int y = __shfl_up_sync(0xffffffffu, t, o);
       if (lane >= o) t += y;
     }
-    if (lane < NT / 32) warp_tot[lane] = t;  // inclusive prefix of warp totals
+    if (lane < NT / 32) warp_tot[lane] = t;
   }
   __syncthreads();
   int base = wid > 0 ? warp_tot[wid - 1] : 0;
@@ -110,71 +135,64 @@ __device__ __forceinline__ int block_exscan(int v, int *warp_tot, int &total) {
   return base + x - v;
 }
 
-struct GatherSmem {
-  // rows padded to T+1 floats: lanes that walk a near-vertical line of
-  // samples hit rows two apart, which with a stride of T (a multiple of the 32
-  // banks) would all fall into one bank
-  float accr[T][T + 1];
-  float acci[T][T + 1];
-  int seg_p[MAXSEG];     // angle | image << 20
-  int seg_i0[MAXSEG];
-  int seg_start[MAXSEG + 1];
-  int warp_tot[NT / 32];
-};
-
-// Gridding of the polar spectrum onto the periodic (2n)^2 grid.
-//   G: [nz, nproj, n] complex, plain forward FFT of each projection
-//   grid: [nz, 2n, 2n] complex, output (fftshift sign included)
-__global__ void __launch_bounds__(NT) gather_tiles(const float2 *__restrict__ G,
-                                                   float2 *__restrict__ grid,
-                                                   const float2 *__restrict__ cs,
-                                                   const float *__restrict__ rtab,
-                                                   const float *__restrict__ etab,
-                                                   const int *__restrict__ tile_order,
-                                                   Geom geo) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  GatherSmem &sm = *reinterpret_cast<GatherSmem *>(smem_raw);
-  const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
-  const int z = blockIdx.x % geo.nz;
-  const int tile = tile_order[blockIdx.x / geo.nz];
-  const int ix0 = (tile % geo.ntx) * T, iy0 = (tile / geo.ntx) * T;
-  const int tw = min(T, twon - ix0), th = min(T, twon - iy0);
-  // centred cell coordinates of the tile: X = ix - n
-  const int X0 = ix0 - n, Y0 = iy0 - n;
-
-  for (int k = threadIdx.x; k < T * (T + 1); k += NT) {
-    (&sm.accr[0][0])[k] = 0.f;
-    (&sm.acci[0][0])[k] = 0.f;
+// Tile-local range [a, b] of the footprint cells (periodic grid) along one
+// axis; returns false when the footprint misses the tile.
+__device__ __forceinline__ bool local_range(int f, int origin, int width, int twon, int &a,
+                                            int &b) {
+  int s = f - M - origin;  // centred cells: footprint start relative to the tile
+  s %= twon;
+  if (s < 0) s += twon;
+  if (s < width) {
+    a = s;
+    b = min(s + 2 * M, width - 1);
+    return true;
   }
+  if (s + 2 * M >= twon) {  // wraps around into the tile's start
+    a = 0;
+    b = s + 2 * M - twon;
+    if (b >= width) b = width - 1;
+    return true;
+  }
+  return false;
+}
 
-  // Periodic images of the sample footprint that can reach this tile.
+// ---- per-geometry sample lists ------------------------------------------
+// pass 0: count the samples whose footprint reaches each tile;
+// pass 1: write them (packed p*n+i) in angle-then-radius order.
+__global__ void __launch_bounds__(SETUP_NT)
+    list_tile_samples(const float2 *__restrict__ cs, const float *__restrict__ rtab, Geom geo,
+                      int pass, int *__restrict__ counts, const long long *__restrict__ offs,
+                      int *__restrict__ list) {
+  __shared__ int warp_tot[SETUP_NT / 32];
+  const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
+  const int tile = blockIdx.x;
+  const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
+  const int tw = min(TX, twon - ix0), th = min(TY, twon - iy0);
+  const int X0 = ix0 - n, Y0 = iy0 - n;
+  const float twonf = (float)(2 * n);
   int kx_lo = 1, kx_hi = -1, ky_lo = 1, ky_hi = -1;
   for (int k = -1; k <= 1; k++) {
-    // footprint cells ell in [fx-M, fx+M], fx in [-n, n-1]; ell + 2n*k in tile
     int lo = X0 - 2 * n * k, hi = X0 + tw - 1 - 2 * n * k;
-    if (hi >= -n - M && lo <= n - 1 + M) { kx_lo = min(kx_lo, k); kx_hi = max(kx_hi, k); }
+    if (hi >= -n - M - 1 && lo <= n - 1 + M) { kx_lo = min(kx_lo, k); kx_hi = max(kx_hi, k); }
     lo = Y0 - 2 * n * k; hi = Y0 + th - 1 - 2 * n * k;
-    if (hi >= -n - M && lo <= n - 1 + M) { ky_lo = min(ky_lo, k); ky_hi = max(ky_hi, k); }
+    if (hi >= -n - M - 1 && lo <= n - 1 + M) { ky_lo = min(ky_lo, k); ky_hi = max(ky_hi, k); }
   }
-
-  const float2 *Gz = G + (size_t)z * nproj * n;
-  const float twonf = (float)(2 * n);
-  const int half = n / 2;
-
-  for (int pc = 0; pc < nproj; pc += CHUNK) {
-    // ---- enumerate (angle, image) segments of candidate samples ----
+  long long base = pass ? offs[tile] : 0;
+  int running = 0;
+  for (int pc = 0; pc < nproj; pc += SETUP_NT) {
     int p = pc + threadIdx.x;
-    int my_i0[4], my_len[4], my_img[4];
-    int nseg = 0, ncand = 0;
+    int cnt = 0;
+    int i0s[4], i1s[4], ks[4];
+    int nr = 0;
     if (p < nproj) {
-      float2 csp = cs[p];
+      float2 c = cs[p];
       for (int ky = ky_lo; ky <= ky_hi; ky++)
         for (int kx = kx_lo; kx <= kx_hi; kx++) {
-          float ax = (float)(X0 - M - 2 * n * kx - 2), bx = (float)(X0 + tw - 1 + M - 2 * n * kx + 2);
-          float ay = (float)(Y0 - M - 2 * n * ky - 2), by = (float)(Y0 + th - 1 + M - 2 * n * ky + 2);
+          float ax = (float)(X0 - M - 2 * n * kx - 3), bx = (float)(X0 + tw - 1 + M - 2 * n * kx + 3);
+          float ay = (float)(Y0 - M - 2 * n * ky - 3), by = (float)(Y0 + th - 1 + M - 2 * n * ky + 3);
           float lo0, hi0, lo1, hi1;
-          u_interval(csp.x, ax, bx, lo0, hi0);   // fx ~ u*cos
-          u_interval(-csp.y, ay, by, lo1, hi1);  // fy ~ -u*sin
+          u_interval(c.x, ax, bx, lo0, hi0);   // fx ~ u*cos, u = 2i - n
+          u_interval(-c.y, ay, by, lo1, hi1);  // fy ~ -u*sin
           float lo = fmaxf(lo0, lo1), hi = fminf(hi0, hi1);
           if (lo > hi) continue;
           lo = fmaxf(lo, -2.f * n);
@@ -182,107 +200,222 @@ __global__ void __launch_bounds__(NT) gather_tiles(const float2 *__restrict__ G,
           int i0 = max(0, (int)floorf((lo + n) * 0.5f) - 1);
           int i1 = min(n - 1, (int)ceilf((hi + n) * 0.5f) + 1);
           if (i1 < i0) continue;
-          my_i0[nseg] = i0;
-          my_len[nseg] = i1 - i0 + 1;
-          my_img[nseg] = (kx + 1) + 3 * (ky + 1);
-          ncand += i1 - i0 + 1;
-          nseg++;
+          i0s[nr] = i0; i1s[nr] = i1; ks[nr] = (kx + 1) + 3 * (ky + 1);
+          nr++;
         }
-    }
-    int seg_total, cand_total;
-    int seg_off = block_exscan(nseg, sm.warp_tot, seg_total);
-    int cand_off = block_exscan(ncand, sm.warp_tot, cand_total);
-    if (cand_total == 0) continue;  // uniform across the block
-    {
-      int c = cand_off;
-      for (int k = 0; k < nseg; k++) {
-        sm.seg_p[seg_off + k] = p | (my_img[k] << 20);
-        sm.seg_i0[seg_off + k] = my_i0[k];
-        sm.seg_start[seg_off + k] = c;
-        c += my_len[k];
+      for (int q = 0; q < nr; q++) {
+        int kx = ks[q] % 3 - 1, ky = ks[q] / 3 - 1;
+        for (int i = i0s[q]; i <= i1s[q]; i++) {
+          float x0, y0;
+          int fx, fy;
+          sample_pos(cs, rtab, p, i, twonf, x0, y0, fx, fy);
+          int ax = fx - M + 2 * n * kx, ay = fy - M + 2 * n * ky;
+          if (ax <= X0 + tw - 1 && ax + 2 * M >= X0 && ay <= Y0 + th - 1 && ay + 2 * M >= Y0)
+            cnt++;
+        }
       }
-      if (threadIdx.x == 0) sm.seg_start[seg_total] = cand_total;
+    }
+    int total;
+    int off = block_exscan<SETUP_NT>(cnt, warp_tot, total);
+    if (pass && p < nproj && cnt > 0) {
+      int w = 0;
+      for (int q = 0; q < nr; q++) {
+        int kx = ks[q] % 3 - 1, ky = ks[q] / 3 - 1;
+        for (int i = i0s[q]; i <= i1s[q]; i++) {
+          float x0, y0;
+          int fx, fy;
+          sample_pos(cs, rtab, p, i, twonf, x0, y0, fx, fy);
+          int ax = fx - M + 2 * n * kx, ay = fy - M + 2 * n * ky;
+          if (ax <= X0 + tw - 1 && ax + 2 * M >= X0 && ay <= Y0 + th - 1 && ay + 2 * M >= Y0)
+            list[base + running + off + (w++)] = p * n + i;
+        }
+      }
+    }
+    running += total;
+  }
+  if (!pass && threadIdx.x == 0) counts[tile] = running;
+}
+
+// pass 0: count, for each 8x4 block of each tile, the tile samples reaching
+// it; pass 1: write their tile-local indices (ascending).
+__global__ void __launch_bounds__(NTH)
+    list_block_samples(const float2 *__restrict__ cs, const float *__restrict__ rtab, Geom geo,
+                       const long long *__restrict__ toffs, const int *__restrict__ tlist,
+                       int pass, int *__restrict__ counts, const long long *__restrict__ boffs,
+                       int *__restrict__ blist) {
+  __shared__ int wcnt[NREG][NTH / 32];
+  __shared__ int run[NREG];
+  const int n = geo.n, twon = geo.twon;
+  const int tile = blockIdx.x;
+  const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
+  const int tw = min(TX, twon - ix0), th = min(TY, twon - iy0);
+  const int X0 = ix0 - n, Y0 = iy0 - n;
+  const float twonf = (float)(2 * n);
+  const long long t0 = toffs[tile];
+  const int S = (int)(toffs[tile + 1] - t0);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x < NREG) run[threadIdx.x] = 0;
+  __syncthreads();
+  for (int base = 0; base < S; base += NTH) {
+    int k = base + threadIdx.x;
+    unsigned mask = 0;
+    if (k < S) {
+      int s = tlist[t0 + k];
+      int p = s / n, i = s % n;
+      float x0, y0;
+      int fx, fy, xa, xb, ya, yb;
+      sample_pos(cs, rtab, p, i, twonf, x0, y0, fx, fy);
+      if (local_range(fx, X0, tw, twon, xa, xb) && local_range(fy, Y0, th, twon, ya, yb)) {
+        for (int ry = ya / RY; ry <= yb / RY; ry++)
+          for (int rx = xa / RX; rx <= xb / RX; rx++) mask |= 1u << (ry * NRX + rx);
+      }
+    }
+    unsigned ballots[NREG];
+#pragma unroll
+    for (int r = 0; r < NREG; r++) {
+      ballots[r] = __ballot_sync(0xffffffffu, (mask >> r) & 1u);
+      if (lane == 0) wcnt[r][wid] = __popc(ballots[r]);
     }
     __syncthreads();
-
-    // ---- scatter the candidates into the shared tile ----
-    for (int j = threadIdx.x; j < cand_total; j += NT) {
-      int lo = 0, hi = seg_total - 1;
-      while (lo < hi) {  // last segment with start <= j
-        int mid = (lo + hi + 1) >> 1;
-        if (sm.seg_start[mid] <= j) lo = mid; else hi = mid - 1;
+    if (threadIdx.x < NREG) {  // exclusive offsets of each warp within this chunk
+      int r = threadIdx.x, acc = run[r];
+      for (int w = 0; w < NTH / 32; w++) {
+        int c = wcnt[r][w];
+        wcnt[r][w] = acc;
+        acc += c;
       }
-      int pp = sm.seg_p[lo];
-      int img = pp >> 20;
-      int ang = pp & 0xFFFFF;
-      int i = sm.seg_i0[lo] + (j - sm.seg_start[lo]);
-      float2 csa = cs[ang];
-      float r = rtab[i];
-      // sample position exactly as takexy computes it
-      float x0 = r * csa.x;
-      float y0 = -(r * csa.y);
-      if (x0 >= 0.5f) x0 = 0.5f - 1e-5;
-      if (y0 >= 0.5f) y0 = 0.5f - 1e-5;
-      int b0 = (int)floorf(twonf * x0) - M;
-      int b1 = (int)floorf(twonf * y0) - M;
-      int kx = img % 3 - 1, ky = img / 3 - 1;
-      // tile-local coordinates of the footprint corner
-      int lx0 = b0 + 2 * n * kx - X0;
-      int ly0 = b1 + 2 * n * ky - Y0;
-      if (lx0 > tw - 1 || lx0 + 2 * M < 0 || ly0 > th - 1 || ly0 + 2 * M < 0) continue;
-      // spectrum value with the ifftshift pair folded in: (-1)^i G[(i+n/2) mod n]
-      int ii = i + half;
-      if (ii >= n) ii -= n;
-      float2 gv = Gz[(size_t)ang * n + ii];
-      float sg = (i & 1) ? -geo.scale : geo.scale;
-      float gx = gv.x * sg, gy = gv.y * sg;
-      float k0[2 * M + 1], k1[2 * M + 1];
+      run[r] = acc;
+    }
+    __syncthreads();
+    if (pass) {
+      unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-      for (int t = 0; t < 2 * M + 1; t++) {
-        float w0 = etab[b0 + t + n + M + EPAD] - x0;
-        k0[t] = __expf(geo.coeff1 * w0 * w0);
-        float w1 = etab[b1 + t + n + M + EPAD] - y0;
-        k1[t] = __expf(geo.coeff1 * w1 * w1);
-      }
-      if (lx0 >= 0 && lx0 + 2 * M < tw && ly0 >= 0 && ly0 + 2 * M < th) {
-#pragma unroll
-        for (int t1 = 0; t1 < 2 * M + 1; t1++) {
-#pragma unroll
-          for (int t0 = 0; t0 < 2 * M + 1; t0++) {
-            float w = geo.coeff0 * (k0[t0] * k1[t1]);
-            atomicAdd(&sm.accr[ly0 + t1][lx0 + t0], w * gx);
-            atomicAdd(&sm.acci[ly0 + t1][lx0 + t0], w * gy);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int t1 = 0; t1 < 2 * M + 1; t1++) {
-          int ly = ly0 + t1;
-          if (ly < 0 || ly >= th) continue;
-#pragma unroll
-          for (int t0 = 0; t0 < 2 * M + 1; t0++) {
-            int lx = lx0 + t0;
-            if (lx < 0 || lx >= tw) continue;
-            float w = geo.coeff0 * (k0[t0] * k1[t1]);
-            atomicAdd(&sm.accr[ly][lx], w * gx);
-            atomicAdd(&sm.acci[ly][lx], w * gy);
-          }
-        }
-      }
+      for (int r = 0; r < NREG; r++)
+        if ((mask >> r) & 1u)
+          blist[boffs[tile * NREG + r] + wcnt[r][wid] + __popc(ballots[r] & lt)] = k;
     }
     __syncthreads();
   }
+  if (!pass && threadIdx.x < NREG) counts[tile * NREG + threadIdx.x] = run[threadIdx.x];
+}
 
-  // ---- store the tile with the pre-FFT fftshift sign ----
-  float2 *gz = grid + (size_t)z * twon * twon;
-  for (int k = threadIdx.x; k < T * T; k += NT) {
-    int ly = k / T, lx = k % T;
-    if (ly >= th || lx >= tw) continue;
-    int ix = ix0 + lx, iy = iy0 + ly;
-    // sign of fftshiftc on the (2n+2m)^2 buffer at index (ix+m, iy+m)
-    int sx = 1 - 2 * ((ix + M + 1) % 2), sy = 1 - 2 * ((iy + M + 1) % 2);
-    float sgn = (float)(sx * sy);
-    gz[(size_t)iy * twon + ix] = make_float2(sm.accr[ly][lx] * sgn, sm.acci[ly][lx] * sgn);
+// ---- gridding --------------------------------------------------------------
+// G: [nz, nproj, n] complex, plain forward FFT of each projection.
+// grid: [nz, 2n, 2n] complex (fftshift sign included).
+template <int Z>
+struct GridSmem {
+  float4 g[Z / 2][SC];  // (g_z.x, g_z.y, g_z+1.x, g_z+1.y) of each staged sample
+  float4 pos[SC];       // x0, y0, fx, fy (ints stored bitwise)
+};
+
+template <int Z>
+__global__ void __launch_bounds__(NTH, 2)
+    grid_blocks(const float2 *__restrict__ G, float2 *__restrict__ grid,
+                const float2 *__restrict__ cs, const float *__restrict__ rtab,
+                const float *__restrict__ etab, const int *__restrict__ tile_order,
+                const long long *__restrict__ toffs, const int *__restrict__ tlist,
+                const long long *__restrict__ boffs, const int *__restrict__ blist, Geom geo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GridSmem<Z> &sm = *reinterpret_cast<GridSmem<Z> *>(smem_raw);
+  const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
+  const int zgroups = (geo.nz + Z - 1) / Z;
+  const int tile = tile_order[blockIdx.x / zgroups];
+  const int z0 = (blockIdx.x % zgroups) * Z;
+  const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // this lane's cell
+  const int cx = ix0 + (wid % NRX) * RX + (lane % RX);
+  const int cy = iy0 + (wid / NRX) * RY + (lane / RX);
+  const int X = cx - n, Y = cy - n;
+  const float twonf = (float)(2 * n);
+  const int half = n / 2;
+  float ar[Z], ai[Z];
+#pragma unroll
+  for (int z = 0; z < Z; z++) ar[z] = ai[z] = 0.f;
+
+  const long long t0 = toffs[tile];
+  const int S = (int)(toffs[tile + 1] - t0);
+  long long bcur = boffs[tile * NREG + wid];
+  const long long bend = boffs[tile * NREG + wid + 1];
+
+  for (int c0 = 0; c0 < S; c0 += SC) {
+    const int cnt = min(SC, S - c0);
+    // stage positions
+    for (int k = threadIdx.x; k < cnt; k += NTH) {
+      int s = tlist[t0 + c0 + k];
+      int p = s / n, i = s % n;
+      float x0, y0;
+      int fx, fy;
+      sample_pos(cs, rtab, p, i, twonf, x0, y0, fx, fy);
+      sm.pos[k] = make_float4(x0, y0, __int_as_float(fx), __int_as_float(fy));
+    }
+    // stage spectrum values of Z pairs, pair-innermost; consecutive threads
+    // read consecutive samples of one pair (coalesced along the radius)
+    for (int e = threadIdx.x; e < cnt * (Z / 2); e += NTH) {
+      int k = e % cnt, zp = e / cnt;
+      int s = tlist[t0 + c0 + k];
+      int p = s / n, i = s % n;
+      int ii = i + half;
+      if (ii >= n) ii -= n;
+      float sg = (i & 1) ? -geo.scale : geo.scale;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      int za = z0 + 2 * zp, zb = za + 1;
+      if (za < geo.nz) {
+        float2 a = G[((size_t)za * nproj + p) * n + ii];
+        v.x = a.x * sg;
+        v.y = a.y * sg;
+      }
+      if (zb < geo.nz) {
+        float2 b = G[((size_t)zb * nproj + p) * n + ii];
+        v.z = b.x * sg;
+        v.w = b.y * sg;
+      }
+      sm.g[zp][k] = v;
+    }
+    __syncthreads();
+    // this warp's samples within the chunk (block list is ascending)
+    const int cend = c0 + cnt;
+    while (bcur < bend) {
+      int idx = (bcur + lane < bend) ? blist[bcur + lane] : 0x7fffffff;
+      unsigned inb = __ballot_sync(0xffffffffu, idx < cend);
+      int m = __popc(inb);
+      for (int t = 0; t < m; t++) {
+        int j = __shfl_sync(0xffffffffu, idx, t) - c0;
+        float4 ps = sm.pos[j];
+        int fx = __float_as_int(ps.z), fy = __float_as_int(ps.w);
+        // periodic offset of this lane's cell inside the footprint
+        int dx = X - (fx - M);
+        if (dx < 0) dx += twon; else if (dx >= twon) dx -= twon;
+        int dy = Y - (fy - M);
+        if (dy < 0) dy += twon; else if (dy >= twon) dy -= twon;
+        float w = 0.f;
+        if (dx <= 2 * M && dy <= 2 * M) {
+          float w0 = etab[fx - M + dx + n + M + EPAD] - ps.x;
+          float w1 = etab[fy - M + dy + n + M + EPAD] - ps.y;
+          w = __expf(geo.coeff1 * w0 * w0) * __expf(geo.coeff1 * w1 * w1);
+        }
+#pragma unroll
+        for (int zp = 0; zp < Z / 2; zp++) {
+          float4 v = sm.g[zp][j];
+          ar[2 * zp] = fmaf(w, v.x, ar[2 * zp]);
+          ai[2 * zp] = fmaf(w, v.y, ai[2 * zp]);
+          ar[2 * zp + 1] = fmaf(w, v.z, ar[2 * zp + 1]);
+          ai[2 * zp + 1] = fmaf(w, v.w, ai[2 * zp + 1]);
+        }
+      }
+      bcur += m;
+      if (m < 32) break;
+    }
+    __syncthreads();
+  }
+  // store with coeff0 and the pre-FFT fftshift sign of the (2n+2m)^2 buffer
+  if (cx < twon && cy < twon) {
+    int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
+    float sgn = (float)(sx * sy) * geo.coeff0;
+#pragma unroll
+    for (int z = 0; z < Z; z++)
+      if (z0 + z < geo.nz)
+        grid[((size_t)(z0 + z) * twon + cy) * twon + cx] = make_float2(ar[z] * sgn, ai[z] * sgn);
   }
 }
 
@@ -354,10 +487,15 @@ struct tcb_fourierrec {
   float *rtab = nullptr;
   float *etab = nullptr;
   int *tile_order = nullptr;
+  long long *toffs = nullptr;  // [ntiles+1] offsets into tlist
+  int *tlist = nullptr;        // samples per tile (p*n+i)
+  long long *boffs = nullptr;  // [ntiles*16+1] offsets into blist
+  int *blist = nullptr;        // tile-local sample indices per 8x4 block
   float2 *grid = nullptr;
   float2 *g32 = nullptr;  // fp32 staging of g (FLOAT16 only)
   cufftHandle plan1d = 0, plan2d = 0;
   int ntiles = 0;
+  size_t list_bytes = 0;
 };
 
 using namespace tcb;
@@ -372,16 +510,32 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->rtab);
   cudaFree(h->etab);
   cudaFree(h->tile_order);
+  cudaFree(h->toffs);
+  cudaFree(h->tlist);
+  cudaFree(h->boffs);
+  cudaFree(h->blist);
   cudaFree(h->grid);
   cudaFree(h->g32);
   h->plan1d = h->plan2d = 0;
   h->cs = nullptr;
   h->rtab = h->etab = nullptr;
   h->tile_order = nullptr;
+  h->toffs = h->boffs = nullptr;
+  h->tlist = h->blist = nullptr;
   h->grid = h->g32 = nullptr;
 }
 
-constexpr size_t kGatherSmem = sizeof(GatherSmem);
+template <int Z>
+int launch_grid(tcb_fourierrec *h, const float2 *gc, cudaStream_t s) {
+  const Geom &geo = h->geo;
+  unsigned zgroups = (unsigned)((h->nz + Z - 1) / Z);
+  grid_blocks<Z><<<(unsigned)h->ntiles * zgroups, NTH, sizeof(GridSmem<Z>), s>>>(
+      gc, h->grid, h->cs, h->rtab, h->etab, h->tile_order, h->toffs, h->tlist, h->boffs,
+      h->blist, geo);
+  TCB_LAUNCH_CHECK();
+  count_launch();
+  return TCB_OK;
+}
 
 int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   TCB_CHECK_ARG(h, "fourierrec: null handle");
@@ -405,10 +559,12 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   }
   {
     StageTimer st("fr_gather", s);
-    gather_tiles<<<(unsigned)(h->ntiles * h->nz), NT, kGatherSmem, s>>>(
-        gc, h->grid, h->cs, h->rtab, h->etab, h->tile_order, geo);
-    TCB_LAUNCH_CHECK();
-    count_launch();
+    int rc;
+    if (h->nz >= 16) rc = launch_grid<16>(h, gc, s);
+    else if (h->nz >= 8) rc = launch_grid<8>(h, gc, s);
+    else if (h->nz >= 4) rc = launch_grid<4>(h, gc, s);
+    else rc = launch_grid<2>(h, gc, s);
+    if (rc != TCB_OK) return rc;
   }
   {
     StageTimer st("fr_fft2d", s);
@@ -428,6 +584,60 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   return TCB_OK;
 }
 
+// Exclusive prefix sums of device counts -> device offsets (setup only).
+int scan_counts(const int *d_counts, long long *d_offs, size_t count, long long &total) {
+  std::vector<int> c(count);
+  std::vector<long long> o(count + 1);
+  TCB_CUDA(cudaMemcpy(c.data(), d_counts, count * sizeof(int), cudaMemcpyDeviceToHost));
+  o[0] = 0;
+  for (size_t k = 0; k < count; k++) o[k + 1] = o[k] + c[k];
+  TCB_CUDA(cudaMemcpy(d_offs, o.data(), (count + 1) * sizeof(long long),
+                      cudaMemcpyHostToDevice));
+  total = o[count];
+  return TCB_OK;
+}
+
+// Build the per-tile and per-block sample lists (depends on theta and n only).
+int build_lists(tcb_fourierrec *h) {
+  const Geom &geo = h->geo;
+  const int nt = h->ntiles;
+  int *counts = nullptr;
+  TCB_CUDA(cudaMalloc(&counts, (size_t)nt * NREG * sizeof(int)));
+  int st = TCB_OK;
+  long long ntot = 0, nbtot = 0;
+  do {
+    list_tile_samples<<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 0, counts, nullptr, nullptr);
+    if (cudaGetLastError() != cudaSuccess) { st = TCB_ERR_CUDA; break; }
+    if ((st = scan_counts(counts, h->toffs, nt, ntot)) != TCB_OK) break;
+    if (cudaMalloc(&h->tlist, std::max<long long>(ntot, 1) * sizeof(int)) != cudaSuccess) {
+      st = TCB_ERR_OUT_OF_MEMORY;
+      break;
+    }
+    list_tile_samples<<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 1, nullptr, h->toffs, h->tlist);
+    list_block_samples<<<nt, NTH>>>(h->cs, h->rtab, geo, h->toffs, h->tlist, 0, counts,
+                                    nullptr, nullptr);
+    if (cudaGetLastError() != cudaSuccess) { st = TCB_ERR_CUDA; break; }
+    if ((st = scan_counts(counts, h->boffs, (size_t)nt * NREG, nbtot)) != TCB_OK) break;
+    if (cudaMalloc(&h->blist, std::max<long long>(nbtot, 1) * sizeof(int)) != cudaSuccess) {
+      st = TCB_ERR_OUT_OF_MEMORY;
+      break;
+    }
+    list_block_samples<<<nt, NTH>>>(h->cs, h->rtab, geo, h->toffs, h->tlist, 1, nullptr,
+                                    h->boffs, h->blist);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      set_error("fourierrec: list construction failed: %s", cudaGetErrorString(e));
+      st = TCB_ERR_CUDA;
+      break;
+    }
+  } while (0);
+  cudaFree(counts);
+  if (st == TCB_ERR_OUT_OF_MEMORY) set_error("fourierrec: out of memory for sample lists");
+  if (st == TCB_ERR_CUDA && tcb_last_error()[0] == 0) set_error("fourierrec: list kernel failed");
+  h->list_bytes = (size_t)(ntot + nbtot) * sizeof(int);
+  return st;
+}
+
 }  // namespace
 
 extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t nz,
@@ -435,14 +645,15 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   TCB_CHECK_ARG(out, "tcb_fourierrec_create: null out");
   *out = nullptr;
   TCB_CHECK_ARG(theta, "tcb_fourierrec_create: null theta");
-  // n >= T keeps at most two periodic images of a footprint per grid axis
-  // inside one tile (the enumeration below stores up to four segments per angle).
-  TCB_CHECK_ARG(n >= (size_t)T && n % 2 == 0 && n <= 32768,
-                "tcb_fourierrec_create: n=%zu must be even and in [%d, 32768]", n, T);
+  // n >= TX keeps a 9-cell footprint from reaching one tile through two
+  // periodic images.
+  TCB_CHECK_ARG(n >= (size_t)TX && n % 2 == 0 && n <= 32768,
+                "tcb_fourierrec_create: n=%zu must be even and in [%d, 32768]", n, TX);
   TCB_CHECK_ARG(nproj >= 1 && nproj < (1u << 20), "tcb_fourierrec_create: bad nproj %zu",
                 nproj);
   TCB_CHECK_ARG(nz >= 1, "tcb_fourierrec_create: nz must be >= 1");
-  TCB_CHECK_ARG(nproj * nz < (1ull << 31), "tcb_fourierrec_create: nproj*nz too large");
+  TCB_CHECK_ARG(nproj * nz < (1ull << 31) && nproj * n < (1ull << 31),
+                "tcb_fourierrec_create: nproj*nz or nproj*n too large");
   TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
                 "tcb_fourierrec_create: bad precision %d", precision);
   // Constants exactly as the reference constructor computes them
@@ -463,12 +674,13 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   geo.nproj = (int)nproj;
   geo.nz = (int)nz;
   geo.twon = (int)(2 * n);
-  geo.ntx = (int)ceil_div(2 * n, T);
+  geo.ntx = (int)ceil_div(2 * n, TX);
+  geo.nty = (int)ceil_div(2 * n, TY);
   geo.mu = mu;
   geo.coeff0 = TCB_PI_F / (mu * (4 * n * n));
   geo.coeff1 = -TCB_PI_F * TCB_PI_F / mu;
   geo.scale = 4.0f / n;
-  h->ntiles = geo.ntx * geo.ntx;
+  h->ntiles = geo.ntx * geo.nty;
 
   auto fail = [&](int code) {
     fr_release(h);
@@ -488,6 +700,8 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   FR_ALLOC(h->rtab, n * sizeof(float));
   FR_ALLOC(h->etab, (2 * n + 2 * M + 1 + 2 * EPAD) * sizeof(float));
   FR_ALLOC(h->tile_order, h->ntiles * sizeof(int));
+  FR_ALLOC(h->toffs, (h->ntiles + 1) * sizeof(long long));
+  FR_ALLOC(h->boffs, ((size_t)h->ntiles * NREG + 1) * sizeof(long long));
   FR_ALLOC(h->grid, nz * 4 * n * n * sizeof(float2));
   if (precision == TCB_FLOAT16) FR_ALLOC(h->g32, nz * nproj * n * sizeof(float2));
 #undef FR_ALLOC
@@ -497,8 +711,8 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   std::vector<float> dist(h->ntiles);
   for (int t = 0; t < h->ntiles; t++) {
     order[t] = t;
-    float cx = (t % geo.ntx) * T + 0.5f * T - (float)n;
-    float cy = (t / geo.ntx) * T + 0.5f * T - (float)n;
+    float cx = (t % geo.ntx) * TX + 0.5f * TX - (float)n;
+    float cy = (t / geo.ntx) * TY + 0.5f * TY - (float)n;
     dist[t] = cx * cx + cy * cy;
   }
   std::stable_sort(order.begin(), order.end(),
@@ -518,8 +732,13 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
     set_error("tcb_fourierrec_create: table setup failed: %s", cudaGetErrorString(e));
     return fail(TCB_ERR_CUDA);
   }
-  e = cudaFuncSetAttribute(gather_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kGatherSmem);
+  int st = build_lists(h);
+  if (st != TCB_OK) return fail(st);
+  e = cudaFuncSetAttribute(grid_blocks<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(GridSmem<16>));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(grid_blocks<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(GridSmem<8>));
   if (e != cudaSuccess) {
     set_error("tcb_fourierrec_create: smem attribute failed: %s", cudaGetErrorString(e));
     return fail(TCB_ERR_CUDA);
