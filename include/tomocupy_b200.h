@@ -104,6 +104,26 @@ int tcb_prep_rows(float *out, const void *in, const float *dark0, const float *f
                   size_t out_zstride, size_t out_pstride, size_t out_poff,
                   size_t out_xoff, size_t out_width, unsigned flags, void *stream);
 
+/* Dark/flat normalisation (+ optional -log and edge padding) of a contiguous
+ * [nproj, nz, n] frame stack, exactly as tcb_darkflat_stats followed by
+ * tcb_prep_rows (flat_linear excluded), but without any device allocation.
+ * This entry point has no counterpart in the reference.  It is for callers
+ * that cannot allocate device memory where they normalise frames (e.g. an
+ * acquisition loop that must not allocate once streaming, or code inside a
+ * runtime that owns the device allocator).  The dark/flat statistics live in
+ * a fixed array inside the library (2 * TCB_NOALLOC_MAX_PLANE floats, 8 MiB
+ * per device, kept until the process exits); nz*n above
+ * TCB_NOALLOC_MAX_PLANE is rejected with TCB_ERR_INVALID_ARGUMENT.  All
+ * calls share that array: calls that overlap on the GPU race.  The first call
+ * on each device looks up the array's address with that device current; make
+ * it before any stream capture.  Inputs and outputs are the caller's. */
+#define TCB_NOALLOC_MAX_PLANE (1u << 20)
+int tcb_prep_noalloc(float *out, const void *data, const void *dark, const void *flat,
+                     size_t nproj, size_t nz, size_t n, size_t ndark, size_t nflat,
+                     int in_dtype, float bright_ratio, size_t out_zstride,
+                     size_t out_pstride, size_t out_poff, size_t out_xoff,
+                     size_t out_width, unsigned flags, void *stream);
+
 /* ------------------------------------------------------------------------
  * FBP filter.  Replaces cfunc_filter (src/include/cfunc_filter.cuh:9-23,
  * src/cuda/cfunc_filter.i:9-21): g real [nz, nproj, n] filtered in place

@@ -52,6 +52,8 @@ SIGNATURES: dict[str, list] = {
     "tcb_launch_count": [C.POINTER(C.c_uint64)],
     "tcb_darkflat_stats": [vp, vp, vp, vp, vp, sz, sz, sz, sz, i32, f32, i32, vp],
     "tcb_prep_rows": [vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, sz, sz, sz, u32, vp],
+    "tcb_prep_noalloc": [vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, f32, sz, sz, sz, sz, sz, u32,
+                         vp],
     "tcb_filter_create": [C.POINTER(vp), sz, sz, sz, i32],
     "tcb_filter_apply": [vp, vp, vp, vp],
     "tcb_filter_destroy": [vp],

@@ -6,6 +6,8 @@
 // Every CuPy elementwise step there is a separate kernel, so no multiply-add
 // is ever contracted; the explicit __f*_rn intrinsics below keep nvcc from
 // contracting either, which makes the fp32 results bit-identical.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace tcb {
@@ -235,5 +237,107 @@ extern "C" int tcb_prep_rows(float *out, const void *in, const float *dark0,
       return TCB_ERR_INVALID_ARGUMENT;
   }
   TCB_LAUNCH_CHECK();
+  return TCB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Frame normalisation without any device allocation.
+//
+// Some callers cannot allocate device memory at the point where they
+// normalise frames: acquisition loops that must not allocate once streaming
+// has started, code running inside another runtime that owns the device
+// allocator, or work recorded into a CUDA graph.  tcb_prep_rows needs the
+// dark/flat statistics in caller-provided device buffers; this entry point
+// keeps them in a fixed array in the library's own device memory instead.
+// The array holds 2 * TCB_NOALLOC_MAX_PLANE floats (8 MiB) on every device
+// that loads the library, for the life of the process.  All calls share it,
+// so calls that overlap on the GPU (different streams or threads) race; each
+// call rewrites every statistic it uses, so nothing is carried over from the
+// previous call.  The first call on a device looks up the array's device
+// address (cudaGetSymbolAddress) with that device current; make that first
+// call before any stream capture.
+namespace tcb {
+namespace {
+__device__ __align__(256) float g_noalloc_stats[2 * TCB_NOALLOC_MAX_PLANE];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float *g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_stats_ptr(float **out) {
+  int dev = 0;
+  TCB_CUDA(cudaGetDevice(&dev));
+  TCB_CHECK_ARG(dev >= 0 && dev < kMaxDevices, "tcb_prep_noalloc: device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    TCB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_stats));
+    g_noalloc_ptr[dev] = static_cast<float *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return TCB_OK;
+}
+}  // namespace
+}  // namespace tcb
+
+extern "C" int tcb_prep_noalloc(float *out, const void *data, const void *dark,
+                                const void *flat, size_t nproj, size_t nz, size_t n,
+                                size_t ndark, size_t nflat, int in_dtype, float bright_ratio,
+                                size_t out_zstride, size_t out_pstride, size_t out_poff,
+                                size_t out_xoff, size_t out_width, unsigned flags,
+                                void *stream) {
+  TCB_CHECK_ARG(out && data && dark && flat, "tcb_prep_noalloc: null pointer");
+  TCB_CHECK_ARG(ndark >= 1 && nflat >= 1, "tcb_prep_noalloc: need >=1 dark and flat");
+  TCB_CHECK_ARG(!(flags & TCB_PREP_FLAT_LINEAR),
+                "tcb_prep_noalloc: flat_linear is not supported without allocation");
+  TCB_CHECK_ARG((flags & ~(unsigned)(TCB_PREP_DARKFLAT | TCB_PREP_MINUS_LOG |
+                                     TCB_PREP_EDGE_PAD)) == 0,
+                "tcb_prep_noalloc: unknown flags 0x%x", flags);
+  TCB_CHECK_ARG(nz * n <= (size_t)TCB_NOALLOC_MAX_PLANE,
+                "tcb_prep_noalloc: nz*n = %zu exceeds the fixed scratch of %u elements; "
+                "split the rows into smaller chunks or use tcb_prep_rows",
+                nz * n, (unsigned)TCB_NOALLOC_MAX_PLANE);
+  TCB_CHECK_ARG(!(flags & TCB_PREP_EDGE_PAD) || out_width >= out_xoff + n,
+                "tcb_prep_noalloc: out_width < out_xoff + n");
+  TCB_CHECK_ARG(nproj < (1u << 31) && nproj * nz < (1ull << 31),
+                "tcb_prep_noalloc: too many rows in one call");
+  TCB_CHECK_ARG(in_dtype == TCB_U16 || in_dtype == TCB_U8 || in_dtype == TCB_F32,
+                "tcb_prep_noalloc: unknown dtype %d", in_dtype);
+  if (nproj == 0 || nz == 0 || n == 0) return TCB_OK;
+  float *stats = nullptr;
+  int st = noalloc_stats_ptr(&stats);
+  if (st != TCB_OK) return st;
+  float *dark0 = stats, *flat0 = stats + TCB_NOALLOC_MAX_PLANE;
+  size_t plane = nz * n;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned sgrid = ceil_div(plane, 256);
+  PrepArgs a{out, data, dark0, flat0, nullptr, (int)nproj, (int)nz, (int)n, nz * n, n,
+             out_zstride, out_pstride, out_poff, out_xoff, out_width,
+             flags | TCB_PREP_DARKFLAT};
+  unsigned rows = (unsigned)(nproj * nz);
+  switch (in_dtype) {
+    case TCB_U16:
+      darkflat_stats_kernel<uint16_t><<<sgrid, 256, 0, s>>>(
+          dark0, flat0, nullptr, (const uint16_t *)dark, (const uint16_t *)flat, (int)ndark,
+          (int)nflat, plane, bright_ratio, 0);
+      TCB_LAUNCH_CHECK();
+      prep_rows_kernel<uint16_t><<<rows, 256, 0, s>>>(a);
+      break;
+    case TCB_U8:
+      darkflat_stats_kernel<uint8_t><<<sgrid, 256, 0, s>>>(
+          dark0, flat0, nullptr, (const uint8_t *)dark, (const uint8_t *)flat, (int)ndark,
+          (int)nflat, plane, bright_ratio, 0);
+      TCB_LAUNCH_CHECK();
+      prep_rows_kernel<uint8_t><<<rows, 256, 0, s>>>(a);
+      break;
+    default:
+      darkflat_stats_kernel<float><<<sgrid, 256, 0, s>>>(
+          dark0, flat0, nullptr, (const float *)dark, (const float *)flat, (int)ndark,
+          (int)nflat, plane, bright_ratio, 0);
+      TCB_LAUNCH_CHECK();
+      prep_rows_kernel<float><<<rows, 256, 0, s>>>(a);
+  }
+  TCB_LAUNCH_CHECK();
+  count_launch(2);
   return TCB_OK;
 }
