@@ -180,6 +180,24 @@ int tcb_linerec_backprojection_try_lamino(tcb_linerec *h, void *f, const void *g
 int tcb_linerec_destroy(tcb_linerec *h);
 
 /* ------------------------------------------------------------------------
+ * Log-polar backprojector.  Replaces cfunc_lprec
+ * (src/include/cfunc_lprec.cuh:9-49, src/cuda/cfunc_lprec.i:11-29).
+ * setgrids borrows the caller's device grids for the handle's lifetime (as
+ * the reference does); backprojection zeroes f [nz, n, n] and accumulates
+ * the three spans; g [nz, nproj, n] is overwritten by its spline
+ * coefficients (as in the reference).
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_lprec tcb_lprec;
+int tcb_lprec_create(tcb_lprec **out, size_t nproj, size_t nz, size_t n, size_t ntheta,
+                     size_t nrho, int precision);
+int tcb_lprec_setgrids(tcb_lprec *h, const void *fz, const float *lp2p1, const float *lp2p2,
+                       const float *lp2p1w, const float *lp2p2w, const float *C2lp1,
+                       const float *C2lp2, const int *lpids, const int *wids,
+                       const int *cids, size_t nlpids, size_t nwids, size_t ncids);
+int tcb_lprec_backprojection(tcb_lprec *h, void *f, void *g, void *stream);
+int tcb_lprec_destroy(tcb_lprec *h);
+
+/* ------------------------------------------------------------------------
  * Laminography Fourier chain.
  * ------------------------------------------------------------------------ */
 

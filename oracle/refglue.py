@@ -170,6 +170,38 @@ class RefLineRec(_Handle):
                                              theta.data_ptr(), phi.data_ptr(), sz, _s(stream))
 
 
+class RefLpRec(_Handle):
+    """reconstruction/lprec.py:292-335 over the reference cfunc_lprec.  ``grids``
+    holds the Padj arrays (fZ, lp2p1, ..., cids) as NumPy arrays: the golden
+    fixtures produced by the reference's own Python, or a restatement."""
+    op = "lprec"
+
+    def __init__(self, n, nproj, nz, grids, dtype="float32"):
+        ntheta = 2 ** int(round(math.log2(nproj)))
+        nrho = 2 * 2 ** int(round(math.log2(n)))
+        super().__init__(dtype == "float16", nproj, nz, n, ntheta, nrho)
+        import numpy as np
+        dev = torch.device("cuda")
+        tdt = torch.float16 if dtype == "float16" else torch.float32
+        self.t = {}
+        for k in ("lp2p1", "lp2p2", "lp2p1w", "lp2p2w", "C2lp1", "C2lp2", "lpids", "wids",
+                  "cids"):
+            self.t[k] = torch.as_tensor(np.ascontiguousarray(grids[k]), device=dev)
+        fz = np.ascontiguousarray(grids["fZ"]).view("float32")
+        self.t["fZ"] = torch.as_tensor(fz, device=dev).to(tdt).contiguous()
+        t = self.t
+        self.L.ref_setgrids(self.h, t["fZ"].data_ptr(), t["lp2p1"].data_ptr(),
+                            t["lp2p2"].data_ptr(), t["lp2p1w"].data_ptr(), t["lp2p2w"].data_ptr(),
+                            t["C2lp1"].data_ptr(), t["C2lp2"].data_ptr(), t["lpids"].data_ptr(),
+                            t["wids"].data_ptr(), t["cids"].data_ptr(), len(grids["lpids"]),
+                            len(grids["wids"]), len(grids["cids"]))
+
+    def backprojection(self, obj, data, stream=None):
+        data = data.contiguous()
+        self.L.ref_backprojection(self.h, obj.data_ptr(), data.data_ptr(), _s(stream))
+        return obj
+
+
 def ref_darkflat_minus_log(data, dark, flat, bright_ratio=1.0, minus_log=True):
     """proc_functions.py:55-83 in torch, operation by operation (float32)."""
     dark0 = dark.to(torch.float32)

@@ -146,7 +146,28 @@ def gen_cpu(ref: Path):
                     "args_after": {k: getattr(gv.args, k) for k in
                                    ("end_row", "end_proj", "end_column")}})
     (HERE / "sizes_cases.json").write_text(json.dumps(out, indent=1, default=str))
-    print("wrote filter_spectra.npz and sizes_cases.json")
+
+    # log-polar grids of LpRec (lprec.py:82-289)
+    sys.modules["cupy"]._default_memory_pool = types.SimpleNamespace(free_all_blocks=lambda: None)
+    for sub in ("cfunc_lprec", "cfunc_lprecfp16"):
+        m = types.ModuleType(f"tomocupy.{sub}")
+        sys.modules[f"tomocupy.{sub}"] = m
+        setattr(sys.modules["tomocupy"], sub, m)
+    lp = _load(ref / "src/tomocupy/reconstruction/lprec.py", "ref_lprec")
+    grids = {}
+    for n, nproj in LPREC_CASES:
+        ntheta = 2 ** int(np.round(np.log2(nproj)))
+        nrho = 2 * 2 ** int(np.round(np.log2(n)))
+        P = lp.create_gl(n, nproj, ntheta, nrho)
+        A = lp.create_adj(P)
+        for name in ("fZ", "lp2p1", "lp2p2", "lp2p1w", "lp2p2w", "C2lp1", "C2lp2", "cids",
+                     "lpids", "wids"):
+            grids[f"{name}_{n}_{nproj}"] = np.asarray(getattr(A, name))
+    np.savez_compressed(HERE / "lprec_grids.npz", **grids)
+    print("wrote filter_spectra.npz, sizes_cases.json and lprec_grids.npz")
+
+
+LPREC_CASES = [(128, 90), (200, 128)]
 
 
 GPU_CASES = dict(n=128, nproj=90, nz=4, seed=7)

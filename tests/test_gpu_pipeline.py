@@ -35,6 +35,12 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
     filt = ref.RefFilter(ne, P, ncz)
     if algorithm == "fourierrec":
         rec = ref.RefFourierRec(n, P, ncz, th)
+    elif algorithm == "lprec":
+        from tomocupy_b200.reconstruction import lprec_grids as L
+        ntheta, nrho = L.lp_sizes(n, P)
+        A = L.create_adj(L.create_gl(n, P, ntheta, nrho))  # pinned by lprec_grids.npz
+        rec = ref.RefLpRec(n, P, ncz, vars(A))
+        center = center + 0.5  # BackprojFunctions (backproj_functions.py:70-71)
     else:
         rec = ref.RefLineRec(th, P, P, ncz, ncz, n)
     out = torch.zeros((nz, n, n), dtype=torch.float32, device=dev)
@@ -92,6 +98,15 @@ def test_c1_linerec_matches_reference(cuda, ref, c1):
     d, dk, fl = data[:, :4], dark[:, :4], flat[:, :4]
     ours = run_ours(d, dk, fl, theta, algorithm="linerec", ncz=4)
     theirs = reference_chain(ref, d, dk, fl, theta, algorithm="linerec", ncz=4)
+    err = rel_l2(ours, theirs)
+    assert err < 1e-5, err
+
+
+def test_c1_lprec_matches_reference(cuda, ref, c1):
+    data, dark, flat, theta, _ = c1
+    d, dk, fl = data[:, :4], dark[:, :4], flat[:, :4]
+    ours = run_ours(d, dk, fl, theta, algorithm="lprec", ncz=4)
+    theirs = reference_chain(ref, d, dk, fl, theta, algorithm="lprec", ncz=4)
     err = rel_l2(ours, theirs)
     assert err < 1e-5, err
 

@@ -67,6 +67,10 @@ SIGNATURES: dict[str, list] = {
     "tcb_linerec_backprojection_try": [vp, vp, vp, vp, vp, f32, i32, vp],
     "tcb_linerec_backprojection_try_lamino": [vp, vp, vp, vp, vp, i32, vp],
     "tcb_linerec_destroy": [vp],
+    "tcb_lprec_create": [C.POINTER(vp), sz, sz, sz, sz, sz, i32],
+    "tcb_lprec_setgrids": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, sz, sz],
+    "tcb_lprec_backprojection": [vp, vp, vp, vp],
+    "tcb_lprec_destroy": [vp],
     "tcb_fft2d_create": [C.POINTER(vp), sz, sz, sz],
     "tcb_fft2d_fwd": [vp, vp, vp, vp],
     "tcb_fft2d_destroy": [vp],

@@ -302,11 +302,26 @@ __global__ void __launch_bounds__(NTH)
 // ---- gridding --------------------------------------------------------------
 // G: [nz, nproj, n] complex, plain forward FFT of each projection.
 // grid: [nz, 2n, 2n] complex (fftshift sign included).
+constexpr int KREC = 2 + 2 * (2 * M + 2);  // staged record: origin + 10 x-weights + 10 y-weights
 template <int Z>
 struct GridSmem {
   float4 g[Z / 2][SC];  // (g_z.x, g_z.y, g_z+1.x, g_z+1.y) of each staged sample
-  float4 pos[SC];       // x0, y0, fx, fy (ints stored bitwise)
+  // per staged sample: [0] tile-local footprint origin (lx0 | ly0 << 16),
+  // [2..11] x-weights exp(c1 (ell/2n - x0)^2) for the 9 footprint columns and
+  // a trailing 0, [12..21] the same along y.  A lane reads the weight of its
+  // own column/row, so the exps are computed once per staged sample instead
+  // of once per lane.
+  int rec[SC][KREC];
 };
+
+// Footprint origin relative to the tile on a periodic axis, in [-2M, twon-2M-1].
+__device__ __forceinline__ int tile_origin(int f, int origin, int twon) {
+  int t = f - M - origin;
+  t %= twon;
+  if (t < 0) t += twon;
+  if (t > twon - 2 * M - 1) t -= twon;
+  return t;
+}
 
 template <int Z>
 __global__ void __launch_bounds__(NTH, 2)
@@ -323,10 +338,11 @@ __global__ void __launch_bounds__(NTH, 2)
   const int z0 = (blockIdx.x % zgroups) * Z;
   const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  // this lane's cell
-  const int cx = ix0 + (wid % NRX) * RX + (lane % RX);
-  const int cy = iy0 + (wid / NRX) * RY + (lane / RX);
-  const int X = cx - n, Y = cy - n;
+  // this lane's cell, tile-local and global
+  const int lx = (wid % NRX) * RX + (lane % RX);
+  const int ly = (wid / NRX) * RY + (lane / RX);
+  const int cx = ix0 + lx, cy = iy0 + ly;
+  const int X0 = ix0 - n, Y0 = iy0 - n;
   const float twonf = (float)(2 * n);
   const int half = n / 2;
   float ar[Z], ai[Z];
@@ -340,14 +356,25 @@ __global__ void __launch_bounds__(NTH, 2)
 
   for (int c0 = 0; c0 < S; c0 += SC) {
     const int cnt = min(SC, S - c0);
-    // stage positions
+    // stage footprint origins and separable weights
     for (int k = threadIdx.x; k < cnt; k += NTH) {
       int s = tlist[t0 + c0 + k];
       int p = s / n, i = s % n;
       float x0, y0;
       int fx, fy;
       sample_pos(cs, rtab, p, i, twonf, x0, y0, fx, fy);
-      sm.pos[k] = make_float4(x0, y0, __int_as_float(fx), __int_as_float(fy));
+      int *r = sm.rec[k];
+      r[0] = (tile_origin(fx, X0, twon) & 0xFFFF) | (tile_origin(fy, Y0, twon) << 16);
+      r[1] = 0;
+#pragma unroll
+      for (int d = 0; d < 2 * M + 1; d++) {
+        float w0 = etab[fx - M + d + n + M + EPAD] - x0;
+        float w1 = etab[fy - M + d + n + M + EPAD] - y0;
+        r[2 + d] = __float_as_int(__expf(geo.coeff1 * w0 * w0));
+        r[2 + 2 * M + 2 + d] = __float_as_int(__expf(geo.coeff1 * w1 * w1));
+      }
+      r[2 + 2 * M + 1] = 0;
+      r[2 + 2 * (2 * M + 1) + 1] = 0;
     }
     // stage spectrum values of Z pairs, pair-innermost; consecutive threads
     // read consecutive samples of one pair (coalesced along the radius)
@@ -381,19 +408,12 @@ __global__ void __launch_bounds__(NTH, 2)
       int m = __popc(inb);
       for (int t = 0; t < m; t++) {
         int j = __shfl_sync(0xffffffffu, idx, t) - c0;
-        float4 ps = sm.pos[j];
-        int fx = __float_as_int(ps.z), fy = __float_as_int(ps.w);
-        // periodic offset of this lane's cell inside the footprint
-        int dx = X - (fx - M);
-        if (dx < 0) dx += twon; else if (dx >= twon) dx -= twon;
-        int dy = Y - (fy - M);
-        if (dy < 0) dy += twon; else if (dy >= twon) dy -= twon;
-        float w = 0.f;
-        if (dx <= 2 * M && dy <= 2 * M) {
-          float w0 = etab[fx - M + dx + n + M + EPAD] - ps.x;
-          float w1 = etab[fy - M + dy + n + M + EPAD] - ps.y;
-          w = __expf(geo.coeff1 * w0 * w0) * __expf(geo.coeff1 * w1 * w1);
-        }
+        const int *r = sm.rec[j];
+        int o = r[0];
+        // offset of this lane's cell in the footprint; outside -> the 0 weight
+        unsigned dx = min((unsigned)(lx - (int)(short)(o & 0xFFFF)), (unsigned)(2 * M + 1));
+        unsigned dy = min((unsigned)(ly - (o >> 16)), (unsigned)(2 * M + 1));
+        float w = __int_as_float(r[2 + dx]) * __int_as_float(r[2 + 2 * M + 2 + dy]);
 #pragma unroll
         for (int zp = 0; zp < Z / 2; zp++) {
           float4 v = sm.g[zp][j];

@@ -32,13 +32,15 @@ from .reconstruction.fbp_filter import calc_filter
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
                  algorithm="fourierrec", minus_log=True, device="cuda"):
-        if algorithm not in ("fourierrec", "linerec"):
+        if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if algorithm == "fourierrec" and ncz % 2:
             raise ValueError("fourierrec needs an even number of rows per chunk")
         self.device = torch.device(device)
         self.n, self.nproj, self.ncz = int(n), int(nproj), int(ncz)
-        self.center = float(center)
+        # lprec reconstructs about centre + 0.5, as BackprojFunctions sets it
+        # (reconstruction/backproj_functions.py:70-71)
+        self.center = float(center) + (0.5 if algorithm == "lprec" else 0.0)
         self.algorithm = algorithm
         self.minus_log = minus_log
         self.ne = 4 * self.n
@@ -56,8 +58,13 @@ class SinoPipeline:
             self.g = torch.empty((self.ncz // 2, self.nproj, self.n, 2), dtype=torch.float32,
                                  device=self.device)
         else:
-            self.lr = cfunc_linerec.cfunc_linerec(self.nproj, self.ncz, self.n, self.nproj,
-                                                  self.ncz)
+            if algorithm == "linerec":
+                self.lr = cfunc_linerec.cfunc_linerec(self.nproj, self.ncz, self.n, self.nproj,
+                                                      self.ncz)
+            else:
+                from .reconstruction.lprec import LpRec
+                self.lp = LpRec(self.n, self.nproj, self.ncz, theta, "float32",
+                                device=self.device)
             self.crop = torch.empty((self.ncz, self.nproj, self.n), dtype=torch.float32,
                                     device=self.device)
 
@@ -95,8 +102,12 @@ class SinoPipeline:
             s = torch.cuda.current_stream() if stream is None else stream
             with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
                 self.crop.copy_(self.rows[:, :, self.pad:self.pad + self.n])
-                out.zero_()
-            self.lr.backprojection(out, self.crop, self.theta, math.pi / 2, 0, stream)
+                if self.algorithm == "linerec":
+                    out.zero_()
+            if self.algorithm == "linerec":
+                self.lr.backprojection(out, self.crop, self.theta, math.pi / 2, 0, stream)
+            else:
+                self.lp.fslv.backprojection(out, self.crop, stream)
         return out
 
     def reconstruct(self, out, data, dark0=None, flat0=None, z_lo=0, sht=None, stream=None):
