@@ -125,6 +125,21 @@ int tcb_prep_noalloc(float *out, const void *data, const void *dark, const void 
                      size_t out_width, unsigned flags, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Fourier-wavelet ring removal.  Replaces remove_stripe_fw with DWTForward /
+ * DWTInverse / afb1d / sfb1d (src/tomocupy/processing/remove_stripe.py:51-293).
+ * create: sizes of the sinogram chunk, DWT levels, damping sigma and the
+ * wavelet filter bank (host float64 arrays of length L, PyWavelets order).
+ * apply_sino: in place on padded sinograms [nz][nproj + nproj/8][ni] (slice
+ * stride sstride), data rows starting at (nproj/8)/2, other rows zero.
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_stripe_fw tcb_stripe_fw;
+int tcb_stripe_fw_create(tcb_stripe_fw **out, size_t nproj, size_t nz, size_t ni, int level,
+                         float sigma, const double *dec_lo, const double *dec_hi,
+                         const double *rec_lo, const double *rec_hi, int L);
+int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t sstride, void *stream);
+int tcb_stripe_fw_destroy(tcb_stripe_fw *h);
+
+/* ------------------------------------------------------------------------
  * FBP filter.  Replaces cfunc_filter (src/include/cfunc_filter.cuh:9-23,
  * src/cuda/cfunc_filter.i:9-21): g real [nz, nproj, n] filtered in place
  * with w complex [nz, n/2+1] (one spectrum per slice).

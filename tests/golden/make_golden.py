@@ -164,7 +164,53 @@ def gen_cpu(ref: Path):
                      "lpids", "wids"):
             grids[f"{name}_{n}_{nproj}"] = np.asarray(getattr(A, name))
     np.savez_compressed(HERE / "lprec_grids.npz", **grids)
-    print("wrote filter_spectra.npz, sizes_cases.json and lprec_grids.npz")
+
+    # Fourier-wavelet ring removal (remove_stripe.py:51-293).  PyWavelets is
+    # absent: a stub serves the filter banks derived by
+    # tomocupy_b200.processing.wavelets, so these fixtures pin the algorithm,
+    # not the taps.
+    from tomocupy_b200.processing import wavelets as W
+
+    class _Wavelet:
+        def __init__(self, name):
+            self.dec_lo, self.dec_hi, self.rec_lo, self.rec_hi = (list(a) for a in
+                                                                  W.filter_bank(name))
+    pywt = types.ModuleType("pywt")
+    pywt.Wavelet = _Wavelet
+    pywt.dwt_coeff_len = lambda n, L, mode="symmetric": W.dwt_coeff_len(n, L)
+    sys.modules["pywt"] = pywt
+    import scipy.ndimage as ndi
+    cx = types.ModuleType("cupyx")
+    cxs = types.ModuleType("cupyx.scipy")
+    cxn = types.ModuleType("cupyx.scipy.ndimage")
+    for f in ("median_filter", "binary_dilation", "uniform_filter1d"):
+        setattr(cxn, f, getattr(ndi, f))
+    sys.modules.update({"cupyx": cx, "cupyx.scipy": cxs, "cupyx.scipy.ndimage": cxn})
+    rs = _load(ref / "src/tomocupy/processing/remove_stripe.py", "ref_remove_stripe")
+    fw = {}
+    for i, (nproj, nz, n, level, sigma, wname, seed) in enumerate(FW_CASES):
+        data = fw_input(nproj, nz, n, seed)
+        fw[f"in_{i}"] = data
+        fw[f"out_{i}"] = np.asarray(rs.remove_stripe_fw(data.copy(), sigma, wname, level),
+                                    dtype=np.float32)
+    np.savez_compressed(HERE / "fw_stripe.npz", **fw)
+    print("wrote filter_spectra.npz, sizes_cases.json, lprec_grids.npz and fw_stripe.npz")
+
+
+# (nproj, nz, ni, level, sigma, wavelet, seed)
+FW_CASES = [(90, 2, 64, 3, 1.0, "sym16", 1), (120, 3, 96, 4, 2.0, "db5", 2),
+            (64, 1, 80, 2, 1.0, "haar", 3), (100, 2, 128, 7, 1.0, "sym16", 4)]
+
+
+def fw_input(nproj, nz, n, seed):
+    """Normalised sinogram-like data with vertical stripes, float32 [nproj, nz, n]."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(-1, 1, n)
+    base = np.exp(-4 * x ** 2)[None, None, :] * (1 + 0.1 * np.sin(
+        np.linspace(0, 6, nproj))[:, None, None])
+    stripes = 1 + 0.05 * rng.standard_normal(n) * (rng.uniform(size=n) < 0.2)
+    noise = 0.01 * rng.standard_normal((nproj, nz, n))
+    return (base * stripes[None, None, :] + noise).astype(np.float32)
 
 
 LPREC_CASES = [(128, 90), (200, 128)]

@@ -23,7 +23,7 @@ def c1():
 
 
 def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
-                    fbp="parzen", center=None, sht=None):
+                    fbp="parzen", center=None, sht=None, stripe=None):
     from oracle import np_tomo
     dev = torch.device("cuda")
     P, nz, n = data.shape
@@ -46,7 +46,14 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
     out = torch.zeros((nz, n, n), dtype=torch.float32, device=dev)
     for z0 in range(0, nz, ncz):
         d = ref.ref_darkflat_minus_log(data[:, z0:z0 + ncz].to(dev), dark[:, z0:z0 + ncz].to(dev),
-                                       flat[:, z0:z0 + ncz].to(dev))
+                                       flat[:, z0:z0 + ncz].to(dev), minus_log=stripe is None)
+        if stripe is not None:
+            # proc_sino: ring removal on the dark/flat corrected frames (checked on
+            # its own against the reference's remove_stripe_fw), then proc_proj: -log
+            from tomocupy_b200.processing.remove_stripe import remove_stripe_fw
+            d = remove_stripe_fw(d.contiguous(), *stripe)
+            d = torch.where(d <= 0, torch.ones((), device=dev), d)
+            d = torch.nan_to_num(-torch.log(d), nan=6.0, posinf=0.0, neginf=0.0)
         d = d.permute(1, 0, 2).contiguous()
         s = torch.zeros(ncz, device=dev) if sht is None else sht
         d = ref.ref_fbp_filter_center(filt, d, wf, t, center, s, n, ne)
@@ -99,6 +106,23 @@ def test_c1_linerec_matches_reference(cuda, ref, c1):
     ours = run_ours(d, dk, fl, theta, algorithm="linerec", ncz=4)
     theirs = reference_chain(ref, d, dk, fl, theta, algorithm="linerec", ncz=4)
     err = rel_l2(ours, theirs)
+    assert err < 1e-5, err
+
+
+def test_c1_fw_ring_removal_pipeline(cuda, ref, c1):
+    """dark/flat -> fw ring removal (level 7, sym16) -> -log -> filter -> fourierrec."""
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    data, dark, flat, theta, _ = c1
+    d, dk, fl = data[:, :8], dark[:, :8], flat[:, :8]
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=8,
+                      remove_stripe_method="fw", fw_sigma=1.0, fw_filter="sym16", fw_level=7)
+    reader = ArrayReader(d, dk, fl, theta=theta, pin=True)
+    writer = ArrayWriter(device="cpu", pin=True)
+    GPURec(reader, writer).recon_all()
+    theirs = reference_chain(ref, d, dk, fl, theta, ncz=8, stripe=(1.0, "sym16", 7))
+    err = rel_l2(writer.rec, theirs)
     assert err < 1e-5, err
 
 

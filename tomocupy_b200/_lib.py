@@ -54,6 +54,9 @@ SIGNATURES: dict[str, list] = {
     "tcb_prep_rows": [vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, sz, sz, sz, u32, vp],
     "tcb_prep_noalloc": [vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, f32, sz, sz, sz, sz, sz, u32,
                          vp],
+    "tcb_stripe_fw_create": [C.POINTER(vp), sz, sz, sz, i32, f32, vp, vp, vp, vp, i32],
+    "tcb_stripe_fw_apply_sino": [vp, vp, sz, vp],
+    "tcb_stripe_fw_destroy": [vp],
     "tcb_filter_create": [C.POINTER(vp), sz, sz, sz, i32],
     "tcb_filter_apply": [vp, vp, vp, vp],
     "tcb_filter_destroy": [vp],

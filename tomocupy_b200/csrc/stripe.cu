@@ -1,0 +1,404 @@
+// Fourier-wavelet ring removal (remove_stripe_fw).
+//
+// Same algorithm as the reference (src/tomocupy/processing/remove_stripe.py:
+// _reflect/_mypad 51-84, afb1d 86-128, sfb1d 131-155, DWTForward 157-200,
+// DWTInverse 202-246, remove_stripe_fw 253-293): the sinograms, padded along
+// the angles to nproj + nproj/8 with zeros, go through `level` 2D DWT levels
+// (stride-2 correlation with the reversed analysis filters along the
+// detector, then along the angles, half-sample symmetric extension, output
+// length floor((N + L - 1)/2)); at every level the band that is high-pass
+// along the detector and low-pass along the angles (vertical stripes) is
+// Fourier transformed along the angles, multiplied by
+// -expm1(-k^2 / (2 sigma^2)) and transformed back; the inverse DWT (stride-2
+// transposed convolution with the synthesis filters, cropped by L-2 on both
+// sides) rebuilds the sinograms.
+//
+// Every tap is accumulated in the reference's order with explicit
+// round-to-nearest multiplies and adds (no contraction), so the wavelet
+// stages reproduce its float32 arithmetic; the band FFTs use cuFFT.
+// B200 design: one kernel per filter pass over all slices of the chunk,
+// both output channels of a pass from one read of the input window, the
+// pyramid kept in HBM, the damped band transposed so the angle FFTs are
+// contiguous batched transforms, 1/N of the inverse FFT folded into the
+// damping factors.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace tcb {
+namespace sw {
+
+constexpr int MAXL = 64;
+
+struct Taps {
+  float h0[MAXL], h1[MAXL];  // analysis: dec_lo, dec_hi reversed
+  float g0[MAXL], g1[MAXL];  // synthesis: rec_lo, rec_hi
+  int L;
+};
+
+__device__ __forceinline__ int reflect(int m, int n) {
+  int p = 2 * n;
+  m %= p;
+  if (m < 0) m += p;
+  return m >= n ? p - 1 - m : m;
+}
+
+// afb1d along the last axis: x [B][H][W] (row stride sx, slice stride sz) ->
+// out [B][2][H][Wo] (lo, hi).
+__global__ void afb_rows(const float *__restrict__ x, long long sz, int sx, float *__restrict__ out,
+                         int B, int H, int W, int Wo, int padl, const Taps *__restrict__ taps) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = (long long)B * H * Wo;
+  if (idx >= total) return;
+  int j = (int)(idx % Wo);
+  long long r = idx / Wo;
+  int h = (int)(r % H);
+  int b = (int)(r / H);
+  const float *row = x + b * sz + (long long)h * sx;
+  const int L = taps->L;
+  float lo = 0.f, hi = 0.f;
+  for (int k = 0; k < L; k++) {
+    float v = row[reflect(2 * j + k - padl, W)];
+    if (k == 0) {
+      lo = __fmul_rn(taps->h0[0], v);
+      hi = __fmul_rn(taps->h1[0], v);
+    } else {
+      lo = __fadd_rn(lo, __fmul_rn(taps->h0[k], v));
+      hi = __fadd_rn(hi, __fmul_rn(taps->h1[k], v));
+    }
+  }
+  long long o = (((long long)b * 2) * H + h) * Wo + j;
+  out[o] = lo;
+  out[o + (long long)H * Wo] = hi;
+}
+
+// afb1d along the rows axis for both channels: in [B][2][H][W] ->
+// out [B][4][Ho][W] (channel c -> 2c lo, 2c+1 hi).
+__global__ void afb_cols(const float *__restrict__ in, float *__restrict__ out, int B, int H,
+                         int W, int Ho, int padl, const Taps *__restrict__ taps) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = (long long)B * 2 * Ho * W;
+  if (idx >= total) return;
+  int j = (int)(idx % W);
+  long long r = idx / W;
+  int i = (int)(r % Ho);
+  long long bc = r / Ho;  // b*2 + c
+  const float *col = in + bc * H * W + j;
+  const int L = taps->L;
+  float lo = 0.f, hi = 0.f;
+  for (int k = 0; k < L; k++) {
+    float v = col[(long long)reflect(2 * i + k - padl, H) * W];
+    if (k == 0) {
+      lo = __fmul_rn(taps->h0[0], v);
+      hi = __fmul_rn(taps->h1[0], v);
+    } else {
+      lo = __fadd_rn(lo, __fmul_rn(taps->h0[k], v));
+      hi = __fadd_rn(hi, __fmul_rn(taps->h1[k], v));
+    }
+  }
+  long long b = bc / 2, c = bc % 2;
+  long long o = ((b * 4 + 2 * c) * Ho + i) * W + j;
+  out[o] = lo;
+  out[o + (long long)Ho * W] = hi;
+}
+
+// sfb1d along the rows axis: channel 0 = synth(lo0, hi0), 1 = synth(lo1, hi1)
+// with lo0 = LL (stride sll), hi0 = band0, lo1 = band1, hi1 = band2 of a
+// [B][4][Hi][Wb] pyramid level; LL may be cropped (Hi, W used).  Output
+// [B][2][Ho][W], Ho = 2 Hi - L + 2.
+__global__ void sfb_cols(const float *__restrict__ y, long long bstride, int Hi, int Wb, int W,
+                         float *__restrict__ out, int B, int Ho, const Taps *__restrict__ taps) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = (long long)B * 2 * Ho * W;
+  if (idx >= total) return;
+  int j = (int)(idx % W);
+  long long r = idx / W;
+  int t = (int)(r % Ho);
+  long long bc = r / Ho;
+  int b = (int)(bc / 2), c = (int)(bc % 2);
+  const int L = taps->L;
+  const long long plane = (long long)Hi * Wb;
+  const float *base = y + b * bstride;
+  const float *lo = base + (c == 0 ? 0 : 2) * plane + j;  // LL or band1 (HL)
+  const float *hi = base + (c == 0 ? 1 : 3) * plane + j;  // band0 (LH) or band2 (HH)
+  int tt = t + L - 2;  // position in the uncropped output
+  float acc = 0.f;
+  for (int k = tt & 1; k < L; k += 2) {
+    int h = (tt - k) >> 1;
+    if (h < 0 || h >= Hi) continue;
+    float v = __fadd_rn(__fmul_rn(taps->g0[k], lo[(long long)h * Wb]),
+                        __fmul_rn(taps->g1[k], hi[(long long)h * Wb]));
+    acc = __fadd_rn(acc, v);
+  }
+  out[(bc * Ho + t) * W + j] = acc;
+}
+
+// sfb1d along the last axis: in [B][2][H][Wi] -> out rows (b, h) of width
+// Wo = 2 Wi - L + 2, written to dst[b*dsz + h*dsx + w] for h < Hd, w < Wd.
+__global__ void sfb_rows(const float *__restrict__ in, int H, int Wi, float *__restrict__ dst,
+                         long long dsz, int dsx, int Hd, int Wd, int B,
+                         const Taps *__restrict__ taps) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = (long long)B * Hd * Wd;
+  if (idx >= total) return;
+  int w = (int)(idx % Wd);
+  long long r = idx / Wd;
+  int h = (int)(r % Hd);
+  int b = (int)(r / Hd);
+  const int L = taps->L;
+  const float *lo = in + (((long long)b * 2) * H + h) * Wi;
+  const float *hi = lo + (long long)H * Wi;
+  int tt = w + L - 2;
+  float acc = 0.f;
+  for (int k = tt & 1; k < L; k += 2) {
+    int q = (tt - k) >> 1;
+    if (q < 0 || q >= Wi) continue;
+    float v = __fadd_rn(__fmul_rn(taps->g0[k], lo[q]), __fmul_rn(taps->g1[k], hi[q]));
+    acc = __fadd_rn(acc, v);
+  }
+  dst[b * dsz + (long long)h * dsx + w] = acc;
+}
+
+// [B][R][C] <-> [B][C][R] (32x32 tiles)
+__global__ void transpose_bands(const float *__restrict__ in, long long istride,
+                                float *__restrict__ out, long long ostride, int R, int C) {
+  __shared__ float t[32][33];
+  int b = blockIdx.z;
+  int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const float *src = in + b * istride;
+  float *dst = out + b * ostride;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < R && c < C) t[k][threadIdx.x] = src[(long long)r * C + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < R && c < C) dst[(long long)c * R + r] = t[threadIdx.x][k];
+  }
+}
+
+__global__ void damp_kernel(float2 *__restrict__ spec, const float *__restrict__ damp, int nc,
+                            long long total) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  float d = damp[i % nc];
+  float2 v = spec[i];
+  spec[i] = make_float2(v.x * d, v.y * d);
+}
+
+}  // namespace sw
+}  // namespace tcb
+
+using namespace tcb;
+using namespace tcb::sw;
+
+struct tcb_stripe_fw {
+  int nproj, nz, ni, level, nproj_pad, L;
+  std::vector<int> H, W;  // level sizes: H[0] = nproj_pad, W[0] = ni
+  std::vector<float *> Y; // per level [nz][4][H[k+1]][W[k+1]]
+  std::vector<float *> damp;  // per level damping factors (with 1/H)
+  std::vector<cufftHandle> r2c, c2r;
+  float *tmp = nullptr;    // [nz][2][H][W] scratch
+  float *bt = nullptr;     // transposed band scratch
+  float2 *spec = nullptr;  // band spectrum scratch
+  Taps *taps = nullptr;    // device copy
+  size_t tmp_elems = 0;
+};
+
+static void fw_release(tcb_stripe_fw *h) {
+  for (auto p : h->Y) cudaFree(p);
+  for (auto p : h->damp) cudaFree(p);
+  for (auto p : h->r2c) if (p) cufftDestroy(p);
+  for (auto p : h->c2r) if (p) cufftDestroy(p);
+  h->Y.clear();
+  h->damp.clear();
+  h->r2c.clear();
+  h->c2r.clear();
+  cudaFree(h->tmp);
+  cudaFree(h->bt);
+  cudaFree(h->spec);
+  cudaFree(h->taps);
+  h->tmp = h->bt = nullptr;
+  h->spec = nullptr;
+  h->taps = nullptr;
+}
+
+extern "C" int tcb_stripe_fw_create(tcb_stripe_fw **out, size_t nproj, size_t nz, size_t ni,
+                                    int level, float sigma, const double *dec_lo,
+                                    const double *dec_hi, const double *rec_lo,
+                                    const double *rec_hi, int L) {
+  TCB_CHECK_ARG(out, "tcb_stripe_fw_create: null out");
+  *out = nullptr;
+  TCB_CHECK_ARG(nproj >= 2 && nz >= 1 && ni >= 2 && level >= 1 && level <= 16,
+                "tcb_stripe_fw_create: bad sizes");
+  TCB_CHECK_ARG(L >= 2 && L <= MAXL && dec_lo && dec_hi && rec_lo && rec_hi,
+                "tcb_stripe_fw_create: bad filter bank (L=%d)", L);
+  TCB_CHECK_ARG(sigma > 0, "tcb_stripe_fw_create: sigma must be > 0");
+  tcb_stripe_fw *h = new tcb_stripe_fw();
+  h->nproj = (int)nproj;
+  h->nz = (int)nz;
+  h->ni = (int)ni;
+  h->level = level;
+  h->nproj_pad = (int)(nproj + nproj / 8);
+  h->L = L;
+  h->H.push_back(h->nproj_pad);
+  h->W.push_back((int)ni);
+  for (int k = 0; k < level; k++) {
+    h->H.push_back((h->H[k] + L - 1) / 2);
+    h->W.push_back((h->W[k] + L - 1) / 2);
+  }
+  auto fail = [&](int code, const char *what) {
+    set_error("tcb_stripe_fw_create: %s", what);
+    fw_release(h);
+    delete h;
+    return code;
+  };
+  Taps t{};
+  t.L = L;
+  for (int k = 0; k < L; k++) {  // float32 taps, analysis filters reversed
+    t.h0[k] = (float)dec_lo[L - 1 - k];
+    t.h1[k] = (float)dec_hi[L - 1 - k];
+    t.g0[k] = (float)rec_lo[k];
+    t.g1[k] = (float)rec_hi[k];
+  }
+  if (cudaMalloc(&h->taps, sizeof(Taps)) != cudaSuccess)
+    return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+  if (cudaMemcpy(h->taps, &t, sizeof(Taps), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(TCB_ERR_CUDA, "cudaMemcpy failed");
+  size_t maxband = 0, maxtmp = 0;
+  for (int k = 0; k < level; k++) {
+    int Ho = h->H[k + 1], Wo = h->W[k + 1];
+    float *y = nullptr;
+    if (cudaMalloc(&y, (size_t)nz * 4 * Ho * Wo * sizeof(float)) != cudaSuccess)
+      return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    h->Y.push_back(y);
+    // damping factors (remove_stripe.py:270-274), 1/Ho of the inverse FFT folded in
+    int nc = Ho / 2 + 1;
+    std::vector<double> yh(Ho);
+    for (int q = 0; q < Ho; q++) yh[q] = ((-Ho + 2 * q) + 1) / 2.0;
+    std::vector<float> d(nc);
+    for (int q = 0; q < nc; q++) {
+      double v = yh[(q + Ho / 2) % Ho];  // ifftshift, first nc entries
+      d[q] = (float)(-std::expm1(-v * v / (2.0 * (double)sigma * sigma)) / Ho);
+    }
+    float *dd = nullptr;
+    if (cudaMalloc(&dd, nc * sizeof(float)) != cudaSuccess)
+      return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    h->damp.push_back(dd);
+    if (cudaMemcpy(dd, d.data(), nc * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(TCB_ERR_CUDA, "cudaMemcpy failed");
+    cufftHandle p1 = 0, p2 = 0;
+    int len[1] = {Ho};
+    int batch = (int)(nz * Wo);
+    if (cufftPlanMany(&p1, 1, len, nullptr, 1, Ho, nullptr, 1, nc, CUFFT_R2C, batch) !=
+            CUFFT_SUCCESS ||
+        cufftPlanMany(&p2, 1, len, nullptr, 1, nc, nullptr, 1, Ho, CUFFT_C2R, batch) !=
+            CUFFT_SUCCESS)
+      return fail(TCB_ERR_CUFFT, "cufftPlanMany failed");
+    h->r2c.push_back(p1);
+    h->c2r.push_back(p2);
+    maxband = std::max(maxband, (size_t)nz * Ho * Wo);
+    maxtmp = std::max(maxtmp, (size_t)nz * 2 * h->H[k] * Wo);          // afb rows output
+    maxtmp = std::max(maxtmp, (size_t)nz * 2 * (2 * Ho - L + 2) * Wo);  // sfb cols output
+  }
+  if (cudaMalloc(&h->tmp, maxtmp * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->bt, maxband * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->spec, (maxband / 2 + (size_t)nz * h->W[1] + 16) * sizeof(float2)) !=
+          cudaSuccess)
+    return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+  h->tmp_elems = maxtmp;
+  *out = h;
+  return TCB_OK;
+}
+
+// Ring removal in place on padded sinograms sino [nz][nproj_pad][ni] (slice
+// stride sstride elements): rows [(pad)/2, (pad)/2 + nproj) hold the data,
+// the other rows must be zero on entry (they are overwritten).
+extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t sstride,
+                                        void *stream) {
+  TCB_CHECK_ARG(h && h->taps, "tcb_stripe_fw_apply_sino: null or freed handle");
+  TCB_CHECK_ARG(sino, "tcb_stripe_fw_apply_sino: null pointer");
+  TCB_CHECK_ARG(sstride >= (size_t)h->nproj_pad * h->ni, "tcb_stripe_fw_apply_sino: stride");
+  cudaStream_t s = (cudaStream_t)stream;
+  StageTimer st("stripe_fw", s);
+  const int B = h->nz, L = h->L;
+  // forward
+  for (int k = 0; k < h->level; k++) {
+    int Hk = h->H[k], Wk = h->W[k], Ho = h->H[k + 1], Wo = h->W[k + 1];
+    const float *x;
+    long long xsz;
+    int xsx;
+    if (k == 0) {
+      x = sino;
+      xsz = (long long)sstride;
+      xsx = Wk;
+    } else {
+      x = h->Y[k - 1];  // LL channel of the previous level
+      xsz = 4LL * Hk * Wk;
+      xsx = Wk;
+    }
+    int pw = 2 * (Wo - 1) - Wk + L, ph = 2 * (Ho - 1) - Hk + L;
+    long long n1 = (long long)B * Hk * Wo;
+    afb_rows<<<ceil_div(n1, 256), 256, 0, s>>>(x, xsz, xsx, h->tmp, B, Hk, Wk, Wo, pw / 2,
+                                               h->taps);
+    TCB_LAUNCH_CHECK();
+    long long n2 = (long long)B * 2 * Ho * Wo;
+    afb_cols<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, h->Y[k], B, Hk, Wo, Ho, ph / 2, h->taps);
+    TCB_LAUNCH_CHECK();
+    // damp band 1 (index 2 of the level: high-pass along the detector, low-pass along angles)
+    float *band = h->Y[k] + 2LL * Ho * Wo;
+    dim3 tb(32, 8);
+    dim3 g1(ceil_div(Wo, 32), ceil_div(Ho, 32), B);
+    transpose_bands<<<g1, tb, 0, s>>>(band, 4LL * Ho * Wo, h->bt, (long long)Ho * Wo, Ho, Wo);
+    TCB_LAUNCH_CHECK();
+    TCB_CUFFT(cufftSetStream(h->r2c[k], s));
+    TCB_CUFFT(cufftSetStream(h->c2r[k], s));
+    TCB_CUFFT(cufftExecR2C(h->r2c[k], h->bt, (cufftComplex *)h->spec));
+    int nc = Ho / 2 + 1;
+    long long tot = (long long)B * Wo * nc;
+    damp_kernel<<<ceil_div(tot, 256), 256, 0, s>>>(h->spec, h->damp[k], nc, tot);
+    TCB_LAUNCH_CHECK();
+    TCB_CUFFT(cufftExecC2R(h->c2r[k], (cufftComplex *)h->spec, h->bt));
+    dim3 g2(ceil_div(Ho, 32), ceil_div(Wo, 32), B);
+    transpose_bands<<<g2, tb, 0, s>>>(h->bt, (long long)Ho * Wo, band, 4LL * Ho * Wo, Wo, Ho);
+    TCB_LAUNCH_CHECK();
+    count_launch(5);
+  }
+  // inverse
+  for (int k = h->level - 1; k >= 0; k--) {
+    int Hi = h->H[k + 1], Wi = h->W[k + 1];
+    int Hc = 2 * Hi - L + 2;  // rows after the column synthesis
+    long long n1 = (long long)B * 2 * Hc * Wi;
+    sfb_cols<<<ceil_div(n1, 256), 256, 0, s>>>(h->Y[k], 4LL * Hi * Wi, Hi, Wi, Wi, h->tmp, B,
+                                               Hc, h->taps);
+    TCB_LAUNCH_CHECK();
+    // reconstruction of level k's input, cropped to its size, into the LL
+    // channel of the level above (or into the sinograms)
+    int Hd = h->H[k], Wd = h->W[k];
+    float *dst;
+    long long dsz;
+    if (k == 0) {
+      dst = sino;
+      dsz = (long long)sstride;
+    } else {
+      dst = h->Y[k - 1];
+      dsz = 4LL * Hd * Wd;
+    }
+    int Hrows = std::min(Hd, Hc);
+    long long n2 = (long long)B * Hrows * Wd;
+    sfb_rows<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, Hc, Wi, dst, dsz, Wd, Hrows, Wd, B,
+                                               h->taps);
+    TCB_LAUNCH_CHECK();
+    count_launch(2);
+  }
+  return TCB_OK;
+}
+
+extern "C" int tcb_stripe_fw_destroy(tcb_stripe_fw *h) {
+  if (!h) return TCB_OK;
+  fw_release(h);
+  delete h;
+  return TCB_OK;
+}

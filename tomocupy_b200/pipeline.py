@@ -31,7 +31,7 @@ from .reconstruction.fbp_filter import calc_filter
 
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
-                 algorithm="fourierrec", minus_log=True, device="cuda"):
+                 algorithm="fourierrec", minus_log=True, device="cuda", stripe=None):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if algorithm == "fourierrec" and ncz % 2:
@@ -52,6 +52,16 @@ class SinoPipeline:
                                 device=self.device)
         self.filter = cfunc_filter.cfunc_filter(self.nproj, self.ncz, self.ne)
         self._w_cache: dict = {}
+        # optional Fourier-wavelet ring removal between dark/flat and -log
+        # (ProcFunctions.proc_sino, proc_functions.py:140-160): stripe is
+        # (sigma, wavelet, level)
+        self.fw = None
+        if stripe is not None:
+            from .processing.remove_stripe import StripeFW
+            sigma, wname, level = stripe
+            self.fw = StripeFW(self.nproj, self.ncz, self.n, sigma, wname, level)
+            self.sino = torch.zeros((self.ncz, self.fw.nproj_pad, self.n), dtype=torch.float32,
+                                    device=self.device)
         if algorithm == "fourierrec":
             self.fr = cfunc_fourierrec.cfunc_fourierrec(self.nproj, self.ncz // 2, self.n,
                                                         self.theta)
@@ -87,6 +97,20 @@ class SinoPipeline:
         assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.n
         d0 = dark0[z_lo:z_lo + nz] if dark0 is not None else None
         f0 = flat0[z_lo:z_lo + nz] if flat0 is not None else None
+        if self.fw is not None:
+            fw = self.fw
+            s = torch.cuda.current_stream() if stream is None else stream
+            with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
+                self.sino.zero_()
+            prep_rows(self.sino, data, d0, f0, darkflat=dark0 is not None, minus_log=False,
+                      out_zstride=fw.nproj_pad * self.n, out_pstride=self.n,
+                      out_poff=fw.poff, stream=stream)
+            fw.apply_sino(self.sino, stream)
+            src = self.sino[:nz, fw.poff:fw.poff + self.nproj].permute(1, 0, 2)
+            prep_rows(self.rows, src, darkflat=False, minus_log=self.minus_log,
+                      out_zstride=self.nproj * self.ne, out_pstride=self.ne, out_xoff=self.pad,
+                      out_width=self.ne, edge_pad=True, stream=stream)
+            return
         prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                   minus_log=self.minus_log, out_zstride=self.nproj * self.ne,
                   out_pstride=self.ne, out_xoff=self.pad, out_width=self.ne, edge_pad=True,

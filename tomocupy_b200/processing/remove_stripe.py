@@ -1,0 +1,64 @@
+"""Fourier-wavelet ring removal (``remove_stripe_fw``) over the native operator.
+
+Same function signature and result layout as the reference
+(src/tomocupy/processing/remove_stripe.py:253-293): data [nproj, nz, ni]
+float32 -> ring-corrected copy.  ``StripeFW`` is the reusable operator for a
+fixed chunk shape, working in place on padded sinograms
+[nz, nproj + nproj//8, ni] (the layout the fused pipeline produces).
+The wavelet filters come from :mod:`.wavelets`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import functools
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._handle import NativeHandle
+from . import wavelets
+from .proc_functions import prep_rows
+
+
+class StripeFW(NativeHandle):
+    _destroy = "tcb_stripe_fw_destroy"
+
+    def __init__(self, nproj, nz, ni, sigma=1.0, wname="sym16", level=7):
+        dl, dh, rl, rh = (np.ascontiguousarray(a, dtype=np.float64)
+                          for a in wavelets.filter_bank(wname))
+        P = C.POINTER(C.c_double)
+        self._set(_lib.create("tcb_stripe_fw_create", int(nproj), int(nz), int(ni), int(level),
+                              float(sigma), dl.ctypes.data_as(P), dh.ctypes.data_as(P),
+                              rl.ctypes.data_as(P), rh.ctypes.data_as(P), len(rl)))
+        self.nproj, self.nz, self.ni, self.level = int(nproj), int(nz), int(ni), int(level)
+        self.nproj_pad = self.nproj + self.nproj // 8
+        self.poff = (self.nproj_pad - self.nproj) // 2
+
+    def apply_sino(self, sino, stream=None):
+        """In place on sino [nz, nproj_pad, ni] float32 (pad rows zero on entry)."""
+        assert sino.dtype == torch.float32 and sino.stride(2) == 1 and sino.stride(1) == self.ni
+        _lib.call("tcb_stripe_fw_apply_sino", self._live(), sino.data_ptr(), sino.stride(0),
+                  _lib.stream_ptr(stream))
+        return sino
+
+
+@functools.lru_cache(maxsize=8)
+def _operator(nproj, nz, ni, sigma, wname, level, device_index):
+    return StripeFW(nproj, nz, ni, sigma, wname, level)
+
+
+def remove_stripe_fw(data, sigma, wname, level):
+    """Remove stripes with wavelet filtering: data [nproj, nz, ni] -> new tensor."""
+    nproj, nz, ni = data.shape
+    op = _operator(nproj, nz, ni, float(sigma), str(wname), int(level),
+                   data.device.index or 0)
+    sino = torch.zeros((nz, op.nproj_pad, ni), dtype=torch.float32, device=data.device)
+    src = data if data.dtype == torch.float32 else data.to(torch.float32)
+    # [nproj, nz, ni] -> rows poff.. of [nz, nproj_pad, ni]
+    prep_rows(sino, src, darkflat=False, minus_log=False, out_zstride=op.nproj_pad * ni,
+              out_pstride=ni, out_poff=op.poff)
+    op.apply_sino(sino)
+    out = torch.empty((nproj, nz, ni), dtype=data.dtype, device=data.device)
+    out.copy_(sino[:, op.poff:op.poff + nproj].permute(1, 0, 2))
+    return out

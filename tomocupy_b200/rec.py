@@ -23,9 +23,9 @@ from .processing.proc_functions import darkflat_stats
 
 
 def _supported():
-    if args.remove_stripe_method not in ("none",):
+    if args.remove_stripe_method not in ("none", "fw"):
         raise NotImplementedError(
-            f"remove_stripe_method={args.remove_stripe_method!r} in the fused driver")
+            f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
     if args.file_type != "standard" or args.binning != 0:
         raise NotImplementedError("double_fov / binning are not part of tomocupy_b200")
     if args.dtype != "float32":
@@ -40,9 +40,13 @@ class GPURec:
         self.device = torch.device(device)
         self.cl_reader = cl_reader
         self.cl_writer = cl_writer
+        stripe = None
+        if args.remove_stripe_method == "fw":
+            stripe = (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
         self.pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                  params.center, args.fbp_filter, args.reconstruction_algorithm,
-                                 minus_log=args.minus_log == "True", device=self.device)
+                                 minus_log=args.minus_log == "True", device=self.device,
+                                 stripe=stripe)
         self.stream1 = torch.cuda.Stream(self.device)
         self.stream2 = torch.cuda.Stream(self.device)
         self.stream3 = torch.cuda.Stream(self.device)
