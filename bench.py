@@ -129,6 +129,12 @@ def stage_bytes(stage, n, nproj, ncz):
     return table.get(stage)
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch from
+# the committed ncu captures, keyed by (stage, n, nproj, rows per chunk);
+# see profiles/fr_gather_grid_blocks_2048x1500_16pairs.md
+NCU_TRAFFIC = {("fr_gather", 2048, 1500, 32): 533.82e6 + 2104.92e6}
+
+
 def setup_dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -243,7 +249,8 @@ def run_ours(a, ws, rank, local):
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": round(achieved / peaks["hbm_gbs"], 4),
-                    "traffic": None, "algorithmic_bytes_per_launch": algo,
+                    "traffic": NCU_TRAFFIC.get((dom, a.n, a.nproj, a.ncz)),
+                    "algorithmic_bytes_per_launch": algo,
                     "ms_per_launch": round(per_launch_ms, 4),
                     "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)"
                     if peaks_kind == "measured" else "fallback 6.65 TB/s"}
