@@ -45,15 +45,18 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
         rec = ref.RefLineRec(th, P, P, ncz, ncz, n)
     out = torch.zeros((nz, n, n), dtype=torch.float32, device=dev)
     for z0 in range(0, nz, ncz):
-        d = ref.ref_darkflat_minus_log(data[:, z0:z0 + ncz].to(dev), dark[:, z0:z0 + ncz].to(dev),
-                                       flat[:, z0:z0 + ncz].to(dev), minus_log=stripe is None)
+        # dark/flat in CuPy's float32 operation order (NumPy restatement,
+        # bit-exact with the native kernel), -log with the device logf
+        d = np_tomo.darkflat(np.asarray(data[:, z0:z0 + ncz]), np.asarray(dark[:, z0:z0 + ncz]),
+                             np.asarray(flat[:, z0:z0 + ncz]))
+        d = torch.as_tensor(np.ascontiguousarray(d), device=dev)
         if stripe is not None:
             # proc_sino: ring removal on the dark/flat corrected frames (checked on
             # its own against the reference's remove_stripe_fw), then proc_proj: -log
             from tomocupy_b200.processing.remove_stripe import remove_stripe_fw
             d = remove_stripe_fw(d.contiguous(), *stripe)
-            d = torch.where(d <= 0, torch.ones((), device=dev), d)
-            d = torch.nan_to_num(-torch.log(d), nan=6.0, posinf=0.0, neginf=0.0)
+        d = torch.where(d <= 0, torch.ones((), device=dev), d)
+        d = torch.nan_to_num(-torch.log(d), nan=6.0, posinf=0.0, neginf=0.0)
         d = d.permute(1, 0, 2).contiguous()
         s = torch.zeros(ncz, device=dev) if sht is None else sht
         d = ref.ref_fbp_filter_center(filt, d, wf, t, center, s, n, ne)
