@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -125,6 +126,8 @@ def stage_bytes(stage, n, nproj, ncz):
         "fr_gather": pairs * (nproj * n * 8 + (2 * n) ** 2 * 8),
         "fr_deapod": pairs * (n * n * 8 + 2 * n * n * 4),
         "linerec": ncz * (nproj * n * 4 + n * n * 8),
+        # tensor-core filter: FLOPs (3 split products of 2 n^2 per row), not bytes
+        "tc_filter": 3 * 2 * ncz * nproj * n * n,
     }
     return table.get(stage)
 
@@ -193,28 +196,17 @@ def cpu_baseline(a, data_cpu, dark, flat, theta):
             "seconds": secs}
 
 
-def run_ours(a, ws, rank, local):
+def _time_path(a, ws, dtype, data, dark, flat, theta, dark0, flat0, out, dev, local):
+    """Warm up, then time a.steps whole-volume reconstructions on the device."""
     import torch
     from tomocupy_b200 import _lib, global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
-    from tomocupy_b200.global_vars import params
-    from tomocupy_b200.processing.proc_functions import darkflat_stats
     from tomocupy_b200.rec import GPURec
-
-    dev = torch.device("cuda", local)
-    t_gen = time.perf_counter()
-    data, dark, flat, theta, _ = make_data(a, dev)
-    torch.cuda.synchronize()
-    log(f"[rank {rank}] generated {tuple(data.shape)} in {time.perf_counter() - t_gen:.1f} s")
     global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
-                      nsino_per_chunk=a.ncz)
-    reader = ArrayReader(data, dark, flat, theta=theta)
-    writer = ArrayWriter(device=dev)
-    rec = GPURec(reader, writer, device=dev)
-    dark0, flat0, _ = darkflat_stats(dark, flat)
-    out = torch.empty((params.nz, params.n, params.n), dtype=torch.float32, device=dev)
+                      nsino_per_chunk=a.ncz, dtype=dtype)
+    rec = GPURec(ArrayReader(data, dark, flat, theta=theta), ArrayWriter(device=dev),
+                 device=dev)
     stream = torch.cuda.current_stream(dev)
-
     for _ in range(a.warmup):
         rec.recon_device(data, dark0, flat0, out)
     barrier(ws)
@@ -231,30 +223,86 @@ def run_ours(a, ws, rank, local):
     launches = _lib.launch_count() - l0
     stages = _lib.profile_report()
     _lib.profile_enable(False)
-    ms_total = barrier_max(ev0.elapsed_time(ev1), ws)
-    ms_step = ms_total / a.steps
+    ms_step = barrier_max(ev0.elapsed_time(ev1), ws) / a.steps
+    del rec
+    return ms_step, stages, launches, clk.summary()
+
+
+def _roofline(stages, a, peaks, peaks_kind, kernel=None):
+    """Roofline of the dominant (or the named) native stage."""
+    own = {k: v for k, v in stages.items() if stage_bytes(k, a.n, a.nproj, a.ncz) is not None}
+    dom = kernel if kernel in own else (max(own, key=lambda k: own[k]["ms"]) if own else None)
+    if dom is None:
+        return None
+    per_launch_ms = own[dom]["ms"] / own[dom]["count"]
+    algo = stage_bytes(dom, a.n, a.nproj, a.ncz)
+    if dom == "tc_filter":  # tensor-bound: algorithmic flops, fp16 dense = bf16 dense rate
+        achieved = algo / (per_launch_ms / 1e3) / 1e12
+        peak = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
+        return {"bound": "tensor", "kernel": dom, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                "traffic": NCU_TRAFFIC.get((dom, a.n, a.nproj, a.ncz)),
+                "algorithmic_flops_per_launch": algo, "ms_per_launch": round(per_launch_ms, 4),
+                "peak_source": (f"{peaks_kind} (MEASURED_PEAKS.json bf16_tflops_sustained, "
+                                "kernel timed inside a long step)")
+                if peaks_kind == "measured" else "fallback 1.4 PFLOP/s sustained"}
+    achieved = algo / (per_launch_ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+            "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peaks["hbm_gbs"], 4),
+            "traffic": NCU_TRAFFIC.get((dom, a.n, a.nproj, a.ncz)),
+            "algorithmic_bytes_per_launch": algo, "ms_per_launch": round(per_launch_ms, 4),
+            "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)"
+            if peaks_kind == "measured" else "fallback 6.65 TB/s"}
+
+
+def run_ours(a, ws, rank, local):
+    import torch
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.processing.proc_functions import darkflat_stats
+
+    dev = torch.device("cuda", local)
+    t_gen = time.perf_counter()
+    data, dark, flat, theta, _ = make_data(a, dev)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] generated {tuple(data.shape)} in {time.perf_counter() - t_gen:.1f} s")
+    dark0, flat0, _ = darkflat_stats(dark, flat)
+    out = torch.empty((a.nz, a.n, a.n), dtype=torch.float32, device=dev)
+    peaks, peaks_kind = load_peaks()
     vox = float(a.n) ** 2 * a.nz * a.nproj
+
+    # primary path (the drop-in fp32 by default) and the other precision beside it
+    primary = a.precision
+    other = "mixed" if primary == "float32" else "float32"
+    ms_step, stages, launches, clocks = _time_path(a, ws, primary, data, dark, flat, theta,
+                                                   dark0, flat0, out, dev, local)
     value = ws * vox / (ms_step / 1e3) / 1e9
     slices_s = ws * a.nz / (ms_step / 1e3)
-
-    # dominant native stage and its roofline
-    peaks, peaks_kind = load_peaks()
-    own = {k: v for k, v in stages.items() if stage_bytes(k, a.n, a.nproj, a.ncz) is not None}
-    dom = max(own, key=lambda k: own[k]["ms"]) if own else None
-    roofline = None
-    if dom:
-        per_launch_ms = own[dom]["ms"] / own[dom]["count"]
-        algo = stage_bytes(dom, a.n, a.nproj, a.ncz)
-        achieved = algo / (per_launch_ms / 1e3) / 1e9
-        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
-                    "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                    "frac": round(achieved / peaks["hbm_gbs"], 4),
-                    "traffic": NCU_TRAFFIC.get((dom, a.n, a.nproj, a.ncz)),
-                    "algorithmic_bytes_per_launch": algo,
-                    "ms_per_launch": round(per_launch_ms, 4),
-                    "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                    if peaks_kind == "measured" else "fallback 6.65 TB/s"}
-    clocks = clk.summary()
+    roofline = _roofline(stages, a, peaks, peaks_kind)
+    side = None
+    if not a.no_mixed:
+        out2 = torch.empty_like(out)
+        ms2, st2, l2, clk2 = _time_path(a, ws, other, data, dark, flat, theta, dark0, flat0,
+                                        out2, dev, local)
+        # whole-volume agreement of the two precisions (both outputs resident)
+        diff = 0.0
+        ref2 = 0.0
+        for z0 in range(0, a.nz, 64):
+            diff += float(torch.sum((out2[z0:z0 + 64] - out[z0:z0 + 64]).double() ** 2))
+            ref2 += float(torch.sum(out[z0:z0 + 64].double() ** 2))
+        del out2
+        v2 = ws * vox / (ms2 / 1e3) / 1e9
+        mixed_ms, fp32_ms = (ms2, ms_step) if other == "mixed" else (ms_step, ms2)
+        mst = st2 if other == "mixed" else stages
+        side = {"precision": other, "value": round(v2, 2), "unit": "GUPS",
+                "ms_per_step": round(ms2, 3), "slices_per_s": round(ws * a.nz / (ms2 / 1e3), 1),
+                "mixed_speedup_vs_fp32": round(fp32_ms / mixed_ms, 3),
+                "rel_l2_vs_" + primary: math.sqrt(diff / max(ref2, 1e-300)),
+                "rel_l2_vs_fp64": "see tests/test_gpu_pipeline.py::"
+                                  "test_c1_mixed_fourierrec_vs_fp64_oracle (budget 1e-3)",
+                "gpu_launches": l2, "clocks": clk2,
+                "roofline_tc_filter": _roofline(mst, a, peaks, peaks_kind, "tc_filter"),
+                "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in st2.items()}}
 
     # ---------------- e2e through the public driver with host buffers
     e2e = None
@@ -267,21 +315,26 @@ def run_ours(a, ws, rank, local):
         base = cpu_baseline(a, dcpu, dkc, flc, theta)
 
     if rank == 0:
+        tag = "fp32" if primary == "float32" else "mixed-precision"
         line = {
-            "metric": f"GUPS @{a.n}^2x{a.nproj} ({a.algorithm} fp32 pipeline, 1 GPU rate)",
+            "metric": f"GUPS @{a.n}^2x{a.nproj} ({a.algorithm} {tag} pipeline, 1 GPU rate)",
             "value": round(value, 2), "unit": "GUPS", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if primary == "float32" else "f16x2 operands / f32 accumulate",
+            "data": "synthetic",
             "config": {"workload": f"{a.nz} rows x {a.nproj} angles x {a.n} cols uint16 -> "
                                    f"{a.nz}x{a.n}^2 f32 volume; dark/flat, -log, {a.filter} "
                                    f"filter, {a.algorithm}; ring removal off",
                        "n": a.n, "nproj": a.nproj, "nz": a.nz, "ncz": a.ncz,
+                       "precision": primary,
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "inputs (12.6 GB frames) larger than L2; no flush"},
             "slices_per_s": round(slices_s, 1),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": base,
             "clocks": clocks, "gpu_launches": launches,
             "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in stages.items()},
+            other if other == "mixed" else "fp32": side,
         }
         print(json.dumps(line), flush=True)
 
@@ -305,7 +358,7 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank):
     dk_host = dark[:, :nz_e2e].cpu().pin_memory()
     fl_host = flat[:, :nz_e2e].cpu().pin_memory()
     global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
-                      nsino_per_chunk=a.ncz)
+                      nsino_per_chunk=a.ncz, dtype=a.precision)
     reader = ArrayReader(d_host, dk_host, fl_host, theta=theta)
     writer = ArrayWriter(device="cpu", pin=True)
     rec = GPURec(reader, writer, device=dev)
@@ -419,6 +472,9 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", choices=["float32", "mixed"], default="float32",
+                    help="path reported as value (the other one is timed beside it)")
+    ap.add_argument("--no-mixed", action="store_true", help="time only --precision")
     a = ap.parse_args()
     if a.warmup < 3:
         log("note: warmup < 3 requested; using 3")

@@ -151,6 +151,51 @@ int tcb_filter_apply(tcb_filter *h, void *g, const void *w, void *stream);
 int tcb_filter_destroy(tcb_filter *h);
 
 /* ------------------------------------------------------------------------
+ * Mixed-precision filter on the tensor cores.  Same operator as
+ * fbp_filter_center (src/tomocupy/reconstruction/backproj_functions.py:93-109:
+ * edge pad to ne, R2C, x w, C2R, crop) followed by cfunc_filter::filter
+ * (src/cuda/cfunc_filter.cu:49-61), written as the n x n matrix it is and
+ * applied as an fp16 tcgen05 GEMM with fp32 accumulation and a hi/lo
+ * split-precision correction (x_hi T_hi + x_lo T_hi + x_hi T_lo).  The
+ * reference's own half-precision path is cfunc_filterfp16 (fp16 cuFFT).
+ *
+ * create: nproj angles, up to nz slices per apply call, n columns
+ *   (n >= 64, n % 8 == 0), nkern distinct filter kernels (1 = shared by all
+ *   slices; otherwise slice z of a call uses kernel kern0 + z).
+ * set_kernels: hz host float64 [nkern][ne], the unnormalised C2R of each
+ *   kernel's spectrum w (ne = padded length, pad = left padding = ne/2 - n/2
+ *   in the reference); synchronous.
+ * tcb_prep_rows_split16 (below) writes the hi/lo operand planes.
+ * apply: x_hi/x_lo fp16 [nz * nproj][lda] (z-major rows).  out_mode
+ *   TCB_TCF_OUT_ROWS writes fp32 out[(z*nproj + p)*ldo + j];
+ *   TCB_TCF_OUT_PAIRS writes the packed complex layout of
+ *   FourierRec.backprojection (src/tomocupy/reconstruction/fourierrec.py:63-68):
+ *   float2 out[(z % (nz/2))*nproj + p][j], real part from slices < nz/2.
+ * status: 1 in *timed_out when a kernel gave up on a bounded wait (synchronous).
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_tcfilter tcb_tcfilter;
+#define TCB_TCF_OUT_ROWS 0
+#define TCB_TCF_OUT_PAIRS 1
+int tcb_tcfilter_create(tcb_tcfilter **out, size_t nproj, size_t nz, size_t n, size_t nkern);
+int tcb_tcfilter_set_kernels(tcb_tcfilter *h, const double *hz, size_t ne, size_t pad,
+                             void *stream);
+int tcb_tcfilter_apply(tcb_tcfilter *h, const void *x_hi, const void *x_lo, size_t lda,
+                       size_t nz, size_t kern0, void *out, int out_mode, size_t ldo,
+                       void *stream);
+int tcb_tcfilter_status(tcb_tcfilter *h, int *timed_out);
+int tcb_tcfilter_destroy(tcb_tcfilter *h);
+
+/* Split-fp16 variant of tcb_prep_rows (same normalisation chain, same
+ * reference lines), written as hi = fp16(v) and lo = fp16(v - hi) planes
+ * [z*out_zstride + p*out_pstride + x]; no edge padding (the tensor-core
+ * filter folds it into its operator). */
+int tcb_prep_rows_split16(void *hi, void *lo, const void *in, const float *dark0,
+                          const float *flat0, const float *flat1, size_t nproj, size_t nz,
+                          size_t n, size_t in_pstride, size_t in_zstride, int in_dtype,
+                          size_t out_zstride, size_t out_pstride, unsigned flags,
+                          void *stream);
+
+/* ------------------------------------------------------------------------
  * Fourier-gridding backprojector.  Replaces cfunc_fourierrec
  * (src/include/cfunc_fourierrec.cuh:10-36, src/cuda/cfunc_fourierrec.i:9-21).
  *   theta: device fp32 [nproj] (read during create only, as in the reference)

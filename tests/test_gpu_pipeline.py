@@ -67,11 +67,12 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
     return out.cpu()
 
 
-def run_ours(data, dark, flat, theta, algorithm="fourierrec", ncz=8, host=True):
+def run_ours(data, dark, flat, theta, algorithm="fourierrec", ncz=8, host=True,
+             dtype="float32"):
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
-    global_vars.reset(reconstruction_algorithm=algorithm, nsino_per_chunk=ncz)
+    global_vars.reset(reconstruction_algorithm=algorithm, nsino_per_chunk=ncz, dtype=dtype)
     dev = "cpu" if host else "cuda"
     reader = ArrayReader(data.to(dev), dark.to(dev), flat.to(dev), theta=theta, pin=host)
     writer = ArrayWriter(device=dev, pin=host)
@@ -180,3 +181,57 @@ def test_recon_try_matches_reference(cuda, ref, c1):
             ours = writer.tries[(zs, float(params.save_centers[k + kk]))].cpu()
             err = rel_l2(ours, theirs[kk])
             assert err < 1e-5, (k + kk, err)
+
+
+# --------------------------------------------------------------------------
+# Mixed precision: split-fp16 tensor-core filter feeding the fp32 backprojectors.
+# Budget: rel-L2 <= 1e-3 against the FP64 oracle of the same algorithm.
+def _fp64_fourierrec(d, dk, fl, theta, n):
+    from oracle import np_tomo
+    sino = np_tomo.minus_log(np_tomo.darkflat(d.numpy(), dk.numpy(), fl.numpy()))
+    sino = sino.transpose(1, 0, 2).astype(np.float64)
+    wf = np_tomo.calc_filter(4 * n, "parzen")
+    filt = np_tomo.fbp_filter_center(sino, wf, n / 2, 0.0, np.float64)
+    return np_tomo.fourierrec(filt, theta, np.float64)
+
+
+def test_c1_mixed_fourierrec_vs_fp64_oracle(cuda, c1):
+    data, dark, flat, theta, _ = c1
+    d, dk, fl = data[:, :4], dark[:, :4], flat[:, :4]
+    mixed = run_ours(d, dk, fl, theta, ncz=4, dtype="mixed").numpy()
+    fp32 = run_ours(d, dk, fl, theta, ncz=4).numpy()
+    want = _fp64_fourierrec(d, dk, fl, theta, N)
+    e_mixed, e_fp32 = rel_l2(mixed, want), rel_l2(fp32, want)
+    assert e_mixed < 1e-3, e_mixed
+    # the filter's extra error is small next to the gridding's own
+    assert e_mixed < 2 * e_fp32 + 1e-5, (e_mixed, e_fp32)
+
+
+@pytest.mark.parametrize("algorithm", ["linerec", "lprec"])
+def test_c1_mixed_matches_fp32_path(cuda, c1, algorithm):
+    data, dark, flat, theta, _ = c1
+    d, dk, fl = data[:, :4], dark[:, :4], flat[:, :4]
+    mixed = run_ours(d, dk, fl, theta, algorithm=algorithm, ncz=4, dtype="mixed")
+    fp32 = run_ours(d, dk, fl, theta, algorithm=algorithm, ncz=4)
+    err = rel_l2(mixed, fp32)
+    assert err < 1e-4, err
+
+
+def test_recon_try_mixed_matches_fp32(cuda, c1):
+    """Per-centre filter kernels (one operator per slice) in the try sweep."""
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.rec import GPURec
+    data, dark, flat, theta, _ = c1
+    res = {}
+    for dtype in ("float32", "mixed"):
+        global_vars.reset(reconstruction_type="try", center_search_width=2.0,
+                          center_search_step=0.5, nsino="0.5", nsino_per_chunk=4, dtype=dtype)
+        writer = ArrayWriter(device="cuda")
+        GPURec(ArrayReader(data, dark, flat, theta=theta), writer).recon_try()
+        res[dtype] = {k: v.cpu() for k, v in writer.tries.items()}
+    assert res["float32"].keys() == res["mixed"].keys() and len(res["mixed"]) == 8
+    for k in res["mixed"]:
+        err = rel_l2(res["mixed"][k], res["float32"][k])
+        assert err < 1e-4, (k, err)

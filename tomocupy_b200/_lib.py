@@ -23,6 +23,9 @@ PREP_MINUS_LOG = 2
 PREP_FLAT_LINEAR = 4
 PREP_EDGE_PAD = 8
 
+TCF_OUT_ROWS = 0
+TCF_OUT_PAIRS = 1
+
 STATUS_NAMES = {
     0: "TCB_OK", 1: "TCB_ERR_INVALID_ARGUMENT", 2: "TCB_ERR_CUDA", 3: "TCB_ERR_CUFFT",
     4: "TCB_ERR_OUT_OF_MEMORY", 5: "TCB_ERR_NOT_SUPPORTED", 6: "TCB_ERR_FREED",
@@ -60,6 +63,12 @@ SIGNATURES: dict[str, list] = {
     "tcb_filter_create": [C.POINTER(vp), sz, sz, sz, i32],
     "tcb_filter_apply": [vp, vp, vp, vp],
     "tcb_filter_destroy": [vp],
+    "tcb_tcfilter_create": [C.POINTER(vp), sz, sz, sz, sz],
+    "tcb_tcfilter_set_kernels": [vp, vp, sz, sz, vp],
+    "tcb_tcfilter_apply": [vp, vp, vp, sz, sz, sz, vp, i32, sz, vp],
+    "tcb_tcfilter_status": [vp, C.POINTER(i32)],
+    "tcb_tcfilter_destroy": [vp],
+    "tcb_prep_rows_split16": [vp, vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, u32, vp],
     "tcb_fourierrec_create": [C.POINTER(vp), sz, sz, sz, vp, i32],
     "tcb_fourierrec_backprojection": [vp, vp, vp, vp],
     "tcb_fourierrec_backprojection_slices": [vp, vp, vp, vp],

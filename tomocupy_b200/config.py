@@ -15,7 +15,7 @@ DEFAULTS = {
     "reconstruction_type": "full",          # 'full' | 'try' | 'try_lamino'
     "reconstruction_algorithm": "fourierrec",  # 'fourierrec' | 'lprec' | 'linerec'
     "fbp_filter": "parzen",
-    "dtype": "float32",                     # 'float32' | 'float16'
+    "dtype": "float32",                     # 'float32' | 'float16' | 'mixed' (tensor-core filter)
     "rotation_axis": -1.0,
     "center_search_width": 50.0,
     "center_search_step": 0.5,

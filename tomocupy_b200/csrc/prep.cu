@@ -6,6 +6,8 @@
 // Every CuPy elementwise step there is a separate kernel, so no multiply-add
 // is ever contracted; the explicit __f*_rn intrinsics below keep nvcc from
 // contracting either, which makes the fp32 results bit-identical.
+#include <cuda_fp16.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -50,6 +52,7 @@ __global__ void darkflat_stats_kernel(float *__restrict__ dark0, float *__restri
 
 struct PrepArgs {
   float *out;
+  __half *hi, *lo;  // split-fp16 output planes (tcb_prep_rows_split16)
   const void *in;
   const float *dark0, *flat0, *flat1;
   int nproj, nz, n;
@@ -108,24 +111,37 @@ __device__ __forceinline__ float prep_scalar(const PrepArgs &a, const T *src, in
   return prep_apply(a.flags, to_f32(src[x]), d0, f0, f1, vlin);
 }
 
+// v = hi + lo with hi = fp16(v) and lo = fp16(v - hi): 22 significant bits
+// in two fp16 planes, the operand format of the tensor-core filter.
+__device__ __forceinline__ void split16(float v, __half &h, __half &l) {
+  h = __float2half_rn(v);
+  l = __float2half_rn(__fsub_rn(v, __half2float(h)));
+}
+
 // One CTA per output row (z, p); rows are enumerated z-major so consecutive
-// CTAs write consecutive output rows.
-template <typename T>
+// CTAs write consecutive output rows.  SPLIT writes the row as two fp16
+// planes (hi, lo) instead of fp32.
+template <typename T, bool SPLIT>
 __global__ void __launch_bounds__(256) prep_rows_kernel(PrepArgs a) {
   size_t row = blockIdx.x;
   int z = (int)(row / a.nproj);
   int p = (int)(row % a.nproj);
   const T *src = (const T *)a.in + (size_t)p * a.in_pstride + (size_t)z * a.in_zstride;
-  float *dst = a.out + (size_t)z * a.out_zstride + (size_t)(p + a.out_poff) * a.out_pstride;
+  const size_t orow = (size_t)z * a.out_zstride + (size_t)(p + a.out_poff) * a.out_pstride;
+  float *dst = SPLIT ? nullptr : a.out + orow;
+  __half *dhi = SPLIT ? a.hi + orow + a.out_xoff : nullptr;
+  __half *dlo = SPLIT ? a.lo + orow + a.out_xoff : nullptr;
   double vlin = 0.0;
   if (a.flags & TCB_PREP_FLAT_LINEAR)
     vlin = (p == a.nproj - 1) ? 1.0 : __dmul_rn((double)p, 1.0 / (double)(a.nproj - 1));
   const int n = a.n;
-  float *row_out = dst + a.out_xoff;
+  float *row_out = SPLIT ? nullptr : dst + a.out_xoff;
   const bool df = (a.flags & TCB_PREP_DARKFLAT) != 0;
   const bool lin = (a.flags & TCB_PREP_FLAT_LINEAR) != 0;
+  const bool out_al = SPLIT ? ((((uintptr_t)dhi) & 7) == 0 && (((uintptr_t)dlo) & 7) == 0)
+                            : ((((uintptr_t)row_out) & 15) == 0);
   // Vector path: 4 elements per thread per step when everything is aligned.
-  bool vec = (n % 4 == 0) && ((((uintptr_t)row_out) & 15) == 0) &&
+  bool vec = (n % 4 == 0) && out_al &&
              ((((uintptr_t)src) & (sizeof(T) * 4 - 1)) == 0) &&
              (!df || ((((uintptr_t)(a.dark0 + (size_t)z * n)) & 15) == 0 &&
                       (((uintptr_t)(a.flat0 + (size_t)z * n)) & 15) == 0 &&
@@ -147,13 +163,26 @@ __global__ void __launch_bounds__(256) prep_rows_kernel(PrepArgs a) {
       r.y = prep_apply(a.flags, (float)raw.y, d0.y, f0.y, f1.y, vlin);
       r.z = prep_apply(a.flags, (float)raw.z, d0.z, f0.z, f1.z, vlin);
       r.w = prep_apply(a.flags, (float)raw.w, d0.w, f0.w, f1.w, vlin);
-      *reinterpret_cast<float4 *>(row_out + x) = r;
+      if constexpr (SPLIT) {
+        __half h[4], l[4];
+        split16(r.x, h[0], l[0]);
+        split16(r.y, h[1], l[1]);
+        split16(r.z, h[2], l[2]);
+        split16(r.w, h[3], l[3]);
+        *reinterpret_cast<uint2 *>(dhi + x) = *reinterpret_cast<const uint2 *>(h);
+        *reinterpret_cast<uint2 *>(dlo + x) = *reinterpret_cast<const uint2 *>(l);
+      } else {
+        *reinterpret_cast<float4 *>(row_out + x) = r;
+      }
     }
   } else {
-    for (int x = threadIdx.x; x < n; x += blockDim.x)
-      row_out[x] = prep_scalar<T>(a, src, z, x, vlin);
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+      float v = prep_scalar<T>(a, src, z, x, vlin);
+      if constexpr (SPLIT) split16(v, dhi[x], dlo[x]);
+      else row_out[x] = v;
+    }
   }
-  if (a.flags & TCB_PREP_EDGE_PAD) {
+  if (!SPLIT && (a.flags & TCB_PREP_EDGE_PAD)) {
     float left = prep_scalar<T>(a, src, z, 0, vlin);
     float right = prep_scalar<T>(a, src, z, n - 1, vlin);
     size_t xo = a.out_xoff, xe = a.out_xoff + n;
@@ -223,17 +252,54 @@ extern "C" int tcb_prep_rows(float *out, const void *in, const float *dark0,
   if (nproj == 0 || nz == 0 || n == 0) return TCB_OK;
   size_t rows = nproj * nz;
   TCB_CHECK_ARG(rows < (1ull << 31), "tcb_prep_rows: too many rows in one call");
-  PrepArgs a{out, in, dark0, flat0, flat1, (int)nproj, (int)nz, (int)n, in_pstride,
-             in_zstride, out_zstride, out_pstride, out_poff, out_xoff, out_width, flags};
+  PrepArgs a{out, nullptr, nullptr, in, dark0, flat0, flat1, (int)nproj, (int)nz, (int)n,
+             in_pstride, in_zstride, out_zstride, out_pstride, out_poff, out_xoff, out_width,
+             flags};
   cudaStream_t s = (cudaStream_t)stream;
   StageTimer st("prep_rows", s);
   count_launch();
   switch (in_dtype) {
-    case TCB_U16: prep_rows_kernel<uint16_t><<<(unsigned)rows, 256, 0, s>>>(a); break;
-    case TCB_U8: prep_rows_kernel<uint8_t><<<(unsigned)rows, 256, 0, s>>>(a); break;
-    case TCB_F32: prep_rows_kernel<float><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_U16: prep_rows_kernel<uint16_t, false><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_U8: prep_rows_kernel<uint8_t, false><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_F32: prep_rows_kernel<float, false><<<(unsigned)rows, 256, 0, s>>>(a); break;
     default:
       set_error("tcb_prep_rows: unknown dtype %d", in_dtype);
+      return TCB_ERR_INVALID_ARGUMENT;
+  }
+  TCB_LAUNCH_CHECK();
+  return TCB_OK;
+}
+
+extern "C" int tcb_prep_rows_split16(void *hi, void *lo, const void *in, const float *dark0,
+                                     const float *flat0, const float *flat1, size_t nproj,
+                                     size_t nz, size_t n, size_t in_pstride,
+                                     size_t in_zstride, int in_dtype, size_t out_zstride,
+                                     size_t out_pstride, unsigned flags, void *stream) {
+  TCB_CHECK_ARG(hi && lo && in, "tcb_prep_rows_split16: null pointer");
+  TCB_CHECK_ARG(!(flags & TCB_PREP_DARKFLAT) || (dark0 && flat0),
+                "tcb_prep_rows_split16: darkflat needs dark0/flat0");
+  TCB_CHECK_ARG(!(flags & TCB_PREP_FLAT_LINEAR) || (flat1 && nproj >= 2),
+                "tcb_prep_rows_split16: flat_linear needs flat1 and nproj>=2");
+  TCB_CHECK_ARG(!(flags & TCB_PREP_EDGE_PAD),
+                "tcb_prep_rows_split16: edge padding is folded into the filter operator");
+  TCB_CHECK_ARG(out_pstride >= n, "tcb_prep_rows_split16: out_pstride < n");
+  TCB_CHECK_ARG(nproj < (1u << 31) && nz < (1u << 31) && n < (1u << 31),
+                "tcb_prep_rows_split16: size too large");
+  if (nproj == 0 || nz == 0 || n == 0) return TCB_OK;
+  size_t rows = nproj * nz;
+  TCB_CHECK_ARG(rows < (1ull << 31), "tcb_prep_rows_split16: too many rows in one call");
+  PrepArgs a{nullptr, (__half *)hi, (__half *)lo, in, dark0, flat0, flat1, (int)nproj,
+             (int)nz, (int)n, in_pstride, in_zstride, out_zstride, out_pstride, 0, 0, n,
+             flags};
+  cudaStream_t s = (cudaStream_t)stream;
+  StageTimer st("prep_rows", s);
+  count_launch();
+  switch (in_dtype) {
+    case TCB_U16: prep_rows_kernel<uint16_t, true><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_U8: prep_rows_kernel<uint8_t, true><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_F32: prep_rows_kernel<float, true><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    default:
+      set_error("tcb_prep_rows_split16: unknown dtype %d", in_dtype);
       return TCB_ERR_INVALID_ARGUMENT;
   }
   TCB_LAUNCH_CHECK();
@@ -311,8 +377,8 @@ extern "C" int tcb_prep_noalloc(float *out, const void *data, const void *dark,
   size_t plane = nz * n;
   cudaStream_t s = (cudaStream_t)stream;
   unsigned sgrid = ceil_div(plane, 256);
-  PrepArgs a{out, data, dark0, flat0, nullptr, (int)nproj, (int)nz, (int)n, nz * n, n,
-             out_zstride, out_pstride, out_poff, out_xoff, out_width,
+  PrepArgs a{out, nullptr, nullptr, data, dark0, flat0, nullptr, (int)nproj, (int)nz, (int)n,
+             nz * n, n, out_zstride, out_pstride, out_poff, out_xoff, out_width,
              flags | TCB_PREP_DARKFLAT};
   unsigned rows = (unsigned)(nproj * nz);
   switch (in_dtype) {
@@ -321,21 +387,21 @@ extern "C" int tcb_prep_noalloc(float *out, const void *data, const void *dark,
           dark0, flat0, nullptr, (const uint16_t *)dark, (const uint16_t *)flat, (int)ndark,
           (int)nflat, plane, bright_ratio, 0);
       TCB_LAUNCH_CHECK();
-      prep_rows_kernel<uint16_t><<<rows, 256, 0, s>>>(a);
+      prep_rows_kernel<uint16_t, false><<<rows, 256, 0, s>>>(a);
       break;
     case TCB_U8:
       darkflat_stats_kernel<uint8_t><<<sgrid, 256, 0, s>>>(
           dark0, flat0, nullptr, (const uint8_t *)dark, (const uint8_t *)flat, (int)ndark,
           (int)nflat, plane, bright_ratio, 0);
       TCB_LAUNCH_CHECK();
-      prep_rows_kernel<uint8_t><<<rows, 256, 0, s>>>(a);
+      prep_rows_kernel<uint8_t, false><<<rows, 256, 0, s>>>(a);
       break;
     default:
       darkflat_stats_kernel<float><<<sgrid, 256, 0, s>>>(
           dark0, flat0, nullptr, (const float *)dark, (const float *)flat, (int)ndark,
           (int)nflat, plane, bright_ratio, 0);
       TCB_LAUNCH_CHECK();
-      prep_rows_kernel<float><<<rows, 256, 0, s>>>(a);
+      prep_rows_kernel<float, false><<<rows, 256, 0, s>>>(a);
   }
   TCB_LAUNCH_CHECK();
   count_launch(2);

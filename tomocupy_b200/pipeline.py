@@ -15,6 +15,13 @@ executed as native kernels on one stream:
     ``tcb_fourierrec_backprojection_slices`` (gridding, 2D FFT, deapodization,
     unpacking into the output slices);
     linerec: crop + ``tcb_linerec_backprojection``.
+
+``precision="mixed"`` replaces steps 1-2 with ``tcb_prep_rows_split16`` (the
+same prep chain written as fp16 hi/lo planes, unpadded) and the tensor-core
+filter ``tcb_tcfilter_apply`` (edge pad + filter + centre shift + crop as one
+split-precision fp16 GEMM), whose epilogue writes the packed complex pairs
+of fourierrec directly (no pack pass) or the cropped rows of linerec/lprec.
+The filter does not modify its input planes.
 """
 from __future__ import annotations
 
@@ -24,16 +31,20 @@ import numpy as np
 import torch
 
 from . import _lib, cfunc_filter, cfunc_fourierrec, cfunc_linerec
-from .processing.proc_functions import in_dtype_code, prep_rows
+from .processing.proc_functions import in_dtype_code, prep_rows, prep_rows_split16
 from .reconstruction.backproj_functions import phase_weights, rfftfreq32
 from .reconstruction.fbp_filter import calc_filter
 
 
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
-                 algorithm="fourierrec", minus_log=True, device="cuda", stripe=None):
+                 algorithm="fourierrec", minus_log=True, device="cuda", stripe=None,
+                 precision="float32"):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
+        if precision not in ("float32", "mixed"):
+            raise NotImplementedError(f"SinoPipeline: precision {precision!r}")
+        self.precision = precision
         if algorithm == "fourierrec" and ncz % 2:
             raise ValueError("fourierrec needs an even number of rows per chunk")
         self.device = torch.device(device)
@@ -46,12 +57,24 @@ class SinoPipeline:
         self.ne = 4 * self.n
         self.pad = self.ne // 2 - self.n // 2
         self.theta = torch.as_tensor(np.asarray(theta, dtype=np.float32), device=self.device)
-        self.wfilter = torch.as_tensor(calc_filter(self.ne, fbp_filter), device=self.device)
+        self.wfilter_np = calc_filter(self.ne, fbp_filter)
+        self.wfilter = torch.as_tensor(self.wfilter_np, device=self.device)
         self.t = rfftfreq32(self.ne, self.device)
-        self.rows = torch.empty((self.ncz, self.nproj, self.ne), dtype=torch.float32,
-                                device=self.device)
-        self.filter = cfunc_filter.cfunc_filter(self.nproj, self.ncz, self.ne)
         self._w_cache: dict = {}
+        if precision == "mixed":
+            from .reconstruction.tcfilter import TCFilter
+            self.npl = -(-self.n // 8) * 8  # fp16 row pitch (16-byte TMA rows)
+            self.xhi = torch.empty((self.ncz, self.nproj, self.npl), dtype=torch.float16,
+                                   device=self.device)
+            self.xlo = torch.empty_like(self.xhi)
+            self.tcf = TCFilter(self.n, self.nproj, self.ncz, 1, self.device)
+            self.tcf.set_kernels(self.wfilter_np, self.ne, self.center, 0.0)
+            self.tcf_sht = None      # per-slice kernels for centre shifts (built on demand)
+            self._sht_key = None
+        else:
+            self.rows = torch.empty((self.ncz, self.nproj, self.ne), dtype=torch.float32,
+                                    device=self.device)
+            self.filter = cfunc_filter.cfunc_filter(self.nproj, self.ncz, self.ne)
         # optional Fourier-wavelet ring removal between dark/flat and -log
         # (ProcFunctions.proc_sino, proc_functions.py:140-160): stripe is
         # (sigma, wavelet, level)
@@ -107,17 +130,77 @@ class SinoPipeline:
                       out_poff=fw.poff, stream=stream)
             fw.apply_sino(self.sino, stream)
             src = self.sino[:nz, fw.poff:fw.poff + self.nproj].permute(1, 0, 2)
+            if self.precision == "mixed":
+                prep_rows_split16(self.xhi, self.xlo, src, darkflat=False,
+                                  minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
+                                  out_pstride=self.npl, stream=stream)
+                return
             prep_rows(self.rows, src, darkflat=False, minus_log=self.minus_log,
                       out_zstride=self.nproj * self.ne, out_pstride=self.ne, out_xoff=self.pad,
                       out_width=self.ne, edge_pad=True, stream=stream)
+            return
+        if self.precision == "mixed":
+            prep_rows_split16(self.xhi, self.xlo, data, d0, f0, darkflat=dark0 is not None,
+                              minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
+                              out_pstride=self.npl, stream=stream)
             return
         prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                   minus_log=self.minus_log, out_zstride=self.nproj * self.ne,
                   out_pstride=self.ne, out_xoff=self.pad, out_width=self.ne, edge_pad=True,
                   stream=stream)
 
+    def replicate_first_row(self):
+        """Copy slice 0 of the loaded rows to every slice (try-centre sweeps)."""
+        if self.precision == "mixed":
+            self.xhi[1:].copy_(self.xhi[:1].expand(self.ncz - 1, -1, -1))
+            self.xlo[1:].copy_(self.xlo[:1].expand(self.ncz - 1, -1, -1))
+        else:
+            self.rows[1:].copy_(self.rows[:1].expand(self.ncz - 1, -1, -1))
+
+    def save_rows(self):
+        """Snapshot of slice 0 needed to refill rows that filtering overwrote (or None)."""
+        return None if self.precision == "mixed" else self.rows[0].clone()
+
+    def restore_rows(self, saved):
+        if saved is not None:
+            self.rows.copy_(saved.expand(self.ncz, -1, -1))
+
+    def _tc_filter(self, sht):
+        """The tensor-core filter for these centre shifts (shared kernel when None)."""
+        if sht is None:
+            return self.tcf
+        from .reconstruction.tcfilter import TCFilter
+        sh = np.asarray(sht, dtype=np.float32).reshape(-1)
+        if sh.size == 1:
+            sh = np.repeat(sh, self.ncz)
+        if self.tcf_sht is None:
+            self.tcf_sht = TCFilter(self.n, self.nproj, self.ncz, self.ncz, self.device)
+        key = sh.tobytes()
+        if key != self._sht_key:
+            self.tcf_sht.set_kernels(self.wfilter_np, self.ne, self.center, sh.astype(np.float64))
+            self._sht_key = key
+        return self.tcf_sht
+
+    def _filter_and_backproject_mixed(self, out, sht, stream):
+        f = self._tc_filter(sht)
+        if self.algorithm == "fourierrec":
+            f.apply(self.xhi, self.xlo, torch.view_as_complex(self.g), pairs=True, stream=stream)
+            self.fr.backprojection_slices(out, self.g, stream)
+            return out
+        f.apply(self.xhi, self.xlo, self.crop, stream=stream)
+        if self.algorithm == "linerec":
+            s = torch.cuda.current_stream() if stream is None else stream
+            with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
+                out.zero_()
+            self.lr.backprojection(out, self.crop, self.theta, math.pi / 2, 0, stream)
+        else:
+            self.lp.fslv.backprojection(out, self.crop, stream)
+        return out
+
     def filter_and_backproject(self, out, sht=None, stream=None):
         """out [ncz, n, n] float32 (contiguous) from the loaded rows."""
+        if self.precision == "mixed":
+            return self._filter_and_backproject_mixed(out, sht, stream)
         self.filter.filter(self.rows, self.weights(sht), stream)
         if self.algorithm == "fourierrec":
             self.fr.pack(self.g, self.rows, self.ne, self.pad, stream)

@@ -67,6 +67,27 @@ def prep_rows(out, data, dark0=None, flat0=None, flat1=None, *, darkflat=True, m
     return out
 
 
+def prep_rows_split16(hi, lo, data, dark0=None, flat0=None, flat1=None, *, darkflat=True,
+                      minus_log=True, flat_linear=False, out_zstride, out_pstride,
+                      stream=None):
+    """tcb_prep_rows_split16: the prep_rows chain written as fp16 hi/lo planes."""
+    nproj, nz, n = data.shape
+    assert data.stride(2) == 1
+    assert hi.dtype == torch.float16 and lo.dtype == torch.float16
+    flags = 0
+    if darkflat:
+        flags |= _lib.PREP_DARKFLAT
+    if minus_log:
+        flags |= _lib.PREP_MINUS_LOG
+    if flat_linear:
+        flags |= _lib.PREP_FLAT_LINEAR
+    _lib.call("tcb_prep_rows_split16", _lib.ptr(hi), _lib.ptr(lo), _lib.ptr(data),
+              _lib.ptr(dark0), _lib.ptr(flat0), _lib.ptr(flat1), nproj, nz, n, data.stride(0),
+              data.stride(1), in_dtype_code(data), out_zstride, out_pstride, flags,
+              _lib.stream_ptr(stream))
+    return hi, lo
+
+
 class ProcFunctions:
     def __init__(self):
         if args.beam_hardening_method != "none":

@@ -28,8 +28,9 @@ def _supported():
             f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
     if args.file_type != "standard" or args.binning != 0:
         raise NotImplementedError("double_fov / binning are not part of tomocupy_b200")
-    if args.dtype != "float32":
-        raise NotImplementedError("the fused driver runs the float32 drop-in path")
+    if args.dtype not in ("float32", "mixed"):
+        raise NotImplementedError(
+            "the fused driver runs the float32 drop-in path or the 'mixed' tensor-core path")
 
 
 class GPURec:
@@ -46,7 +47,8 @@ class GPURec:
         self.pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                  params.center, args.fbp_filter, args.reconstruction_algorithm,
                                  minus_log=args.minus_log == "True", device=self.device,
-                                 stripe=stripe)
+                                 stripe=stripe,
+                                 precision="mixed" if args.dtype == "mixed" else "float32")
         self.stream1 = torch.cuda.Stream(self.device)
         self.stream2 = torch.cuda.Stream(self.device)
         self.stream3 = torch.cuda.Stream(self.device)
@@ -133,14 +135,14 @@ class GPURec:
             d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
             # one prep pass into slice 0 of the padded rows, replicated to all slices
             self.pipe.load_rows(row, d0, f0, 0)
-            self.pipe.rows[1:].copy_(self.pipe.rows[:1].expand(ncz - 1, -1, -1))
-            base = self.pipe.rows[0].clone()
+            self.pipe.replicate_first_row()
+            base = self.pipe.save_rows()
             for k in range(params.nschunk):
                 lk = int(params.lschunk[k])
                 sht = np.zeros(ncz, dtype=np.float32)
                 sht[:lk] = params.shift_array[k * ncz:k * ncz + lk]
                 if k > 0:
-                    self.pipe.rows.copy_(base.expand(ncz, -1, -1))
+                    self.pipe.restore_rows(base)
                 self.pipe.filter_and_backproject(out, sht)
                 for kk in range(lk):
                     self.cl_writer.write_data_try(out[kk], params.save_centers[k * ncz + kk],
