@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -514,6 +515,10 @@ struct tcb_fourierrec {
   float2 *grid = nullptr;
   float2 *g32 = nullptr;  // fp32 staging of g (FLOAT16 only)
   cufftHandle plan1d = 0, plan2d = 0;
+  // Pruned inverse 2D FFT: row transforms over all 2n rows, then column
+  // transforms over only the n columns [n/2, 3n/2) that deapodization reads.
+  cufftHandle plan_rows = 0, plan_cols = 0;
+  bool pruned = false;
   int ntiles = 0;
   size_t list_bytes = 0;
 };
@@ -526,6 +531,8 @@ namespace {
 void fr_release(tcb_fourierrec *h) {
   if (h->plan1d) cufftDestroy(h->plan1d);
   if (h->plan2d) cufftDestroy(h->plan2d);
+  if (h->plan_rows) cufftDestroy(h->plan_rows);
+  if (h->plan_cols) cufftDestroy(h->plan_cols);
   cudaFree(h->cs);
   cudaFree(h->rtab);
   cudaFree(h->etab);
@@ -536,7 +543,7 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->blist);
   cudaFree(h->grid);
   cudaFree(h->g32);
-  h->plan1d = h->plan2d = 0;
+  h->plan1d = h->plan2d = h->plan_rows = h->plan_cols = 0;
   h->cs = nullptr;
   h->rtab = h->etab = nullptr;
   h->tile_order = nullptr;
@@ -572,7 +579,12 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     gc = h->g32;
   }
   TCB_CUFFT(cufftSetStream(h->plan1d, s));
-  TCB_CUFFT(cufftSetStream(h->plan2d, s));
+  if (h->pruned) {
+    TCB_CUFFT(cufftSetStream(h->plan_rows, s));
+    TCB_CUFFT(cufftSetStream(h->plan_cols, s));
+  } else {
+    TCB_CUFFT(cufftSetStream(h->plan2d, s));
+  }
   {
     StageTimer st("fr_fft1d", s);
     TCB_CUFFT(cufftExecC2C(h->plan1d, (cufftComplex *)gc, (cufftComplex *)gc, CUFFT_FORWARD));
@@ -588,8 +600,19 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   }
   {
     StageTimer st("fr_fft2d", s);
-    TCB_CUFFT(cufftExecC2C(h->plan2d, (cufftComplex *)h->grid, (cufftComplex *)h->grid,
-                           CUFFT_INVERSE));
+    if (h->pruned) {
+      // separable: all rows along x, then the kept columns along y, per pair
+      TCB_CUFFT(cufftExecC2C(h->plan_rows, (cufftComplex *)h->grid, (cufftComplex *)h->grid,
+                             CUFFT_INVERSE));
+      const size_t plane = (size_t)geo.twon * geo.twon;
+      for (size_t z = 0; z < h->nz; z++) {
+        cufftComplex *c = (cufftComplex *)(h->grid + z * plane + h->n / 2);
+        TCB_CUFFT(cufftExecC2C(h->plan_cols, c, c, CUFFT_INVERSE));
+      }
+    } else {
+      TCB_CUFFT(cufftExecC2C(h->plan2d, (cufftComplex *)h->grid, (cufftComplex *)h->grid,
+                             CUFFT_INVERSE));
+    }
   }
   {
     StageTimer st("fr_deapod", s);
@@ -767,8 +790,22 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   cufftResult r = cufftPlanMany(&h->plan1d, 1, len1, nullptr, 1, 0, nullptr, 1, 0,
                                 CUFFT_C2C, (int)(nproj * nz));
   int len2[2] = {(int)(2 * n), (int)(2 * n)};
-  if (r == CUFFT_SUCCESS)
+  // The deapodization reads only rows and columns [n/2, 3n/2 + 1) of the
+  // inverse 2D transform, so the column pass runs on n of the 2n columns.
+  // TCB_FOURIERREC_FULL_FFT2D=1 selects one full 2D transform instead.
+  const char *full = getenv("TCB_FOURIERREC_FULL_FFT2D");
+  h->pruned = !(full && full[0] == '1');
+  if (r == CUFFT_SUCCESS && !h->pruned)
     r = cufftPlanMany(&h->plan2d, 2, len2, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, (int)nz);
+  if (r == CUFFT_SUCCESS && h->pruned) {
+    int lr[1] = {(int)(2 * n)};
+    r = cufftPlanMany(&h->plan_rows, 1, lr, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C,
+                      (int)(2 * n * nz));
+    int emb[1] = {(int)(2 * n)};
+    if (r == CUFFT_SUCCESS)
+      r = cufftPlanMany(&h->plan_cols, 1, lr, emb, (int)(2 * n), 1, emb, (int)(2 * n), 1,
+                        CUFFT_C2C, (int)n);
+  }
   if (r != CUFFT_SUCCESS) {
     set_error("tcb_fourierrec_create: cufftPlanMany failed: %d", (int)r);
     return fail(r == CUFFT_ALLOC_FAILED ? TCB_ERR_OUT_OF_MEMORY : TCB_ERR_CUFFT);

@@ -264,35 +264,32 @@ __global__ void __launch_bounds__(128, 1)
   __syncwarp();
   tc_fence_after();
 
-  // Epilogue: warp w owns accumulator rows (TMEM lanes) 32w .. 32w+31.
-  const int m = warp * 32 + lane;
-  const int p = p0 + m;
-  const bool row_ok = ok && p < g.nproj && z < g.nz;
+  // Epilogue: warp w owns accumulator rows (TMEM lanes) 32w .. 32w+31.  Each
+  // 32 x 32 block goes through shared memory (the pipeline buffers are idle
+  // now) so that one warp store covers 32 consecutive columns of one row.
+  float *tb = reinterpret_cast<float *>(smem) + warp * (32 * 33);
+  const bool wok = __all_sync(0xffffffffu, ok) && z < g.nz;
   for (int c0 = 0; c0 < BN; c0 += 32) {
     float v[32];
     tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-    const int j0 = nt * BN + c0;
-    if (!row_ok || j0 >= g.n) continue;
-    if (MODE == OUT_ROWS) {
-      float *dst = g.out + ((size_t)z * g.nproj + p) * g.ldo + j0;
-      if (j0 + 32 <= g.n && ((uintptr_t)dst & 15) == 0) {
 #pragma unroll
-        for (int i = 0; i < 32; i += 4)
-          *reinterpret_cast<float4 *>(dst + i) =
-              make_float4(v[i] * g.inv_scale, v[i + 1] * g.inv_scale, v[i + 2] * g.inv_scale,
-                          v[i + 3] * g.inv_scale);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 32; i++)
-          if (j0 + i < g.n) dst[i] = v[i] * g.inv_scale;
-      }
-    } else {
+    for (int i = 0; i < 32; i++) tb[i * 33 + lane] = v[i];
+    __syncwarp();
+    const int j = nt * BN + c0 + lane;
+    if (wok && nt * BN + c0 < g.n) {
       const int q = z % g.zh, comp = z / g.zh;
-      float *dst = g.out + ((((size_t)q * g.nproj + p) * g.n + j0) * 2 + comp);
-#pragma unroll
-      for (int i = 0; i < 32; i++)
-        if (j0 + i < g.n) dst[2 * i] = v[i] * g.inv_scale;
+#pragma unroll 4
+      for (int r = 0; r < 32; r++) {
+        const int p = p0 + warp * 32 + r;
+        if (p >= g.nproj || j >= g.n) continue;
+        const float val = tb[lane * 33 + r] * g.inv_scale;
+        if (MODE == OUT_ROWS)
+          g.out[((size_t)z * g.nproj + p) * g.ldo + j] = val;
+        else
+          g.out[(((size_t)q * g.nproj + p) * g.n + j) * 2 + comp] = val;
+      }
     }
+    __syncwarp();
   }
   if (!ok) atomicOr(g.err, 1);
   tc_fence_before();
