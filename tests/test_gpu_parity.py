@@ -119,6 +119,8 @@ FR_CASES = [
     (512, 360, 8, "uniform"),
     (200, 120, 3, "random"),   # 2n not a multiple of the tile: partial tiles
     (256, 401, 1, "random"),
+    (2048, 150, 2, "uniform"),  # 2n = 4096: the production FFT length
+    (4096, 64, 1, "random"),    # 2n = 8192: radix-16^3 x 2
 ]
 
 
@@ -139,6 +141,26 @@ def test_fourierrec_dropin_vs_reference(cuda, ref, n, nproj, nz, kind):
     L.ref_destroy(h)
     err = rel_l2(f_ours.cpu(), f_ref.cpu())
     assert err < FR_TOL, err
+
+
+@pytest.mark.parametrize("n,nproj,nz", [(128, 60, 2), (256, 90, 3), (512, 100, 2),
+                                        (1024, 64, 2), (2048, 40, 1), (4096, 24, 1)])
+def test_fourierrec_own_fft_matches_cufft(cuda, monkeypatch, n, nproj, nz):
+    """The own pruned inverse FFT (+ fused deapodization) against cuFFT's pruned path."""
+    from tomocupy_b200 import cfunc_fourierrec
+    theta = torch.as_tensor(_theta(nproj, "random"), device=cuda)
+    g = torch.randn((nz, nproj, n, 2), device=cuda)
+    out = {}
+    for mode in ("own", "cufft"):  # the own FFT is opt-in
+        monkeypatch.setenv("TCB_FOURIERREC_FFT", mode)
+        op = cfunc_fourierrec.cfunc_fourierrec(nproj, nz, n, theta)
+        f = torch.empty((nz, n, n, 2), device=cuda)
+        op.backprojection(f, g.clone(), None)
+        torch.cuda.synchronize()
+        out[mode] = f.cpu()
+        op.free()
+    err = rel_l2(out["own"], out["cufft"])
+    assert err < 1e-6, err
 
 
 def test_fourierrec_backprojection_slices_matches_dropin(cuda):

@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fft_pow2.cuh"
 
 #define TCB_PI_F 3.1415926535f
 
@@ -443,16 +444,13 @@ __global__ void __launch_bounds__(NTH, 2)
 // fftshift after the 2D FFT + divphi + circ (+ optional unpacking).
 //   grid: [nz, 2n, 2n]; f complex [nz, n, n] (unpack == 0) or
 //   f real [2nz, n, n] (unpack == 1).
-template <typename OutT>
-__global__ void deapod_kernel(const float2 *__restrict__ grid, OutT *__restrict__ f,
-                              Geom geo, int unpack) {
-  const int n = geo.n, twon = geo.twon;
-  int tx = blockIdx.x * blockDim.x + threadIdx.x;
-  int ty = blockIdx.y * blockDim.y + threadIdx.y;
-  int tz = blockIdx.z;
-  if (tx >= n || ty >= n) return;
+// Deapodization of one output pixel (tx, ty) from the inverse-FFT value at
+// grid index (tx + n/2, ty + 1 + n/2): the post-FFT fftshift sign, divphi
+// with its (1 - n%4) sign and 1/nproj, and the circle mask, in the
+// reference's operation order (kernels_fourierrec.cuh divphi + circ).
+__device__ __forceinline__ float2 deapod_value(float2 v, int tx, int ty, const Geom &geo) {
+  const int n = geo.n;
   int ix = tx + n / 2, iy = ty + 1 + n / 2;
-  float2 v = grid[(size_t)tz * twon * twon + (size_t)iy * twon + ix];
   int sx = 1 - 2 * ((ix + M + 1) % 2), sy = 1 - 2 * ((iy + M + 1) % 2);
   float sgn = (float)(sx * sy);
   v.x *= sgn;
@@ -468,6 +466,13 @@ __global__ void deapod_kernel(const float2 *__restrict__ grid, OutT *__restrict_
   float lam = (float)((4 * x * x + 4 * y * y) < 1);
   v.x *= lam;
   v.y *= lam;
+  return v;
+}
+
+template <typename OutT>
+__device__ __forceinline__ void store_out(OutT *f, float2 v, int tx, int ty, int tz, const Geom &geo,
+                                          int unpack) {
+  const int n = geo.n;
   size_t plane = (size_t)n * n;
   size_t o = (size_t)ty * n + tx;
   if (unpack) {
@@ -476,6 +481,107 @@ __global__ void deapod_kernel(const float2 *__restrict__ grid, OutT *__restrict_
   } else {
     f[2 * ((size_t)tz * plane + o)] = (OutT)v.x;
     f[2 * ((size_t)tz * plane + o) + 1] = (OutT)v.y;
+  }
+}
+
+// fftshift after the 2D FFT + divphi + circ (+ optional unpacking).
+//   grid: [nz, 2n, 2n]; f complex [nz, n, n] (unpack == 0) or
+//   f real [2nz, n, n] (unpack == 1).
+template <typename OutT>
+__global__ void deapod_kernel(const float2 *__restrict__ grid, OutT *__restrict__ f,
+                              Geom geo, int unpack) {
+  const int n = geo.n, twon = geo.twon;
+  int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  int ty = blockIdx.y * blockDim.y + threadIdx.y;
+  int tz = blockIdx.z;
+  if (tx >= n || ty >= n) return;
+  int ix = tx + n / 2, iy = ty + 1 + n / 2;
+  float2 v = grid[(size_t)tz * twon * twon + (size_t)iy * twon + ix];
+  store_out(f, deapod_value(v, tx, ty, geo), tx, ty, tz, geo, unpack);
+}
+
+// Own pruned inverse 2D FFT for power-of-two 2n (N = 2n).
+// Pass 1 (columns): CPC adjacent columns x of one pair's N x N grid per
+// block; the inverse FFT along y keeps rows y' in [n/2 + 1, 3n/2 + 1), the
+// only ones deapodization reads, in t1[pair][y' - n/2 - 1][x] (n x N).
+template <int N>
+__global__ void __launch_bounds__(1024) ifft_cols(const float2 *__restrict__ grid,
+                                                 float2 *__restrict__ t1,
+                                                 const float2 *__restrict__ tw, int cpc) {
+  extern __shared__ float2 fsm[];
+  constexpr int SSTR = fftk::Plan<N>::PADDED + 4;
+  const int c = threadIdx.x % cpc, tid = threadIdx.x / cpc;
+  const int ncb = N / cpc;
+  const int z = blockIdx.x / ncb, x = (blockIdx.x % ncb) * cpc + c;
+  const float2 *src = grid + (size_t)z * N * N + x;
+  float2 *dst = t1 + (size_t)z * (N / 2) * N + x;
+  auto in = [src](int e) { return __ldg(src + (size_t)e * N); };
+  auto out = [dst](int o, float2 v) {
+    const unsigned r = (unsigned)(o - (N / 4 + 1));
+    if (r < (unsigned)(N / 2)) dst[(size_t)r * N] = v;
+  };
+  fftk::ifft<N>(fsm + c * SSTR, tid, tw, in, out);
+}
+
+// Pass 2 (rows): one kept row ty of t1 per block; the inverse FFT along x
+// keeps x' in [n/2, 3n/2) and applies deapodization and the output layout.
+template <int N, typename OutT>
+__global__ void __launch_bounds__(N / 16) ifft_rows_deapod(const float2 *__restrict__ t1,
+                                                          OutT *__restrict__ f,
+                                                          const float2 *__restrict__ tw,
+                                                          Geom geo, int unpack) {
+  extern __shared__ float2 fsm[];
+  constexpr int n = N / 2;
+  const int ty = blockIdx.x % n, z = blockIdx.x / n;
+  const float2 *src = t1 + ((size_t)z * n + ty) * N;
+  auto in = [src](int e) { return __ldg(src + e); };
+  auto out = [&](int o, float2 v) {
+    const unsigned tx = (unsigned)(o - N / 4);
+    if (tx < (unsigned)n) store_out(f, deapod_value(v, (int)tx, ty, geo), (int)tx, ty, z, geo,
+                                    unpack);
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
+}
+
+inline int cols_per_block(int N) { return std::min(16384 / N, 16); }
+inline size_t cols_smem(int N) {
+  return (size_t)cols_per_block(N) * (N + N / 16 + 4) * sizeof(float2);
+}
+inline size_t rows_smem(int N) { return (size_t)(N + N / 16) * sizeof(float2); }
+
+template <int N>
+cudaError_t own_fft_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(ifft_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)cols_smem(N));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_rows_deapod<N, float>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(N));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_rows_deapod<N, __half>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(N));
+  return e;
+}
+
+template <int N>
+void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, void *f, bool half,
+                    const Geom &geo, int unpack, size_t nz, cudaStream_t s) {
+  const int cpc = cols_per_block(N);
+  {
+    StageTimer st("fr_ifft_cols", s);
+    ifft_cols<N><<<(unsigned)((N / cpc) * nz), cpc * (N / 16), cols_smem(N), s>>>(grid, t1, tw,
+                                                                                 cpc);
+    count_launch();
+  }
+  {
+    StageTimer st("fr_ifft_rows_deapod", s);
+    const unsigned blocks = (unsigned)((N / 2) * nz);
+    if (half)
+      ifft_rows_deapod<N, __half><<<blocks, N / 16, rows_smem(N), s>>>(t1, (__half *)f, tw, geo,
+                                                                       unpack);
+    else
+      ifft_rows_deapod<N, float><<<blocks, N / 16, rows_smem(N), s>>>(t1, (float *)f, tw, geo,
+                                                                      unpack);
+    count_launch();
   }
 }
 
@@ -519,6 +625,11 @@ struct tcb_fourierrec {
   // transforms over only the n columns [n/2, 3n/2) that deapodization reads.
   cufftHandle plan_rows = 0, plan_cols = 0;
   bool pruned = false;
+  // Own pruned FFT (columns pass, then rows pass fused with deapodization)
+  // when 2n is a power of two in [256, 8192]: own_n = 2n, else 0.
+  int own_n = 0;
+  float2 *t1 = nullptr;  // [nz][n][2n] column-pass output
+  float2 *tw = nullptr;  // [2n] exp(2 pi i m / 2n)
   int ntiles = 0;
   size_t list_bytes = 0;
 };
@@ -543,6 +654,9 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->blist);
   cudaFree(h->grid);
   cudaFree(h->g32);
+  cudaFree(h->t1);
+  cudaFree(h->tw);
+  h->t1 = h->tw = nullptr;
   h->plan1d = h->plan2d = h->plan_rows = h->plan_cols = 0;
   h->cs = nullptr;
   h->rtab = h->etab = nullptr;
@@ -579,7 +693,8 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     gc = h->g32;
   }
   TCB_CUFFT(cufftSetStream(h->plan1d, s));
-  if (h->pruned) {
+  if (h->own_n) {
+  } else if (h->pruned) {
     TCB_CUFFT(cufftSetStream(h->plan_rows, s));
     TCB_CUFFT(cufftSetStream(h->plan_cols, s));
   } else {
@@ -597,6 +712,19 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     else if (h->nz >= 4) rc = launch_grid<4>(h, gc, s);
     else rc = launch_grid<2>(h, gc, s);
     if (rc != TCB_OK) return rc;
+  }
+  if (h->own_n) {
+    const bool half = h->precision == TCB_FLOAT16;
+    switch (h->own_n) {
+      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+    }
+    TCB_LAUNCH_CHECK();
+    return TCB_OK;
   }
   {
     StageTimer st("fr_fft2d", s);
@@ -793,11 +921,48 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   // The deapodization reads only rows and columns [n/2, 3n/2 + 1) of the
   // inverse 2D transform, so the column pass runs on n of the 2n columns.
   // TCB_FOURIERREC_FULL_FFT2D=1 selects one full 2D transform instead.
+  // TCB_FOURIERREC_FFT=own selects the library's own pruned FFT with fused
+  // deapodization (power-of-two 2n in [256, 8192]).  It is exact to cuFFT
+  // within fp32 round-off but, at 2n = 4096 on B200, slower than cuFFT's
+  // pruned pair of passes (139 vs 128 ms per 2048-slice volume), so cuFFT
+  // stays the default.
   const char *full = getenv("TCB_FOURIERREC_FULL_FFT2D");
+  const char *fsel = getenv("TCB_FOURIERREC_FFT");
   h->pruned = !(full && full[0] == '1');
+  const size_t N2 = 2 * n;
+  if (h->pruned && (fsel && strcmp(fsel, "own") == 0) && N2 >= 256 && N2 <= 8192 &&
+      (N2 & (N2 - 1)) == 0) {
+    std::vector<float2> twh(N2);
+    for (size_t m = 0; m < N2; m++) {
+      double a = 2.0 * M_PI * (double)m / (double)N2;
+      twh[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    if (cudaMalloc(&h->tw, N2 * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&h->t1, nz * n * N2 * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("tcb_fourierrec_create: out of device memory for the FFT buffers");
+      return fail(TCB_ERR_OUT_OF_MEMORY);
+    }
+    e = cudaMemcpy(h->tw, twh.data(), N2 * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      switch (N2) {
+        case 256: e = own_fft_attrs<256>(); break;
+        case 512: e = own_fft_attrs<512>(); break;
+        case 1024: e = own_fft_attrs<1024>(); break;
+        case 2048: e = own_fft_attrs<2048>(); break;
+        case 4096: e = own_fft_attrs<4096>(); break;
+        default: e = own_fft_attrs<8192>(); break;
+      }
+    }
+    if (e != cudaSuccess) {
+      set_error("tcb_fourierrec_create: FFT setup failed: %s", cudaGetErrorString(e));
+      return fail(TCB_ERR_CUDA);
+    }
+    h->own_n = (int)N2;
+  }
   if (r == CUFFT_SUCCESS && !h->pruned)
     r = cufftPlanMany(&h->plan2d, 2, len2, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, (int)nz);
-  if (r == CUFFT_SUCCESS && h->pruned) {
+  if (r == CUFFT_SUCCESS && h->pruned && !h->own_n) {
     int lr[1] = {(int)(2 * n)};
     r = cufftPlanMany(&h->plan_rows, 1, lr, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C,
                       (int)(2 * n * nz));
