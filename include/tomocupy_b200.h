@@ -219,6 +219,10 @@ int tcb_fourierrec_backprojection_slices(tcb_fourierrec *h, void *f, void *g,
  * backproj_functions.py:107). */
 int tcb_fourierrec_pack(tcb_fourierrec *h, void *g, const void *src,
                         size_t row_stride, size_t xoff, void *stream);
+/* Tuning knob (no reference counterpart): slice pairs accumulated per
+ * gridding block, 2/4/8/16, or 0 for the largest that the handle's nz allows.
+ * Results do not depend on it beyond fp32 summation order. */
+int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs);
 int tcb_fourierrec_destroy(tcb_fourierrec *h);
 
 /* ------------------------------------------------------------------------

@@ -73,6 +73,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_fourierrec_backprojection": [vp, vp, vp, vp],
     "tcb_fourierrec_backprojection_slices": [vp, vp, vp, vp],
     "tcb_fourierrec_pack": [vp, vp, vp, sz, sz, vp],
+    "tcb_fourierrec_set_pairs_per_block": [vp, i32],
     "tcb_fourierrec_destroy": [vp],
     "tcb_linerec_create": [C.POINTER(vp), sz, sz, sz, sz, sz, i32],
     "tcb_linerec_backprojection": [vp, vp, vp, vp, f32, i32, vp],

@@ -41,6 +41,11 @@ class cfunc_fourierrec:
         _lib.call("tcb_fourierrec_pack", self._h, _lib.ptr(g), _lib.ptr(src), int(row_stride),
                   int(xoff), _lib.stream_ptr(stream))
 
+    def set_pairs_per_block(self, pairs: int) -> None:
+        """Tuning knob (not in the reference): slice pairs per gridding block, 0 = auto."""
+        self._check()
+        _lib.call("tcb_fourierrec_set_pairs_per_block", self._h, int(pairs))
+
     def _check(self):
         if self._h is None:
             raise _lib.TcbError(6, type(self).__name__, "object was freed")

@@ -628,6 +628,7 @@ struct tcb_fourierrec {
   // Own pruned FFT (columns pass, then rows pass fused with deapodization)
   // when 2n is a power of two in [256, 8192]: own_n = 2n, else 0.
   int own_n = 0;
+  int zblock = 0;  // pairs per gridding block (2/4/8/16; 0 = largest that fits nz)
   float2 *t1 = nullptr;  // [nz][n][2n] column-pass output
   float2 *tw = nullptr;  // [2n] exp(2 pi i m / 2n)
   int ntiles = 0;
@@ -707,9 +708,10 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   {
     StageTimer st("fr_gather", s);
     int rc;
-    if (h->nz >= 16) rc = launch_grid<16>(h, gc, s);
-    else if (h->nz >= 8) rc = launch_grid<8>(h, gc, s);
-    else if (h->nz >= 4) rc = launch_grid<4>(h, gc, s);
+    const size_t zb = h->zblock ? (size_t)h->zblock : 16;
+    if (h->nz >= 16 && zb >= 16) rc = launch_grid<16>(h, gc, s);
+    else if (h->nz >= 8 && zb >= 8) rc = launch_grid<8>(h, gc, s);
+    else if (h->nz >= 4 && zb >= 4) rc = launch_grid<4>(h, gc, s);
     else rc = launch_grid<2>(h, gc, s);
     if (rc != TCB_OK) return rc;
   }
@@ -1003,6 +1005,14 @@ extern "C" int tcb_fourierrec_pack(tcb_fourierrec *h, void *g, const void *src,
                                          (int)h->nproj, (int)h->n, row_stride, xoff);
   TCB_LAUNCH_CHECK();
   count_launch();
+  return TCB_OK;
+}
+
+extern "C" int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs) {
+  TCB_CHECK_ARG(h, "tcb_fourierrec_set_pairs_per_block: null handle");
+  TCB_CHECK_ARG(pairs == 0 || pairs == 2 || pairs == 4 || pairs == 8 || pairs == 16,
+                "tcb_fourierrec_set_pairs_per_block: pairs must be 0, 2, 4, 8 or 16");
+  h->zblock = pairs;
   return TCB_OK;
 }
 

@@ -41,17 +41,29 @@ class GPURec:
         self.device = torch.device(device)
         self.cl_reader = cl_reader
         self.cl_writer = cl_writer
-        stripe = None
-        if args.remove_stripe_method == "fw":
-            stripe = (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
-        self.pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
-                                 params.center, args.fbp_filter, args.reconstruction_algorithm,
-                                 minus_log=args.minus_log == "True", device=self.device,
-                                 stripe=stripe,
-                                 precision="mixed" if args.dtype == "mixed" else "float32")
+        self._pipe = None
+        self.sweep = None
         self.stream1 = torch.cuda.Stream(self.device)
         self.stream2 = torch.cuda.Stream(self.device)
         self.stream3 = torch.cuda.Stream(self.device)
+
+    @property
+    def precision(self) -> str:
+        return "mixed" if args.dtype == "mixed" else "float32"
+
+    @property
+    def pipe(self) -> SinoPipeline:
+        """The chunk pipeline (built on first use; try-centre sweeps do not need it)."""
+        if self._pipe is None:
+            stripe = None
+            if args.remove_stripe_method == "fw":
+                stripe = (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
+            self._pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
+                                      params.center, args.fbp_filter,
+                                      args.reconstruction_algorithm,
+                                      minus_log=args.minus_log == "True", device=self.device,
+                                      stripe=stripe, precision=self.precision)
+        return self._pipe
 
     # ------------------------------------------------------------------ helpers
     def _stats(self, dark, flat, stream):
@@ -124,29 +136,32 @@ class GPURec:
 
     # ------------------------------------------------------------------ try
     def recon_try(self):
-        """Reconstruct slice(s) ``params.id_slices`` for every centre in ``params.shift_array``."""
+        """Reconstruct slice(s) ``params.id_slices`` for every centre in ``params.shift_array``.
+
+        The sweep over all centres is one CUDA graph (TryCenterSweep), recorded
+        once and replayed for each requested slice.
+        """
+        from .trycenter import TryCenterSweep
+        if args.reconstruction_algorithm != "fourierrec" or args.remove_stripe_method != "none":
+            raise NotImplementedError("try-centre sweeps run fourierrec without ring removal")
         data, dark, flat = self.cl_reader.frames()
-        ncz, n, nproj = params.ncz, params.n, params.nproj
         dev = self.device
-        out = torch.empty((ncz, n, n), dtype=torch.float32, device=dev)
+        if self.sweep is None:
+            self.sweep = TryCenterSweep(params.n, params.nproj, params.theta, params.center,
+                                        params.shift_array, args.fbp_filter, self.precision,
+                                        params.ncz, device=dev,
+                                        minus_log=args.minus_log == "True")
+        sw = self.sweep
         for id_slice in params.id_slices:
             z = int(id_slice)
             row = data[:, z:z + 1].to(dev)
             d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
-            # one prep pass into slice 0 of the padded rows, replicated to all slices
-            self.pipe.load_rows(row, d0, f0, 0)
-            self.pipe.replicate_first_row()
-            base = self.pipe.save_rows()
-            for k in range(params.nschunk):
-                lk = int(params.lschunk[k])
-                sht = np.zeros(ncz, dtype=np.float32)
-                sht[:lk] = params.shift_array[k * ncz:k * ncz + lk]
-                if k > 0:
-                    self.pipe.restore_rows(base)
-                self.pipe.filter_and_backproject(out, sht)
-                for kk in range(lk):
-                    self.cl_writer.write_data_try(out[kk], params.save_centers[k * ncz + kk],
-                                                  id_slice)
+            sw.load(row, d0, f0)
+            if sw.graph is None:
+                sw.capture()
+            out = sw.run()
+            for k in range(sw.S):
+                self.cl_writer.write_data_try(out[k], params.save_centers[k], id_slice)
         torch.cuda.synchronize(dev)
 
     # ------------------------------------------------------------------ device
