@@ -256,6 +256,57 @@ def _roofline(stages, a, peaks, peaks_kind, kernel=None):
             if peaks_kind == "measured" else "fallback 6.65 TB/s"}
 
 
+def run_try(a, dev):
+    """Try-centre sweep: 1 slice x a.try_n cols x a.try_nproj angles x a.try_centers centres.
+
+    Centres 2096 - 0.375 k (k < 256) around rotation axis 2048 for n = 4096;
+    fourierrec, Parzen filter.  Each precision is autotuned (chunk size x
+    gridding depth), captured as one CUDA graph and timed by graph replays.
+    """
+    import torch
+    from tomocupy_b200 import synthetic
+    from tomocupy_b200.processing.proc_functions import darkflat_stats
+    from tomocupy_b200.trycenter import TryCenterSweep, autotune, per_center_errors
+    n, P, S = a.try_n, a.try_nproj, a.try_centers
+    data, dark, flat, theta, _ = synthetic.make_dataset(P, 1, n, seed=a.seed, device=dev)
+    d0, f0, _ = darkflat_stats(dark, flat)
+    center = n / 2
+    shifts = (center + 48.0) - 0.375 * np.arange(S) - center  # centres 2096 - 0.375 k at n=4096
+    shifts = -shifts  # the filter places the axis at center - sht
+    res = {"workload": f"1 slice x {n} cols x {P} angles, {S} centres "
+                       f"[{center + 48.0 - 0.375 * (S - 1):.3f}, {center + 48.0:.3f}] step 0.375",
+           "unit": "GUPS (n^2 * nproj * centres / t)"}
+    outs = {}
+    for prec in ("float32", "mixed"):
+        tune = autotune(n, P, theta, center, shifts, data, d0, f0, fbp_filter="parzen",
+                        precision=prec, candidates=[(16, 8), (32, 8), (32, 16)], reps=1)
+        sw = TryCenterSweep(n, P, theta, center, shifts, "parzen", prec, tune["ncz"],
+                            tune["pairs_per_block"], dev)
+        sw.load(data, d0, f0)
+        sw.capture()
+        sw.time_ms(1)
+        ms = sw.time_ms(3)
+        outs[prec] = sw.run().clone()
+        res[prec] = {"ms_per_sweep": round(ms, 3),
+                     "value": round(float(n) ** 2 * P * S / (ms / 1e3) / 1e9, 2),
+                     "graph_launches_per_sweep": 1, "ncz": tune["ncz"],
+                     "pairs_per_block": tune["pairs_per_block"], "autotune": tune["table"]}
+        sw.free()
+        del sw
+        torch.cuda.empty_cache()
+    rel, mx = per_center_errors(outs["mixed"].cpu(), outs["float32"].cpu())
+    res["mixed_vs_fp32_per_center"] = {"rel_l2_max": float(rel.max()),
+                                       "rel_l2_median": float(np.median(rel)),
+                                       "max_abs_max": float(mx.max())}
+    res["mixed_speedup_vs_fp32"] = round(res["float32"]["ms_per_sweep"] /
+                                         res["mixed"]["ms_per_sweep"], 3)
+    res["fp64_oracle"] = ("per-centre rel-L2 vs FP64 in "
+                          "tests/test_gpu_trycenter.py::test_mixed_sweep_vs_fp64_oracle_per_center")
+    del outs
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_ours(a, ws, rank, local):
     import torch
     from tomocupy_b200.global_vars import params
@@ -309,6 +360,12 @@ def run_ours(a, ws, rank, local):
     if not a.no_e2e:
         e2e = run_e2e(a, data, dark, flat, theta, dev, ws, rank)
 
+    trycenter = None
+    if not a.no_try:
+        del out
+        torch.cuda.empty_cache()
+        trycenter = run_try(a, dev)
+
     base = None
     if rank == 0 and ws == 1 and not a.no_cpu:
         dcpu, dkc, flc = data.cpu().numpy(), dark.cpu().numpy(), flat.cpu().numpy()
@@ -335,6 +392,7 @@ def run_ours(a, ws, rank, local):
             "clocks": clocks, "gpu_launches": launches,
             "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in stages.items()},
             other if other == "mixed" else "fp32": side,
+            "try_center": trycenter,
         }
         print(json.dumps(line), flush=True)
 
@@ -475,6 +533,10 @@ def main():
     ap.add_argument("--precision", choices=["float32", "mixed"], default="float32",
                     help="path reported as value (the other one is timed beside it)")
     ap.add_argument("--no-mixed", action="store_true", help="time only --precision")
+    ap.add_argument("--no-try", action="store_true", help="skip the try-centre sweep")
+    ap.add_argument("--try-n", type=int, default=4096)
+    ap.add_argument("--try-nproj", type=int, default=3000)
+    ap.add_argument("--try-centers", type=int, default=256)
     a = ap.parse_args()
     if a.warmup < 3:
         log("note: warmup < 3 requested; using 3")
