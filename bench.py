@@ -307,6 +307,75 @@ def run_try(a, dev):
     return res
 
 
+def run_serving(a, dev):
+    """Serving leg: a seeded Poisson stream of uneven reconstructions.
+
+    Arrivals at a.serve_rate req/s; width from {512, 1024, 2048, 4096},
+    angles from {180, 720, 1500, 3000}, slices U{1..64}, uint16 frames,
+    fp32 : mixed = 1 : 1.  Frames come from pinned host stacks (one per
+    width x angles, 64 slices; a request takes a slab), results go to pinned
+    host buffers.  Geometries are made resident before the stream.
+    """
+    import torch
+    from tomocupy_b200 import synthetic
+    from tomocupy_b200.serving import Request, Server, latency_summary, poisson_stream
+    specs = poisson_stream(rate=a.serve_rate, count=a.serve_requests, seed=a.seed)
+    pool, outs = {}, {}
+    for _, n, P, _, _ in specs:
+        if (n, P) not in pool:
+            d, dk, fl, th, _ = synthetic.make_dataset(P, 64, n, seed=a.seed, device=dev)
+            pool[(n, P)] = (d.cpu().pin_memory(), dk.cpu().pin_memory(), fl.cpu().pin_memory(),
+                            th)
+            del d, dk, fl
+        if n not in outs:
+            outs[n] = torch.empty((64, n, n), dtype=torch.float32, pin_memory=True)
+
+    def make(precision=None):
+        reqs = []
+        for k, (t, n, P, nz, prec) in enumerate(specs):
+            d, dk, fl, th = pool[(n, P)]
+            reqs.append(Request(k, d[:, :nz], dk[:, :nz], fl[:, :nz], th, n / 2,
+                                precision or prec, "parzen", arrival=t, out=outs[n][:nz]))
+        return reqs
+
+    res = {"workload": f"{len(specs)} requests, Poisson {a.serve_rate}/s (seed {a.seed}), "
+                       "n in {512,1024,2048,4096}, nproj in {180,720,1500,3000}, nz U{1..64}, "
+                       "fp32:mixed 1:1, uint16 pinned host frames -> pinned host volumes",
+           "hbm_budget_gb": a.serve_budget_gb}
+    srv = Server(dev, hbm_budget=a.serve_budget_gb * 1e9, ncz=a.serve_ncz)
+    srv.warm(make())
+    srv.warm(make("float32"))
+    # single-request latency: each request alone on the warm server
+    alone = make()
+    for r in alone:
+        r.arrival = 0.0
+        srv.serve([r], realtime=False)
+    single = np.array([r.latency for r in alone]) * 1e3
+    res["single_request"] = {"p50_ms": float(np.percentile(single, 50)),
+                             "p99_ms": float(np.percentile(single, 99))}
+    mix = make()
+    srv.serve(mix, realtime=True)
+    res["continuous_batching"] = latency_summary(mix)
+    res["continuous_batching"]["peak_admitted"] = srv.peak_active
+    res["continuous_batching"]["peak_resident_gb"] = round(srv.peak_bytes / 1e9, 2)
+    ratio = np.array([m.latency / s.latency for m, s in zip(mix, alone)])
+    res["latency_in_mix_over_alone"] = {"p50": float(np.percentile(ratio, 50)),
+                                        "p99": float(np.percentile(ratio, 99))}
+    res["p99_over_single_p99"] = round(res["continuous_batching"]["p99_ms"] /
+                                       res["single_request"]["p99_ms"], 3)
+    base = Server(dev, hbm_budget=a.serve_budget_gb * 1e9, ncz=a.serve_ncz, max_active=1)
+    base.geoms = srv.geoms  # same resident geometries
+    base.geom_bytes = srv.geom_bytes
+    seq = make("float32")
+    base.serve(seq, realtime=True)
+    res["one_at_a_time_fp32"] = latency_summary(seq)
+    res["GUPS_vs_one_at_a_time_fp32"] = round(res["continuous_batching"]["GUPS"] /
+                                              res["one_at_a_time_fp32"]["GUPS"], 3)
+    del srv, base, pool, outs
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_ours(a, ws, rank, local):
     import torch
     from tomocupy_b200.global_vars import params
@@ -360,16 +429,21 @@ def run_ours(a, ws, rank, local):
     if not a.no_e2e:
         e2e = run_e2e(a, data, dark, flat, theta, dev, ws, rank)
 
-    trycenter = None
-    if not a.no_try:
-        del out
-        torch.cuda.empty_cache()
-        trycenter = run_try(a, dev)
-
     base = None
     if rank == 0 and ws == 1 and not a.no_cpu:
         dcpu, dkc, flc = data.cpu().numpy(), dark.cpu().numpy(), flat.cpu().numpy()
         base = cpu_baseline(a, dcpu, dkc, flc, theta)
+        del dcpu, dkc, flc
+
+    # the remaining legs need the device memory of the volume workload
+    del out, data, dark, flat, dark0, flat0
+    torch.cuda.empty_cache()
+    trycenter = None
+    if not a.no_try and ws == 1:
+        trycenter = run_try(a, dev)
+    serving = None
+    if not a.no_serve and ws == 1:
+        serving = run_serving(a, dev)
 
     if rank == 0:
         tag = "fp32" if primary == "float32" else "mixed-precision"
@@ -393,6 +467,7 @@ def run_ours(a, ws, rank, local):
             "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in stages.items()},
             other if other == "mixed" else "fp32": side,
             "try_center": trycenter,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
 
@@ -534,6 +609,11 @@ def main():
                     help="path reported as value (the other one is timed beside it)")
     ap.add_argument("--no-mixed", action="store_true", help="time only --precision")
     ap.add_argument("--no-try", action="store_true", help="skip the try-centre sweep")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving stream")
+    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-ncz", type=int, default=16)
     ap.add_argument("--try-n", type=int, default=4096)
     ap.add_argument("--try-nproj", type=int, default=3000)
     ap.add_argument("--try-centers", type=int, default=256)

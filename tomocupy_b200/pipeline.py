@@ -149,6 +149,24 @@ class SinoPipeline:
                   out_pstride=self.ne, out_xoff=self.pad, out_width=self.ne, edge_pad=True,
                   stream=stream)
 
+    def clear_rows(self, lz: int, stream=None) -> None:
+        """Zero the filter input rows of slices [lz, ncz) (a partial chunk).
+
+        fourierrec pairs slice k with slice k + ncz/2, so leftover rows of an
+        earlier chunk would leak into a partial chunk through the packing's
+        real/imaginary crosstalk; zero rows make every chunk depend on its own
+        slices only.
+        """
+        if lz >= self.ncz:
+            return
+        s = torch.cuda.current_stream() if stream is None else stream
+        with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
+            if self.precision == "mixed":
+                self.xhi[lz:].zero_()
+                self.xlo[lz:].zero_()
+            else:
+                self.rows[lz:].zero_()
+
     def replicate_first_row(self):
         """Copy slice 0 of the loaded rows to every slice (try-centre sweeps)."""
         if self.precision == "mixed":
