@@ -135,7 +135,9 @@ def stage_bytes(stage, n, nproj, ncz):
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch from
 # the committed ncu captures, keyed by (stage, n, nproj, rows per chunk);
 # see profiles/fr_gather_grid_blocks_2048x1500_16pairs.md
-NCU_TRAFFIC = {("fr_gather", 2048, 1500, 32): 533.82e6 + 2104.92e6}
+NCU_TRAFFIC = {("fr_gather", 2048, 1500, 32): 533.82e6 + 2104.92e6,
+               # profiles/tc_filter_tcf_gemm_2048x1500_32slices.md
+               ("tc_filter", 2048, 1500, 32): 411.44e6 + 359.14e6}
 
 
 def setup_dist():
