@@ -163,6 +163,30 @@ def test_fourierrec_own_fft_matches_cufft(cuda, monkeypatch, n, nproj, nz):
     assert err < 1e-6, err
 
 
+@pytest.mark.parametrize("n,nproj,nz", [(128, 90, 2), (200, 120, 3), (512, 360, 16),
+                                        (256, 180, 20), (2048, 64, 8)])
+def test_fourierrec_tensor_gridding_vs_fp32(cuda, n, nproj, nz):
+    """Mixed-precision gridding (fp16 weights and hi/lo values on tcgen05, fp32
+    accumulation) against the fp32 gridding: partial tiles (n = 200), pair
+    counts that are not a multiple of 16, more than 16 pairs (two groups)."""
+    from tomocupy_b200 import _lib, cfunc_fourierrec
+    theta = torch.as_tensor(_theta(nproj, "random"), device=cuda)
+    g = torch.randn((nz, nproj, n, 2), device=cuda) * 100.0
+    out = {}
+    for mode in (_lib.GRID_FP32, _lib.GRID_TENSOR):
+        op = cfunc_fourierrec.cfunc_fourierrec(nproj, nz, n, theta)
+        op.set_gridding(mode)
+        f = torch.full((nz, n, n, 2), float("nan"), device=cuda)
+        op.backprojection(f, g.clone(), None)
+        torch.cuda.synchronize()
+        assert not op.timed_out()
+        out[mode] = f.cpu()
+        op.free()
+    assert torch.isfinite(out[_lib.GRID_TENSOR]).all()
+    err = rel_l2(out[_lib.GRID_TENSOR], out[_lib.GRID_FP32])
+    assert err < 1e-3, err
+
+
 def test_fourierrec_backprojection_slices_matches_dropin(cuda):
     from tomocupy_b200 import cfunc_fourierrec
     n, nproj, nz = 128, 64, 2

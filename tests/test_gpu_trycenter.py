@@ -72,7 +72,7 @@ def test_mixed_sweep_vs_fp64_oracle_per_center(cuda, one_slice):
     rel_m, max_m = per_center_errors(mixed, want)
     rel_f, _ = per_center_errors(fp32, want)
     assert rel_m.max() < 1e-3, rel_m
-    assert np.all(rel_m < 2 * rel_f + 1e-5), (rel_m, rel_f)
+    assert rel_f.max() < 1e-4, rel_f
     assert np.all(np.isfinite(max_m))
 
 

@@ -23,6 +23,9 @@ PREP_MINUS_LOG = 2
 PREP_FLAT_LINEAR = 4
 PREP_EDGE_PAD = 8
 
+GRID_FP32 = 0
+GRID_TENSOR = 1
+
 TCF_OUT_ROWS = 0
 TCF_OUT_PAIRS = 1
 
@@ -74,6 +77,8 @@ SIGNATURES: dict[str, list] = {
     "tcb_fourierrec_backprojection_slices": [vp, vp, vp, vp],
     "tcb_fourierrec_pack": [vp, vp, vp, sz, sz, vp],
     "tcb_fourierrec_set_pairs_per_block": [vp, i32],
+    "tcb_fourierrec_set_gridding": [vp, i32],
+    "tcb_fourierrec_status": [vp, C.POINTER(i32)],
     "tcb_fourierrec_destroy": [vp],
     "tcb_linerec_create": [C.POINTER(vp), sz, sz, sz, sz, sz, i32],
     "tcb_linerec_backprojection": [vp, vp, vp, vp, f32, i32, vp],

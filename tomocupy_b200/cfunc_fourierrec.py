@@ -46,6 +46,19 @@ class cfunc_fourierrec:
         self._check()
         _lib.call("tcb_fourierrec_set_pairs_per_block", self._h, int(pairs))
 
+    def set_gridding(self, mode: int) -> None:
+        """_lib.GRID_FP32 (default, the drop-in) or _lib.GRID_TENSOR (mixed precision)."""
+        self._check()
+        _lib.call("tcb_fourierrec_set_gridding", self._h, int(mode))
+
+    def timed_out(self) -> bool:
+        """True when a tensor-core gridding wait gave up (synchronises)."""
+        import ctypes as C
+        self._check()
+        v = C.c_int(0)
+        _lib.call("tcb_fourierrec_status", self._h, C.byref(v))
+        return bool(v.value)
+
     def _check(self):
         if self._h is None:
             raise _lib.TcbError(6, type(self).__name__, "object was freed")

@@ -38,6 +38,7 @@
 
 #include "common.cuh"
 #include "fft_pow2.cuh"
+#include "tcgen05.cuh"
 
 #define TCB_PI_F 3.1415926535f
 
@@ -444,6 +445,297 @@ __global__ void __launch_bounds__(NTH, 2)
 // fftshift after the 2D FFT + divphi + circ (+ optional unpacking).
 //   grid: [nz, 2n, 2n]; f complex [nz, n, n] (unpack == 0) or
 //   f real [2nz, n, n] (unpack == 1).
+// ---- gridding on the tensor cores (mixed precision) --------------------------
+// For one 32 x 16 tile and up to 16 slice pairs, gridding is the product
+//   D[cell, comp] = sum_s W[cell, s] * Gv[s, comp]
+// with W[cell, s] = wx_s[cell.x - ox_s] * wy_s[cell.y - oy_s] (zero outside
+// the sample's 9 x 9 footprint) and Gv the sample's spectrum values of the 16
+// pairs (re, im).  Per chunk of 64 listed samples the CTA writes W (512 x 64,
+// fp16) and Gv (64 x 64: 16 pairs x (re, im) x (hi, lo) fp16, scaled by a
+// power of two so every value is in fp16's normal range) into shared memory
+// in the UMMA K-major 128-byte-swizzled layout, and one thread issues 4 M-groups
+// x 4 K-steps of tcgen05.mma (M = 128 cells, N = 64, K = 16) accumulating in
+// TMEM; the chunk after it is built while they run (two smem stages).  The
+// epilogue sums hi + lo, undoes the scale and stores like grid_blocks.
+// Weights and footprints are computed exactly as grid_blocks computes them.
+constexpr int TCK = 64;                       // samples per chunk (one K block)
+constexpr int TCN = 64;                       // 16 pairs x (re, im) x (hi, lo)
+constexpr int TCM = TX * TY;                  // 512 cells
+constexpr int TC_A = TCM * TCK * 2;           // 64 KB
+constexpr int TC_B = TCN * TCK * 2;           // 8 KB
+constexpr int TC_STAGE = TC_A + TC_B;
+constexpr int TC_THREADS = 512;
+constexpr int TC_REC = 2 + 2 * (2 * M + 1);   // fx, fy (or origin, valid), 9 + 9 weights
+
+// Per-sample footprint record, computed once per geometry with exactly the
+// arithmetic of grid_blocks: [0] fx, [1] fy (grid cells of the footprint
+// centre), [2..10] x-weights, [11..19] y-weights.
+__global__ void sample_records(const float2 *__restrict__ cs, const float *__restrict__ rtab,
+                               const float *__restrict__ etab, Geom geo,
+                               int *__restrict__ recs) {
+  const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = geo.n;
+  if (s >= (size_t)geo.nproj * n) return;
+  const int p = (int)(s / n), i = (int)(s % n);
+  float x0, y0;
+  int fx, fy;
+  sample_pos(cs, rtab, p, i, (float)(2 * n), x0, y0, fx, fy);
+  int *r = recs + s * TC_REC;
+  r[0] = fx;
+  r[1] = fy;
+#pragma unroll
+  for (int d = 0; d < 2 * M + 1; d++) {
+    float w0 = etab[fx - M + d + n + M + EPAD] - x0;
+    float w1 = etab[fy - M + d + n + M + EPAD] - y0;
+    r[2 + d] = __float_as_int(__expf(geo.coeff1 * w0 * w0));
+    r[2 + 2 * M + 1 + d] = __float_as_int(__expf(geo.coeff1 * w1 * w1));
+  }
+}
+// One smem stage per CTA and two CTAs per SM (2 x 256 TMEM columns = all 512):
+// one CTA builds its next chunk while the other's MMAs and loads are in flight.
+constexpr int TC_STAGES = 1;
+constexpr int TC_SMEM = TC_STAGES * TC_STAGE + TC_STAGES * TCK * TC_REC * 4 + 64 + 1024;
+constexpr uint32_t TC_IDESC = tc::idesc_f16_f32(128, TCN);
+
+__global__ void absmax_kernel(const float2 *__restrict__ g, size_t total,
+                              unsigned *__restrict__ out) {
+  float m = 0.f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float2 v = g[i];
+    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));  // m >= 0: int order
+}
+
+__device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
+  h = __float2half_rn(v);
+  l = __float2half_rn(v - __half2float(h));
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 2)
+    grid_tc(const float2 *__restrict__ G, float2 *__restrict__ grid,
+            const float2 *__restrict__ cs, const float *__restrict__ rtab,
+            const float *__restrict__ etab, const int *__restrict__ tile_order,
+            const long long *__restrict__ toffs, const int *__restrict__ tlist,
+            const int *__restrict__ recs, const unsigned *__restrict__ amax_bits, Geom geo,
+            int *__restrict__ err) {
+  using namespace tcb::tc;
+  extern __shared__ uint8_t tsm_raw[];
+  uint8_t *sm = tsm_raw + ((1024u - (smem_u32(tsm_raw) & 1023u)) & 1023u);
+  int *rec = reinterpret_cast<int *>(sm + TC_STAGES * TC_STAGE);   // [stages][TCK][TC_REC]
+  uint64_t *mma_done = reinterpret_cast<uint64_t *>(rec + TC_STAGES * TCK * TC_REC);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 2);
+  const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
+  const int zgroups = (geo.nz + ZMAX - 1) / ZMAX;
+  const int tile = tile_order[blockIdx.x / zgroups];
+  const int z0 = (blockIdx.x % zgroups) * ZMAX;
+  const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
+  const int X0 = ix0 - n, Y0 = iy0 - n;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float twonf = (float)(2 * n);
+  const int half = n / 2;
+  // power-of-two scale that puts max |G| in [2^13, 2^14)
+  const float amax = __uint_as_float(*amax_bits);
+  int ex = 0;
+  if (amax > 0.f) frexpf(amax, &ex);
+  const float gsc = ldexpf(1.f, 14 - ex), unsc = ldexpf(1.f, ex - 14);
+
+  if (tid == 0) {
+    mbar_init(&mma_done[0], 1);
+    mbar_init(&mma_done[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const long long t0 = toffs[tile];
+  const int S = (int)(toffs[tile + 1] - t0);
+  const int nch = (S + TCK - 1) / TCK;
+  // Register prefetch of one chunk: this thread's record words (e = tid + j*TC_THREADS
+  // of TCK x TC_REC) and spectrum values (e = tid + j*TC_THREADS of TCK x ZMAX).
+  constexpr int NRW = (TCK * TC_REC + TC_THREADS - 1) / TC_THREADS;  // 3
+  constexpr int NGV = (TCK * ZMAX + TC_THREADS - 1) / TC_THREADS;    // 2
+  int pr[NRW], pr1[NRW];
+  float2 pg[NGV];
+  int pc[NGV];
+  auto prefetch = [&](int cc) {
+#pragma unroll
+    for (int j = 0; j < NRW; j++) {
+      const int e = tid + j * TC_THREADS;
+      pr[j] = 0;
+      pr1[j] = 0;
+      if (e < TCK * TC_REC) {
+        const int k = e / TC_REC, w = e % TC_REC;
+        const int idx = cc * TCK + k;
+        if (idx < S) {
+          const int sidx = tlist[t0 + idx];
+          if (w >= 2) {
+            pr[j] = recs[(size_t)sidx * TC_REC + w];
+          } else if (w == 0) {
+            pr[j] = recs[(size_t)sidx * TC_REC];
+            pr1[j] = recs[(size_t)sidx * TC_REC + 1];
+          } else {
+            pr[j] = sidx + 1;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NGV; j++) {
+      const int e = tid + j * TC_THREADS;
+      pc[j] = 0;
+      pg[j] = make_float2(0.f, 0.f);
+      if (e < TCK * ZMAX) {
+        const int k = e % TCK, pz = e / TCK;
+        const int idx = cc * TCK + k;
+        if (idx < S && z0 + pz < geo.nz) {
+          const int sidx = tlist[t0 + idx];
+          const int pp = sidx / n, i = sidx % n;
+          int ii = i + half;
+          if (ii >= n) ii -= n;
+          pc[j] = 1 + (i & 1);
+          pg[j] = G[(size_t)(z0 + pz) * nproj * n + (size_t)pp * n + ii];
+        }
+      }
+    }
+  };
+  bool ok = true;
+  if (nch > 0) prefetch(0);
+  for (int c = 0; c < nch; c++) {
+    const int st = c % TC_STAGES;
+    uint8_t *A = sm + st * TC_STAGE, *B = A + TC_A;
+    int *R = rec + st * TCK * TC_REC;
+    // the MMAs that last read this stage (chunk c - TC_STAGES) must be done
+    if (c >= TC_STAGES && !mbar_wait(&mma_done[st], ((c / TC_STAGES) - 1) & 1)) ok = false;
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+    // (1) records and (3) spectrum values of this chunk from the prefetch registers
+#pragma unroll
+    for (int j = 0; j < NRW; j++) {
+      const int e = tid + j * TC_THREADS;
+      if (e < TCK * TC_REC) {
+        const int w = e % TC_REC;
+        int v = pr[j];
+        if (w == 0) {
+          const int k = e / TC_REC;
+          v = (c * TCK + k < S) ? ((tile_origin(pr[j], X0, twon) & 0xFFFF) |
+                                   (tile_origin(pr1[j], Y0, twon) << 16))
+                                : 0;
+        }
+        R[e] = v;  // e == k * TC_REC + w
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NGV; j++) {
+      const int e = tid + j * TC_THREADS;
+      if (e < TCK * ZMAX) {
+        const int k = e % TCK, pz = e / TCK;
+        __half rh = __float2half_rn(0.f), rl = rh, ih = rh, il = rh;
+        if (pc[j]) {
+          const float sg = ((pc[j] == 2) ? -geo.scale : geo.scale) * gsc;
+          split_half(pg[j].x * sg, rh, rl);
+          split_half(pg[j].y * sg, ih, il);
+        }
+        const int row = pz * 4;
+        *reinterpret_cast<__half *>(B + sw128_offset(row + 0, k)) = rh;
+        *reinterpret_cast<__half *>(B + sw128_offset(row + 1, k)) = ih;
+        *reinterpret_cast<__half *>(B + sw128_offset(row + 2, k)) = rl;
+        *reinterpret_cast<__half *>(B + sw128_offset(row + 3, k)) = il;
+      }
+    }
+    // (2) clear W (most entries are outside every footprint)
+    {
+      uint4 zero = make_uint4(0, 0, 0, 0);
+      uint4 *a4 = reinterpret_cast<uint4 *>(A);
+      for (int q = tid; q < TC_A / 16; q += TC_THREADS) a4[q] = zero;
+    }
+    __syncthreads();
+    // the next chunk's loads fly while this one is scattered and multiplied
+    if (c + 1 < nch) prefetch(c + 1);
+    // (4) scatter the footprint weights into W[cell][sample]: one thread per
+    // (sample, footprint row); consecutive threads take consecutive samples
+    for (int e = tid; e < TCK * (2 * M + 1); e += TC_THREADS) {
+      const int k = e % TCK, dy = e / TCK;
+      const int *r = R + k * TC_REC;
+      if (!r[1]) continue;
+      const int o = r[0];
+      const int ly = (o >> 16) + dy;
+      if ((unsigned)ly >= (unsigned)TY) continue;
+      const float wyv = __int_as_float(r[2 + 2 * M + 1 + dy]);
+      const int ox = (int)(short)(o & 0xFFFF);
+      const uint32_t kcol = (uint32_t)((k & 7) << 1);
+      const int kchunk = k >> 3;
+#pragma unroll
+      for (int dx = 0; dx < 2 * M + 1; dx++) {
+        const int lx = ox + dx;
+        if ((unsigned)lx < (unsigned)TX) {
+          const int m = ly * TX + lx;  // row of W (cell); rows of one tile row share 8-row groups
+          const float w = __int_as_float(r[2 + dx]) * wyv;
+          *reinterpret_cast<__half *>(A + (m >> 3) * 1024 + (m & 7) * 128 +
+                                      (((kchunk ^ m) & 7) << 4) + kcol) = __float2half_rn(w);
+        }
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    // (5) one thread issues the chunk's MMAs; the next chunk is built meanwhile
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+#pragma unroll
+      for (int g = 0; g < 4; g++)
+#pragma unroll
+        for (int kk = 0; kk < TCK / 16; kk++)
+          mma_f16(tmem + g * TCN, sdesc(a0 + g * 16384 + kk * 32), sdesc(b0 + kk * 32),
+                  TC_IDESC, (c > 0 || kk > 0) ? 1u : 0u);
+      mma_commit(&mma_done[st]);
+    }
+  }
+  if (ok && nch > 0 &&
+      !mbar_wait(&mma_done[(nch - 1) % TC_STAGES], ((nch - 1) / TC_STAGES) & 1))
+    ok = false;
+  ok = __syncthreads_and(ok);
+  tc_fence_after();
+  // Epilogue: warp w reads TMEM lanes 32(w%4).. of M-group w/4 (16 warps, 4 groups).
+  const int q = warp & 3;
+  {
+    const int g = warp >> 2;
+    const int m = g * 128 + q * 32 + lane;
+    const int cx = ix0 + (m % TX), cy = iy0 + (m / TX);
+    int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
+    const float sgn = (float)(sx * sy) * geo.coeff0 * unsc;
+    for (int c0 = 0; c0 < TCN; c0 += 32) {
+      float v[32];
+      if (nch > 0) {
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * TCN + c0), v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) v[j] = 0.f;
+      }
+      if (!ok || cx >= twon || cy >= twon) continue;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int pz = c0 / 4 + j;
+        if (z0 + pz < geo.nz)
+          grid[((size_t)(z0 + pz) * twon + cy) * twon + cx] =
+              make_float2((v[4 * j] + v[4 * j + 2]) * sgn, (v[4 * j + 1] + v[4 * j + 3]) * sgn);
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicOr(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
 // Deapodization of one output pixel (tx, ty) from the inverse-FFT value at
 // grid index (tx + n/2, ty + 1 + n/2): the post-FFT fftshift sign, divphi
 // with its (1 - n%4) sign and 1/nproj, and the circle mask, in the
@@ -629,6 +921,10 @@ struct tcb_fourierrec {
   // when 2n is a power of two in [256, 8192]: own_n = 2n, else 0.
   int own_n = 0;
   int zblock = 0;  // pairs per gridding block (2/4/8/16; 0 = largest that fits nz)
+  int grid_mode = 0;          // TCB_GRID_FP32 or TCB_GRID_TENSOR
+  unsigned *amax = nullptr;   // max |G| bits for the tensor-core gridding scale
+  int *recs = nullptr;        // per-sample footprint records (tensor-core gridding)
+  int *tc_err = nullptr;      // set by a tensor-core gridding wait that timed out
   float2 *t1 = nullptr;  // [nz][n][2n] column-pass output
   float2 *tw = nullptr;  // [2n] exp(2 pi i m / 2n)
   int ntiles = 0;
@@ -657,7 +953,13 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->g32);
   cudaFree(h->t1);
   cudaFree(h->tw);
+  cudaFree(h->amax);
+  cudaFree(h->tc_err);
+  cudaFree(h->recs);
+  h->recs = nullptr;
   h->t1 = h->tw = nullptr;
+  h->amax = nullptr;
+  h->tc_err = nullptr;
   h->plan1d = h->plan2d = h->plan_rows = h->plan_cols = 0;
   h->cs = nullptr;
   h->rtab = h->etab = nullptr;
@@ -705,7 +1007,19 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     StageTimer st("fr_fft1d", s);
     TCB_CUFFT(cufftExecC2C(h->plan1d, (cufftComplex *)gc, (cufftComplex *)gc, CUFFT_FORWARD));
   }
-  {
+  if (h->grid_mode == TCB_GRID_TENSOR) {
+    StageTimer st("fr_gather_tc", s);
+    const size_t gtot = h->nz * h->nproj * h->n;
+    TCB_CUDA(cudaMemsetAsync(h->amax, 0, sizeof(unsigned), s));
+    absmax_kernel<<<std::min<unsigned>(ceil_div(gtot, 256), 148u * 16u), 256, 0, s>>>(gc, gtot,
+                                                                                      h->amax);
+    const unsigned zgroups = (unsigned)((h->nz + ZMAX - 1) / ZMAX);
+    grid_tc<<<(unsigned)h->ntiles * zgroups, TC_THREADS, TC_SMEM, s>>>(
+        gc, h->grid, h->cs, h->rtab, h->etab, h->tile_order, h->toffs, h->tlist, h->recs, h->amax,
+        geo, h->tc_err);
+    TCB_LAUNCH_CHECK();
+    count_launch(2);
+  } else {
     StageTimer st("fr_gather", s);
     int rc;
     const size_t zb = h->zblock ? (size_t)h->zblock : 16;
@@ -1013,6 +1327,38 @@ extern "C" int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs) 
   TCB_CHECK_ARG(pairs == 0 || pairs == 2 || pairs == 4 || pairs == 8 || pairs == 16,
                 "tcb_fourierrec_set_pairs_per_block: pairs must be 0, 2, 4, 8 or 16");
   h->zblock = pairs;
+  return TCB_OK;
+}
+
+extern "C" int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode) {
+  TCB_CHECK_ARG(h, "tcb_fourierrec_set_gridding: null handle");
+  TCB_CHECK_ARG(h->grid, "tcb_fourierrec_set_gridding: handle was freed");
+  TCB_CHECK_ARG(mode == TCB_GRID_FP32 || mode == TCB_GRID_TENSOR,
+                "tcb_fourierrec_set_gridding: unknown mode %d", mode);
+  if (mode == TCB_GRID_TENSOR && !h->amax) {
+    const size_t nsamp = h->nproj * h->n;
+    if (cudaMalloc(&h->amax, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&h->tc_err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h->recs, nsamp * TC_REC * sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("tcb_fourierrec_set_gridding: out of device memory");
+      return TCB_ERR_OUT_OF_MEMORY;
+    }
+    TCB_CUDA(cudaMemset(h->tc_err, 0, sizeof(int)));
+    TCB_CUDA(cudaFuncSetAttribute(grid_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TC_SMEM));
+    sample_records<<<ceil_div(nsamp, 256), 256>>>(h->cs, h->rtab, h->etab, h->geo, h->recs);
+    count_launch();
+    TCB_CUDA(cudaDeviceSynchronize());
+  }
+  h->grid_mode = mode;
+  return TCB_OK;
+}
+
+extern "C" int tcb_fourierrec_status(tcb_fourierrec *h, int *timed_out) {
+  TCB_CHECK_ARG(h && timed_out, "tcb_fourierrec_status: null pointer");
+  *timed_out = 0;
+  if (h->tc_err) TCB_CUDA(cudaMemcpy(timed_out, h->tc_err, sizeof(int), cudaMemcpyDeviceToHost));
   return TCB_OK;
 }
 

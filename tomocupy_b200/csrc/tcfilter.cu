@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 struct tcb_tcfilter {
   size_t nproj, nz, n, nkern;
@@ -52,6 +53,7 @@ struct tcb_tcfilter {
 
 namespace tcb {
 namespace tcf {
+using namespace tcb::tc;
 
 constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;
@@ -59,10 +61,7 @@ constexpr int B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr uint32_t TMEM_COLS = 256;
-constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s at 1.9 GHz
-// Instruction descriptor: D f32 (bits 4-5 = 1), A/B f16, both K-major,
-// N = 256 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
-constexpr uint32_t IDESC = (1u << 4) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+constexpr uint32_t IDESC = tc::idesc_f16_f32(BM, BN);  // M = 128, N = 256
 
 enum { OUT_ROWS = 0, OUT_PAIRS = 1 };
 
@@ -75,106 +74,6 @@ struct GemmArgs {
   float inv_scale;
   int *err;
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t cnt) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(cnt));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: false when the clock budget ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
-  long long t0 = clock64();
-  while (!mbar_try_wait(b, parity))
-    if (clock64() - t0 > WAIT_CYCLES) return false;
-  return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
-                                            int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor for a K-major tile written by TMA with
-// SWIZZLE_128B: rows of 128 B, 8-row groups 1024 B apart (SBO), descriptor
-// version 1, layout type 2 (128-byte swizzle).
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(1024 >> 4) << 32;
-  d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
-  return d;
-}
-
-__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                        uint32_t accumulate) {
-  uint32_t z = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-          tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// 32 consecutive fp32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-      "%28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-        "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(128, 1)
@@ -254,7 +153,7 @@ __global__ void __launch_bounds__(128, 1)
       const uint32_t sa = smem_u32(smem + s * STAGE_BYTES), sb = sa + A_BYTES;
 #pragma unroll
       for (int k = 0; k < BK / 16; k++)
-        mma_f16(tmem, sdesc(sa + k * 32), sdesc(sb + k * 32), (kb > 0 || k > 0) ? 1u : 0u);
+        mma_f16(tmem, sdesc(sa + k * 32), sdesc(sb + k * 32), IDESC, (kb > 0 || k > 0) ? 1u : 0u);
       mma_commit(&empty[s]);
     }
     mma_commit(done);

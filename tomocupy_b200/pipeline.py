@@ -20,8 +20,10 @@ executed as native kernels on one stream:
 same prep chain written as fp16 hi/lo planes, unpadded) and the tensor-core
 filter ``tcb_tcfilter_apply`` (edge pad + filter + centre shift + crop as one
 split-precision fp16 GEMM), whose epilogue writes the packed complex pairs
-of fourierrec directly (no pack pass) or the cropped rows of linerec/lprec.
-The filter does not modify its input planes.
+of fourierrec directly (no pack pass) or the cropped rows of linerec/lprec,
+and grids fourierrec on the tensor cores (``TCB_GRID_TENSOR``: fp16 weights
+and hi/lo values, fp32 accumulation).  The filter does not modify its input
+planes.
 """
 from __future__ import annotations
 
@@ -88,6 +90,8 @@ class SinoPipeline:
         if algorithm == "fourierrec":
             self.fr = cfunc_fourierrec.cfunc_fourierrec(self.nproj, self.ncz // 2, self.n,
                                                         self.theta)
+            if precision == "mixed":  # fp16 weights/values, fp32 accumulation in TMEM
+                self.fr.set_gridding(_lib.GRID_TENSOR)
             self.g = torch.empty((self.ncz // 2, self.nproj, self.n, 2), dtype=torch.float32,
                                  device=self.device)
         else:
