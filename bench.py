@@ -378,6 +378,64 @@ def run_serving(a, dev):
     return res
 
 
+def _lamino_setup(a, dtype):
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.global_vars import params
+    ntheta, n, rh, tilt = a.lam_nproj, a.lam_n, a.lam_rh, 30.0
+    theta = (np.arange(ntheta) * 2 * np.pi / ntheta).astype(np.float32)
+    global_vars.reset(lamino_angle=tilt, reconstruction_algorithm="fourierrec",
+                      nsino_per_chunk=32, nproj_per_chunk=60, fbp_filter="shepp", dtype=dtype)
+    params.n, params.nz, params.nproj, params.ncproj, params.ncz = n, n, ntheta, 60, 32
+    params.rh, params.center, params.theta, params.lamino_angle = rh, n / 2, theta, tilt
+    return theta
+
+
+def _lamino_data(a, dev):
+    """Seeded smooth projections [nproj, n, n] (content does not change the timing)."""
+    import torch
+    from tomocupy_b200.synthetic import smooth_field
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(a.seed)
+    base = smooth_field(a.lam_n, a.lam_n, 24.0, gen, dev).abs()
+    ang = torch.arange(a.lam_nproj, device=dev, dtype=torch.float32)
+    return (base[None] * (1.0 + 0.1 * torch.cos(ang * 2 * np.pi / a.lam_nproj))[:, None, None]
+            ).contiguous()
+
+
+def run_lamino(a, dev):
+    """Laminography leg: fp32 chain and fp16 stage storage, device-resident."""
+    import torch
+    from tomocupy_b200.reconstruction.backproj_lamfourier_parallel import \
+        BackprojLamFourierParallel
+    data = _lamino_data(a, dev)
+    vox = float(a.lam_rh) * a.lam_n * a.lam_n * a.lam_nproj
+    res = {"workload": f"{a.lam_nproj} angles over [0, 2pi) x {a.lam_n}^2 fp32 projections, "
+                       f"tilt 30 deg, rh {a.lam_rh} -> {a.lam_rh}x{a.lam_n}^2 volume "
+                       "(seeded smooth projections)", "unit": "GUPS (rh*n^2*nproj/t)"}
+    outs = {}
+    for dtype in ("float32", "mixed"):
+        _lamino_setup(a, dtype)
+        bp = BackprojLamFourierParallel(device=dev)
+        bp.rec_lam(data)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(2):
+            out = bp.rec_lam(data)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 2
+        key = "fp32" if dtype == "float32" else "fp16_storage"
+        res[key] = {"ms": round(ms, 2), "value": round(vox / (ms / 1e3) / 1e9, 2)}
+        outs[key] = out
+        del bp
+    d = (outs["fp16_storage"].double() - outs["fp32"].double()).norm()
+    res["fp16_storage_rel_l2_vs_fp32"] = float(d / outs["fp32"].double().norm())
+    del outs, data
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_ours(a, ws, rank, local):
     import torch
     from tomocupy_b200.global_vars import params
@@ -446,6 +504,9 @@ def run_ours(a, ws, rank, local):
     serving = None
     if not a.no_serve and ws == 1:
         serving = run_serving(a, dev)
+    lamino = None
+    if not a.no_lamino and ws == 1:
+        lamino = run_lamino(a, dev)
 
     if rank == 0:
         tag = "fp32" if primary == "float32" else "mixed-precision"
@@ -470,6 +531,7 @@ def run_ours(a, ws, rank, local):
             other if other == "mixed" else "fp32": side,
             "try_center": trycenter,
             "serving": serving,
+            "lamino": lamino,
         }
         print(json.dumps(line), flush=True)
 
@@ -571,6 +633,25 @@ def run_reference(a, ws, rank, local):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / a.steps
     value = float(n) ** 2 * rows * P / (ms / 1e3) / 1e9
+    lam = None
+    if not a.no_lamino:
+        _lamino_setup(a, "float32")
+        ld = _lamino_data(a, dev)
+        th = torch.as_tensor((np.arange(a.lam_nproj) * 2 * np.pi / a.lam_nproj).astype(np.float32),
+                             device=dev)
+        wl = torch.as_tensor(np_tomo.calc_filter(4 * a.lam_n, "shepp"), device=dev)
+        refglue.ref_rec_lam(ld, th, a.lam_n / 2, 30.0, a.lam_rh, wl, nthetac=60, dethc=32, n1c=32)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        refglue.ref_rec_lam(ld, th, a.lam_n / 2, 30.0, a.lam_rh, wl, nthetac=60, dethc=32, n1c=32)
+        e1.record()
+        torch.cuda.synchronize()
+        lms = e0.elapsed_time(e1)
+        lam = {"ms": round(lms, 2), "unit": "GUPS (rh*n^2*nproj/t)",
+               "value": round(float(a.lam_rh) * a.lam_n ** 2 * a.lam_nproj / (lms / 1e3) / 1e9, 2),
+               "workload": "laminography, same as our lamino leg (reference CUDA operators)"}
+        del ld
     line = {"impl": "reference",
             "metric": f"GUPS @{a.n}^2x{a.nproj} ({a.algorithm} fp32 pipeline, 1 GPU rate)",
             "value": round(value, 2), "unit": "GUPS", "n_gpus": 1, "steps": a.steps,
@@ -586,7 +667,8 @@ def run_reference(a, ws, rank, local):
                                        f"on the B200, {rows} rows per step, driven by 1 host "
                                        f"thread; the reference has no CPU implementation"},
             "e2e": {"value": round(value, 2), "unit": "GUPS", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "lamino": lam}
     print(json.dumps(line), flush=True)
 
 
@@ -616,6 +698,10 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-ncz", type=int, default=16)
+    ap.add_argument("--no-lamino", action="store_true", help="skip the laminography leg")
+    ap.add_argument("--lam-n", type=int, default=1024)
+    ap.add_argument("--lam-nproj", type=int, default=1200)
+    ap.add_argument("--lam-rh", type=int, default=512)
     ap.add_argument("--try-n", type=int, default=4096)
     ap.add_argument("--try-nproj", type=int, default=3000)
     ap.add_argument("--try-centers", type=int, default=256)

@@ -301,6 +301,11 @@ int tcb_usfft2d_adj(tcb_usfft2d *h, void *f, const void *g, const float *theta, 
  * of backproj_lamfourier_parallel.py:197-215 and the host copies). */
 int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1, const float *theta,
                          float phi, int row0, int nrows, int deth_full, void *stream);
+/* fp16 storage (no reference counterpart; the reference's laminography path
+ * is fp32 only): TCB_FLOAT16 makes the stage-1 spectrum input and the output
+ * of adj/adj_rows complex fp16 (__half2) arrays; gridding, FFTs and
+ * deapodization compute in fp32. */
+int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision);
 int tcb_usfft2d_destroy(tcb_usfft2d *h);
 
 /* Replaces cfunc_usfft1d (src/include/cfunc_usfft1d.cuh:7-34,
@@ -310,6 +315,8 @@ int tcb_usfft2d_destroy(tcb_usfft2d *h);
 typedef struct tcb_usfft1d tcb_usfft1d;
 int tcb_usfft1d_create(tcb_usfft1d **out, size_t n0, size_t n1, size_t n2, size_t deth);
 int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi, void *stream);
+/* fp16 storage of the input g (complex fp16); output and arithmetic fp32. */
+int tcb_usfft1d_set_storage(tcb_usfft1d *h, int precision);
 int tcb_usfft1d_destroy(tcb_usfft1d *h);
 
 #ifdef __cplusplus

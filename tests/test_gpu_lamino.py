@@ -115,3 +115,28 @@ def test_rec_lam_vs_reference(cuda, ref):
     torch.cuda.synchronize()
     err = rel_l2(ours.cpu(), theirs.cpu())
     assert err < 1e-5, err
+
+
+def test_rec_lam_fp16_storage_vs_fp32(cuda):
+    """Mixed precision for laminography: the stage-1 spectrum and the stage-2
+    array in complex fp16, every kernel computing in fp32.  Error stated
+    against the fp32 chain (which matches the reference build to 1e-5)."""
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.reconstruction.backproj_lamfourier_parallel import \
+        BackprojLamFourierParallel
+    ntheta, deth, detw, rh = 90, 96, 128, 48
+    rng = np.random.default_rng(5)
+    data = torch.as_tensor(rng.standard_normal((ntheta, deth, detw)).astype(np.float32),
+                           device=cuda)
+    theta = (np.arange(ntheta) * 2 * np.pi / ntheta).astype(np.float32)
+    out = {}
+    for dtype in ("float32", "mixed"):
+        global_vars.reset(lamino_angle=TILT, reconstruction_algorithm="fourierrec",
+                          nsino_per_chunk=8, nproj_per_chunk=8, fbp_filter="shepp", dtype=dtype)
+        params.n, params.nz, params.nproj, params.ncproj, params.ncz = detw, deth, ntheta, 8, 8
+        params.rh, params.center, params.theta, params.lamino_angle = rh, detw / 2, theta, TILT
+        out[dtype] = BackprojLamFourierParallel().rec_lam(data.clone()).cpu()
+    err = rel_l2(out["mixed"], out["float32"])
+    assert torch.isfinite(out["mixed"]).all()
+    assert err < 1e-3, err

@@ -19,5 +19,9 @@ class cfunc_usfft1d(NativeHandle):
         _lib.call("tcb_usfft1d_adj", self._live(), _lib.ptr(f_), _lib.ptr(g_), float(phi),
                   _lib.stream_ptr(stream_))
 
+    def set_storage(self, precision: int) -> None:
+        """Not in the reference: _lib.TCB_FLOAT16 stores the stage arrays in complex fp16."""
+        _lib.call("tcb_usfft1d_set_storage", self._live(), int(precision))
+
     def fwd(self, *a, **k):
         raise NotImplementedError("usfft1d forward is not on the reconstruction path")

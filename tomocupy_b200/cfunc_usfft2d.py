@@ -26,5 +26,9 @@ class cfunc_usfft2d(NativeHandle):
                   _lib.ptr(theta), float(phi), int(row0), int(nrows), int(deth_full),
                   _lib.stream_ptr(stream_))
 
+    def set_storage(self, precision: int) -> None:
+        """Not in the reference: _lib.TCB_FLOAT16 stores the stage arrays in complex fp16."""
+        _lib.call("tcb_usfft2d_set_storage", self._live(), int(precision))
+
     def fwd(self, *a, **k):
         raise NotImplementedError("usfft2d forward is not on the reconstruction path")

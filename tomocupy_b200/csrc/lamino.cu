@@ -147,8 +147,16 @@ __device__ __forceinline__ void u2_pos(const U2Geom &g, float2 csa, int tx, int 
   y = (float)fmin(fmax((double)y, -0.5f + 1e-5), 0.5f - 1e-5);
 }
 
+// Storage of the stage arrays: complex fp32 (float2) or complex fp16
+// (__half2, "fp16 storage"); arithmetic is fp32 either way.
+__device__ __forceinline__ float2 ld2(const float2 *p) { return *p; }
+__device__ __forceinline__ float2 ld2(const __half2 *p) { return __half22float2(*p); }
+__device__ __forceinline__ void st2(float2 *p, float2 v) { *p = v; }
+__device__ __forceinline__ void st2(__half2 *p, float2 v) { *p = __floats2half2_rn(v.x, v.y); }
+
 // Value of sample (tx, ty, tz) with the conjugate mirror of gather2d.
-__device__ __forceinline__ float2 u2_val(const U2Geom &g, const float2 *__restrict__ src, int tx,
+template <typename S>
+__device__ __forceinline__ float2 u2_val(const U2Geom &g, const S *__restrict__ src, int tx,
                                          int ty, int tz) {
   const int wc = g.detw / 2 + 1;
   if (!g.fused) {
@@ -160,21 +168,21 @@ __device__ __forceinline__ float2 u2_val(const U2Geom &g, const float2 *__restri
       tzs = tz + g.ntheta;
       conj = -1.f;
     }
-    float2 v = src[(size_t)txs + (size_t)tys * wc + (size_t)tzs * wc * g.deth];
+    float2 v = ld2(src + (size_t)txs + (size_t)tys * wc + (size_t)tzs * wc * g.deth);
     v.y *= conj;
     return v;
   }
   int row = g.row0 + ty;
-  if (tx <= g.detw / 2) return src[(size_t)tx + (size_t)row * wc + (size_t)tz * wc * g.deth_full];
+  if (tx <= g.detw / 2) return ld2(src + (size_t)tx + (size_t)row * wc + (size_t)tz * wc * g.deth_full);
   int mrow = g.deth_full - row;
   if (mrow >= g.deth_full) mrow -= g.deth_full;
-  float2 v = src[(size_t)(g.detw - tx) + (size_t)mrow * wc + (size_t)tz * wc * g.deth_full];
+  float2 v = ld2(src + (size_t)(g.detw - tx) + (size_t)mrow * wc + (size_t)tz * wc * g.deth_full);
   v.y = -v.y;
   return v;
 }
 
-template <int M0, int M1>
-__global__ void __launch_bounds__(NT) u2_gather(const float2 *__restrict__ src,
+template <int M0, int M1, typename S>
+__global__ void __launch_bounds__(NT) u2_gather(const S *__restrict__ src,
                                                 float2 *__restrict__ grid,
                                                 const float2 *__restrict__ cs,
                                                 const float *__restrict__ ex,
@@ -328,7 +336,8 @@ __global__ void u2_tables(float2 *__restrict__ cs, float *__restrict__ ex, float
 
 // divker2d (direction 1) with the post-FFT fftshift sign; f[ty][slab][tx] layout
 // [n1][fstride_slabs][n0], slab offset fslab0.
-__global__ void u2_deapod(const float2 *__restrict__ grid, float2 *__restrict__ f, U2Geom geo,
+template <typename S>
+__global__ void u2_deapod(const float2 *__restrict__ grid, S *__restrict__ f, U2Geom geo,
                           int nslab, int fslabs, int fslab0) {
   const int n0 = geo.n0, n1 = geo.n1;
   int tx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -344,8 +353,8 @@ __global__ void u2_deapod(const float2 *__restrict__ grid, float2 *__restrict__ 
   v.x *= s;
   v.y *= s;
   float nn = (float)(n0 * n1);
-  f[(size_t)tx + (size_t)(fslab0 + tz) * n0 + (size_t)ty * n0 * fslabs] =
-      make_float2(v.x / ker / nn, v.y / ker / nn);
+  st2(f + (size_t)tx + (size_t)(fslab0 + tz) * n0 + (size_t)ty * n0 * fslabs,
+      make_float2(v.x / ker / nn, v.y / ker / nn));
 }
 
 // ------------------------------------------------------------------ usfft1d
@@ -359,7 +368,8 @@ struct U1Geom {
 // Gather form of gather1d(direction 1) + wrap1d + fftshiftc1d: grid cell
 // (z, y, x) of the periodic [2n2][n1][n0] grid sums the height samples whose
 // footprint reaches it.  g: [n1][deth/2+1][n0] (row stride gstride rows).
-__global__ void u1_gather(const float2 *__restrict__ g, float2 *__restrict__ grid,
+template <typename S>
+__global__ void u1_gather(const S *__restrict__ g, float2 *__restrict__ grid,
                           const float *__restrict__ zt, const float *__restrict__ ez, U1Geom geo,
                           float zslope, float zoff) {
   const int n0 = geo.n0, n1 = geo.n1, n2 = geo.n2, M = geo.m2, deth = geo.deth;
@@ -396,7 +406,7 @@ __global__ void u1_gather(const float2 *__restrict__ g, float2 *__restrict__ gri
         ts = t - 2 * (t - deth / 2);
         conj = -1.f;
       }
-      float2 v = g[(size_t)tx + (size_t)ts * n0 + (size_t)ty * n0 * hc];
+      float2 v = ld2(g + (size_t)tx + (size_t)ts * n0 + (size_t)ty * n0 * hc);
       sr += w * v.x;
       si += w * conj * v.y;
     }
@@ -505,6 +515,7 @@ struct tcb_usfft2d {
   float2 *cs = nullptr;
   float *ex = nullptr, *ey = nullptr;
   cufftHandle plan = 0;
+  int storage = TCB_FLOAT32;  // of the stage-1 input and the output
 };
 
 static void u2_release(tcb_usfft2d *h) {
@@ -565,14 +576,14 @@ extern "C" int tcb_usfft2d_create(tcb_usfft2d **out, size_t n0_, size_t n1_, siz
   if (cufftPlanMany(&h->plan, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, (int)n2) !=
       CUFFT_SUCCESS)
     return fail(TCB_ERR_CUFFT, "cufftPlanMany failed");
-  if (cudaFuncSetAttribute(u2_gather<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(u2_gather<4, 4, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sizeof(U2Smem)) != cudaSuccess)
     return fail(TCB_ERR_CUDA, "smem attribute failed");
   *out = h;
   return TCB_OK;
 }
 
-static int u2_run(tcb_usfft2d *h, float2 *f, const float2 *g, const float *theta, float phi,
+static int u2_run(tcb_usfft2d *h, void *f, const void *g, const float *theta, float phi,
                   int k, int deth0, int fused, int row0, int deth_full, int nslab, int fslabs,
                   int fslab0, cudaStream_t s) {
   U2Geom geo = h->geo;
@@ -591,7 +602,12 @@ static int u2_run(tcb_usfft2d *h, float2 *f, const float2 *g, const float *theta
   {
     StageTimer st("usfft2d_gather", s);
     unsigned blocks = (unsigned)(geo.ntx * geo.nty * nslab);
-    u2_gather<4, 4><<<blocks, NT, sizeof(U2Smem), s>>>(g, h->grid, h->cs, h->ex, h->ey, geo);
+    if (h->storage == TCB_FLOAT16)
+      u2_gather<4, 4, __half2><<<blocks, NT, sizeof(U2Smem), s>>>((const __half2 *)g, h->grid,
+                                                                 h->cs, h->ex, h->ey, geo);
+    else
+      u2_gather<4, 4, float2><<<blocks, NT, sizeof(U2Smem), s>>>((const float2 *)g, h->grid,
+                                                                h->cs, h->ex, h->ey, geo);
     TCB_LAUNCH_CHECK();
     count_launch();
   }
@@ -604,7 +620,10 @@ static int u2_run(tcb_usfft2d *h, float2 *f, const float2 *g, const float *theta
   {
     StageTimer st("usfft2d_deapod", s);
     dim3 blk(32, 8), grd(ceil_div(geo.n0, 32), ceil_div(geo.n1, 8), (unsigned)nslab);
-    u2_deapod<<<grd, blk, 0, s>>>(h->grid, f, geo, nslab, fslabs, fslab0);
+    if (h->storage == TCB_FLOAT16)
+      u2_deapod<__half2><<<grd, blk, 0, s>>>(h->grid, (__half2 *)f, geo, nslab, fslabs, fslab0);
+    else
+      u2_deapod<float2><<<grd, blk, 0, s>>>(h->grid, (float2 *)f, geo, nslab, fslabs, fslab0);
     TCB_LAUNCH_CHECK();
     count_launch();
   }
@@ -618,7 +637,7 @@ extern "C" int tcb_usfft2d_adj(tcb_usfft2d *h, void *f, const void *g, const flo
   TCB_CHECK_ARG(h && h->grid, "tcb_usfft2d_adj: null or freed handle");
   TCB_CHECK_ARG(f && g && theta, "tcb_usfft2d_adj: null pointer");
   TCB_CHECK_ARG((size_t)h->geo.deth == h->n2, "tcb_usfft2d_adj: deth must equal n2 slabs");
-  return u2_run(h, (float2 *)f, (const float2 *)g, theta, phi, k, deth0, 0, 0, 0,
+  return u2_run(h, f, g, theta, phi, k, deth0, 0, 0, 0,
                 (int)h->n2, (int)h->n2, 0, (cudaStream_t)stream);
 }
 
@@ -637,9 +656,21 @@ extern "C" int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1,
   // express row0 as k*deth via a geometry with deth = 1.
   tcb_usfft2d tmp = *h;
   tmp.geo.deth = 1;
-  int st = u2_run(&tmp, (float2 *)S2, (const float2 *)S1, theta, phi, row0, deth_full, 1, row0,
+  int st = u2_run(&tmp, S2, S1, theta, phi, row0, deth_full, 1, row0,
                   deth_full, nrows, deth_full / 2 + 1, row0, (cudaStream_t)stream);
   return st;
+}
+
+extern "C" int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision) {
+  TCB_CHECK_ARG(h && h->grid, "tcb_usfft2d_set_storage: null or freed handle");
+  TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
+                "tcb_usfft2d_set_storage: unknown precision %d", precision);
+  if (precision == TCB_FLOAT16)
+    TCB_CUDA(cudaFuncSetAttribute(u2_gather<4, 4, __half2>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(U2Smem)));
+  h->storage = precision;
+  return TCB_OK;
 }
 
 extern "C" int tcb_usfft2d_destroy(tcb_usfft2d *h) {
@@ -652,6 +683,7 @@ extern "C" int tcb_usfft2d_destroy(tcb_usfft2d *h) {
 // ====================================================================== usfft1d
 struct tcb_usfft1d {
   U1Geom geo;
+  int storage = TCB_FLOAT32;  // of the input g
   float2 *grid = nullptr;
   float *zt = nullptr, *ez = nullptr;
   cufftHandle plan = 0;
@@ -723,7 +755,12 @@ extern "C" int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi
   {
     StageTimer st("usfft1d_gather", s);
     dim3 blk(128), grd(ceil_div(geo.n0, 128), (unsigned)geo.n1, (unsigned)(2 * geo.n2));
-    u1_gather<<<grd, blk, 0, s>>>((const float2 *)g, h->grid, h->zt, h->ez, geo, zslope, zoff);
+    if (h->storage == TCB_FLOAT16)
+      u1_gather<__half2><<<grd, blk, 0, s>>>((const __half2 *)g, h->grid, h->zt, h->ez, geo,
+                                             zslope, zoff);
+    else
+      u1_gather<float2><<<grd, blk, 0, s>>>((const float2 *)g, h->grid, h->zt, h->ez, geo,
+                                            zslope, zoff);
     TCB_LAUNCH_CHECK();
     count_launch();
   }
@@ -740,6 +777,14 @@ extern "C" int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi
     TCB_LAUNCH_CHECK();
     count_launch();
   }
+  return TCB_OK;
+}
+
+extern "C" int tcb_usfft1d_set_storage(tcb_usfft1d *h, int precision) {
+  TCB_CHECK_ARG(h && h->grid, "tcb_usfft1d_set_storage: null or freed handle");
+  TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
+                "tcb_usfft1d_set_storage: unknown precision %d", precision);
+  h->storage = precision;
   return TCB_OK;
 }
 

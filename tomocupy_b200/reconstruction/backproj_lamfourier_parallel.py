@@ -23,6 +23,7 @@ import math
 import numpy as np
 import torch
 
+from .. import _lib
 from ..global_vars import args, params
 from ..processing.proc_functions import prep_rows
 from ..reconstruction.backproj_functions import rfftfreq32
@@ -75,7 +76,13 @@ class BackprojLamFourierParallel:
         theta = torch.as_tensor(np.asarray(params.theta, dtype=np.float32), device=dev)
         nthetac, deth, detw = self.nthetac, self.deth, self.detw
         w = self._weights(nthetac)
-        s1 = torch.empty((self.ntheta, deth, detw // 2 + 1), dtype=torch.complex64, device=dev)
+        # fp16 storage of the two stage arrays (fp32 arithmetic) in mixed precision
+        half = args.dtype == "mixed"
+        sdt = torch.float16 if half else torch.float32
+        prec = _lib.TCB_FLOAT16 if half else _lib.TCB_FLOAT32
+        self.cl_lamfourier.cl_usfft2d.set_storage(prec)
+        self.cl_lamfourier.cl_usfft1d.set_storage(prec)
+        s1 = torch.empty((self.ntheta, deth, detw // 2 + 1, 2), dtype=sdt, device=dev)
         g1 = torch.empty((nthetac, deth, detw // 2 + 1), dtype=torch.complex64, device=dev)
         # stage 1
         for st in range(0, self.ntheta, nthetac):
@@ -91,10 +98,10 @@ class BackprojLamFourierParallel:
             self.cl_filter.fslv.filter(self._rows, w, stream)
             self._crop.copy_(self._rows[:, :, self.pad:self.pad + detw])
             self.cl_lamfourier.fft2d_fwd(g1, self._crop, stream)
-            s1[st:end] = g1[:end - st]
+            s1[st:end] = torch.view_as_real(g1[:end - st])
         # stage 2
         nrow = deth // 2 + 1
-        s2 = torch.empty((self.n1, nrow, self.n2), dtype=torch.complex64, device=dev)
+        s2 = torch.empty((self.n1, nrow, self.n2, 2), dtype=sdt, device=dev)
         for st in range(0, nrow, self.dethc):
             nr = min(self.dethc, nrow - st)
             self.cl_lamfourier.cl_usfft2d.adj_rows(s2, s1, theta, phi, st, nr, deth, stream)
@@ -102,7 +109,7 @@ class BackprojLamFourierParallel:
         # stage 3
         s3 = torch.empty((self.n1, self.n0, self.n2), dtype=torch.float32, device=dev)
         o1 = torch.empty((self.n1c, self.n0, self.n2), dtype=torch.float32, device=dev)
-        gin = torch.zeros((self.n1c, nrow, self.n2), dtype=torch.complex64, device=dev)
+        gin = torch.zeros((self.n1c, nrow, self.n2, 2), dtype=sdt, device=dev)
         for st in range(0, self.n1, self.n1c):
             end = min(self.n1, st + self.n1c)
             if end - st == self.n1c:
