@@ -610,8 +610,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     const int st = c % TC_STAGES;
     uint8_t *A = sm + st * TC_STAGE, *B = A + TC_A;
     int *R = rec + st * TCK * TC_REC;
-    // the MMAs that last read this stage (chunk c - TC_STAGES) must be done
-    if (c >= TC_STAGES && !mbar_wait(&mma_done[st], ((c / TC_STAGES) - 1) & 1)) ok = false;
+    // the MMAs that last read this stage (chunk c - TC_STAGES) must be done; one
+    // thread polls the mbarrier, the others wait at the block barrier
+    if (tid == 0 && c >= TC_STAGES && !mbar_wait(&mma_done[st], ((c / TC_STAGES) - 1) & 1))
+      ok = false;
     ok = __syncthreads_and(ok);
     if (!ok) break;
     // (1) records and (3) spectrum values of this chunk from the prefetch registers
@@ -696,7 +698,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       mma_commit(&mma_done[st]);
     }
   }
-  if (ok && nch > 0 &&
+  if (tid == 0 && ok && nch > 0 &&
       !mbar_wait(&mma_done[(nch - 1) % TC_STAGES], ((nch - 1) / TC_STAGES) & 1))
     ok = false;
   ok = __syncthreads_and(ok);
