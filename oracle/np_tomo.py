@@ -290,3 +290,135 @@ def direct_fbp64(filtered, theta, n):
             row = filtered[z, p].astype(np.float64)
             out[z] += np.where(ok, row[i0c] * (1 - fr) + row[i0c + 1] * fr, 0)
     return out * np.pi / nproj
+
+
+# --------------------------------------------------------------------------
+# laminography Fourier chain in float64 (src/cuda/cfunc_fft2d.cu:52-63,
+# src/include/kernels_fft2d.cu, src/cuda/cfunc_usfft2d.cu:72-89 with
+# src/include/kernels_usfft2d.cu, src/cuda/cfunc_usfft1d.cu:68-86 with
+# src/include/kernels_usfft1d.cu, glue of
+# src/tomocupy/reconstruction/backproj_lamfourier_parallel.py:185-304).
+# The frequency-row chunk packing of the glue is replaced by its meaning:
+# row r of the half spectrum, with the conjugate mirror for tx > detw/2.
+# --------------------------------------------------------------------------
+def _usfft_params(n, eps=1e-3):
+    mu = -np.log(eps) / (2.0 * n * n)
+    m = int(np.ceil(2 * n / np.pi * np.sqrt(-mu * np.log(eps) + (mu * n) * (mu * n) / 4)))
+    return mu, m
+
+
+def _checker(nx, ny):
+    """(1-2((tx+1)%2)) (1-2((ty+1)%2)) over [ny, nx]."""
+    sx = 1 - 2 * ((np.arange(nx) + 1) % 2)
+    sy = 1 - 2 * ((np.arange(ny) + 1) % 2)
+    return (sy[:, None] * sx[None, :]).astype(np.float64)
+
+
+def fft2d64(f):
+    """cfunc_fft2d.fwd: sign flip, R2C 2D, sign flip with -1, / (deth*detw)."""
+    ntheta, deth, detw = f.shape
+    g = np.fft.rfft2(f * _checker(detw, deth)[None])
+    wc = detw // 2 + 1
+    return g * (-_checker(wc, deth))[None] / (deth * detw)
+
+
+def usfft2d_adj64(s1, theta, phi, n):
+    """All frequency rows r in [0, deth/2] of the half spectrum s1
+    [ntheta, deth, detw/2+1] -> s2 [n1 = n, nrow, n0 = n] (usfft2d.adj)."""
+    ntheta, deth, wc = s1.shape
+    detw = 2 * (wc - 1)
+    n0 = n1 = n
+    mu0, m0 = _usfft_params(n0)
+    mu1, m1 = _usfft_params(n1)
+    P0, P1 = 2 * n0 + 2 * m0, 2 * n1 + 2 * m1
+    nrow = deth // 2 + 1
+    out = np.empty((n1, nrow, n0), dtype=np.complex128)
+    th = np.asarray(theta, np.float64)[:, None]
+    tx = np.arange(detw)[None, :]
+    ku = (tx - detw / 2.0) / detw
+    i0 = np.arange(2 * m0 + 1)
+    i1 = np.arange(2 * m1 + 1)
+    for r in range(nrow):
+        kv = (r - deth / 2.0) / deth
+        x = ku * np.cos(th) + kv * np.sin(th) * np.cos(phi)
+        y = ku * np.sin(th) - kv * np.cos(th) * np.cos(phi)
+        x = np.clip(x, -0.5 + 1e-5, 0.5 - 1e-5).ravel()
+        y = np.clip(y, -0.5 + 1e-5, 0.5 - 1e-5).ravel()
+        # sample values with the conjugate mirror of gather2d
+        mrow = (deth - r) % deth
+        v = np.where(tx <= detw // 2, s1[:, r, np.minimum(tx, wc - 1)[0]],
+                     np.conj(s1[:, mrow, np.clip(detw - tx, 0, wc - 1)[0]])).ravel()
+        ell0 = np.floor(2 * n0 * x).astype(np.int64)[:, None] - m0 + i0[None, :]
+        ell1 = np.floor(2 * n1 * y).astype(np.int64)[:, None] - m1 + i1[None, :]
+        w0 = ell0 / (2.0 * n0) - x[:, None]
+        w1 = ell1 / (2.0 * n1) - y[:, None]
+        w = (np.pi / np.sqrt(mu0 * mu1 * ntheta) *
+             np.exp(-np.pi ** 2 / mu0 * w0[:, None, :] ** 2 - np.pi ** 2 / mu1 * w1[:, :, None] ** 2))
+        idx = (n0 + m0 + ell0[:, None, :]) + P0 * (n1 + m1 + ell1[:, :, None])
+        val = (w * v[:, None, None]).ravel()
+        idx = idx.ravel()
+        grid = (np.bincount(idx, val.real, P0 * P1) + 1j * np.bincount(idx, val.imag, P0 * P1))
+        grid = grid.reshape(P1, P0)
+        # wrap2d (adjoint): fold the padding into the periodic 2n grid
+        core = np.zeros((2 * n1, 2 * n0), dtype=np.complex128)
+        yy = (np.arange(P1) - m1) % (2 * n1)
+        xx = (np.arange(P0) - m0) % (2 * n0)
+        np.add.at(core, (yy[:, None], xx[None, :]), grid)
+        grid = np.zeros((P1, P0), dtype=np.complex128)
+        grid[m1:m1 + 2 * n1, m0:m0 + 2 * n0] = core
+        grid *= _checker(P0, P1)
+        inner = grid[m1:m1 + 2 * n1, m0:m0 + 2 * n0]
+        grid[m1:m1 + 2 * n1, m0:m0 + 2 * n0] = np.fft.ifft2(inner) * (4 * n0 * n1)
+        grid *= _checker(P0, P1)
+        # divker2d (direction 1): f[ty][slab][tx] with the n1-ty-1 row flip
+        ty = np.arange(n1)[:, None]
+        txo = np.arange(n0)[None, :]
+        ker = np.exp(-mu0 * (txo - n0 // 2) ** 2 - mu1 * (ty - n1 // 2) ** 2)
+        gv = grid[n1 - ty - 1 + n1 // 2 + m1, txo + n0 // 2 + m0]
+        out[:, r, :] = gv / ker / (n0 * n1)
+    return out
+
+
+def usfft1d_adj64(s2, phi, rh, deth):
+    """s2 [n1, deth/2+1, n0] -> f [n1, rh, n0] real (usfft1d.adj along the height)."""
+    n1, hc, n0 = s2.shape
+    n2 = rh
+    mu2, m2 = _usfft_params(n2)
+    P2 = 2 * n2 + 2 * m2
+    tz = np.arange(deth)
+    z = (tz - deth / 2.0) / deth * np.sin(phi)
+    tzs = np.where(tz > deth // 2, deth - tz, tz)
+    conj = np.where(tz > deth // 2, -1.0, 1.0)
+    g = s2[:, tzs, :]                                  # [n1, deth, n0]
+    g = g.real + 1j * (g.imag * conj[None, :, None])
+    i2 = np.arange(2 * m2 + 1)
+    ell2 = np.floor(2 * n2 * z).astype(np.int64)[:, None] - m2 + i2[None, :]   # [deth, 2m2+1]
+    w = np.sqrt(np.pi / (mu2 * n0)) * np.exp(-np.pi ** 2 / mu2 * (ell2 / (2.0 * n2) - z[:, None]) ** 2)
+    grid = np.zeros((n1, P2, n0), dtype=np.complex128)
+    for t in range(deth):
+        for j in range(2 * m2 + 1):
+            grid[:, n2 + m2 + ell2[t, j], :] += w[t, j] * g[:, t, :]
+    core = np.zeros((n1, 2 * n2, n0), dtype=np.complex128)
+    zz = (np.arange(P2) - m2) % (2 * n2)
+    for k in range(P2):
+        core[:, zz[k], :] += grid[:, k, :]
+    grid[:] = 0
+    grid[:, m2:m2 + 2 * n2, :] = core
+    s = (1 - 2 * ((np.arange(P2) + 1) % 2)).astype(np.float64)[None, :, None]
+    grid *= s
+    grid[:, m2:m2 + 2 * n2, :] = np.fft.ifft(grid[:, m2:m2 + 2 * n2, :], axis=1) * (2 * n2)
+    grid *= s
+    tzo = np.arange(n2)
+    ker = np.exp(-mu2 * (tzo - n2 // 2) ** 2)
+    return grid[:, tzo + n2 // 2 + m2, :].real / ker[None, :, None] / (2 * n2)
+
+
+def rec_lam64(data, theta, center, lamino_angle, rh, wfilter):
+    """FP64 laminographic reconstruction [rh, detw, detw] of data [ntheta, deth, detw]."""
+    ntheta, deth, detw = data.shape
+    phi = np.pi / 2 + lamino_angle / 180 * np.pi
+    filt = fbp_filter_center(np.asarray(data, np.float64), wfilter, center, 0.0, np.float64)
+    s1 = fft2d64(filt)
+    s2 = usfft2d_adj64(s1, theta, phi, detw)
+    s3 = usfft1d_adj64(s2, phi, rh, deth)
+    return np.ascontiguousarray(s3.transpose(1, 0, 2))

@@ -140,3 +140,49 @@ def test_rec_lam_fp16_storage_vs_fp32(cuda):
     err = rel_l2(out["mixed"], out["float32"])
     assert torch.isfinite(out["mixed"]).all()
     assert err < 1e-3, err
+
+
+@pytest.fixture(scope="module")
+def lam_case():
+    from oracle import np_tomo
+    ntheta, deth, detw, rh = 90, 96, 128, 48
+    rng = np.random.default_rng(5)
+    data = rng.standard_normal((ntheta, deth, detw)).astype(np.float32)
+    theta = (np.arange(ntheta) * 2 * np.pi / ntheta).astype(np.float32)
+    wf = np_tomo.calc_filter(4 * detw, "shepp")
+    want = np_tomo.rec_lam64(data, theta, detw / 2, TILT, rh, wf)
+    return data, theta, wf, want, (ntheta, deth, detw, rh)
+
+
+def _ours_lam(data, theta, sizes, dtype):
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.reconstruction.backproj_lamfourier_parallel import \
+        BackprojLamFourierParallel
+    ntheta, deth, detw, rh = sizes
+    global_vars.reset(lamino_angle=TILT, reconstruction_algorithm="fourierrec",
+                      nsino_per_chunk=8, nproj_per_chunk=8, fbp_filter="shepp", dtype=dtype)
+    params.n, params.nz, params.nproj, params.ncproj, params.ncz = detw, deth, ntheta, 8, 8
+    params.rh, params.center, params.theta, params.lamino_angle = rh, detw / 2, theta, TILT
+    return BackprojLamFourierParallel().rec_lam(torch.as_tensor(data, device="cuda")).cpu()
+
+
+def test_rec_lam_vs_fp64_oracle(cuda, ref, lam_case):
+    """Error statement of the laminography chain against the FP64 restatement:
+    ours fp32, the reference build, and ours with fp16 stage storage."""
+    data, theta, wf, want, sizes = lam_case
+    want = torch.as_tensor(want)
+    ours = _ours_lam(data, theta, sizes, "float32")
+    mixed = _ours_lam(data, theta, sizes, "mixed")
+    ntheta, deth, detw, rh = sizes
+    theirs = ref.ref_rec_lam(torch.as_tensor(data, device="cuda"),
+                             torch.as_tensor(theta, device="cuda"), detw / 2, TILT, rh,
+                             torch.as_tensor(wf, device="cuda"), nthetac=8, dethc=8,
+                             n1c=8).cpu()
+    e_ours, e_ref, e_mixed = rel_l2(ours, want), rel_l2(theirs, want), rel_l2(mixed, want)
+    print(f"lamino rel-L2 vs FP64: ours {e_ours:.3e}, reference {e_ref:.3e}, "
+          f"fp16 storage {e_mixed:.3e}")
+    # measured on B200: 5.8e-6, 5.8e-6, 2.9e-4
+    assert e_ours < 2e-5, e_ours
+    assert e_ref < 2e-5, e_ref
+    assert e_mixed < 1e-3, e_mixed
