@@ -436,6 +436,48 @@ def run_lamino(a, dev):
     return res
 
 
+def run_methods(a, data, dark, flat, theta, dev):
+    """The rest of the production configuration, fp32 drop-in path, frames resident:
+    fourierrec with Fourier-wavelet ring removal (level 7, sigma 1, sym16) on the
+    whole volume, and lprec / linerec on a bounded slab of rows."""
+    import torch
+    from tomocupy_b200 import _lib, global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.processing.proc_functions import darkflat_stats
+    from tomocupy_b200.rec import GPURec
+    res = {}
+    legs = [("fourierrec+fw", "fourierrec", a.nz, dict(remove_stripe_method="fw", fw_sigma=1.0,
+                                                         fw_filter="sym16", fw_level=7)),
+            ("lprec", "lprec", min(a.nz, a.slab_rows), {}),
+            ("linerec", "linerec", min(a.nz, a.slab_rows), {})]
+    for name, alg, rows, extra in legs:
+        d, dk, fl = data[:, :rows], dark[:, :rows], flat[:, :rows]
+        global_vars.reset(reconstruction_algorithm=alg, fbp_filter=a.filter,
+                          nsino_per_chunk=a.ncz, **extra)
+        rec = GPURec(ArrayReader(d, dk, fl, theta=theta), ArrayWriter(device=dev), device=dev)
+        d0, f0, _ = darkflat_stats(dk, fl)
+        out = torch.empty((params.nz, params.n, params.n), dtype=torch.float32, device=dev)
+        rec.recon_device(d, d0, f0, out)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rec.recon_device(d, d0, f0, out)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        _lib.profile_enable(True)
+        rec.recon_device(d, d0, f0, out)
+        stages = _lib.profile_report()
+        _lib.profile_enable(False)
+        res[name] = {"rows": rows, "ms": round(ms, 2), "unit": "GUPS",
+                     "value": round(float(a.n) ** 2 * rows * a.nproj / (ms / 1e3) / 1e9, 2),
+                     "stages_ms": {k: round(v["ms"], 2) for k, v in stages.items()}}
+        del rec, out
+        torch.cuda.empty_cache()
+    return res
+
+
 def run_ours(a, ws, rank, local):
     import torch
     from tomocupy_b200.global_vars import params
@@ -484,6 +526,10 @@ def run_ours(a, ws, rank, local):
                 "roofline_tc_filter": _roofline(mst, a, peaks, peaks_kind, "tc_filter"),
                 "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in st2.items()}}
 
+    methods = None
+    if not a.no_methods and ws == 1:
+        methods = run_methods(a, data, dark, flat, theta, dev)
+
     # ---------------- e2e through the public driver with host buffers
     e2e = None
     if not a.no_e2e:
@@ -529,6 +575,7 @@ def run_ours(a, ws, rank, local):
             "clocks": clocks, "gpu_launches": launches,
             "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in stages.items()},
             other if other == "mixed" else "fp32": side,
+            "methods": methods,
             "try_center": trycenter,
             "serving": serving,
             "lamino": lamino,
@@ -699,6 +746,10 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-ncz", type=int, default=16)
     ap.add_argument("--no-lamino", action="store_true", help="skip the laminography leg")
+    ap.add_argument("--no-methods", action="store_true",
+                    help="skip ring removal / lprec / linerec legs")
+    ap.add_argument("--slab-rows", type=int, default=256,
+                    help="rows of the lprec and linerec legs")
     ap.add_argument("--lam-n", type=int, default=1024)
     ap.add_argument("--lam-nproj", type=int, default=1200)
     ap.add_argument("--lam-rh", type=int, default=512)

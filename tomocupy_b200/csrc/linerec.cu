@@ -96,6 +96,115 @@ __global__ void __launch_bounds__(BX *BY)
   *o = from_f32<T>(ld(o) + f0 * c);
 }
 
+// FULL mode, ZS consecutive slices per thread, sinogram footprints staged in
+// shared memory.  For each angle the CTA's 32 x 8 x ZS voxels read detector
+// samples u in a window of at most 32|cos| + 8|sin| + 2 and, in tomography
+// (cos(phi) ~ 0), rows vr in [tz0 + sz - 1, tz0 + sz + ZS]; a box of UW x VR
+// samples per angle is loaded cooperatively for AC angles at a time.  Every
+// voxel evaluates exactly the expressions of backproject_kernel (u, v, their
+// truncation and weights) and reads the same sinogram values -- from the box
+// when inside it, from global memory otherwise -- so the sums are
+// bit-identical for any geometry; only the speed depends on the box holding
+// the samples (tomography).
+constexpr int ZS = 4;
+constexpr int UW = 48, VR = ZS + 2, AC = 32;
+template <typename T>
+__global__ void __launch_bounds__(BX *BY)
+    backproject_full_zs(T *__restrict__ f, const T *__restrict__ data,
+                        const float *__restrict__ theta, float phi, float c, int sz, int ncz,
+                        int n, int nz, int nproj) {
+  __shared__ float s_c[AC], s_s[AC];
+  __shared__ int s_u0[AC], s_v0[AC];
+  __shared__ float box[AC][VR][UW];
+  const int tx = blockIdx.x * BX + threadIdx.x;
+  const int ty = blockIdx.y * BY + threadIdx.y;
+  const int tz0 = blockIdx.z * ZS;
+  const bool active = tx < n && ty < n;
+  const float cphi = __cosf(phi);
+  const float sphi = __sinf(phi);
+  float acc[ZS];
+#pragma unroll
+  for (int s = 0; s < ZS; s++) acc[s] = 0.f;
+  const int tid = threadIdx.y * BX + threadIdx.x;
+  const int x0 = blockIdx.x * BX - n / 2, y0 = blockIdx.y * BY - n / 2;
+  for (int t0 = 0; t0 < nproj; t0 += AC) {
+    const int cnt = min(AC, nproj - t0);
+    __syncthreads();
+    if (tid < cnt) {
+      float th = theta[t0 + tid];
+      float ct = __cosf(th), st = __sinf(th);
+      s_c[tid] = ct;
+      s_s[tid] = st;
+      // smallest u of the tile's corners, one sample of margin
+      float umin = fminf(fminf(ct * x0 + st * y0, ct * (x0 + BX - 1) + st * y0),
+                         fminf(ct * x0 + st * (y0 + BY - 1),
+                               ct * (x0 + BX - 1) + st * (y0 + BY - 1))) + n / 2;
+      s_u0[tid] = (int)floorf(umin) - 1;
+      s_v0[tid] = tz0 + sz - 1;
+    }
+    __syncthreads();
+    // stage the boxes: cnt x VR rows of UW samples (zeros outside the sinogram)
+    for (int e = tid; e < cnt * VR * UW; e += BX * BY) {
+      const int a = e / (VR * UW), r = (e / UW) % VR, w = e % UW;
+      const int uu = s_u0[a] + w, vv = s_v0[a] + r;
+      float val = 0.f;
+      if (uu >= 0 && uu < n && vv >= 0 && vv < nz)
+        val = ld(data + uu + (size_t)(t0 + a) * n + (size_t)vv * n * nproj);
+      box[a][r][w] = val;
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (int k = 0; k < cnt; k++) {
+      const int t = t0 + k;
+      float ctheta = s_c[k];
+      float stheta = s_s[k];
+      float R0 = ctheta, R1 = stheta;
+      float R3 = stheta * cphi, R4 = -ctheta * cphi, R5 = sphi;
+      float u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2;
+      int ur = (int)(u - 1e-5f);
+      if (!((ur >= 0) & (ur < n - 1))) continue;
+      u = u - ur;
+      const int bu = ur - s_u0[k];
+      const bool uin = (bu >= 0) & (bu < UW - 1);
+#pragma unroll
+      for (int s = 0; s < ZS; s++) {
+        const int tz = tz0 + s;
+        const int zz = tz + sz - nz / 2;
+        float v = R3 * (tx - n / 2) + R4 * (ty - n / 2) + R5 * zz + nz / 2;
+        int vr = (int)(v - 1e-5f);
+        if ((tz < ncz) & (vr >= 0) & (vr < nz - 1)) {
+          v = v - vr;
+          const int bv = vr - s_v0[k];
+          float x00, x01, x10, x11;
+          if (uin & (bv >= 0) & (bv < VR - 1)) {
+            x00 = box[k][bv][bu];
+            x01 = box[k][bv][bu + 1];
+            x10 = box[k][bv + 1][bu];
+            x11 = box[k][bv + 1][bu + 1];
+          } else {
+            const T *d0 = data + ur + (size_t)t * n + (size_t)vr * n * nproj;
+            const T *d1 = d0 + (size_t)n * nproj;
+            x00 = ld(d0);
+            x01 = ld(d0 + 1);
+            x10 = ld(d1);
+            x11 = ld(d1 + 1);
+          }
+          acc[s] += x00 * ((1 - u) * (1 - v)) + x01 * ((0 + u) * (1 - v)) +
+                    x10 * ((1 - u) * (0 + v)) + x11 * ((0 + u) * (0 + v));
+        }
+      }
+    }
+  }
+  if (!active) return;
+#pragma unroll
+  for (int s = 0; s < ZS; s++) {
+    const int tz = tz0 + s;
+    if (tz >= ncz) break;
+    T *o = f + tx + (size_t)(n - ty - 1) * n + (size_t)tz * n * n;
+    *o = from_f32<T>(ld(o) + acc[s] * c);
+  }
+}
+
 template <typename T>
 int launch(tcb_linerec *h, int mode, void *f, const void *g, const float *theta,
            float phi, const float *phi_v, const float *sh, int sz, cudaStream_t s) {
@@ -105,10 +214,12 @@ int launch(tcb_linerec *h, int mode, void *f, const void *g, const float *theta,
   float c = 4.0f / h->nproj;
   int n = (int)h->n, nz = (int)h->nz, ncz = (int)h->ncz, np = (int)h->ncproj;
   switch (mode) {
-    case FULL:
-      backproject_kernel<T, FULL><<<grd, blk, 0, s>>>((T *)f, (const T *)g, theta, phi,
-                                                      nullptr, nullptr, c, sz, ncz, n, nz, np);
+    case FULL: {
+      dim3 grz(ceil_div(h->n, BX), ceil_div(h->n, BY), ceil_div(h->ncz, ZS));
+      backproject_full_zs<T><<<grz, blk, 0, s>>>((T *)f, (const T *)g, theta, phi, c, sz, ncz,
+                                                  n, nz, np);
       break;
+    }
     case TRY:
       backproject_kernel<T, TRY><<<grd, blk, 0, s>>>((T *)f, (const T *)g, theta, phi,
                                                      nullptr, sh, c, sz, ncz, n, nz, np);

@@ -44,10 +44,29 @@ __device__ __forceinline__ int reflect(int m, int n) {
   return m >= n ? p - 1 - m : m;
 }
 
+// The filter-bank kernels keep the reference's per-tap operation order
+// (round-to-nearest multiply then add, tap by tap), so results are
+// bit-identical; the taps live in shared memory and the symmetric reflection
+// is only evaluated for outputs whose support crosses an edge.
+struct SmemTaps {
+  float a[MAXL], b[MAXL];
+};
+
+__device__ __forceinline__ void load_taps(SmemTaps &st, const float *a, const float *b, int L) {
+  for (int k = threadIdx.x + threadIdx.y * blockDim.x; k < L; k += blockDim.x * blockDim.y) {
+    st.a[k] = a[k];
+    st.b[k] = b[k];
+  }
+  __syncthreads();
+}
+
 // afb1d along the last axis: x [B][H][W] (row stride sx, slice stride sz) ->
 // out [B][2][H][Wo] (lo, hi).
 __global__ void afb_rows(const float *__restrict__ x, long long sz, int sx, float *__restrict__ out,
                          int B, int H, int W, int Wo, int padl, const Taps *__restrict__ taps) {
+  __shared__ SmemTaps st;
+  const int L = taps->L;
+  load_taps(st, taps->h0, taps->h1, L);
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = (long long)B * H * Wo;
   if (idx >= total) return;
@@ -56,16 +75,20 @@ __global__ void afb_rows(const float *__restrict__ x, long long sz, int sx, floa
   int h = (int)(r % H);
   int b = (int)(r / H);
   const float *row = x + b * sz + (long long)h * sx;
-  const int L = taps->L;
-  float lo = 0.f, hi = 0.f;
-  for (int k = 0; k < L; k++) {
-    float v = row[reflect(2 * j + k - padl, W)];
-    if (k == 0) {
-      lo = __fmul_rn(taps->h0[0], v);
-      hi = __fmul_rn(taps->h1[0], v);
-    } else {
-      lo = __fadd_rn(lo, __fmul_rn(taps->h0[k], v));
-      hi = __fadd_rn(hi, __fmul_rn(taps->h1[k], v));
+  const int base = 2 * j - padl;
+  float v = row[base >= 0 && base < W ? base : reflect(base, W)];
+  float lo = __fmul_rn(st.a[0], v), hi = __fmul_rn(st.b[0], v);
+  if (base >= 0 && base + L <= W) {
+    for (int k = 1; k < L; k++) {
+      v = row[base + k];
+      lo = __fadd_rn(lo, __fmul_rn(st.a[k], v));
+      hi = __fadd_rn(hi, __fmul_rn(st.b[k], v));
+    }
+  } else {
+    for (int k = 1; k < L; k++) {
+      v = row[reflect(base + k, W)];
+      lo = __fadd_rn(lo, __fmul_rn(st.a[k], v));
+      hi = __fadd_rn(hi, __fmul_rn(st.b[k], v));
     }
   }
   long long o = (((long long)b * 2) * H + h) * Wo + j;
@@ -77,6 +100,9 @@ __global__ void afb_rows(const float *__restrict__ x, long long sz, int sx, floa
 // out [B][4][Ho][W] (channel c -> 2c lo, 2c+1 hi).
 __global__ void afb_cols(const float *__restrict__ in, float *__restrict__ out, int B, int H,
                          int W, int Ho, int padl, const Taps *__restrict__ taps) {
+  __shared__ SmemTaps st;
+  const int L = taps->L;
+  load_taps(st, taps->h0, taps->h1, L);
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = (long long)B * 2 * Ho * W;
   if (idx >= total) return;
@@ -85,16 +111,21 @@ __global__ void afb_cols(const float *__restrict__ in, float *__restrict__ out, 
   int i = (int)(r % Ho);
   long long bc = r / Ho;  // b*2 + c
   const float *col = in + bc * H * W + j;
-  const int L = taps->L;
-  float lo = 0.f, hi = 0.f;
-  for (int k = 0; k < L; k++) {
-    float v = col[(long long)reflect(2 * i + k - padl, H) * W];
-    if (k == 0) {
-      lo = __fmul_rn(taps->h0[0], v);
-      hi = __fmul_rn(taps->h1[0], v);
-    } else {
-      lo = __fadd_rn(lo, __fmul_rn(taps->h0[k], v));
-      hi = __fadd_rn(hi, __fmul_rn(taps->h1[k], v));
+  const int base = 2 * i - padl;
+  float v = col[(long long)(base >= 0 && base < H ? base : reflect(base, H)) * W];
+  float lo = __fmul_rn(st.a[0], v), hi = __fmul_rn(st.b[0], v);
+  if (base >= 0 && base + L <= H) {
+    const float *c0 = col + (long long)base * W;
+    for (int k = 1; k < L; k++) {
+      v = c0[(long long)k * W];
+      lo = __fadd_rn(lo, __fmul_rn(st.a[k], v));
+      hi = __fadd_rn(hi, __fmul_rn(st.b[k], v));
+    }
+  } else {
+    for (int k = 1; k < L; k++) {
+      v = col[(long long)reflect(base + k, H) * W];
+      lo = __fadd_rn(lo, __fmul_rn(st.a[k], v));
+      hi = __fadd_rn(hi, __fmul_rn(st.b[k], v));
     }
   }
   long long b = bc / 2, c = bc % 2;
@@ -109,6 +140,9 @@ __global__ void afb_cols(const float *__restrict__ in, float *__restrict__ out, 
 // [B][2][Ho][W], Ho = 2 Hi - L + 2.
 __global__ void sfb_cols(const float *__restrict__ y, long long bstride, int Hi, int Wb, int W,
                          float *__restrict__ out, int B, int Ho, const Taps *__restrict__ taps) {
+  __shared__ SmemTaps st;
+  const int L = taps->L;
+  load_taps(st, taps->g0, taps->g1, L);
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = (long long)B * 2 * Ho * W;
   if (idx >= total) return;
@@ -117,7 +151,6 @@ __global__ void sfb_cols(const float *__restrict__ y, long long bstride, int Hi,
   int t = (int)(r % Ho);
   long long bc = r / Ho;
   int b = (int)(bc / 2), c = (int)(bc % 2);
-  const int L = taps->L;
   const long long plane = (long long)Hi * Wb;
   const float *base = y + b * bstride;
   const float *lo = base + (c == 0 ? 0 : 2) * plane + j;  // LL or band1 (HL)
@@ -127,8 +160,8 @@ __global__ void sfb_cols(const float *__restrict__ y, long long bstride, int Hi,
   for (int k = tt & 1; k < L; k += 2) {
     int h = (tt - k) >> 1;
     if (h < 0 || h >= Hi) continue;
-    float v = __fadd_rn(__fmul_rn(taps->g0[k], lo[(long long)h * Wb]),
-                        __fmul_rn(taps->g1[k], hi[(long long)h * Wb]));
+    float v = __fadd_rn(__fmul_rn(st.a[k], lo[(long long)h * Wb]),
+                        __fmul_rn(st.b[k], hi[(long long)h * Wb]));
     acc = __fadd_rn(acc, v);
   }
   out[(bc * Ho + t) * W + j] = acc;
@@ -139,6 +172,9 @@ __global__ void sfb_cols(const float *__restrict__ y, long long bstride, int Hi,
 __global__ void sfb_rows(const float *__restrict__ in, int H, int Wi, float *__restrict__ dst,
                          long long dsz, int dsx, int Hd, int Wd, int B,
                          const Taps *__restrict__ taps) {
+  __shared__ SmemTaps st;
+  const int L = taps->L;
+  load_taps(st, taps->g0, taps->g1, L);
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = (long long)B * Hd * Wd;
   if (idx >= total) return;
@@ -146,7 +182,6 @@ __global__ void sfb_rows(const float *__restrict__ in, int H, int Wi, float *__r
   long long r = idx / Wd;
   int h = (int)(r % Hd);
   int b = (int)(r / Hd);
-  const int L = taps->L;
   const float *lo = in + (((long long)b * 2) * H + h) * Wi;
   const float *hi = lo + (long long)H * Wi;
   int tt = w + L - 2;
@@ -154,7 +189,7 @@ __global__ void sfb_rows(const float *__restrict__ in, int H, int Wi, float *__r
   for (int k = tt & 1; k < L; k += 2) {
     int q = (tt - k) >> 1;
     if (q < 0 || q >= Wi) continue;
-    float v = __fadd_rn(__fmul_rn(taps->g0[k], lo[q]), __fmul_rn(taps->g1[k], hi[q]));
+    float v = __fadd_rn(__fmul_rn(st.a[k], lo[q]), __fmul_rn(st.b[k], hi[q]));
     acc = __fadd_rn(acc, v);
   }
   dst[b * dsz + (long long)h * dsx + w] = acc;
@@ -322,7 +357,6 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
   TCB_CHECK_ARG(sino, "tcb_stripe_fw_apply_sino: null pointer");
   TCB_CHECK_ARG(sstride >= (size_t)h->nproj_pad * h->ni, "tcb_stripe_fw_apply_sino: stride");
   cudaStream_t s = (cudaStream_t)stream;
-  StageTimer st("stripe_fw", s);
   const int B = h->nz, L = h->L;
   // forward
   for (int k = 0; k < h->level; k++) {
@@ -341,12 +375,20 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     }
     int pw = 2 * (Wo - 1) - Wk + L, ph = 2 * (Ho - 1) - Hk + L;
     long long n1 = (long long)B * Hk * Wo;
-    afb_rows<<<ceil_div(n1, 256), 256, 0, s>>>(x, xsz, xsx, h->tmp, B, Hk, Wk, Wo, pw / 2,
-                                               h->taps);
+    {
+      StageTimer st("fw_afb_rows", s);
+      afb_rows<<<ceil_div(n1, 256), 256, 0, s>>>(x, xsz, xsx, h->tmp, B, Hk, Wk, Wo, pw / 2,
+                                                 h->taps);
+    }
     TCB_LAUNCH_CHECK();
     long long n2 = (long long)B * 2 * Ho * Wo;
-    afb_cols<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, h->Y[k], B, Hk, Wo, Ho, ph / 2, h->taps);
+    {
+      StageTimer st("fw_afb_cols", s);
+      afb_cols<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, h->Y[k], B, Hk, Wo, Ho, ph / 2,
+                                                 h->taps);
+    }
     TCB_LAUNCH_CHECK();
+    StageTimer std_("fw_damp", s);
     // damp band 1 (index 2 of the level: high-pass along the detector, low-pass along angles)
     float *band = h->Y[k] + 2LL * Ho * Wo;
     dim3 tb(32, 8);
@@ -371,8 +413,11 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     int Hi = h->H[k + 1], Wi = h->W[k + 1];
     int Hc = 2 * Hi - L + 2;  // rows after the column synthesis
     long long n1 = (long long)B * 2 * Hc * Wi;
-    sfb_cols<<<ceil_div(n1, 256), 256, 0, s>>>(h->Y[k], 4LL * Hi * Wi, Hi, Wi, Wi, h->tmp, B,
-                                               Hc, h->taps);
+    {
+      StageTimer st("fw_sfb_cols", s);
+      sfb_cols<<<ceil_div(n1, 256), 256, 0, s>>>(h->Y[k], 4LL * Hi * Wi, Hi, Wi, Wi, h->tmp, B,
+                                                 Hc, h->taps);
+    }
     TCB_LAUNCH_CHECK();
     // reconstruction of level k's input, cropped to its size, into the LL
     // channel of the level above (or into the sinograms)
@@ -388,6 +433,7 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     }
     int Hrows = std::min(Hd, Hc);
     long long n2 = (long long)B * Hrows * Wd;
+    StageTimer st("fw_sfb_rows", s);
     sfb_rows<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, Hc, Wi, dst, dsz, Wd, Hrows, Wd, B,
                                                h->taps);
     TCB_LAUNCH_CHECK();
