@@ -534,6 +534,10 @@ def run_ours(a, ws, rank, local):
     e2e = None
     if not a.no_e2e:
         e2e = run_e2e(a, data, dark, flat, theta, dev, ws, rank)
+        if side is not None and ws == 1:
+            # the mixed path end to end, with fp16 output slices (half the D2H bytes)
+            side["e2e_fp16_out"] = run_e2e(a, data, dark, flat, theta, dev, ws, rank,
+                                           precision="mixed", out_dtype="float16")
 
     base = None
     if rank == 0 and ws == 1 and not a.no_cpu:
@@ -583,7 +587,7 @@ def run_ours(a, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def run_e2e(a, data, dark, flat, theta, dev, ws, rank):
+def run_e2e(a, data, dark, flat, theta, dev, ws, rank, precision=None, out_dtype="float32"):
     import torch
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
@@ -595,16 +599,18 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank):
                 avail = int(ln.split()[1]) * 1024
     except OSError:
         pass
-    full_bytes = data.numel() * 2 + a.nz * a.n * a.n * 4
+    osz = 2 if out_dtype == "float16" else 4
+    full_bytes = data.numel() * 2 + a.nz * a.n * a.n * osz
     nz_e2e = a.nz if (avail > 3 * full_bytes * ws) else min(a.nz, a.e2e_slab)
     nz_e2e -= nz_e2e % a.ncz
     d_host = data[:, :nz_e2e].cpu().pin_memory()
     dk_host = dark[:, :nz_e2e].cpu().pin_memory()
     fl_host = flat[:, :nz_e2e].cpu().pin_memory()
     global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
-                      nsino_per_chunk=a.ncz, dtype=a.precision)
+                      nsino_per_chunk=a.ncz, dtype=precision or a.precision, out_dtype=out_dtype)
     reader = ArrayReader(d_host, dk_host, fl_host, theta=theta)
-    writer = ArrayWriter(device="cpu", pin=True)
+    writer = ArrayWriter(device="cpu", pin=True,
+                         dtype=torch.float16 if out_dtype == "float16" else torch.float32)
     rec = GPURec(reader, writer, device=dev)
     for _ in range(max(1, min(a.warmup, 2))):
         rec.recon_all()
@@ -621,11 +627,12 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank):
     ms = barrier_max(ev0.elapsed_time(ev1) / a.steps, ws)
     vox = float(a.n) ** 2 * nz_e2e * a.nproj
     h2d = d_host.numel() * 2 + dk_host.numel() * 2 + fl_host.numel() * 2
-    d2h = nz_e2e * a.n * a.n * 4
+    d2h = nz_e2e * a.n * a.n * osz
     return {"value": round(ws * vox / (ms / 1e3) / 1e9, 2), "unit": "GUPS",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "rows": nz_e2e, "ms_per_step": round(ms, 2), "wall_ms_per_step": round(wall * 1e3, 2),
-            "api": "GPURec.recon_all (pinned host frames -> pinned host volume)"}
+            "api": "GPURec.recon_all (pinned host frames -> pinned host volume)",
+            "precision": precision or a.precision, "out_dtype": out_dtype}
 
 
 def run_reference(a, ws, rank, local):

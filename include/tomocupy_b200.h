@@ -232,6 +232,10 @@ int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs);
 #define TCB_GRID_FP32 0
 #define TCB_GRID_TENSOR 1
 int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode);
+/* Output precision (no reference counterpart): TCB_FLOAT16 writes the
+ * reconstructed slices in fp16 while the input g stays fp32 (a FLOAT16 handle
+ * has fp16 input and output). */
+int tcb_fourierrec_set_output(tcb_fourierrec *h, int precision);
 int tcb_fourierrec_status(tcb_fourierrec *h, int *timed_out);
 int tcb_fourierrec_destroy(tcb_fourierrec *h);
 

@@ -68,14 +68,16 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
 
 
 def run_ours(data, dark, flat, theta, algorithm="fourierrec", ncz=8, host=True,
-             dtype="float32"):
+             dtype="float32", out_dtype="float32"):
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
-    global_vars.reset(reconstruction_algorithm=algorithm, nsino_per_chunk=ncz, dtype=dtype)
+    global_vars.reset(reconstruction_algorithm=algorithm, nsino_per_chunk=ncz, dtype=dtype,
+                      out_dtype=out_dtype)
     dev = "cpu" if host else "cuda"
     reader = ArrayReader(data.to(dev), dark.to(dev), flat.to(dev), theta=theta, pin=host)
-    writer = ArrayWriter(device=dev, pin=host)
+    writer = ArrayWriter(device=dev, pin=host,
+                         dtype=torch.float16 if out_dtype == "float16" else torch.float32)
     GPURec(reader, writer).recon_all()
     return writer.rec.cpu()
 
@@ -234,3 +236,17 @@ def test_recon_try_mixed_matches_fp32(cuda, c1):
     for k in res["mixed"]:
         err = rel_l2(res["mixed"][k], res["float32"][k])
         assert err < 1e-4, (k, err)
+
+
+def test_c1_mixed_fp16_output_vs_fp64_oracle(cuda, c1):
+    """Mixed precision with fp16 output slices (half the device-to-host bytes)."""
+    data, dark, flat, theta, _ = c1
+    d, dk, fl = data[:, :4], dark[:, :4], flat[:, :4]
+    out16 = run_ours(d, dk, fl, theta, ncz=4, dtype="mixed", out_dtype="float16")
+    out32 = run_ours(d, dk, fl, theta, ncz=4, dtype="mixed")
+    assert out16.dtype == torch.float16
+    want = _fp64_fourierrec(d, dk, fl, theta, N)
+    e16 = rel_l2(out16.float().numpy(), want)
+    assert e16 < 1e-3, e16
+    # the fp16 rounding of the output is the only difference
+    assert rel_l2(out16.float(), out32) < 5e-4

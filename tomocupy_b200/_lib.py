@@ -79,6 +79,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_fourierrec_set_pairs_per_block": [vp, i32],
     "tcb_fourierrec_set_gridding": [vp, i32],
     "tcb_fourierrec_status": [vp, C.POINTER(i32)],
+    "tcb_fourierrec_set_output": [vp, i32],
     "tcb_fourierrec_destroy": [vp],
     "tcb_linerec_create": [C.POINTER(vp), sz, sz, sz, sz, sz, i32],
     "tcb_linerec_backprojection": [vp, vp, vp, vp, f32, i32, vp],

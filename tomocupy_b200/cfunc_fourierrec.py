@@ -51,6 +51,11 @@ class cfunc_fourierrec:
         self._check()
         _lib.call("tcb_fourierrec_set_gridding", self._h, int(mode))
 
+    def set_output(self, precision: int) -> None:
+        """_lib.TCB_FLOAT16: fp16 output slices from fp32 input (not in the reference)."""
+        self._check()
+        _lib.call("tcb_fourierrec_set_output", self._h, int(precision))
+
     def timed_out(self) -> bool:
         """True when a tensor-core gridding wait gave up (synchronises)."""
         import ctypes as C

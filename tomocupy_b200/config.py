@@ -16,6 +16,7 @@ DEFAULTS = {
     "reconstruction_algorithm": "fourierrec",  # 'fourierrec' | 'lprec' | 'linerec'
     "fbp_filter": "parzen",
     "dtype": "float32",                     # 'float32' | 'float16' | 'mixed' (tensor-core filter)
+    "out_dtype": "float32",                 # 'float32' | 'float16' output slices (fourierrec)
     "rotation_axis": -1.0,
     "center_search_width": 50.0,
     "center_search_step": 0.5,

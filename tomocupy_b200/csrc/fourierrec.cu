@@ -924,6 +924,7 @@ struct tcb_fourierrec {
   int own_n = 0;
   int zblock = 0;  // pairs per gridding block (2/4/8/16; 0 = largest that fits nz)
   int grid_mode = 0;          // TCB_GRID_FP32 or TCB_GRID_TENSOR
+  bool out_f16 = false;       // fp16 output slices (set_output) with fp32 input
   unsigned *amax = nullptr;   // max |G| bits for the tensor-core gridding scale
   int *recs = nullptr;        // per-sample footprint records (tensor-core gridding)
   int *tc_err = nullptr;      // set by a tensor-core gridding wait that timed out
@@ -1031,8 +1032,9 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     else rc = launch_grid<2>(h, gc, s);
     if (rc != TCB_OK) return rc;
   }
+  const bool out_half = h->precision == TCB_FLOAT16 || h->out_f16;
   if (h->own_n) {
-    const bool half = h->precision == TCB_FLOAT16;
+    const bool half = out_half;
     switch (h->own_n) {
       case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
       case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
@@ -1063,7 +1065,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   {
     StageTimer st("fr_deapod", s);
     dim3 blk(32, 8), grd(ceil_div(h->n, 32), ceil_div(h->n, 8), (unsigned)h->nz);
-    if (h->precision == TCB_FLOAT16)
+    if (out_half)
       deapod_kernel<__half><<<grd, blk, 0, s>>>(h->grid, (__half *)f, geo, unpack);
     else
       deapod_kernel<float><<<grd, blk, 0, s>>>(h->grid, (float *)f, geo, unpack);
@@ -1354,6 +1356,14 @@ extern "C" int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode) {
     TCB_CUDA(cudaDeviceSynchronize());
   }
   h->grid_mode = mode;
+  return TCB_OK;
+}
+
+extern "C" int tcb_fourierrec_set_output(tcb_fourierrec *h, int precision) {
+  TCB_CHECK_ARG(h, "tcb_fourierrec_set_output: null handle");
+  TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
+                "tcb_fourierrec_set_output: unknown precision %d", precision);
+  h->out_f16 = precision == TCB_FLOAT16;
   return TCB_OK;
 }
 

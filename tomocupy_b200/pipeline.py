@@ -41,12 +41,17 @@ from .reconstruction.fbp_filter import calc_filter
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
                  algorithm="fourierrec", minus_log=True, device="cuda", stripe=None,
-                 precision="float32"):
+                 precision="float32", out_dtype="float32"):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if precision not in ("float32", "mixed"):
             raise NotImplementedError(f"SinoPipeline: precision {precision!r}")
         self.precision = precision
+        if out_dtype not in ("float32", "float16"):
+            raise NotImplementedError(f"SinoPipeline: out_dtype {out_dtype!r}")
+        if out_dtype == "float16" and algorithm != "fourierrec":
+            raise NotImplementedError("fp16 output slices: fourierrec only")
+        self.out_dtype = torch.float16 if out_dtype == "float16" else torch.float32
         if algorithm == "fourierrec" and ncz % 2:
             raise ValueError("fourierrec needs an even number of rows per chunk")
         self.device = torch.device(device)
@@ -92,6 +97,8 @@ class SinoPipeline:
                                                         self.theta)
             if precision == "mixed":  # fp16 weights/values, fp32 accumulation in TMEM
                 self.fr.set_gridding(_lib.GRID_TENSOR)
+            if out_dtype == "float16":
+                self.fr.set_output(_lib.TCB_FLOAT16)
             self.g = torch.empty((self.ncz // 2, self.nproj, self.n, 2), dtype=torch.float32,
                                  device=self.device)
         else:
@@ -220,7 +227,8 @@ class SinoPipeline:
         return out
 
     def filter_and_backproject(self, out, sht=None, stream=None):
-        """out [ncz, n, n] float32 (contiguous) from the loaded rows."""
+        """out [ncz, n, n] of self.out_dtype (contiguous) from the loaded rows."""
+        assert out.dtype == self.out_dtype, (out.dtype, self.out_dtype)
         if self.precision == "mixed":
             return self._filter_and_backproject_mixed(out, sht, stream)
         self.filter.filter(self.rows, self.weights(sht), stream)

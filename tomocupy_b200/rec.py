@@ -62,7 +62,8 @@ class GPURec:
                                       params.center, args.fbp_filter,
                                       args.reconstruction_algorithm,
                                       minus_log=args.minus_log == "True", device=self.device,
-                                      stripe=stripe, precision=self.precision)
+                                      stripe=stripe, precision=self.precision,
+                                      out_dtype=args.out_dtype)
         return self._pipe
 
     # ------------------------------------------------------------------ helpers
@@ -94,7 +95,10 @@ class GPURec:
         host_in = data.device.type == "cpu"
         host_out = rec_out.device.type == "cpu"
         dbuf = [torch.empty((nproj, ncz, n), dtype=data.dtype, device=dev) for _ in range(2)]
-        rbuf = [torch.empty((ncz, n, n), dtype=torch.float32, device=dev) for _ in range(2)]
+        odt = self.pipe.out_dtype
+        if rec_out.dtype != odt:
+            raise ValueError(f"writer dtype {rec_out.dtype} != output dtype {odt} (args.out_dtype)")
+        rbuf = [torch.empty((ncz, n, n), dtype=odt, device=dev) for _ in range(2)]
         h2d_done = [torch.cuda.Event() for _ in range(2)]
         comp_done = [torch.cuda.Event() for _ in range(2)]
         d2h_done = [torch.cuda.Event() for _ in range(2)]
@@ -176,7 +180,7 @@ class GPURec:
                 self.pipe.reconstruct(out[z0:z0 + ncz], data[:, z0:z0 + ncz], dark0, flat0,
                                       z_lo=z0, stream=stream)
             else:
-                tmp = torch.empty((ncz, params.n, params.n), dtype=torch.float32,
+                tmp = torch.empty((ncz, params.n, params.n), dtype=out.dtype,
                                   device=out.device)
                 self.pipe.reconstruct(tmp, data[:, z0:z0 + lz], dark0, flat0, z_lo=z0,
                                       stream=stream)
