@@ -329,20 +329,26 @@ def run_serving(a, dev):
             pool[(n, P)] = (d.cpu().pin_memory(), dk.cpu().pin_memory(), fl.cpu().pin_memory(),
                             th)
             del d, dk, fl
-        if n not in outs:
-            outs[n] = torch.empty((64, n, n), dtype=torch.float32, pin_memory=True)
+        for dt in (torch.float32, torch.float16):
+            if (n, dt) not in outs:
+                outs[(n, dt)] = torch.empty((64, n, n), dtype=dt, pin_memory=True)
 
     def make(precision=None):
+        # mixed-precision requests return fp16 volumes, fp32 requests fp32
         reqs = []
         for k, (t, n, P, nz, prec) in enumerate(specs):
             d, dk, fl, th = pool[(n, P)]
-            reqs.append(Request(k, d[:, :nz], dk[:, :nz], fl[:, :nz], th, n / 2,
-                                precision or prec, "parzen", arrival=t, out=outs[n][:nz]))
+            prec = precision or prec
+            odt = "float16" if prec == "mixed" else "float32"
+            out = outs[(n, torch.float16 if odt == "float16" else torch.float32)][:nz]
+            reqs.append(Request(k, d[:, :nz], dk[:, :nz], fl[:, :nz], th, n / 2, prec, "parzen",
+                                arrival=t, out=out, out_dtype=odt))
         return reqs
 
     res = {"workload": f"{len(specs)} requests, Poisson {a.serve_rate}/s (seed {a.seed}), "
                        "n in {512,1024,2048,4096}, nproj in {180,720,1500,3000}, nz U{1..64}, "
-                       "fp32:mixed 1:1, uint16 pinned host frames -> pinned host volumes",
+                       "fp32:mixed 1:1 (mixed requests return fp16 volumes), uint16 pinned host "
+                       "frames -> pinned host volumes",
            "hbm_budget_gb": a.serve_budget_gb}
     srv = Server(dev, hbm_budget=a.serve_budget_gb * 1e9, ncz=a.serve_ncz)
     srv.warm(make())

@@ -49,7 +49,8 @@ class Request:
     precision: str = "float32"    # "float32" | "mixed"
     fbp_filter: str = "parzen"
     arrival: float = 0.0          # seconds after the start of the stream
-    out: torch.Tensor | None = None   # pinned host float32 [nz, n, n] (given or allocated)
+    out: torch.Tensor | None = None   # pinned host [nz, n, n] (given or allocated)
+    out_dtype: str = "float32"    # "float16": fp16 slices (half the result bytes)
     # filled in by the server
     t_admit: float = float("nan")
     t_done: float = float("nan")
@@ -72,7 +73,7 @@ def _geometry_key(req: Request, ncz: int):
     nproj, _, n = req.frames.shape
     th = np.asarray(req.theta, dtype=np.float32)
     return (n, nproj, hash(th.tobytes()), float(req.center), req.fbp_filter, req.precision,
-            ncz)
+            req.out_dtype, ncz)
 
 
 @dataclass
@@ -141,11 +142,12 @@ class Server:
         torch.cuda.synchronize(self.device)
         before = self._free_dev()
         pipe = SinoPipeline(n, nproj, self.ncz, req.theta, req.center, req.fbp_filter,
-                            "fourierrec", device=self.device, precision=req.precision)
-        tmp = [torch.empty((self.ncz, n, n), dtype=torch.float32, device=self.device)
+                            "fourierrec", device=self.device, precision=req.precision,
+                            out_dtype=req.out_dtype)
+        tmp = [torch.empty((self.ncz, n, n), dtype=pipe.out_dtype, device=self.device)
                for _ in range(2)]
         torch.cuda.synchronize(self.device)
-        nb = max(before - self._free_dev(), 2 * tmp[0].numel() * 4)
+        nb = max(before - self._free_dev(), 2 * tmp[0].numel() * tmp[0].element_size())
         g = _Geometry(pipe, tmp, torch.cuda.Stream(self.device), torch.cuda.Stream(self.device),
                       nb)
         self.geoms[key] = g
@@ -207,7 +209,9 @@ class Server:
             ready = torch.cuda.Event()
             ready.record(cs)
         if req.out is None:
-            req.out = torch.empty((nz, n, n), dtype=torch.float32, pin_memory=True)
+            req.out = torch.empty((nz, n, n), pin_memory=True,
+                                  dtype=torch.float16 if req.out_dtype == "float16"
+                                  else torch.float32)
         chunks = [(z0, min(self.ncz, nz - z0)) for z0 in range(0, nz, self.ncz)]
         self.req_bytes += need
         g.users += 1
