@@ -155,22 +155,16 @@ def setup_dist():
 
 
 def barrier_max(t_ms, ws):
+    """Maximum of the ranks' device times (NCCL all-reduce when ws > 1)."""
     import torch
-    if ws == 1:
-        return t_ms
-    import torch.distributed as dist
-    x = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-    dist.all_reduce(x, op=dist.ReduceOp.MAX)
-    return float(x.item())
+    from tomocupy_b200.multigpu import max_over_ranks
+    return max_over_ranks(t_ms, torch.device("cuda", torch.cuda.current_device()))
 
 
 def barrier(ws):
     import torch
-    torch.cuda.synchronize()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
+    from tomocupy_b200.multigpu import barrier as mbarrier
+    mbarrier(torch.device("cuda", torch.cuda.current_device()))
 
 
 def make_data(a, device):
