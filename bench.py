@@ -199,7 +199,7 @@ def _time_path(a, ws, dtype, data, dark, flat, theta, dark0, flat0, out, dev, lo
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
     global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
-                      nsino_per_chunk=a.ncz, dtype=dtype)
+                      nsino_per_chunk=a.ncz, dtype=dtype, **_ring_removal(a))
     rec = GPURec(ArrayReader(data, dark, flat, theta=theta), ArrayWriter(device=dev),
                  device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -222,6 +222,13 @@ def _time_path(a, ws, dtype, data, dark, flat, theta, dark0, flat0, out, dev, lo
     ms_step = barrier_max(ev0.elapsed_time(ev1), ws) / a.steps
     del rec
     return ms_step, stages, launches, clk.summary()
+
+
+def _ring_removal(a):
+    """Options of the Fourier-wavelet ring removal of the production pipeline."""
+    if not a.ring_removal:
+        return {}
+    return dict(remove_stripe_method="fw", fw_sigma=1.0, fw_filter="sym16", fw_level=7)
 
 
 def _roofline(stages, a, peaks, peaks_kind, kernel=None):
@@ -569,7 +576,8 @@ def run_ours(a, ws, rank, local):
             "data": "synthetic",
             "config": {"workload": f"{a.nz} rows x {a.nproj} angles x {a.n} cols uint16 -> "
                                    f"{a.nz}x{a.n}^2 f32 volume; dark/flat, -log, {a.filter} "
-                                   f"filter, {a.algorithm}; ring removal off",
+                                   f"filter, {a.algorithm}; ring removal "
+                                   f"{'fw level 7 sigma 1 sym16' if a.ring_removal else 'off'}",
                        "n": a.n, "nproj": a.nproj, "nz": a.nz, "ncz": a.ncz,
                        "precision": primary,
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
@@ -607,7 +615,8 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank, precision=None, out_dtype
     dk_host = dark[:, :nz_e2e].cpu().pin_memory()
     fl_host = flat[:, :nz_e2e].cpu().pin_memory()
     global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
-                      nsino_per_chunk=a.ncz, dtype=precision or a.precision, out_dtype=out_dtype)
+                      nsino_per_chunk=a.ncz, dtype=precision or a.precision, out_dtype=out_dtype,
+                      **_ring_removal(a))
     reader = ArrayReader(d_host, dk_host, fl_host, theta=theta)
     writer = ArrayWriter(device="cpu", pin=True,
                          dtype=torch.float16 if out_dtype == "float16" else torch.float32)
@@ -753,6 +762,8 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-ncz", type=int, default=16)
     ap.add_argument("--no-lamino", action="store_true", help="skip the laminography leg")
+    ap.add_argument("--ring-removal", action="store_true",
+                    help="main leg with Fourier-wavelet ring removal (level 7, sigma 1, sym16)")
     ap.add_argument("--no-methods", action="store_true",
                     help="skip ring removal / lprec / linerec legs")
     ap.add_argument("--slab-rows", type=int, default=256,
