@@ -308,8 +308,14 @@ int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1, const float *
 /* fp16 storage (no reference counterpart; the reference's laminography path
  * is fp32 only): TCB_FLOAT16 makes the stage-1 spectrum input and the output
  * of adj/adj_rows complex fp16 (__half2) arrays; gridding, FFTs and
- * deapodization compute in fp32. */
-int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision);
+ * deapodization compute in fp32.  in_scale (device, [ntheta], or NULL): the
+ * input of angle t was stored multiplied by 1/in_scale[t] and is multiplied
+ * back on load.  out_inv_scale (device, [rows of the output], or NULL): each
+ * call multiplies its output by a power of two that keeps it below 2^14 and
+ * writes the inverse factor for each of its rows there.  The arrays are the
+ * caller's and must outlive the calls. */
+int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision, const float *in_scale,
+                            float *out_inv_scale);
 int tcb_usfft2d_destroy(tcb_usfft2d *h);
 
 /* Replaces cfunc_usfft1d (src/include/cfunc_usfft1d.cuh:7-34,
@@ -319,8 +325,10 @@ int tcb_usfft2d_destroy(tcb_usfft2d *h);
 typedef struct tcb_usfft1d tcb_usfft1d;
 int tcb_usfft1d_create(tcb_usfft1d **out, size_t n0, size_t n1, size_t n2, size_t deth);
 int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi, void *stream);
-/* fp16 storage of the input g (complex fp16); output and arithmetic fp32. */
-int tcb_usfft1d_set_storage(tcb_usfft1d *h, int precision);
+/* fp16 storage of the input g (complex fp16); output and arithmetic fp32.
+ * in_scale (device, [deth/2+1], or NULL): row r of g is multiplied by
+ * in_scale[r] on load (the out_inv_scale rows written by usfft2d). */
+int tcb_usfft1d_set_storage(tcb_usfft1d *h, int precision, const float *in_scale);
 int tcb_usfft1d_destroy(tcb_usfft1d *h);
 
 #ifdef __cplusplus

@@ -19,9 +19,10 @@ class cfunc_usfft1d(NativeHandle):
         _lib.call("tcb_usfft1d_adj", self._live(), _lib.ptr(f_), _lib.ptr(g_), float(phi),
                   _lib.stream_ptr(stream_))
 
-    def set_storage(self, precision: int) -> None:
-        """Not in the reference: _lib.TCB_FLOAT16 stores the stage arrays in complex fp16."""
-        _lib.call("tcb_usfft1d_set_storage", self._live(), int(precision))
+    def set_storage(self, precision: int, in_scale=None) -> None:
+        """Not in the reference: _lib.TCB_FLOAT16 stores the stage arrays in complex
+        fp16, with optional per-angle / per-row power-of-two scale arrays."""
+        _lib.call("tcb_usfft1d_set_storage", self._live(), int(precision), _lib.ptr(in_scale))
 
     def fwd(self, *a, **k):
         raise NotImplementedError("usfft1d forward is not on the reconstruction path")

@@ -26,9 +26,10 @@ class cfunc_usfft2d(NativeHandle):
                   _lib.ptr(theta), float(phi), int(row0), int(nrows), int(deth_full),
                   _lib.stream_ptr(stream_))
 
-    def set_storage(self, precision: int) -> None:
-        """Not in the reference: _lib.TCB_FLOAT16 stores the stage arrays in complex fp16."""
-        _lib.call("tcb_usfft2d_set_storage", self._live(), int(precision))
+    def set_storage(self, precision: int, in_scale=None, out_inv_scale=None) -> None:
+        """Not in the reference: _lib.TCB_FLOAT16 stores the stage arrays in complex
+        fp16, with optional per-angle / per-row power-of-two scale arrays."""
+        _lib.call("tcb_usfft2d_set_storage", self._live(), int(precision), _lib.ptr(in_scale), _lib.ptr(out_inv_scale))
 
     def fwd(self, *a, **k):
         raise NotImplementedError("usfft2d forward is not on the reconstruction path")

@@ -89,6 +89,7 @@ struct U2Geom {
   int fused;                // 0: packed [2*ntheta][deth][detw/2+1]; 1: full stage-1 array
   int row0;                 // fused: first frequency row of this call
   int deth_full;            // fused: rows of the stage-1 array
+  const float *in_scale;    // fp16 storage: per-angle factor of the input (or null)
 };
 
 struct U2Smem {
@@ -172,13 +173,16 @@ __device__ __forceinline__ float2 u2_val(const U2Geom &g, const S *__restrict__ 
     v.y *= conj;
     return v;
   }
+  const float sc = g.in_scale ? g.in_scale[tz] : 1.f;
   int row = g.row0 + ty;
-  if (tx <= g.detw / 2) return ld2(src + (size_t)tx + (size_t)row * wc + (size_t)tz * wc * g.deth_full);
+  if (tx <= g.detw / 2) {
+    float2 v = ld2(src + (size_t)tx + (size_t)row * wc + (size_t)tz * wc * g.deth_full);
+    return make_float2(v.x * sc, v.y * sc);
+  }
   int mrow = g.deth_full - row;
   if (mrow >= g.deth_full) mrow -= g.deth_full;
   float2 v = ld2(src + (size_t)(g.detw - tx) + (size_t)mrow * wc + (size_t)tz * wc * g.deth_full);
-  v.y = -v.y;
-  return v;
+  return make_float2(v.x * sc, -v.y * sc);
 }
 
 template <int M0, int M1, typename S>
@@ -336,9 +340,33 @@ __global__ void u2_tables(float2 *__restrict__ cs, float *__restrict__ ex, float
 
 // divker2d (direction 1) with the post-FFT fftshift sign; f[ty][slab][tx] layout
 // [n1][fstride_slabs][n0], slab offset fslab0.
+// fp16 storage: the output is multiplied by a power of two chosen from the
+// max |grid| of this call (max_bits), so that |f| < 2^14; the inverse goes to
+// out_inv[fslab0 + slab] for the consumer.
+__device__ __forceinline__ float out_factor(const unsigned *max_bits, int n0, int n1) {
+  if (!max_bits) return 1.f;
+  // |f| <= max|grid| / ker / (n0 n1) with 1/ker < 8 (ker >= eps^(1/4))
+  float bound = __uint_as_float(*max_bits) * 8.f / ((float)n0 * (float)n1);
+  int e = 0;
+  if (bound > 0.f) frexpf(bound, &e);
+  return ldexpf(1.f, 14 - e);
+}
+
+__global__ void absmax_c(const float2 *__restrict__ g, size_t total, unsigned *__restrict__ out) {
+  float m = 0.f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float2 v = g[i];
+    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));
+}
+
 template <typename S>
 __global__ void u2_deapod(const float2 *__restrict__ grid, S *__restrict__ f, U2Geom geo,
-                          int nslab, int fslabs, int fslab0) {
+                          int nslab, int fslabs, int fslab0, const unsigned *max_bits,
+                          float *out_inv) {
   const int n0 = geo.n0, n1 = geo.n1;
   int tx = blockIdx.x * blockDim.x + threadIdx.x;
   int ty = blockIdx.y * blockDim.y + threadIdx.y;
@@ -353,12 +381,15 @@ __global__ void u2_deapod(const float2 *__restrict__ grid, S *__restrict__ f, U2
   v.x *= s;
   v.y *= s;
   float nn = (float)(n0 * n1);
+  const float of = out_factor(max_bits, n0, n1);
+  if (out_inv && tx == 0 && ty == 0) out_inv[fslab0 + tz] = 1.f / of;
   st2(f + (size_t)tx + (size_t)(fslab0 + tz) * n0 + (size_t)ty * n0 * fslabs,
-      make_float2(v.x / ker / nn, v.y / ker / nn));
+      make_float2(v.x / ker / nn * of, v.y / ker / nn * of));
 }
 
 // ------------------------------------------------------------------ usfft1d
 struct U1Geom {
+  const float *in_scale;  // fp16 storage: per-row factor of the input (or null)
   int n0, n1, n2, m2, deth;
   float mu2;
   float wscale;  // sqrt(PI / (mu2 n0))
@@ -407,6 +438,10 @@ __global__ void u1_gather(const S *__restrict__ g, float2 *__restrict__ grid,
         conj = -1.f;
       }
       float2 v = ld2(g + (size_t)tx + (size_t)ts * n0 + (size_t)ty * n0 * hc);
+      if (geo.in_scale) {
+        v.x *= geo.in_scale[ts];
+        v.y *= geo.in_scale[ts];
+      }
       sr += w * v.x;
       si += w * conj * v.y;
     }
@@ -516,6 +551,9 @@ struct tcb_usfft2d {
   float *ex = nullptr, *ey = nullptr;
   cufftHandle plan = 0;
   int storage = TCB_FLOAT32;  // of the stage-1 input and the output
+  const float *in_scale = nullptr;  // fp16 storage scales (caller's device arrays)
+  float *out_inv = nullptr;
+  unsigned *maxbits = nullptr;
 };
 
 static void u2_release(tcb_usfft2d *h) {
@@ -524,9 +562,11 @@ static void u2_release(tcb_usfft2d *h) {
   cudaFree(h->cs);
   cudaFree(h->ex);
   cudaFree(h->ey);
+  cudaFree(h->maxbits);
   h->plan = 0;
   h->grid = h->cs = nullptr;
   h->ex = h->ey = nullptr;
+  h->maxbits = nullptr;
 }
 
 extern "C" int tcb_usfft2d_create(tcb_usfft2d **out, size_t n0_, size_t n1_, size_t n2_,
@@ -587,6 +627,7 @@ static int u2_run(tcb_usfft2d *h, void *f, const void *g, const float *theta, fl
                   int k, int deth0, int fused, int row0, int deth_full, int nslab, int fslabs,
                   int fslab0, cudaStream_t s) {
   U2Geom geo = h->geo;
+  geo.in_scale = h->storage == TCB_FLOAT16 ? h->in_scale : nullptr;
   geo.k = k;
   geo.deth0 = deth0;
   geo.cphi = cosf(phi);
@@ -620,10 +661,22 @@ static int u2_run(tcb_usfft2d *h, void *f, const void *g, const float *theta, fl
   {
     StageTimer st("usfft2d_deapod", s);
     dim3 blk(32, 8), grd(ceil_div(geo.n0, 32), ceil_div(geo.n1, 8), (unsigned)nslab);
-    if (h->storage == TCB_FLOAT16)
-      u2_deapod<__half2><<<grd, blk, 0, s>>>(h->grid, (__half2 *)f, geo, nslab, fslabs, fslab0);
-    else
-      u2_deapod<float2><<<grd, blk, 0, s>>>(h->grid, (float2 *)f, geo, nslab, fslabs, fslab0);
+    if (h->storage == TCB_FLOAT16) {
+      const unsigned *mb = nullptr;
+      if (h->out_inv) {
+        const size_t gtot = (size_t)nslab * (2 * geo.n0) * (2 * geo.n1);
+        TCB_CUDA(cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned), s));
+        absmax_c<<<std::min<unsigned>(ceil_div(gtot, 256), 148u * 16u), 256, 0, s>>>(
+            h->grid, gtot, h->maxbits);
+        count_launch();
+        mb = h->maxbits;
+      }
+      u2_deapod<__half2><<<grd, blk, 0, s>>>(h->grid, (__half2 *)f, geo, nslab, fslabs, fslab0,
+                                             mb, h->out_inv);
+    } else {
+      u2_deapod<float2><<<grd, blk, 0, s>>>(h->grid, (float2 *)f, geo, nslab, fslabs, fslab0,
+                                            nullptr, nullptr);
+    }
     TCB_LAUNCH_CHECK();
     count_launch();
   }
@@ -661,10 +714,18 @@ extern "C" int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1,
   return st;
 }
 
-extern "C" int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision) {
+extern "C" int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision, const float *in_scale,
+                                       float *out_inv_scale) {
   TCB_CHECK_ARG(h && h->grid, "tcb_usfft2d_set_storage: null or freed handle");
   TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
                 "tcb_usfft2d_set_storage: unknown precision %d", precision);
+  h->in_scale = in_scale;
+  h->out_inv = out_inv_scale;
+  if (out_inv_scale && !h->maxbits && cudaMalloc(&h->maxbits, sizeof(unsigned)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("tcb_usfft2d_set_storage: out of device memory");
+    return TCB_ERR_OUT_OF_MEMORY;
+  }
   if (precision == TCB_FLOAT16)
     TCB_CUDA(cudaFuncSetAttribute(u2_gather<4, 4, __half2>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -780,11 +841,12 @@ extern "C" int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi
   return TCB_OK;
 }
 
-extern "C" int tcb_usfft1d_set_storage(tcb_usfft1d *h, int precision) {
+extern "C" int tcb_usfft1d_set_storage(tcb_usfft1d *h, int precision, const float *in_scale) {
   TCB_CHECK_ARG(h && h->grid, "tcb_usfft1d_set_storage: null or freed handle");
   TCB_CHECK_ARG(precision == TCB_FLOAT32 || precision == TCB_FLOAT16,
                 "tcb_usfft1d_set_storage: unknown precision %d", precision);
   h->storage = precision;
+  h->geo.in_scale = precision == TCB_FLOAT16 ? in_scale : nullptr;
   return TCB_OK;
 }
 

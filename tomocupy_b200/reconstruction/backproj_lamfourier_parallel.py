@@ -80,8 +80,13 @@ class BackprojLamFourierParallel:
         half = args.dtype == "mixed"
         sdt = torch.float16 if half else torch.float32
         prec = _lib.TCB_FLOAT16 if half else _lib.TCB_FLOAT32
-        self.cl_lamfourier.cl_usfft2d.set_storage(prec)
-        self.cl_lamfourier.cl_usfft1d.set_storage(prec)
+        nrow = deth // 2 + 1
+        # fp16 stage arrays carry power-of-two scales: inv1 per angle, inv2 per
+        # frequency row (written by usfft2d), so values stay in fp16's normal range
+        inv1 = torch.ones(self.ntheta, dtype=torch.float32, device=dev) if half else None
+        inv2 = torch.ones(nrow, dtype=torch.float32, device=dev) if half else None
+        self.cl_lamfourier.cl_usfft2d.set_storage(prec, inv1, inv2)
+        self.cl_lamfourier.cl_usfft1d.set_storage(prec, inv2)
         s1 = torch.empty((self.ntheta, deth, detw // 2 + 1, 2), dtype=sdt, device=dev)
         g1 = torch.empty((nthetac, deth, detw // 2 + 1), dtype=torch.complex64, device=dev)
         # stage 1
@@ -98,9 +103,15 @@ class BackprojLamFourierParallel:
             self.cl_filter.fslv.filter(self._rows, w, stream)
             self._crop.copy_(self._rows[:, :, self.pad:self.pad + detw])
             self.cl_lamfourier.fft2d_fwd(g1, self._crop, stream)
-            s1[st:end] = torch.view_as_real(g1[:end - st])
+            gr = torch.view_as_real(g1[:end - st])
+            if half:
+                _, e = torch.frexp(gr.abs().amax())
+                sig = torch.ldexp(torch.ones((), device=dev), 14 - e)
+                s1[st:end] = gr * sig
+                inv1[st:end] = 1.0 / sig
+            else:
+                s1[st:end] = gr
         # stage 2
-        nrow = deth // 2 + 1
         s2 = torch.empty((self.n1, nrow, self.n2, 2), dtype=sdt, device=dev)
         for st in range(0, nrow, self.dethc):
             nr = min(self.dethc, nrow - st)
