@@ -125,6 +125,12 @@ def stage_bytes(stage, n, nproj, ncz):
         "fr_pack": ncz * nproj * n * 4 + pairs * nproj * n * 8,
         "fr_gather": pairs * (nproj * n * 8 + (2 * n) ** 2 * 8),
         "fr_deapod": pairs * (n * n * 8 + 2 * n * n * 4),
+        # own pruned 2D inverse FFT: rows pass (all 2n rows in, n kept columns
+        # out), columns pass with deapodization (n columns in, n x n slices out)
+        # fused filter: fp32 rows in, packed complex pairs (or their spectra) out
+        "fft_filter": ncz * nproj * n * 4 + pairs * nproj * n * 8,
+        "fr_ifft_rows": pairs * ((2 * n) ** 2 * 8 + 2 * n * n * 8),
+        "fr_ifft_cols_deapod": pairs * (2 * n * n * 8 + 2 * n * n * 4),
         "linerec": ncz * (nproj * n * 4 + n * n * 8),
         # tensor-core filter: FLOPs (3 split products of 2 n^2 per row), not bytes
         "tc_filter": 3 * 2 * ncz * nproj * n * n,

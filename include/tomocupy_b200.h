@@ -185,6 +185,42 @@ int tcb_tcfilter_apply(tcb_tcfilter *h, const void *x_hi, const void *x_lo, size
 int tcb_tcfilter_status(tcb_tcfilter *h, int *timed_out);
 int tcb_tcfilter_destroy(tcb_tcfilter *h);
 
+/* ------------------------------------------------------------------------
+ * Fused fp32 filter.  Same operator as fbp_filter_center
+ * (src/tomocupy/reconstruction/backproj_functions.py:93-109: edge pad to ne,
+ * R2C, x w, C2R, crop) with cfunc_filter::filter
+ * (src/cuda/cfunc_filter.cu:49-61), computed as a circular convolution of
+ * length L = the power of two >= 2n (two FFTs in shared memory) plus the
+ * folded edge-padding columns, for two slices per complex transform.
+ *
+ * create: nproj angles, up to nz slices per apply call, n columns
+ *   (2 <= n <= 4096), nkern filter kernels (1 = shared; otherwise slice z of
+ *   a call uses kernel kern0 + z).
+ * set_kernels: hz host float64 [nkern][ne], the unnormalised C2R of each
+ *   kernel's spectrum w, pad = left padding (ne/2 - n/2 in the reference);
+ *   synchronous.  Same arguments as tcb_tcfilter_set_kernels.
+ * apply: x fp32 rows x[(z*nproj + p)*ldx + xoff + i], i < n (not modified).
+ *   Slices z < half = ceil(nz/2) pair with slice z + half.
+ *   TCB_FFF_OUT_ROWS: fp32 out[(z*nproj + p)*ldo + j].
+ *   TCB_FFF_OUT_PAIRS (nz even): float2 out[(z*nproj + p)*n + j], z < nz/2,
+ *     the packed layout of FourierRec.backprojection
+ *     (src/tomocupy/reconstruction/fourierrec.py:63-68).
+ *   TCB_FFF_OUT_SPECTRUM (nz even, n a power of two >= 256): the forward
+ *     length-n DFT of each packed row, i.e. the projection FFT of
+ *     cfunc_fourierrec::backprojection (src/cuda/cfunc_fourierrec.cu:67-94);
+ *     pass it to a fourierrec handle with tcb_fourierrec_set_input_spectrum.
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_fftfilter tcb_fftfilter;
+#define TCB_FFF_OUT_ROWS 0
+#define TCB_FFF_OUT_PAIRS 1
+#define TCB_FFF_OUT_SPECTRUM 2
+int tcb_fftfilter_create(tcb_fftfilter **out, size_t nproj, size_t nz, size_t n, size_t nkern);
+int tcb_fftfilter_set_kernels(tcb_fftfilter *h, const double *hz, size_t ne, size_t pad,
+                              void *stream);
+int tcb_fftfilter_apply(tcb_fftfilter *h, const float *x, size_t ldx, size_t xoff, size_t nz,
+                        size_t kern0, void *out, int out_mode, size_t ldo, void *stream);
+int tcb_fftfilter_destroy(tcb_fftfilter *h);
+
 /* Split-fp16 variant of tcb_prep_rows (same normalisation chain, same
  * reference lines), written as hi = fp16(v) and lo = fp16(v - hi) planes
  * [z*out_zstride + p*out_pstride + x]; no edge padding (the tensor-core
@@ -236,6 +272,11 @@ int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode);
  * reconstructed slices in fp16 while the input g stays fp32 (a FLOAT16 handle
  * has fp16 input and output). */
 int tcb_fourierrec_set_output(tcb_fourierrec *h, int precision);
+/* Input form (no reference counterpart): on != 0 means g already holds the
+ * forward length-n DFT of every packed projection row (what
+ * tcb_fftfilter_apply writes with TCB_FFF_OUT_SPECTRUM), so the projection
+ * FFT is skipped.  FLOAT32 handles only. */
+int tcb_fourierrec_set_input_spectrum(tcb_fourierrec *h, int on);
 int tcb_fourierrec_status(tcb_fourierrec *h, int *timed_out);
 int tcb_fourierrec_destroy(tcb_fourierrec *h);
 

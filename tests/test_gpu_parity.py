@@ -146,21 +146,30 @@ def test_fourierrec_dropin_vs_reference(cuda, ref, n, nproj, nz, kind):
 @pytest.mark.parametrize("n,nproj,nz", [(128, 60, 2), (256, 90, 3), (512, 100, 2),
                                         (1024, 64, 2), (2048, 40, 1), (4096, 24, 1)])
 def test_fourierrec_own_fft_matches_cufft(cuda, monkeypatch, n, nproj, nz):
-    """The own pruned inverse FFT (+ fused deapodization) against cuFFT's pruned path."""
+    """The own pruned inverse FFT (+ fused deapodization), rows first and
+    columns first, with the largest and with one column per block, against
+    cuFFT's pruned path."""
     from tomocupy_b200 import cfunc_fourierrec
     theta = torch.as_tensor(_theta(nproj, "random"), device=cuda)
     g = torch.randn((nz, nproj, n, 2), device=cuda)
     out = {}
-    for mode in ("own", "cufft"):  # the own FFT is opt-in
+    for mode, cpc in (("cufft", None), ("own", None), ("own", "1"), ("own_cf", None),
+                      ("own_cf", "2")):
         monkeypatch.setenv("TCB_FOURIERREC_FFT", mode)
+        if cpc is None:
+            monkeypatch.delenv("TCB_FOURIERREC_FFT_CPC", raising=False)
+        else:
+            monkeypatch.setenv("TCB_FOURIERREC_FFT_CPC", cpc)
         op = cfunc_fourierrec.cfunc_fourierrec(nproj, nz, n, theta)
-        f = torch.empty((nz, n, n, 2), device=cuda)
+        f = torch.full((nz, n, n, 2), float("nan"), device=cuda)
         op.backprojection(f, g.clone(), None)
         torch.cuda.synchronize()
-        out[mode] = f.cpu()
+        out[(mode, cpc)] = f.cpu()
         op.free()
-    err = rel_l2(out["own"], out["cufft"])
-    assert err < 1e-6, err
+    want = out.pop(("cufft", None))
+    for key, got in out.items():
+        err = rel_l2(got, want)
+        assert err < 1e-6, (key, err)
 
 
 @pytest.mark.parametrize("n,nproj,nz", [(128, 90, 2), (200, 120, 3), (512, 360, 16),

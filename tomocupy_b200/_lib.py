@@ -29,6 +29,10 @@ GRID_TENSOR = 1
 TCF_OUT_ROWS = 0
 TCF_OUT_PAIRS = 1
 
+FFF_OUT_ROWS = 0
+FFF_OUT_PAIRS = 1
+FFF_OUT_SPECTRUM = 2
+
 STATUS_NAMES = {
     0: "TCB_OK", 1: "TCB_ERR_INVALID_ARGUMENT", 2: "TCB_ERR_CUDA", 3: "TCB_ERR_CUFFT",
     4: "TCB_ERR_OUT_OF_MEMORY", 5: "TCB_ERR_NOT_SUPPORTED", 6: "TCB_ERR_FREED",
@@ -71,6 +75,10 @@ SIGNATURES: dict[str, list] = {
     "tcb_tcfilter_apply": [vp, vp, vp, sz, sz, sz, vp, i32, sz, vp],
     "tcb_tcfilter_status": [vp, C.POINTER(i32)],
     "tcb_tcfilter_destroy": [vp],
+    "tcb_fftfilter_create": [C.POINTER(vp), sz, sz, sz, sz],
+    "tcb_fftfilter_set_kernels": [vp, vp, sz, sz, vp],
+    "tcb_fftfilter_apply": [vp, vp, sz, sz, sz, sz, vp, i32, sz, vp],
+    "tcb_fftfilter_destroy": [vp],
     "tcb_prep_rows_split16": [vp, vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, u32, vp],
     "tcb_fourierrec_create": [C.POINTER(vp), sz, sz, sz, vp, i32],
     "tcb_fourierrec_backprojection": [vp, vp, vp, vp],
@@ -80,6 +88,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_fourierrec_set_gridding": [vp, i32],
     "tcb_fourierrec_status": [vp, C.POINTER(i32)],
     "tcb_fourierrec_set_output": [vp, i32],
+    "tcb_fourierrec_set_input_spectrum": [vp, i32],
     "tcb_fourierrec_destroy": [vp],
     "tcb_linerec_create": [C.POINTER(vp), sz, sz, sz, sz, sz, i32],
     "tcb_linerec_backprojection": [vp, vp, vp, vp, f32, i32, vp],

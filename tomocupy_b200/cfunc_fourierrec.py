@@ -56,6 +56,11 @@ class cfunc_fourierrec:
         self._check()
         _lib.call("tcb_fourierrec_set_output", self._h, int(precision))
 
+    def set_input_spectrum(self, on: bool) -> None:
+        """g holds the projection FFT already (FFTFilter spectrum output; not in the reference)."""
+        self._check()
+        _lib.call("tcb_fourierrec_set_input_spectrum", self._h, int(bool(on)))
+
     def timed_out(self) -> bool:
         """True when a tensor-core gridding wait gave up (synchronises)."""
         import ctypes as C

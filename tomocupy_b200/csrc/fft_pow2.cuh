@@ -12,8 +12,11 @@
 // natural order.  Radix-16 stages (a 4 x 4 register DFT) come first, then
 // one radix-2/4/8 stage when N is not a power of 16.
 //
-// Unnormalised, like cuFFT's CUFFT_INVERSE.  The twiddles come from a table
-// tw[m] = exp(2*pi*i*m/N) computed in float64 on the host.  The first stage
+// Unnormalised, like cuFFT's CUFFT_INVERSE.  The twiddles come from a
+// per-stage table computed in float64 on the host (twiddle_table below):
+// stage S keeps w^(r*k) for r in [1, R), k in [0, Ns) at
+// tw[offset(S) + (r - 1)*Ns + k], so the lanes of a warp, which hold
+// consecutive k, read consecutive entries.  The first stage
 // reads its inputs through a caller functor (global memory), the last stage
 // hands its outputs to another functor (global memory, with any pruning or
 // epilogue the caller wants); the stages in between go through shared
@@ -21,6 +24,9 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
 
 namespace tcb {
 namespace fftk {
@@ -123,64 +129,105 @@ template <int N, int S> constexpr int ns_of() {
   else return ns_of<N, S - 1>() * radix_of<N, S - 1>();
 }
 
+// First twiddle of stage S in the per-stage table (stage 0 needs none).
+template <int N, int S> constexpr int tw_offset() {
+  if constexpr (S <= 1) return 0;
+  else return tw_offset<N, S - 1>() + (radix_of<N, S - 1>() - 1) * ns_of<N, S - 1>();
+}
+
 __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
 // One stage (and, recursively, the ones after it).  sm: this transform's
 // padded shared buffer; tid in [0, T); in(e) -> float2 for stage 0;
-// out(o, value) for the last stage.
-template <int N, int S, class In, class Out>
+// out(o, value) for the last stage.  SYNC_OUT: a block barrier between the
+// last stage's shared reads and the out calls, so out may write sm.  Threads
+// with active == false only take part in the barriers.
+template <int N, int S, bool SYNC_OUT, class In, class Out>
 __device__ __forceinline__ void run_stage(float2 (&v)[16], float2 *sm, int tid,
-                                          const float2 *__restrict__ tw, In &in, Out &out) {
+                                          const float2 *__restrict__ tw, In &in, Out &out,
+                                          bool active) {
   constexpr int R = radix_of<N, S>(), Ns = ns_of<N, S>(), NB = 16 / R;
   constexpr int T = Plan<N>::T;
+  if (active) {
 #pragma unroll
-  for (int q = 0; q < NB; q++) {
+    for (int q = 0; q < NB; q++) {
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-      const int e = tid + q * T + r * (N / R);
-      if constexpr (S == 0) v[q * R + r] = in(e);
-      else v[q * R + r] = sm[pad16(e)];
+      for (int r = 0; r < R; r++) {
+        const int e = tid + q * T + r * (N / R);
+        if constexpr (S == 0) v[q * R + r] = in(e);
+        else v[q * R + r] = sm[pad16(e)];
+      }
     }
-  }
-#pragma unroll
-  for (int q = 0; q < NB; q++) {
-    const int b = tid + q * T;
-    if constexpr (Ns > 1) {
-      const int k = b & (Ns - 1);
-      constexpr int step = N / (Ns * R);
-#pragma unroll
-      for (int r = 1; r < R; r++) v[q * R + r] = cmul(v[q * R + r], __ldg(&tw[r * k * step]));
-    }
-    dft<R>(&v[q * R]);
-  }
-  if constexpr (S == Plan<N>::NST - 1) {
-#pragma unroll
-    for (int q = 0; q < NB; q++)
-#pragma unroll
-      for (int r = 0; r < R; r++) out(tid + q * T + r * Ns, v[q * R + r]);
-  } else {
-    __syncthreads();
 #pragma unroll
     for (int q = 0; q < NB; q++) {
       const int b = tid + q * T;
-      const int base = (b / Ns) * Ns * R + (b & (Ns - 1));
+      if constexpr (Ns > 1) {
+        const int k = b & (Ns - 1);
+        constexpr int off = tw_offset<N, S>();
 #pragma unroll
-      for (int r = 0; r < R; r++) sm[pad16(base + r * Ns)] = v[q * R + r];
+        for (int r = 1; r < R; r++)
+          v[q * R + r] = cmul(v[q * R + r], __ldg(&tw[off + (r - 1) * Ns + k]));
+      }
+      dft<R>(&v[q * R]);
+    }
+  }
+  if constexpr (S == Plan<N>::NST - 1) {
+    if constexpr (SYNC_OUT) __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NB; q++)
+#pragma unroll
+        for (int r = 0; r < R; r++) out(tid + q * T + r * Ns, v[q * R + r]);
+    }
+  } else {
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NB; q++) {
+        const int b = tid + q * T;
+        const int base = (b / Ns) * Ns * R + (b & (Ns - 1));
+#pragma unroll
+        for (int r = 0; r < R; r++) sm[pad16(base + r * Ns)] = v[q * R + r];
+      }
     }
     __syncthreads();
-    run_stage<N, S + 1>(v, sm, tid, tw, in, out);
+    run_stage<N, S + 1, SYNC_OUT>(v, sm, tid, tw, in, out, active);
   }
 }
 
 // Inverse FFT of one length-N transform by its T = N/16 threads.  Every
 // thread of the block must call it the same number of times (it contains
 // __syncthreads); the caller's block may hold several transforms side by
-// side, each with its own sm buffer of Plan<N>::PADDED slots.
-template <int N, class In, class Out>
+// side, each with its own sm buffer of Plan<N>::PADDED slots, or run a
+// transform on part of its threads (active false on the others).
+template <int N, bool SYNC_OUT = false, class In, class Out>
 __device__ __forceinline__ void ifft(float2 *sm, int tid, const float2 *__restrict__ tw, In in,
-                                     Out out) {
+                                     Out out, bool active = true) {
   float2 v[16];
-  run_stage<N, 0>(v, sm, tid, tw, in, out);
+  run_stage<N, 0, SYNC_OUT>(v, sm, tid, tw, in, out, active);
+}
+
+// Host: the per-stage twiddle table of a length-n transform (n a power of
+// two in [256, 8192]), entries exp(2*pi*i*r*k/(Ns*R)) in float64 rounded to
+// float, in the order run_stage reads them.
+inline std::vector<float2> twiddle_table(int n) {
+  int ns16 = 0;
+  while ((16 << (4 * ns16)) <= n) ns16++;
+  const int rl = n >> (4 * ns16);
+  const int nst = ns16 + (rl > 1 ? 1 : 0);
+  std::vector<float2> t;
+  int ns = 1;
+  for (int s = 0; s < nst; s++) {
+    const int r_s = s < ns16 ? 16 : rl;
+    if (s > 0)
+      for (int r = 1; r < r_s; r++)
+        for (int k = 0; k < ns; k++) {
+          const double a = 2.0 * M_PI * (double)r * (double)k / ((double)ns * r_s);
+          t.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+    ns *= r_s;
+  }
+  return t;
 }
 
 }  // namespace fftk

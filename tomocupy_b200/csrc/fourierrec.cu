@@ -820,7 +820,7 @@ __global__ void __launch_bounds__(1024) ifft_cols(const float2 *__restrict__ gri
 // Pass 2 (rows): one kept row ty of t1 per block; the inverse FFT along x
 // keeps x' in [n/2, 3n/2) and applies deapodization and the output layout.
 template <int N, typename OutT>
-__global__ void __launch_bounds__(N / 16) ifft_rows_deapod(const float2 *__restrict__ t1,
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16)) ifft_rows_deapod(const float2 *__restrict__ t1,
                                                           OutT *__restrict__ f,
                                                           const float2 *__restrict__ tw,
                                                           Geom geo, int unpack) {
@@ -837,16 +837,68 @@ __global__ void __launch_bounds__(N / 16) ifft_rows_deapod(const float2 *__restr
   fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
 }
 
-inline int cols_per_block(int N) { return std::min(16384 / N, 16); }
-inline size_t cols_smem(int N) {
-  return (size_t)cols_per_block(N) * (N + N / 16 + 4) * sizeof(float2);
+// Rows-first order.  Pass 1 (rows): one row y of a pair's N x N grid per
+// block; the inverse FFT along x keeps x' in [n/2, 3n/2) in
+// t1[pair][y][x' - n/2] (N x n).  Only n of the N outputs are written.
+template <int N>
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
+    ifft_rows_first(const float2 *__restrict__ grid, float2 *__restrict__ t1,
+                    const float2 *__restrict__ tw) {
+  extern __shared__ float2 fsm[];
+  constexpr int n = N / 2;
+  const size_t row = blockIdx.x;  // pair * N + y
+  const float2 *src = grid + row * N;
+  float2 *dst = t1 + row * n;
+  auto in = [src](int e) { return __ldg(src + e); };
+  auto out = [dst](int o, float2 v) {
+    const unsigned x = (unsigned)(o - N / 4);
+    if (x < (unsigned)n) dst[x] = v;
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
 }
+
+// Pass 2 (columns): CPC adjacent columns tx of t1 per block; the inverse
+// FFT along y keeps y' in [n/2 + 1, 3n/2 + 1) and applies deapodization and
+// the output layout (ty = y' - n/2 - 1).
+template <int N, typename OutT>
+__global__ void __launch_bounds__(1024) ifft_cols_deapod(const float2 *__restrict__ t1,
+                                                         OutT *__restrict__ f,
+                                                         const float2 *__restrict__ tw,
+                                                         Geom geo, int unpack, int cpc) {
+  extern __shared__ float2 fsm[];
+  constexpr int n = N / 2;
+  constexpr int SSTR = fftk::Plan<N>::PADDED + 4;
+  const int c = threadIdx.x % cpc, tid = threadIdx.x / cpc;
+  const int ncb = n / cpc;
+  const int z = blockIdx.x / ncb, tx = (blockIdx.x % ncb) * cpc + c;
+  const float2 *src = t1 + (size_t)z * N * n + tx;
+  auto in = [src](int e) { return __ldg(src + (size_t)e * n); };
+  auto out = [&](int o, float2 v) {
+    const unsigned ty = (unsigned)(o - (N / 4 + 1));
+    if (ty < (unsigned)n) store_out(f, deapod_value(v, tx, (int)ty, geo), tx, (int)ty, z, geo,
+                                    unpack);
+  };
+  fftk::ifft<N>(fsm + c * SSTR, tid, tw, in, out);
+}
+
+inline int cols_per_block(int N) { return std::min(16384 / N, 16); }
+inline size_t cols_smem(int N, int cpc) { return (size_t)cpc * (N + N / 16 + 4) * sizeof(float2); }
 inline size_t rows_smem(int N) { return (size_t)(N + N / 16) * sizeof(float2); }
 
 template <int N>
 cudaError_t own_fft_attrs() {
+  const int csm = (int)cols_smem(N, cols_per_block(N));
   cudaError_t e = cudaFuncSetAttribute(ifft_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)cols_smem(N));
+                                       csm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_cols_deapod<N, float>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_cols_deapod<N, __half>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_rows_first<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rows_smem(N));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(ifft_rows_deapod<N, float>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(N));
@@ -858,12 +910,30 @@ cudaError_t own_fft_attrs() {
 
 template <int N>
 void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, void *f, bool half,
-                    const Geom &geo, int unpack, size_t nz, cudaStream_t s) {
-  const int cpc = cols_per_block(N);
+                    const Geom &geo, int unpack, size_t nz, int cpc, bool rows_first,
+                    cudaStream_t s) {
+  if (rows_first) {
+    {
+      StageTimer st("fr_ifft_rows", s);
+      ifft_rows_first<N><<<(unsigned)(N * nz), N / 16, rows_smem(N), s>>>(grid, t1, tw);
+      count_launch();
+    }
+    StageTimer st("fr_ifft_cols_deapod", s);
+    const unsigned blocks = (unsigned)((N / 2 / cpc) * nz);
+    const size_t sm = cols_smem(N, cpc);
+    if (half)
+      ifft_cols_deapod<N, __half><<<blocks, cpc * (N / 16), sm, s>>>(t1, (__half *)f, tw, geo,
+                                                                      unpack, cpc);
+    else
+      ifft_cols_deapod<N, float><<<blocks, cpc * (N / 16), sm, s>>>(t1, (float *)f, tw, geo,
+                                                                     unpack, cpc);
+    count_launch();
+    return;
+  }
   {
     StageTimer st("fr_ifft_cols", s);
-    ifft_cols<N><<<(unsigned)((N / cpc) * nz), cpc * (N / 16), cols_smem(N), s>>>(grid, t1, tw,
-                                                                                 cpc);
+    ifft_cols<N><<<(unsigned)((N / cpc) * nz), cpc * (N / 16), cols_smem(N, cpc), s>>>(grid, t1,
+                                                                                      tw, cpc);
     count_launch();
   }
   {
@@ -919,17 +989,21 @@ struct tcb_fourierrec {
   // transforms over only the n columns [n/2, 3n/2) that deapodization reads.
   cufftHandle plan_rows = 0, plan_cols = 0;
   bool pruned = false;
-  // Own pruned FFT (columns pass, then rows pass fused with deapodization)
-  // when 2n is a power of two in [256, 8192]: own_n = 2n, else 0.
+  // Own pruned FFT (rows pass, then columns pass fused with deapodization,
+  // or the reverse) when 2n is a power of two in [256, 8192]: own_n = 2n,
+  // else 0.
   int own_n = 0;
+  int own_cpc = 0;  // columns per block of the own column pass
+  bool own_rows_first = true;  // rows pass first (columns pass fused with deapodization)
   int zblock = 0;  // pairs per gridding block (2/4/8/16; 0 = largest that fits nz)
   int grid_mode = 0;          // TCB_GRID_FP32 or TCB_GRID_TENSOR
   bool out_f16 = false;       // fp16 output slices (set_output) with fp32 input
+  bool spectrum_in = false;   // g already holds the projection FFT (set_input_spectrum)
   unsigned *amax = nullptr;   // max |G| bits for the tensor-core gridding scale
   int *recs = nullptr;        // per-sample footprint records (tensor-core gridding)
   int *tc_err = nullptr;      // set by a tensor-core gridding wait that timed out
-  float2 *t1 = nullptr;  // [nz][n][2n] column-pass output
-  float2 *tw = nullptr;  // [2n] exp(2 pi i m / 2n)
+  float2 *t1 = nullptr;  // first-pass output: [nz][2n][n] rows first, [nz][n][2n] columns first
+  float2 *tw = nullptr;  // per-stage twiddle table of the length-2n transforms
   int ntiles = 0;
   size_t list_bytes = 0;
 };
@@ -1006,7 +1080,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   } else {
     TCB_CUFFT(cufftSetStream(h->plan2d, s));
   }
-  {
+  if (!h->spectrum_in) {
     StageTimer st("fr_fft1d", s);
     TCB_CUFFT(cufftExecC2C(h->plan1d, (cufftComplex *)gc, (cufftComplex *)gc, CUFFT_FORWARD));
   }
@@ -1035,13 +1109,15 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   const bool out_half = h->precision == TCB_FLOAT16 || h->out_f16;
   if (h->own_n) {
     const bool half = out_half;
+    const int cpc = h->own_cpc;
+    const bool rf = h->own_rows_first;
     switch (h->own_n) {
-      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
-      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
-      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
-      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
-      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
-      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, s); break;
+      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
     }
     TCB_LAUNCH_CHECK();
     return TCB_OK;
@@ -1239,31 +1315,31 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
                                 CUFFT_C2C, (int)(nproj * nz));
   int len2[2] = {(int)(2 * n), (int)(2 * n)};
   // The deapodization reads only rows and columns [n/2, 3n/2 + 1) of the
-  // inverse 2D transform, so the column pass runs on n of the 2n columns.
-  // TCB_FOURIERREC_FULL_FFT2D=1 selects one full 2D transform instead.
-  // TCB_FOURIERREC_FFT=own selects the library's own pruned FFT with fused
-  // deapodization (power-of-two 2n in [256, 8192]).  It is exact to cuFFT
-  // within fp32 round-off but, at 2n = 4096 on B200, slower than cuFFT's
-  // pruned pair of passes (139 vs 128 ms per 2048-slice volume), so cuFFT
-  // stays the default.
+  // inverse 2D transform, so the 2D inverse FFT is pruned.  For a
+  // power-of-two 2n in [256, 8192] the library's own FFT runs it: a row pass
+  // over all 2n rows that writes only the n kept columns, then a column pass
+  // over those n columns with the deapodization fused into its last stage
+  // (2048-slice volume at 2n = 4096: 87 ms, against 128 ms for cuFFT's
+  // pruned passes plus a deapodization kernel).  Other sizes use cuFFT:
+  // rows over all 2n rows, then columns over the n kept columns.
+  // TCB_FOURIERREC_FFT=cufft forces cuFFT, =own_cf the own FFT with the
+  // column pass first; TCB_FOURIERREC_FULL_FFT2D=1 selects one full cuFFT
+  // 2D transform.
   const char *full = getenv("TCB_FOURIERREC_FULL_FFT2D");
   const char *fsel = getenv("TCB_FOURIERREC_FFT");
   h->pruned = !(full && full[0] == '1');
   const size_t N2 = 2 * n;
-  if (h->pruned && (fsel && strcmp(fsel, "own") == 0) && N2 >= 256 && N2 <= 8192 &&
+  const bool own_sel = !(fsel && strcmp(fsel, "cufft") == 0);
+  if (h->pruned && own_sel && N2 >= 256 && N2 <= 8192 &&
       (N2 & (N2 - 1)) == 0) {
-    std::vector<float2> twh(N2);
-    for (size_t m = 0; m < N2; m++) {
-      double a = 2.0 * M_PI * (double)m / (double)N2;
-      twh[m] = make_float2((float)std::cos(a), (float)std::sin(a));
-    }
-    if (cudaMalloc(&h->tw, N2 * sizeof(float2)) != cudaSuccess ||
+    const std::vector<float2> twh = fftk::twiddle_table((int)N2);
+    if (cudaMalloc(&h->tw, twh.size() * sizeof(float2)) != cudaSuccess ||
         cudaMalloc(&h->t1, nz * n * N2 * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       set_error("tcb_fourierrec_create: out of device memory for the FFT buffers");
       return fail(TCB_ERR_OUT_OF_MEMORY);
     }
-    e = cudaMemcpy(h->tw, twh.data(), N2 * sizeof(float2), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(h->tw, twh.data(), twh.size() * sizeof(float2), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
       switch (N2) {
         case 256: e = own_fft_attrs<256>(); break;
@@ -1279,6 +1355,14 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
       return fail(TCB_ERR_CUDA);
     }
     h->own_n = (int)N2;
+    // columns per block of the column pass: a power of two up to
+    // cols_per_block (TCB_FOURIERREC_FFT_CPC tunes it)
+    h->own_rows_first = !(fsel && strcmp(fsel, "own_cf") == 0);
+    h->own_cpc = cols_per_block((int)N2);
+    if (const char *c = getenv("TCB_FOURIERREC_FFT_CPC")) {
+      const int v = atoi(c);
+      if (v >= 1 && v <= h->own_cpc && (v & (v - 1)) == 0) h->own_cpc = v;
+    }
   }
   if (r == CUFFT_SUCCESS && !h->pruned)
     r = cufftPlanMany(&h->plan2d, 2, len2, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, (int)nz);
@@ -1331,6 +1415,15 @@ extern "C" int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs) 
   TCB_CHECK_ARG(pairs == 0 || pairs == 2 || pairs == 4 || pairs == 8 || pairs == 16,
                 "tcb_fourierrec_set_pairs_per_block: pairs must be 0, 2, 4, 8 or 16");
   h->zblock = pairs;
+  return TCB_OK;
+}
+
+extern "C" int tcb_fourierrec_set_input_spectrum(tcb_fourierrec *h, int on) {
+  TCB_CHECK_ARG(h, "tcb_fourierrec_set_input_spectrum: null handle");
+  TCB_CHECK_ARG(h->grid, "tcb_fourierrec_set_input_spectrum: handle was freed");
+  TCB_CHECK_ARG(h->precision == TCB_FLOAT32,
+                "tcb_fourierrec_set_input_spectrum: FLOAT32 handles only");
+  h->spectrum_in = on != 0;
   return TCB_OK;
 }
 

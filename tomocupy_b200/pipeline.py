@@ -7,14 +7,20 @@
 
 executed as native kernels on one stream:
 
- 1. ``tcb_prep_rows``: uint16 frames -> dark/flat -> -log -> sinogram order,
-    written straight into the edge-padded filter rows (one pass, no
-    temporaries, no separate transpose or pad copies);
- 2. ``tcb_filter_apply``: R2C -> per-slice complex spectrum -> C2R;
- 3. fourierrec: ``tcb_fourierrec_pack`` (crop + complex pairing) and
-    ``tcb_fourierrec_backprojection_slices`` (gridding, 2D FFT, deapodization,
-    unpacking into the output slices);
-    linerec: crop + ``tcb_linerec_backprojection``.
+ 1. ``tcb_prep_rows``: uint16 frames -> dark/flat -> -log -> sinogram order
+    (one pass, no temporaries, no separate transpose copy);
+ 2. ``tcb_fftfilter_apply`` (widths up to 4096): edge pad + filter + centre
+    shift + crop as one length-2n convolution in shared memory, two slices
+    per complex transform, written as FourierRec's packed pairs -- for
+    power-of-two widths already through the projection FFT -- or as the
+    cropped rows of linerec/lprec;
+ 3. fourierrec: ``tcb_fourierrec_backprojection_slices`` (gridding, 2D FFT,
+    deapodization, unpacking into the output slices); linerec/lprec on the
+    filtered rows.
+
+Wider rows take the reference's own route: prep into edge-padded rows of
+length ne = 4n, ``tcb_filter_apply`` (R2C -> per-slice spectrum -> C2R),
+then ``tcb_fourierrec_pack`` (crop + complex pairing) or a crop copy.
 
 ``precision="mixed"`` replaces steps 1-2 with ``tcb_prep_rows_split16`` (the
 same prep chain written as fp16 hi/lo planes, unpadded) and the tensor-core
@@ -35,6 +41,7 @@ import torch
 from . import _lib, cfunc_filter, cfunc_fourierrec, cfunc_linerec
 from .processing.proc_functions import in_dtype_code, prep_rows, prep_rows_split16
 from .reconstruction.backproj_functions import phase_weights, rfftfreq32
+from .reconstruction import fftfilter as _fff
 from .reconstruction.fbp_filter import calc_filter
 
 
@@ -68,6 +75,7 @@ class SinoPipeline:
         self.wfilter = torch.as_tensor(self.wfilter_np, device=self.device)
         self.t = rfftfreq32(self.ne, self.device)
         self._w_cache: dict = {}
+        self.fused = precision == "float32" and _fff.supported(self.n)
         if precision == "mixed":
             from .reconstruction.tcfilter import TCFilter
             self.npl = -(-self.n // 8) * 8  # fp16 row pitch (16-byte TMA rows)
@@ -78,6 +86,14 @@ class SinoPipeline:
             self.tcf.set_kernels(self.wfilter_np, self.ne, self.center, 0.0)
             self.tcf_sht = None      # per-slice kernels for centre shifts (built on demand)
             self._sht_key = None
+        elif _fff.supported(self.n):
+            # fused filter: compact rows, not modified by filtering
+            self.rows = torch.empty((self.ncz, self.nproj, self.n), dtype=torch.float32,
+                                    device=self.device)
+            self.fff = _fff.FFTFilter(self.n, self.nproj, self.ncz, 1, self.device)
+            self.fff.set_kernels(self.wfilter_np, self.ne, self.center, 0.0)
+            self.fff_sht = None      # per-slice kernels for centre shifts (built on demand)
+            self._fff_key = None
         else:
             self.rows = torch.empty((self.ncz, self.nproj, self.ne), dtype=torch.float32,
                                     device=self.device)
@@ -99,6 +115,10 @@ class SinoPipeline:
                 self.fr.set_gridding(_lib.GRID_TENSOR)
             if out_dtype == "float16":
                 self.fr.set_output(_lib.TCB_FLOAT16)
+            # the fused filter hands over the projection FFT already done
+            self.fr_spectrum = self.fused and _fff.spectrum_supported(self.n)
+            if self.fr_spectrum:
+                self.fr.set_input_spectrum(True)
             self.g = torch.empty((self.ncz // 2, self.nproj, self.n, 2), dtype=torch.float32,
                                  device=self.device)
         else:
@@ -146,6 +166,10 @@ class SinoPipeline:
                                   minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
                                   out_pstride=self.npl, stream=stream)
                 return
+            if self.fused:
+                prep_rows(self.rows, src, darkflat=False, minus_log=self.minus_log,
+                          out_zstride=self.nproj * self.n, out_pstride=self.n, stream=stream)
+                return
             prep_rows(self.rows, src, darkflat=False, minus_log=self.minus_log,
                       out_zstride=self.nproj * self.ne, out_pstride=self.ne, out_xoff=self.pad,
                       out_width=self.ne, edge_pad=True, stream=stream)
@@ -154,6 +178,11 @@ class SinoPipeline:
             prep_rows_split16(self.xhi, self.xlo, data, d0, f0, darkflat=dark0 is not None,
                               minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
                               out_pstride=self.npl, stream=stream)
+            return
+        if self.fused:
+            prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
+                      minus_log=self.minus_log, out_zstride=self.nproj * self.n,
+                      out_pstride=self.n, stream=stream)
             return
         prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                   minus_log=self.minus_log, out_zstride=self.nproj * self.ne,
@@ -188,7 +217,7 @@ class SinoPipeline:
 
     def save_rows(self):
         """Snapshot of slice 0 needed to refill rows that filtering overwrote (or None)."""
-        return None if self.precision == "mixed" else self.rows[0].clone()
+        return None if (self.precision == "mixed" or self.fused) else self.rows[0].clone()
 
     def restore_rows(self, saved):
         if saved is not None:
@@ -209,6 +238,39 @@ class SinoPipeline:
             self.tcf_sht.set_kernels(self.wfilter_np, self.ne, self.center, sh.astype(np.float64))
             self._sht_key = key
         return self.tcf_sht
+
+    def _fft_filter(self, sht):
+        """The fused filter for these centre shifts (shared kernel when None)."""
+        if sht is None:
+            return self.fff
+        sh = np.asarray(sht, dtype=np.float32).reshape(-1)
+        if sh.size == 1:
+            sh = np.repeat(sh, self.ncz)
+        if self.fff_sht is None:
+            self.fff_sht = _fff.FFTFilter(self.n, self.nproj, self.ncz, self.ncz, self.device)
+        key = sh.tobytes()
+        if key != self._fff_key:
+            self.fff_sht.set_kernels(self.wfilter_np, self.ne, self.center,
+                                     sh.astype(np.float64))
+            self._fff_key = key
+        return self.fff_sht
+
+    def _filter_and_backproject_fused(self, out, sht, stream, kern0=0, fff=None):
+        f = fff if fff is not None else self._fft_filter(sht)
+        if self.algorithm == "fourierrec":
+            f.apply(self.rows, torch.view_as_complex(self.g),
+                    "spectrum" if self.fr_spectrum else "pairs", kern0=kern0, stream=stream)
+            self.fr.backprojection_slices(out, self.g, stream)
+            return out
+        f.apply(self.rows, self.crop, "rows", kern0=kern0, stream=stream)
+        if self.algorithm == "linerec":
+            s = torch.cuda.current_stream() if stream is None else stream
+            with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
+                out.zero_()
+            self.lr.backprojection(out, self.crop, self.theta, math.pi / 2, 0, stream)
+        else:
+            self.lp.fslv.backprojection(out, self.crop, stream)
+        return out
 
     def _filter_and_backproject_mixed(self, out, sht, stream):
         f = self._tc_filter(sht)
@@ -231,6 +293,8 @@ class SinoPipeline:
         assert out.dtype == self.out_dtype, (out.dtype, self.out_dtype)
         if self.precision == "mixed":
             return self._filter_and_backproject_mixed(out, sht, stream)
+        if self.fused:
+            return self._filter_and_backproject_fused(out, sht, stream)
         self.filter.filter(self.rows, self.weights(sht), stream)
         if self.algorithm == "fourierrec":
             self.fr.pack(self.g, self.rows, self.ne, self.pad, stream)

@@ -8,10 +8,10 @@ Reader.init_sizes_try, src/tomocupy/dataio/reader.py:224-247).
 
 ``TryCenterSweep`` keeps everything of a sweep resident -- the normalised
 slice, per-centre filter operators (the tensor-core Toeplitz operators in
-mixed precision, the complex spectra in fp32), the gridding tables and the
-output stack of all centres -- and records the whole sweep (filter ->
-1D FFT -> gridding -> pruned 2D FFT -> deapodization for every chunk) into
-one CUDA graph.  A sweep is then one graph launch.  ``autotune`` times the
+mixed precision, the fused filter's per-centre convolution spectra in fp32),
+the gridding tables and the output stack of all centres -- and records the
+whole sweep (filter -> 1D FFT -> gridding -> pruned 2D FFT -> deapodization
+for every chunk) into one CUDA graph.  A sweep is then one graph launch.  ``autotune`` times the
 sweep for each candidate chunk size and gridding depth (slice pairs per
 gridding block) on the actual geometry and keeps the fastest.
 """
@@ -78,6 +78,12 @@ class TryCenterSweep:
                                 self.device)
             self.tcf.set_kernels(self.pipe.wfilter_np, self.pipe.ne, self.pipe.center,
                                  self.sht.reshape(-1).astype(np.float64))
+        elif self.pipe.fused:
+            from .reconstruction.fftfilter import FFTFilter
+            self.fff = FFTFilter(self.n, self.nproj, self.ncz, self.nchunks * self.ncz,
+                                 self.device)
+            self.fff.set_kernels(self.pipe.wfilter_np, self.pipe.ne, self.pipe.center,
+                                 self.sht.reshape(-1).astype(np.float64))
         else:
             self.weights = [self.pipe.weights(self.sht[k]) for k in range(self.nchunks)]
         self.saved = None
@@ -90,7 +96,7 @@ class TryCenterSweep:
         with torch.cuda.stream(self._stream):
             self.pipe.load_rows(data, dark0, flat0, 0, self._stream)
             self.pipe.replicate_first_row()
-            if self.precision != "mixed":
+            if self.precision != "mixed" and not self.pipe.fused:
                 # same buffer on every load: a captured graph reads it
                 if self.saved is None:
                     self.saved = self.pipe.rows[0].clone()
@@ -106,6 +112,10 @@ class TryCenterSweep:
             if self.precision == "mixed":
                 self.tcf.apply(p.xhi, p.xlo, torch.view_as_complex(p.g), pairs=True,
                                kern0=k * self.ncz, stream=stream)
+            elif p.fused:  # the fused filter leaves the rows as they are
+                self.fff.apply(p.rows, torch.view_as_complex(p.g),
+                               "spectrum" if p.fr_spectrum else "pairs", kern0=k * self.ncz,
+                               stream=stream)
             else:
                 # the cuFFT filter works in place: refill the rows of every chunk
                 p.rows.copy_(self.saved.expand(self.ncz, -1, -1))
@@ -154,7 +164,7 @@ class TryCenterSweep:
 
     def free(self):
         self.graph = None
-        for name in ("tcf",):
+        for name in ("tcf", "fff"):
             obj = getattr(self, name, None)
             if obj is not None:
                 obj.free()
