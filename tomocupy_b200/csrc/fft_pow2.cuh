@@ -14,9 +14,12 @@
 //
 // Unnormalised, like cuFFT's CUFFT_INVERSE.  The twiddles come from a
 // per-stage table computed in float64 on the host (twiddle_table below):
-// stage S keeps w^(r*k) for r in [1, R), k in [0, Ns) at
-// tw[offset(S) + (r - 1)*Ns + k], so the lanes of a warp, which hold
-// consecutive k, read consecutive entries.  The first stage
+// stage S keeps w^(2^j * k) for j < log2(R), k in [0, Ns) at
+// tw[offset(S) + j*Ns + k], so the lanes of a warp, which hold consecutive
+// k, read consecutive entries; w^(r*k) is the product of the entries of the
+// set bits of r (at most 3 roundings for r < 16).  log2(R) loads instead of
+// R - 1 keep the tables of all stages small enough to stay in L1 next to
+// the data streams.  The first stage
 // reads its inputs through a caller functor (global memory), the last stage
 // hands its outputs to another functor (global memory, with any pruning or
 // epilogue the caller wants); the stages in between go through shared
@@ -132,7 +135,29 @@ template <int N, int S> constexpr int ns_of() {
 // First twiddle of stage S in the per-stage table (stage 0 needs none).
 template <int N, int S> constexpr int tw_offset() {
   if constexpr (S <= 1) return 0;
-  else return tw_offset<N, S - 1>() + (radix_of<N, S - 1>() - 1) * ns_of<N, S - 1>();
+  else return tw_offset<N, S - 1>() + ilog2(radix_of<N, S - 1>()) * ns_of<N, S - 1>();
+}
+
+// w^(r*k) for r in [1, R) from the log2(R) table entries w^(2^j * k).
+template <int R>
+__device__ __forceinline__ void stage_twiddles(const float2 *__restrict__ t, int ns, int k,
+                                               float2 (&w)[16]) {
+  w[1] = __ldg(t + k);
+  if constexpr (R >= 4) {
+    w[2] = __ldg(t + ns + k);
+    w[3] = cmul(w[1], w[2]);
+  }
+  if constexpr (R >= 8) {
+    w[4] = __ldg(t + 2 * ns + k);
+    w[5] = cmul(w[1], w[4]);
+    w[6] = cmul(w[2], w[4]);
+    w[7] = cmul(w[3], w[4]);
+  }
+  if constexpr (R >= 16) {
+    w[8] = __ldg(t + 3 * ns + k);
+#pragma unroll
+    for (int r = 1; r < 8; r++) w[8 + r] = cmul(w[r], w[8]);
+  }
 }
 
 __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
@@ -163,10 +188,10 @@ __device__ __forceinline__ void run_stage(float2 (&v)[16], float2 *sm, int tid,
       const int b = tid + q * T;
       if constexpr (Ns > 1) {
         const int k = b & (Ns - 1);
-        constexpr int off = tw_offset<N, S>();
+        float2 w[16];
+        stage_twiddles<R>(tw + tw_offset<N, S>(), Ns, k, w);
 #pragma unroll
-        for (int r = 1; r < R; r++)
-          v[q * R + r] = cmul(v[q * R + r], __ldg(&tw[off + (r - 1) * Ns + k]));
+        for (int r = 1; r < R; r++) v[q * R + r] = cmul(v[q * R + r], w[r]);
       }
       dft<R>(&v[q * R]);
     }
@@ -208,8 +233,8 @@ __device__ __forceinline__ void ifft(float2 *sm, int tid, const float2 *__restri
 }
 
 // Host: the per-stage twiddle table of a length-n transform (n a power of
-// two in [256, 8192]), entries exp(2*pi*i*r*k/(Ns*R)) in float64 rounded to
-// float, in the order run_stage reads them.
+// two in [256, 8192]), entries exp(2*pi*i*2^j*k/(Ns*R)) in float64 rounded
+// to float, in the order run_stage reads them.
 inline std::vector<float2> twiddle_table(int n) {
   int ns16 = 0;
   while ((16 << (4 * ns16)) <= n) ns16++;
@@ -220,9 +245,9 @@ inline std::vector<float2> twiddle_table(int n) {
   for (int s = 0; s < nst; s++) {
     const int r_s = s < ns16 ? 16 : rl;
     if (s > 0)
-      for (int r = 1; r < r_s; r++)
+      for (int p = 1; p < r_s; p *= 2)
         for (int k = 0; k < ns; k++) {
-          const double a = 2.0 * M_PI * (double)r * (double)k / ((double)ns * r_s);
+          const double a = 2.0 * M_PI * (double)p * (double)k / ((double)ns * r_s);
           t.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
         }
     ns *= r_s;

@@ -44,7 +44,7 @@ struct tcb_fftfilter {
   int L = 0;               // convolution length: next power of two >= 2n
   bool spectrum_ok = false;  // n a power of two in [256, 4096]
   float2 *H = nullptr;     // [nkern][L] DFT_L(h_L) / L
-  float *AB = nullptr;     // [nkern][2][n] folded padding columns A, B
+  float2 *AB = nullptr;    // [nkern][n] folded padding columns (A[j], B[j])
   float2 *twL = nullptr;   // per-stage twiddles of length L
   float2 *twn = nullptr;   // per-stage twiddles of length n (spectrum mode)
   bool ready = false;
@@ -62,7 +62,7 @@ struct Args {
   int nproj, nz, half, n;
   int shared_kern, kern0;
   const float2 *H;
-  const float *AB;
+  const float2 *AB;
   const float2 *twL, *twn;
   void *out;
   size_t ldo;
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(L / 16, (16384 / L < 16 ? 16384 / L : 16))
 
   // 2) y = IDFT_L(Y) (1/L folded into H), then the padding columns
   const float2 *Ha = a.H + (size_t)ka * L, *Hb = a.H + (size_t)kb * L;
-  const float *Aa = a.AB + (size_t)ka * 2 * n, *Ab = a.AB + (size_t)kb * 2 * n;
+  const float2 *ABa = a.AB + (size_t)ka * n, *ABb = a.AB + (size_t)kb * n;
   const float xa0 = __ldg(xa), xan = __ldg(xa + n - 1);
   const float xb0 = hasb ? __ldg(xb) : 0.f, xbn = hasb ? __ldg(xb + n - 1) : 0.f;
   const bool same = ka == kb;
@@ -115,8 +115,10 @@ __global__ void __launch_bounds__(L / 16, (16384 / L < 16 ? 16384 / L : 16))
     return make_float2(u.x + w.x, u.y + w.y);
   };
   auto fix = [&](int o, float2 v) {
-    v.x += xa0 * __ldg(Aa + o) + xan * __ldg(Aa + n + o);
-    v.y += xb0 * __ldg(Ab + o) + xbn * __ldg(Ab + n + o);
+    const float2 ca = __ldg(ABa + o);
+    const float2 cb = same ? ca : __ldg(ABb + o);
+    v.x += xa0 * ca.x + xan * ca.y;
+    v.y += xb0 * cb.x + xbn * cb.y;
     return v;
   };
   if constexpr (MODE == OUT_ROWS) {
@@ -237,7 +239,7 @@ extern "C" int tcb_fftfilter_create(tcb_fftfilter **out, size_t nproj, size_t nz
   if (h->spectrum_ok) twn = fftk::twiddle_table((int)n);
   cudaError_t e = cudaSuccess;
   if (cudaMalloc(&h->H, nkern * (size_t)L * sizeof(float2)) != cudaSuccess ||
-      cudaMalloc(&h->AB, nkern * 2 * n * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->AB, nkern * n * sizeof(float2)) != cudaSuccess ||
       cudaMalloc(&h->twL, twL.size() * sizeof(float2)) != cudaSuccess ||
       (h->spectrum_ok && cudaMalloc(&h->twn, twn.size() * sizeof(float2)) != cudaSuccess)) {
     cudaGetLastError();
@@ -277,7 +279,7 @@ extern "C" int tcb_fftfilter_set_kernels(tcb_fftfilter *h, const double *hz, siz
   TCB_CHECK_ARG(ne >= n && pad + n <= ne, "tcb_fftfilter_set_kernels: need pad + n <= ne");
   TCB_CHECK_ARG(ne < (1u << 30), "tcb_fftfilter_set_kernels: ne too large");
   std::vector<float2> Hh(nk * L);
-  std::vector<float> ABh(nk * 2 * n);
+  std::vector<float2> ABh(nk * n);
   std::vector<double> cs(2 * ne + 1);
   std::vector<std::complex<double>> v(L);
   for (size_t k = 0; k < nk; k++) {
@@ -306,14 +308,14 @@ extern "C" int tcb_fftfilter_set_kernels(tcb_fftfilter *h, const double *hz, siz
       const double col0 = S((long long)j, (long long)(j + pad));
       const double coln = S((long long)j + (long long)pad - (long long)ne + 1,
                             (long long)j - (long long)n + 1);
-      ABh[k * 2 * n + j] = (float)(col0 - hk[j % ne]);
-      ABh[k * 2 * n + n + j] = (float)(coln - hk[(j + ne - (n - 1)) % ne]);
+      ABh[k * n + j] = make_float2((float)(col0 - hk[j % ne]),
+                                   (float)(coln - hk[(j + ne - (n - 1)) % ne]));
     }
   }
   cudaStream_t s = (cudaStream_t)stream;
   TCB_CUDA(cudaMemcpyAsync(h->H, Hh.data(), Hh.size() * sizeof(float2), cudaMemcpyHostToDevice,
                            s));
-  TCB_CUDA(cudaMemcpyAsync(h->AB, ABh.data(), ABh.size() * sizeof(float),
+  TCB_CUDA(cudaMemcpyAsync(h->AB, ABh.data(), ABh.size() * sizeof(float2),
                            cudaMemcpyHostToDevice, s));
   TCB_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
   h->ready = true;
