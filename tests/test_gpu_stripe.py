@@ -34,6 +34,26 @@ def test_fw_matches_reference_fixture(cuda, i):
     assert err < 1e-5, (i, err)
 
 
+@pytest.mark.parametrize("i", range(5))
+def test_fw_filter_banks_reproduce_regression_fixture(cuda, i):
+    """Bit-for-bit against outputs recorded with the one-output-per-thread
+    filter-bank kernels (tests/golden/make_fw_b200.py): the register-blocked
+    kernels keep every output's multiply-then-add tap order."""
+    import sys
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    from make_fw_b200 import CASES
+    from tomocupy_b200.processing.remove_stripe import remove_stripe_fw
+    g = np.load(ROOT / "tests" / "golden" / "fw_stripe_b200.npz")
+    nproj, nz, n, level, sigma, wname, seed = CASES[i]
+    out = remove_stripe_fw(torch.as_tensor(g[f"in_{i}"], device=cuda), sigma, wname, level)
+    torch.cuda.synchronize()
+    want = g[f"out_{i}"]
+    got = out.cpu().numpy()
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), \
+        (i, float(np.abs(got - want).max()))
+
+
 def test_fw_removes_stripes(cuda):
     """Constant-along-angle column offsets are strongly attenuated."""
     from tomocupy_b200.processing.remove_stripe import remove_stripe_fw

@@ -21,6 +21,7 @@
 // pyramid kept in HBM, the damped band transposed so the angle FFTs are
 // contiguous batched transforms, 1/N of the inverse FFT folded into the
 // damping factors.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -195,6 +196,259 @@ __global__ void sfb_rows(const float *__restrict__ in, int H, int Wi, float *__r
   dst[b * dsz + (long long)h * dsx + w] = acc;
 }
 
+// ---- register-blocked filter banks for the supported filter lengths ------
+// Same outputs, bit for bit, as the kernels above (every output keeps its
+// multiply-then-add tap order); the taps come from the kernel parameter
+// space (constant-bank operands of the multiplies, fully unrolled), and each
+// input value is read once per thread window instead of once per tap.
+struct TapPair {
+  float a[MAXL], b[MAXL];
+};
+
+// afb1d along the last axis.  RB rows per block staged in shared memory with
+// the symmetric extension applied (smem[u] = x[reflect(u - padl)]); output j
+// reads smem[2j + k], k < L, as L/2 float2 loads (conflict-free).
+template <int L>
+__global__ void __launch_bounds__(256) afb_rows_t(const float *__restrict__ x, long long sz,
+                                                  int sx, float *__restrict__ out, int B, int H,
+                                                  int W, int Wo, int padl, int RB, int SW,
+                                                  const __grid_constant__ TapPair t) {
+  extern __shared__ float2 srow2[];
+  float *srow = reinterpret_cast<float *>(srow2);
+  const long long row0 = (long long)blockIdx.x * RB;
+  const long long nrows = (long long)B * H;
+  const int nr = (int)min((long long)RB, nrows - row0);
+  for (int r = 0; r < nr; r++) {
+    const long long row = row0 + r;
+    const long long b = row / H, h = row - b * H;
+    const float *xr = x + b * sz + h * sx;
+    float *sr = srow + r * SW;
+    for (int u = threadIdx.x; u < SW; u += blockDim.x) {
+      const int m = u - padl;
+      sr[u] = xr[m >= 0 && m < W ? m : reflect(m, W)];
+    }
+  }
+  __syncthreads();
+  constexpr int RO = 4;                 // outputs per thread
+  constexpr int NV = 2 * RO + L - 2;    // their input window
+  const int ngrp = (Wo + RO - 1) / RO;
+  for (int e = threadIdx.x; e < nr * ngrp; e += blockDim.x) {
+    const int r = e / ngrp, j0 = (e - r * ngrp) * RO;
+    const float2 *p = srow2 + (r * SW) / 2 + j0;  // smem[2 j0 + u] = window u
+    float v[NV];
+#pragma unroll
+    for (int q = 0; q < NV / 2; q++) {
+      const float2 w = p[q];
+      v[2 * q] = w.x;
+      v[2 * q + 1] = w.y;
+    }
+    float lo[RO], hi[RO];
+#pragma unroll
+    for (int o = 0; o < RO; o++) {
+      lo[o] = __fmul_rn(t.a[0], v[2 * o]);
+      hi[o] = __fmul_rn(t.b[0], v[2 * o]);
+    }
+#pragma unroll
+    for (int k = 1; k < L; k++) {
+      const float ak = t.a[k], bk = t.b[k];
+#pragma unroll
+      for (int o = 0; o < RO; o++) {
+        lo[o] = __fadd_rn(lo[o], __fmul_rn(ak, v[2 * o + k]));
+        hi[o] = __fadd_rn(hi[o], __fmul_rn(bk, v[2 * o + k]));
+      }
+    }
+    const long long row = row0 + r;
+    const long long b = row / H, h = row - b * H;
+    float *o0 = out + ((b * 2) * H + h) * Wo;
+    float *o1 = o0 + (long long)H * Wo;
+#pragma unroll
+    for (int o = 0; o < RO; o++)
+      if (j0 + o < Wo) {
+        o0[j0 + o] = lo[o];
+        o1[j0 + o] = hi[o];
+      }
+  }
+}
+
+// Column kernels: a block is a tile of 32 columns x (8 * RO) output rows of
+// one channel plane; the input rows of the tile are staged in shared memory
+// (one coalesced pass), then thread (tx, ty) computes column tx, rows
+// ty*RO .. ty*RO + RO - 1 of the tile from a register window.
+constexpr int CT_X = 32, CT_Y = 8;
+
+// afb1d along the rows axis: in [B][2][H][W] -> out [B][4][Ho][W]; thread =
+// column j and RO consecutive output rows, its 2 RO + L - 2 input rows held
+// in registers (read through L1: the windows of neighbouring row groups
+// overlap).
+template <int L, int RO>
+__global__ void __launch_bounds__(128) afb_cols_t(const float *__restrict__ in,
+                                                  float *__restrict__ out, int B, int H, int W,
+                                                  int Ho, int padl,
+                                                  const __grid_constant__ TapPair t) {
+  const int ncolb = (W + blockDim.x - 1) / blockDim.x;
+  const int ngrp = (Ho + RO - 1) / RO;
+  const long long blk = blockIdx.x;
+  const int j = (int)(blk % ncolb) * blockDim.x + threadIdx.x;
+  const long long rest = blk / ncolb;
+  const long long bc = rest / ngrp;
+  const int i0 = (int)(rest - bc * ngrp) * RO;
+  if (j >= W) return;
+  const float *col = in + bc * H * W + j;
+  constexpr int NV = 2 * RO + L - 2;
+  float v[NV];
+  const int r0 = 2 * i0 - padl;
+  if (r0 >= 0 && r0 + NV <= H) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) v[q] = col[(long long)(r0 + q) * W];
+  } else {
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      const int rr = r0 + q;
+      v[q] = col[(long long)(rr >= 0 && rr < H ? rr : reflect(rr, H)) * W];
+    }
+  }
+  const long long b = bc / 2, c = bc % 2;
+  float *o0 = out + ((b * 4 + 2 * c) * Ho) * (long long)W + j;
+  float *o1 = o0 + (long long)Ho * W;
+  float lo[RO], hi[RO];
+#pragma unroll
+  for (int r = 0; r < RO; r++) {
+    lo[r] = __fmul_rn(t.a[0], v[2 * r]);
+    hi[r] = __fmul_rn(t.b[0], v[2 * r]);
+  }
+#pragma unroll
+  for (int k = 1; k < L; k++) {
+    const float ak = t.a[k], bk = t.b[k];
+#pragma unroll
+    for (int r = 0; r < RO; r++) {
+      lo[r] = __fadd_rn(lo[r], __fmul_rn(ak, v[2 * r + k]));
+      hi[r] = __fadd_rn(hi[r], __fmul_rn(bk, v[2 * r + k]));
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < RO; r++)
+    if (i0 + r < Ho) {
+      o0[(long long)(i0 + r) * W] = lo[r];
+      o1[(long long)(i0 + r) * W] = hi[r];
+    }
+}
+
+// One synthesis output: acc over k of the reference's parity (k = tt & 1,
+// tt & 1 + 2, ...), h = (tt - k)/2 skipped outside [0, Hi).  Windows lo/hi
+// hold h = hb + idx; RO consecutive outputs with tt0 even (L even), so
+// h = hb + L/2 + (r - k)/2.
+template <int L, int RO, bool CHECK>
+__device__ __forceinline__ void synth_outputs(const float (&lo)[L / 2 + RO / 2],
+                                              const float (&hi)[L / 2 + RO / 2], int hb, int Hi,
+                                              const TapPair &t, float (&acc)[RO]) {
+#pragma unroll
+  for (int r = 0; r < RO; r++) acc[r] = 0.f;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const float ak = t.a[k], bk = t.b[k];
+#pragma unroll
+    for (int r = k & 1; r < RO; r += 2) {
+      const int idx = (r - k) / 2 + L / 2;  // h - hb
+      if (CHECK) {
+        const int h = hb + idx;
+        if (h < 0 || h >= Hi) continue;
+      }
+      const float vv = __fadd_rn(__fmul_rn(ak, lo[idx]), __fmul_rn(bk, hi[idx]));
+      acc[r] = __fadd_rn(acc[r], vv);
+    }
+  }
+}
+
+// sfb1d along the rows axis (see sfb_cols): tile rows t0.. (t0 a multiple
+// of 8 * RO, so every thread's first output row is even).
+template <int L, int RO>
+__global__ void __launch_bounds__(CT_X *CT_Y) sfb_cols_t(const float *__restrict__ y,
+                                                         long long bstride, int Hi, int Wb, int W,
+                                                         float *__restrict__ out, int B, int Ho,
+                                                         const __grid_constant__ TapPair t) {
+  static_assert(L % 2 == 0 && RO % 2 == 0, "even filter length and output block");
+  constexpr int TR = CT_Y * RO;
+  constexpr int NW = L / 2 + RO / 2;       // window per thread
+  constexpr int NT = TR / 2 + L / 2;       // window per tile
+  __shared__ float tlo[NT][CT_X], thi[NT][CT_X];
+  const int ncolb = (W + CT_X - 1) / CT_X;
+  const int ngrp = (Ho + TR - 1) / TR;
+  const long long blk = blockIdx.x;
+  const int cb = (int)(blk % ncolb);
+  const long long rest = blk / ncolb;
+  const long long bc = rest / ngrp;
+  const int t0 = (int)(rest - bc * ngrp) * TR;
+  const int tx = threadIdx.x % CT_X, ty = threadIdx.x / CT_X;
+  const int j = cb * CT_X + tx;
+  const int b = (int)(bc / 2), c = (int)(bc % 2);
+  const long long plane = (long long)Hi * Wb;
+  const float *base = y + b * bstride;
+  const float *lop = base + (c == 0 ? 0 : 2) * plane + j;  // LL or band1 (HL)
+  const float *hip = base + (c == 0 ? 1 : 3) * plane + j;  // band0 (LH) or band2 (HH)
+  const int hbt = (t0 + L - 2) / 2 - L / 2;  // h of tile window index 0
+  for (int q = ty; q < NT; q += CT_Y) {
+    const int h = hbt + q;
+    const bool ok = j < W && h >= 0 && h < Hi;
+    tlo[q][tx] = ok ? lop[(long long)h * Wb] : 0.f;
+    thi[q][tx] = ok ? hip[(long long)h * Wb] : 0.f;
+  }
+  __syncthreads();
+  if (j >= W) return;
+  const int hb = hbt + ty * (RO / 2);
+  float lo[NW], hi[NW];
+#pragma unroll
+  for (int q = 0; q < NW; q++) {
+    lo[q] = tlo[ty * (RO / 2) + q][tx];
+    hi[q] = thi[ty * (RO / 2) + q][tx];
+  }
+  float acc[RO];
+  if (hb >= 0 && hb + NW <= Hi)
+    synth_outputs<L, RO, false>(lo, hi, hb, Hi, t, acc);
+  else
+    synth_outputs<L, RO, true>(lo, hi, hb, Hi, t, acc);
+  const int tt0 = t0 + ty * RO;
+#pragma unroll
+  for (int r = 0; r < RO; r++)
+    if (tt0 + r < Ho) out[(bc * Ho + tt0 + r) * W + j] = acc[r];
+}
+
+// sfb1d along the last axis (see sfb_rows): thread = RO consecutive outputs
+// w0.. of one row (w0 a multiple of RO), windows read through L1.
+template <int L, int RO>
+__global__ void __launch_bounds__(128) sfb_rows_t(const float *__restrict__ in, int H, int Wi,
+                                                  float *__restrict__ dst, long long dsz, int dsx,
+                                                  int Hd, int Wd, int B,
+                                                  const __grid_constant__ TapPair t) {
+  const int ngrp = (Wd + RO - 1) / RO;
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)B * Hd * ngrp) return;
+  const int w0 = (int)(g % ngrp) * RO;
+  const long long rowi = g / ngrp;
+  const int h = (int)(rowi % Hd);
+  const int b = (int)(rowi / Hd);
+  const float *lop = in + (((long long)b * 2) * H + h) * Wi;
+  const float *hip = lop + (long long)H * Wi;
+  constexpr int NW = L / 2 + RO / 2;
+  const int hb = (w0 + L - 2) / 2 - L / 2;
+  float lo[NW], hi[NW];
+#pragma unroll
+  for (int q = 0; q < NW; q++) {
+    const int qq = hb + q;
+    const bool ok = qq >= 0 && qq < Wi;
+    lo[q] = ok ? lop[qq] : 0.f;
+    hi[q] = ok ? hip[qq] : 0.f;
+  }
+  float acc[RO];
+  if (hb >= 0 && hb + NW <= Wi)
+    synth_outputs<L, RO, false>(lo, hi, hb, Wi, t, acc);
+  else
+    synth_outputs<L, RO, true>(lo, hi, hb, Wi, t, acc);
+  float *d = dst + b * dsz + (long long)h * dsx;
+#pragma unroll
+  for (int r = 0; r < RO; r++)
+    if (w0 + r < Wd) d[w0 + r] = acc[r];
+}
+
 // [B][R][C] <-> [B][C][R] (32x32 tiles)
 __global__ void transpose_bands(const float *__restrict__ in, long long istride,
                                 float *__restrict__ out, long long ostride, int R, int C) {
@@ -240,7 +494,48 @@ struct tcb_stripe_fw {
   float2 *spec = nullptr;  // band spectrum scratch
   Taps *taps = nullptr;    // device copy
   size_t tmp_elems = 0;
+  TapPair ana{}, syn{};    // by-value taps of the register-blocked kernels
 };
+
+namespace {
+constexpr int FB_RO = 4;  // outputs per thread of the column / synthesis kernels
+
+template <int L>
+void launch_afb_rows(const tcb_stripe_fw *h, const float *x, long long xsz, int xsx, int B,
+                     int Hk, int Wk, int Wo, int padl, cudaStream_t s) {
+  const int SW = 2 * ((Wo + 3) / 4 * 4) + L - 2;  // windows of the last 4-output group
+  const int RB = std::max(1, std::min(16, 1024 / Wo));
+  const long long nb = ((long long)B * Hk + RB - 1) / RB;
+  afb_rows_t<L><<<(unsigned)nb, 256, (size_t)RB * SW * sizeof(float), s>>>(
+      x, xsz, xsx, h->tmp, B, Hk, Wk, Wo, padl, RB, SW, h->ana);
+}
+
+template <int L>
+void launch_afb_cols(const tcb_stripe_fw *h, float *out, int B, int Hk, int Wo, int Ho, int padl,
+                     cudaStream_t s) {
+  const long long nb = (long long)ceil_div(Wo, 128) * (2LL * B) * ((Ho + FB_RO - 1) / FB_RO);
+  afb_cols_t<L, FB_RO><<<(unsigned)nb, 128, 0, s>>>(h->tmp, out, B, Hk, Wo, Ho, padl, h->ana);
+}
+
+template <int L>
+void launch_sfb_cols(const tcb_stripe_fw *h, const float *y, int Hi, int Wi, int B, int Hc,
+                     cudaStream_t s) {
+  const long long nb = (long long)ceil_div(Wi, CT_X) * (2LL * B) *
+                       ((Hc + CT_Y * FB_RO - 1) / (CT_Y * FB_RO));
+  sfb_cols_t<L, FB_RO><<<(unsigned)nb, CT_X * CT_Y, 0, s>>>(y, 4LL * Hi * Wi, Hi, Wi, Wi,
+                                                            h->tmp, B, Hc, h->syn);
+}
+
+template <int L>
+void launch_sfb_rows(const tcb_stripe_fw *h, int Hc, int Wi, float *dst, long long dsz, int Wd,
+                     int Hrows, int B, cudaStream_t s) {
+  const long long thr = (long long)B * Hrows * ((Wd + FB_RO - 1) / FB_RO);
+  sfb_rows_t<L, FB_RO><<<(unsigned)ceil_div(thr, 128), 128, 0, s>>>(h->tmp, Hc, Wi, dst, dsz, Wd,
+                                                                    Hrows, Wd, B, h->syn);
+}
+
+bool blocked_length(int L) { return L == 2 || L == 10 || L == 32; }
+}  // namespace
 
 static void fw_release(tcb_stripe_fw *h) {
   for (auto p : h->Y) cudaFree(p);
@@ -297,6 +592,12 @@ extern "C" int tcb_stripe_fw_create(tcb_stripe_fw **out, size_t nproj, size_t nz
     t.h1[k] = (float)dec_hi[L - 1 - k];
     t.g0[k] = (float)rec_lo[k];
     t.g1[k] = (float)rec_hi[k];
+  }
+  for (int k = 0; k < L; k++) {
+    h->ana.a[k] = t.h0[k];
+    h->ana.b[k] = t.h1[k];
+    h->syn.a[k] = t.g0[k];
+    h->syn.b[k] = t.g1[k];
   }
   if (cudaMalloc(&h->taps, sizeof(Taps)) != cudaSuccess)
     return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
@@ -377,15 +678,27 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     long long n1 = (long long)B * Hk * Wo;
     {
       StageTimer st("fw_afb_rows", s);
-      afb_rows<<<ceil_div(n1, 256), 256, 0, s>>>(x, xsz, xsx, h->tmp, B, Hk, Wk, Wo, pw / 2,
-                                                 h->taps);
+      switch (blocked_length(L) ? L : 0) {
+        case 2: launch_afb_rows<2>(h, x, xsz, xsx, B, Hk, Wk, Wo, pw / 2, s); break;
+        case 10: launch_afb_rows<10>(h, x, xsz, xsx, B, Hk, Wk, Wo, pw / 2, s); break;
+        case 32: launch_afb_rows<32>(h, x, xsz, xsx, B, Hk, Wk, Wo, pw / 2, s); break;
+        default:
+          afb_rows<<<ceil_div(n1, 256), 256, 0, s>>>(x, xsz, xsx, h->tmp, B, Hk, Wk, Wo, pw / 2,
+                                                     h->taps);
+      }
     }
     TCB_LAUNCH_CHECK();
     long long n2 = (long long)B * 2 * Ho * Wo;
     {
       StageTimer st("fw_afb_cols", s);
-      afb_cols<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, h->Y[k], B, Hk, Wo, Ho, ph / 2,
-                                                 h->taps);
+      switch (blocked_length(L) ? L : 0) {
+        case 2: launch_afb_cols<2>(h, h->Y[k], B, Hk, Wo, Ho, ph / 2, s); break;
+        case 10: launch_afb_cols<10>(h, h->Y[k], B, Hk, Wo, Ho, ph / 2, s); break;
+        case 32: launch_afb_cols<32>(h, h->Y[k], B, Hk, Wo, Ho, ph / 2, s); break;
+        default:
+          afb_cols<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, h->Y[k], B, Hk, Wo, Ho, ph / 2,
+                                                     h->taps);
+      }
     }
     TCB_LAUNCH_CHECK();
     StageTimer std_("fw_damp", s);
@@ -415,8 +728,14 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     long long n1 = (long long)B * 2 * Hc * Wi;
     {
       StageTimer st("fw_sfb_cols", s);
-      sfb_cols<<<ceil_div(n1, 256), 256, 0, s>>>(h->Y[k], 4LL * Hi * Wi, Hi, Wi, Wi, h->tmp, B,
-                                                 Hc, h->taps);
+      switch (blocked_length(L) ? L : 0) {
+        case 2: launch_sfb_cols<2>(h, h->Y[k], Hi, Wi, B, Hc, s); break;
+        case 10: launch_sfb_cols<10>(h, h->Y[k], Hi, Wi, B, Hc, s); break;
+        case 32: launch_sfb_cols<32>(h, h->Y[k], Hi, Wi, B, Hc, s); break;
+        default:
+          sfb_cols<<<ceil_div(n1, 256), 256, 0, s>>>(h->Y[k], 4LL * Hi * Wi, Hi, Wi, Wi, h->tmp,
+                                                     B, Hc, h->taps);
+      }
     }
     TCB_LAUNCH_CHECK();
     // reconstruction of level k's input, cropped to its size, into the LL
@@ -434,8 +753,14 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     int Hrows = std::min(Hd, Hc);
     long long n2 = (long long)B * Hrows * Wd;
     StageTimer st("fw_sfb_rows", s);
-    sfb_rows<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, Hc, Wi, dst, dsz, Wd, Hrows, Wd, B,
-                                               h->taps);
+    switch (blocked_length(L) ? L : 0) {
+      case 2: launch_sfb_rows<2>(h, Hc, Wi, dst, dsz, Wd, Hrows, B, s); break;
+      case 10: launch_sfb_rows<10>(h, Hc, Wi, dst, dsz, Wd, Hrows, B, s); break;
+      case 32: launch_sfb_rows<32>(h, Hc, Wi, dst, dsz, Wd, Hrows, B, s); break;
+      default:
+        sfb_rows<<<ceil_div(n2, 256), 256, 0, s>>>(h->tmp, Hc, Wi, dst, dsz, Wd, Hrows, Wd, B,
+                                                   h->taps);
+    }
     TCB_LAUNCH_CHECK();
     count_launch(2);
   }
