@@ -265,6 +265,53 @@ def _roofline(stages, a, peaks, peaks_kind, kernel=None):
             if peaks_kind == "measured" else "fallback 6.65 TB/s"}
 
 
+def run_tc_filter(a, dev, peaks, peaks_kind, reps=10):
+    """The tensor-core Toeplitz filter timed alone on one chunk of this workload.
+
+    ncz slices x nproj rows x n columns (split fp16 operands, packed complex
+    output), CUDA events around reps launches after 3 warm-ups; algorithmic
+    flops 3 * 2 * n^2 per row against the burst bf16 peak (a kernel timed
+    alone).  The pipelines use the fused FFT filter, which does O(n log n)
+    work per row instead of the GEMM's O(n^2), so this leg reports the
+    tensor-core kernel on its own.
+    """
+    import torch
+    from tomocupy_b200.reconstruction.fbp_filter import calc_filter
+    from tomocupy_b200.reconstruction.tcfilter import TCFilter, split16
+    n, P, ncz = a.n, a.nproj, a.ncz
+    g = torch.Generator(device=dev).manual_seed(a.seed)
+    x = torch.rand((ncz, P, n), device=dev, generator=g)
+    hi, lo = split16(x)
+    f = TCFilter(n, P, ncz, 1, dev)
+    f.set_kernels(calc_filter(4 * n, a.filter), 4 * n, n / 2)
+    out = torch.empty((ncz // 2, P, n), dtype=torch.complex64, device=dev)
+    s = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        f.apply(hi, lo, out, pairs=True, stream=s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(s)
+    for _ in range(reps):
+        f.apply(hi, lo, out, pairs=True, stream=s)
+    e1.record(s)
+    torch.cuda.synchronize(dev)
+    timed_out = f.timed_out()
+    f.free()
+    ms = e0.elapsed_time(e1) / reps
+    flops = 3 * 2 * ncz * P * float(n) ** 2
+    achieved = flops / (ms / 1e3) / 1e12
+    peak = peaks["bf16_tflops"]
+    return {"bound": "tensor", "kernel": "tc_filter", "timed": "alone",
+            "workload": f"{ncz} slices x {P} rows x {n} columns, packed pair output",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "TFLOP/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": NCU_TRAFFIC.get(("tc_filter", n, P, ncz)),
+            "algorithmic_flops_per_launch": flops, "ms_per_launch": round(ms, 4),
+            "timed_out": timed_out,
+            "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json bf16_tflops, burst: kernel "
+                           "timed alone)" if peaks_kind == "measured" else "fallback 1.59 PFLOP/s"}
+
+
 def run_try(a, dev):
     """Try-centre sweep: 1 slice x a.try_n cols x a.try_nproj angles x a.try_centers centres.
 
@@ -528,7 +575,6 @@ def run_ours(a, ws, rank, local):
         del out2
         v2 = ws * vox / (ms2 / 1e3) / 1e9
         mixed_ms, fp32_ms = (ms2, ms_step) if other == "mixed" else (ms_step, ms2)
-        mst = st2 if other == "mixed" else stages
         side = {"precision": other, "value": round(v2, 2), "unit": "GUPS",
                 "ms_per_step": round(ms2, 3), "slices_per_s": round(ws * a.nz / (ms2 / 1e3), 1),
                 "mixed_speedup_vs_fp32": round(fp32_ms / mixed_ms, 3),
@@ -536,7 +582,7 @@ def run_ours(a, ws, rank, local):
                 "rel_l2_vs_fp64": "see tests/test_gpu_pipeline.py::"
                                   "test_c1_mixed_fourierrec_vs_fp64_oracle (budget 1e-3)",
                 "gpu_launches": l2, "clocks": clk2,
-                "roofline_tc_filter": _roofline(mst, a, peaks, peaks_kind, "tc_filter"),
+                "roofline_tc_filter": run_tc_filter(a, dev, peaks, peaks_kind),
                 "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in st2.items()}}
 
     methods = None

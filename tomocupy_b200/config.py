@@ -17,6 +17,7 @@ DEFAULTS = {
     "fbp_filter": "parzen",
     "dtype": "float32",                     # 'float32' | 'float16' | 'mixed' (tensor-core filter)
     "out_dtype": "float32",                 # 'float32' | 'float16' output slices (fourierrec)
+    "mixed_filter": "fft",                  # dtype 'mixed': 'fft' (fused fp32) | 'tensor' (tcgen05)
     "rotation_axis": -1.0,
     "center_search_width": 50.0,
     "center_search_step": 0.5,

@@ -738,26 +738,39 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   }
 }
 
-// Deapodization of one output pixel (tx, ty) from the inverse-FFT value at
-// grid index (tx + n/2, ty + 1 + n/2): the post-FFT fftshift sign, divphi
-// with its (1 - n%4) sign and 1/nproj, and the circle mask, in the
-// reference's operation order (kernels_fourierrec.cuh divphi + circ).
-__device__ __forceinline__ float2 deapod_value(float2 v, int tx, int ty, const Geom &geo) {
-  const int n = geo.n;
-  int ix = tx + n / 2, iy = ty + 1 + n / 2;
-  int sx = 1 - 2 * ((ix + M + 1) % 2), sy = 1 - 2 * ((iy + M + 1) % 2);
-  float sgn = (float)(sx * sy);
+// Deapodization of output pixel (tx, ty) from the inverse-FFT value at grid
+// index (tx + n/2, ty + 1 + n/2): the post-FFT fftshift sign, divphi
+// (exp(mu n^2 (dx^2 + dy^2)) / nproj with dx = tx/n - 0.5, and the
+// (1 - n%4) sign) and the circle mask 4x^2 + 4y^2 < 1 with x = (tx - n/2)/n
+// (kernels_fourierrec.cuh divphi + circ).  The per-index terms are computed
+// once per geometry with the same float arithmetic:
+// tab[i] = {i/n - 0.5, (i - n/2)/n, sx(i), sy(i)}, the last two the fftshift
+// signs of column index i and of row index i.  The per-pixel expressions
+// keep their original form, so the circle test rounds (and contracts) as
+// the reference's does on boundary pixels.
+__global__ void deapod_terms(float4 *__restrict__ tab, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float d = i / (float)n - 0.5;
+  const float q = (i - n / 2) / float(n);
+  const int ix = i + n / 2, iy = i + 1 + n / 2;
+  const int sx = 1 - 2 * ((ix + M + 1) % 2), sy = 1 - 2 * ((iy + M + 1) % 2);
+  tab[i] = make_float4(d, q, (float)sx, (float)sy);
+}
+
+// Deapodized value from the terms of column tx (X) and row ty (Y);
+// mun2 = mu * n^2, nsign = 1 - n % 4.
+__device__ __forceinline__ float2 deapod_terms_value(float2 v, const float4 X, const float4 Y,
+                                                     float mun2, int nproj, float nsign) {
+  const float sgn = X.z * Y.w;
   v.x *= sgn;
   v.y *= sgn;
-  float dx = tx / (float)n - 0.5;
-  float dy = ty / (float)n - 0.5;
-  float phi = __expf(geo.mu * (n * n) * (dx * dx + dy * dy)) / geo.nproj;
-  phi *= (1 - n % 4);
+  const float dx = X.x, dy = Y.x, x = X.y, y = Y.y;
+  float phi = __expf(mun2 * (dx * dx + dy * dy)) / nproj;
+  phi *= nsign;
   v.x *= phi;
   v.y *= phi;
-  float x = (tx - n / 2) / float(n);
-  float y = (ty - n / 2) / float(n);
-  float lam = (float)((4 * x * x + 4 * y * y) < 1);
+  const float lam = (float)((4 * x * x + 4 * y * y) < 1);
   v.x *= lam;
   v.y *= lam;
   return v;
@@ -783,7 +796,7 @@ __device__ __forceinline__ void store_out(OutT *f, float2 v, int tx, int ty, int
 //   f real [2nz, n, n] (unpack == 1).
 template <typename OutT>
 __global__ void deapod_kernel(const float2 *__restrict__ grid, OutT *__restrict__ f,
-                              Geom geo, int unpack) {
+                              const float4 *__restrict__ dtab, Geom geo, int unpack) {
   const int n = geo.n, twon = geo.twon;
   int tx = blockIdx.x * blockDim.x + threadIdx.x;
   int ty = blockIdx.y * blockDim.y + threadIdx.y;
@@ -791,7 +804,10 @@ __global__ void deapod_kernel(const float2 *__restrict__ grid, OutT *__restrict_
   if (tx >= n || ty >= n) return;
   int ix = tx + n / 2, iy = ty + 1 + n / 2;
   float2 v = grid[(size_t)tz * twon * twon + (size_t)iy * twon + ix];
-  store_out(f, deapod_value(v, tx, ty, geo), tx, ty, tz, geo, unpack);
+  store_out(f,
+            deapod_terms_value(v, __ldg(dtab + tx), __ldg(dtab + ty), geo.mu * (n * n),
+                               geo.nproj, (float)(1 - n % 4)),
+            tx, ty, tz, geo, unpack);
 }
 
 // Own pruned inverse 2D FFT for power-of-two 2n (N = 2n).
@@ -823,16 +839,20 @@ template <int N, typename OutT>
 __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16)) ifft_rows_deapod(const float2 *__restrict__ t1,
                                                           OutT *__restrict__ f,
                                                           const float2 *__restrict__ tw,
+                                                          const float4 *__restrict__ dtab,
                                                           Geom geo, int unpack) {
   extern __shared__ float2 fsm[];
   constexpr int n = N / 2;
   const int ty = blockIdx.x % n, z = blockIdx.x / n;
   const float2 *src = t1 + ((size_t)z * n + ty) * N;
+  const float4 Y = __ldg(dtab + ty);
+  const float mun2 = geo.mu * (n * n), nsign = (float)(1 - n % 4);
   auto in = [src](int e) { return __ldg(src + e); };
   auto out = [&](int o, float2 v) {
     const unsigned tx = (unsigned)(o - N / 4);
-    if (tx < (unsigned)n) store_out(f, deapod_value(v, (int)tx, ty, geo), (int)tx, ty, z, geo,
-                                    unpack);
+    if (tx < (unsigned)n)
+      store_out(f, deapod_terms_value(v, __ldg(dtab + tx), Y, mun2, geo.nproj, nsign), (int)tx,
+                ty, z, geo, unpack);
   };
   fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
 }
@@ -864,6 +884,7 @@ template <int N, typename OutT>
 __global__ void __launch_bounds__(1024) ifft_cols_deapod(const float2 *__restrict__ t1,
                                                          OutT *__restrict__ f,
                                                          const float2 *__restrict__ tw,
+                                                         const float4 *__restrict__ dtab,
                                                          Geom geo, int unpack, int cpc) {
   extern __shared__ float2 fsm[];
   constexpr int n = N / 2;
@@ -872,11 +893,14 @@ __global__ void __launch_bounds__(1024) ifft_cols_deapod(const float2 *__restric
   const int ncb = n / cpc;
   const int z = blockIdx.x / ncb, tx = (blockIdx.x % ncb) * cpc + c;
   const float2 *src = t1 + (size_t)z * N * n + tx;
+  const float4 X = __ldg(dtab + tx);
+  const float mun2 = geo.mu * (n * n), nsign = (float)(1 - n % 4);
   auto in = [src](int e) { return __ldg(src + (size_t)e * n); };
   auto out = [&](int o, float2 v) {
     const unsigned ty = (unsigned)(o - (N / 4 + 1));
-    if (ty < (unsigned)n) store_out(f, deapod_value(v, tx, (int)ty, geo), tx, (int)ty, z, geo,
-                                    unpack);
+    if (ty < (unsigned)n)
+      store_out(f, deapod_terms_value(v, X, __ldg(dtab + ty), mun2, geo.nproj, nsign), tx,
+                (int)ty, z, geo, unpack);
   };
   fftk::ifft<N>(fsm + c * SSTR, tid, tw, in, out);
 }
@@ -909,9 +933,9 @@ cudaError_t own_fft_attrs() {
 }
 
 template <int N>
-void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, void *f, bool half,
-                    const Geom &geo, int unpack, size_t nz, int cpc, bool rows_first,
-                    cudaStream_t s) {
+void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, const float4 *dtab,
+                    void *f, bool half, const Geom &geo, int unpack, size_t nz, int cpc,
+                    bool rows_first, cudaStream_t s) {
   if (rows_first) {
     {
       StageTimer st("fr_ifft_rows", s);
@@ -922,11 +946,11 @@ void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, void *f, b
     const unsigned blocks = (unsigned)((N / 2 / cpc) * nz);
     const size_t sm = cols_smem(N, cpc);
     if (half)
-      ifft_cols_deapod<N, __half><<<blocks, cpc * (N / 16), sm, s>>>(t1, (__half *)f, tw, geo,
-                                                                      unpack, cpc);
+      ifft_cols_deapod<N, __half><<<blocks, cpc * (N / 16), sm, s>>>(t1, (__half *)f, tw, dtab,
+                                                                      geo, unpack, cpc);
     else
-      ifft_cols_deapod<N, float><<<blocks, cpc * (N / 16), sm, s>>>(t1, (float *)f, tw, geo,
-                                                                     unpack, cpc);
+      ifft_cols_deapod<N, float><<<blocks, cpc * (N / 16), sm, s>>>(t1, (float *)f, tw, dtab,
+                                                                     geo, unpack, cpc);
     count_launch();
     return;
   }
@@ -940,11 +964,11 @@ void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, void *f, b
     StageTimer st("fr_ifft_rows_deapod", s);
     const unsigned blocks = (unsigned)((N / 2) * nz);
     if (half)
-      ifft_rows_deapod<N, __half><<<blocks, N / 16, rows_smem(N), s>>>(t1, (__half *)f, tw, geo,
-                                                                       unpack);
+      ifft_rows_deapod<N, __half><<<blocks, N / 16, rows_smem(N), s>>>(t1, (__half *)f, tw,
+                                                                       dtab, geo, unpack);
     else
-      ifft_rows_deapod<N, float><<<blocks, N / 16, rows_smem(N), s>>>(t1, (float *)f, tw, geo,
-                                                                      unpack);
+      ifft_rows_deapod<N, float><<<blocks, N / 16, rows_smem(N), s>>>(t1, (float *)f, tw, dtab,
+                                                                      geo, unpack);
     count_launch();
   }
 }
@@ -1004,6 +1028,7 @@ struct tcb_fourierrec {
   int *tc_err = nullptr;      // set by a tensor-core gridding wait that timed out
   float2 *t1 = nullptr;  // first-pass output: [nz][2n][n] rows first, [nz][n][2n] columns first
   float2 *tw = nullptr;  // per-stage twiddle table of the length-2n transforms
+  float4 *dtab = nullptr;  // [n] deapodization terms (deapod_terms)
   int ntiles = 0;
   size_t list_bytes = 0;
 };
@@ -1030,6 +1055,8 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->g32);
   cudaFree(h->t1);
   cudaFree(h->tw);
+  cudaFree(h->dtab);
+  h->dtab = nullptr;
   cudaFree(h->amax);
   cudaFree(h->tc_err);
   cudaFree(h->recs);
@@ -1112,12 +1139,12 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     const int cpc = h->own_cpc;
     const bool rf = h->own_rows_first;
     switch (h->own_n) {
-      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
     }
     TCB_LAUNCH_CHECK();
     return TCB_OK;
@@ -1142,9 +1169,9 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     StageTimer st("fr_deapod", s);
     dim3 blk(32, 8), grd(ceil_div(h->n, 32), ceil_div(h->n, 8), (unsigned)h->nz);
     if (out_half)
-      deapod_kernel<__half><<<grd, blk, 0, s>>>(h->grid, (__half *)f, geo, unpack);
+      deapod_kernel<__half><<<grd, blk, 0, s>>>(h->grid, (__half *)f, h->dtab, geo, unpack);
     else
-      deapod_kernel<float><<<grd, blk, 0, s>>>(h->grid, (float *)f, geo, unpack);
+      deapod_kernel<float><<<grd, blk, 0, s>>>(h->grid, (float *)f, h->dtab, geo, unpack);
     TCB_LAUNCH_CHECK();
     count_launch();
   }
@@ -1270,6 +1297,7 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   FR_ALLOC(h->toffs, (h->ntiles + 1) * sizeof(long long));
   FR_ALLOC(h->boffs, ((size_t)h->ntiles * NREG + 1) * sizeof(long long));
   FR_ALLOC(h->grid, nz * 4 * n * n * sizeof(float2));
+  FR_ALLOC(h->dtab, n * sizeof(float4));
   if (precision == TCB_FLOAT16) FR_ALLOC(h->g32, nz * nproj * n * sizeof(float2));
 #undef FR_ALLOC
 
@@ -1293,6 +1321,7 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
   int tab = (int)std::max(std::max(nproj, n), 2 * n + 2 * M + 1 + 2 * EPAD);
   setup_tables<<<ceil_div(tab, 256), 256>>>(h->cs, h->rtab, h->etab, theta, (int)n,
                                             (int)nproj);
+  deapod_terms<<<ceil_div(n, 256), 256>>>(h->dtab, (int)n);
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {

@@ -22,14 +22,16 @@ Wider rows take the reference's own route: prep into edge-padded rows of
 length ne = 4n, ``tcb_filter_apply`` (R2C -> per-slice spectrum -> C2R),
 then ``tcb_fourierrec_pack`` (crop + complex pairing) or a crop copy.
 
-``precision="mixed"`` replaces steps 1-2 with ``tcb_prep_rows_split16`` (the
-same prep chain written as fp16 hi/lo planes, unpadded) and the tensor-core
-filter ``tcb_tcfilter_apply`` (edge pad + filter + centre shift + crop as one
-split-precision fp16 GEMM), whose epilogue writes the packed complex pairs
-of fourierrec directly (no pack pass) or the cropped rows of linerec/lprec,
-and grids fourierrec on the tensor cores (``TCB_GRID_TENSOR``: fp16 weights
-and hi/lo values, fp32 accumulation).  The filter does not modify its input
-planes.
+``precision="mixed"`` grids fourierrec on the tensor cores
+(``TCB_GRID_TENSOR``: fp16 weights and hi/lo values, fp32 accumulation).
+Its filter is the fused fp32 filter (``mixed_filter="fft"``, the default:
+O(n log n) and faster at every supported width) or, with
+``mixed_filter="tensor"``, ``tcb_prep_rows_split16`` (the prep chain written
+as fp16 hi/lo planes) followed by the tensor-core filter
+``tcb_tcfilter_apply`` (edge pad + filter + centre shift + crop as one
+split-precision fp16 GEMM of 3 * 2 n^2 flops per row), whose epilogue writes
+the packed complex pairs of fourierrec or the cropped rows of linerec/lprec.
+Neither filter modifies its input.
 """
 from __future__ import annotations
 
@@ -48,12 +50,14 @@ from .reconstruction.fbp_filter import calc_filter
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
                  algorithm="fourierrec", minus_log=True, device="cuda", stripe=None,
-                 precision="float32", out_dtype="float32"):
+                 precision="float32", out_dtype="float32", mixed_filter="fft"):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if precision not in ("float32", "mixed"):
             raise NotImplementedError(f"SinoPipeline: precision {precision!r}")
         self.precision = precision
+        if mixed_filter not in ("fft", "tensor"):
+            raise NotImplementedError(f"SinoPipeline: mixed_filter {mixed_filter!r}")
         if out_dtype not in ("float32", "float16"):
             raise NotImplementedError(f"SinoPipeline: out_dtype {out_dtype!r}")
         if out_dtype == "float16" and algorithm != "fourierrec":
@@ -75,8 +79,11 @@ class SinoPipeline:
         self.wfilter = torch.as_tensor(self.wfilter_np, device=self.device)
         self.t = rfftfreq32(self.ne, self.device)
         self._w_cache: dict = {}
-        self.fused = precision == "float32" and _fff.supported(self.n)
-        if precision == "mixed":
+        self.fused = _fff.supported(self.n) and (precision == "float32" or
+                                                  mixed_filter == "fft")
+        # the tensor-core filter on split fp16 planes (mixed precision only)
+        self.tensor_filter = precision == "mixed" and not self.fused
+        if self.tensor_filter:
             from .reconstruction.tcfilter import TCFilter
             self.npl = -(-self.n // 8) * 8  # fp16 row pitch (16-byte TMA rows)
             self.xhi = torch.empty((self.ncz, self.nproj, self.npl), dtype=torch.float16,
@@ -161,7 +168,7 @@ class SinoPipeline:
                       out_poff=fw.poff, stream=stream)
             fw.apply_sino(self.sino, stream)
             src = self.sino[:nz, fw.poff:fw.poff + self.nproj].permute(1, 0, 2)
-            if self.precision == "mixed":
+            if self.tensor_filter:
                 prep_rows_split16(self.xhi, self.xlo, src, darkflat=False,
                                   minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
                                   out_pstride=self.npl, stream=stream)
@@ -174,7 +181,7 @@ class SinoPipeline:
                       out_zstride=self.nproj * self.ne, out_pstride=self.ne, out_xoff=self.pad,
                       out_width=self.ne, edge_pad=True, stream=stream)
             return
-        if self.precision == "mixed":
+        if self.tensor_filter:
             prep_rows_split16(self.xhi, self.xlo, data, d0, f0, darkflat=dark0 is not None,
                               minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
                               out_pstride=self.npl, stream=stream)
@@ -201,7 +208,7 @@ class SinoPipeline:
             return
         s = torch.cuda.current_stream() if stream is None else stream
         with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
-            if self.precision == "mixed":
+            if self.tensor_filter:
                 self.xhi[lz:].zero_()
                 self.xlo[lz:].zero_()
             else:
@@ -209,7 +216,7 @@ class SinoPipeline:
 
     def replicate_first_row(self):
         """Copy slice 0 of the loaded rows to every slice (try-centre sweeps)."""
-        if self.precision == "mixed":
+        if self.tensor_filter:
             self.xhi[1:].copy_(self.xhi[:1].expand(self.ncz - 1, -1, -1))
             self.xlo[1:].copy_(self.xlo[:1].expand(self.ncz - 1, -1, -1))
         else:
@@ -217,7 +224,7 @@ class SinoPipeline:
 
     def save_rows(self):
         """Snapshot of slice 0 needed to refill rows that filtering overwrote (or None)."""
-        return None if (self.precision == "mixed" or self.fused) else self.rows[0].clone()
+        return None if (self.tensor_filter or self.fused) else self.rows[0].clone()
 
     def restore_rows(self, saved):
         if saved is not None:
@@ -291,7 +298,7 @@ class SinoPipeline:
     def filter_and_backproject(self, out, sht=None, stream=None):
         """out [ncz, n, n] of self.out_dtype (contiguous) from the loaded rows."""
         assert out.dtype == self.out_dtype, (out.dtype, self.out_dtype)
-        if self.precision == "mixed":
+        if self.tensor_filter:
             return self._filter_and_backproject_mixed(out, sht, stream)
         if self.fused:
             return self._filter_and_backproject_fused(out, sht, stream)

@@ -63,7 +63,8 @@ class GPURec:
                                       args.reconstruction_algorithm,
                                       minus_log=args.minus_log == "True", device=self.device,
                                       stripe=stripe, precision=self.precision,
-                                      out_dtype=args.out_dtype)
+                                      out_dtype=args.out_dtype,
+                                      mixed_filter=args.mixed_filter)
         return self._pipe
 
     # ------------------------------------------------------------------ helpers
@@ -154,7 +155,8 @@ class GPURec:
             self.sweep = TryCenterSweep(params.n, params.nproj, params.theta, params.center,
                                         params.shift_array, args.fbp_filter, self.precision,
                                         params.ncz, device=dev,
-                                        minus_log=args.minus_log == "True")
+                                        minus_log=args.minus_log == "True",
+                                        mixed_filter=args.mixed_filter)
         sw = self.sweep
         for id_slice in params.id_slices:
             z = int(id_slice)

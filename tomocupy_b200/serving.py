@@ -156,10 +156,10 @@ class Server:
 
     def _estimate_geometry_bytes(self, n, nproj, precision) -> int:
         ncz = self.ncz
-        rows = ncz * nproj * n * (4 if precision == "mixed" else 16)
-        grid = (ncz // 2) * (2 * n) ** 2 * 8 * 2     # grid + cuFFT work area
+        rows = ncz * nproj * n * (4 if n <= 4096 else 16)  # fused filter: unpadded rows
+        grid = (ncz // 2) * (2 * n) ** 2 * 8 * 2     # grid + FFT work area
         lists = nproj * n * 4 * 8
-        tc = 2 * n * n * 2 if precision == "mixed" else 0
+        tc = 20 * 4 * 2 * nproj * n if precision == "mixed" else 0  # gridding records
         return rows + grid + lists + tc + 2 * ncz * n * n * 4 + (ncz // 2) * nproj * n * 8
 
     def _evict(self, need: int) -> None:

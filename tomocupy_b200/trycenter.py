@@ -56,7 +56,7 @@ class TryCenterSweep:
 
     def __init__(self, n, nproj, theta, center, shifts, fbp_filter="parzen",
                  precision="float32", ncz=32, pairs_per_block=0, device="cuda",
-                 minus_log=True):
+                 minus_log=True, mixed_filter="fft"):
         self.device = torch.device(device)
         self.n, self.nproj, self.ncz = int(n), int(nproj), int(ncz)
         self.precision = precision
@@ -66,13 +66,13 @@ class TryCenterSweep:
         self.nchunks = self.sht.shape[0]
         self.pipe = SinoPipeline(self.n, self.nproj, self.ncz, theta, center, fbp_filter,
                                  "fourierrec", minus_log=minus_log, device=self.device,
-                                 precision=precision)
+                                 precision=precision, mixed_filter=mixed_filter)
         if pairs_per_block:
             self.pipe.fr.set_pairs_per_block(pairs_per_block)
         self.pairs_per_block = int(pairs_per_block)
         self.out = torch.empty((self.nchunks * self.ncz, self.n, self.n), dtype=torch.float32,
                                device=self.device)
-        if precision == "mixed":
+        if self.pipe.tensor_filter:
             from .reconstruction.tcfilter import TCFilter
             self.tcf = TCFilter(self.n, self.nproj, self.ncz, self.nchunks * self.ncz,
                                 self.device)
@@ -96,7 +96,7 @@ class TryCenterSweep:
         with torch.cuda.stream(self._stream):
             self.pipe.load_rows(data, dark0, flat0, 0, self._stream)
             self.pipe.replicate_first_row()
-            if self.precision != "mixed" and not self.pipe.fused:
+            if not self.pipe.tensor_filter and not self.pipe.fused:
                 # same buffer on every load: a captured graph reads it
                 if self.saved is None:
                     self.saved = self.pipe.rows[0].clone()
@@ -109,7 +109,7 @@ class TryCenterSweep:
         p = self.pipe
         for k in range(self.nchunks):
             outk = self.out[k * self.ncz:(k + 1) * self.ncz]
-            if self.precision == "mixed":
+            if p.tensor_filter:
                 self.tcf.apply(p.xhi, p.xlo, torch.view_as_complex(p.g), pairs=True,
                                kern0=k * self.ncz, stream=stream)
             elif p.fused:  # the fused filter leaves the rows as they are
