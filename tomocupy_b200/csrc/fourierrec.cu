@@ -455,9 +455,11 @@ __global__ void __launch_bounds__(NTH, 2)
 // power of two so every value is in fp16's normal range) into shared memory
 // in the UMMA K-major 128-byte-swizzled layout, and one thread issues 4 M-groups
 // x 4 K-steps of tcgen05.mma (M = 128 cells, N = 64, K = 16) accumulating in
-// TMEM; the chunk after it is built while they run (two smem stages).  The
-// epilogue sums hi + lo, undoes the scale and stores like grid_blocks.
-// Weights and footprints are computed exactly as grid_blocks computes them.
+// TMEM; while they run, the other CTA on the SM builds its chunk (one smem
+// stage per CTA, two CTAs per SM).  The epilogue sums hi + lo, undoes the
+// scale and stores like grid_blocks.  Weights and footprints are computed
+// exactly as grid_blocks computes them, once per geometry, into records laid
+// out in the order of the tile lists (tile_records).
 constexpr int TCK = 64;                       // samples per chunk (one K block)
 constexpr int TCN = 64;                       // 16 pairs x (re, im) x (hi, lo)
 constexpr int TCM = TX * TY;                  // 512 cells
@@ -465,37 +467,51 @@ constexpr int TC_A = TCM * TCK * 2;           // 64 KB
 constexpr int TC_B = TCN * TCK * 2;           // 8 KB
 constexpr int TC_STAGE = TC_A + TC_B;
 constexpr int TC_THREADS = 512;
-constexpr int TC_REC = 2 + 2 * (2 * M + 1);   // fx, fy (or origin, valid), 9 + 9 weights
 
-// Per-sample footprint record, computed once per geometry with exactly the
-// arithmetic of grid_blocks: [0] fx, [1] fy (grid cells of the footprint
-// centre), [2..10] x-weights, [11..19] y-weights.
-__global__ void sample_records(const float2 *__restrict__ cs, const float *__restrict__ rtab,
-                               const float *__restrict__ etab, Geom geo,
-                               int *__restrict__ recs) {
-  const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = geo.n;
-  if (s >= (size_t)geo.nproj * n) return;
-  const int p = (int)(s / n), i = (int)(s % n);
-  float x0, y0;
-  int fx, fy;
-  sample_pos(cs, rtab, p, i, (float)(2 * n), x0, y0, fx, fy);
-  int *r = recs + s * TC_REC;
-  r[0] = fx;
-  r[1] = fy;
+// Per-(tile, sample) record, computed once per geometry with exactly the
+// arithmetic of grid_blocks, in the order of the tile lists:
+// [0] tile-local footprint origin (lx0 | ly0 << 16), [1] index of the
+// sample's spectrum value p*n + (i + n/2) % n with the odd-i sign in bit 31,
+// [2..10] x-weights, [11..19] y-weights.  80 bytes: five int4.
+constexpr int TC_REC = 2 + 2 * (2 * M + 1);
+static_assert(TC_REC * 4 == 80, "record = 5 int4");
+
+__global__ void tile_records(const float2 *__restrict__ cs, const float *__restrict__ rtab,
+                             const float *__restrict__ etab, const long long *__restrict__ toffs,
+                             const int *__restrict__ tlist, Geom geo, int *__restrict__ trec) {
+  const int tile = blockIdx.x;
+  const int n = geo.n, twon = geo.twon;
+  const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
+  const int X0 = ix0 - n, Y0 = iy0 - n;
+  const long long t0 = toffs[tile];
+  const int S = (int)(toffs[tile + 1] - t0);
+  for (int k = threadIdx.x; k < S; k += blockDim.x) {
+    const int sidx = tlist[t0 + k];
+    const int p = sidx / n, i = sidx % n;
+    float x0, y0;
+    int fx, fy;
+    sample_pos(cs, rtab, p, i, (float)(2 * n), x0, y0, fx, fy);
+    int *r = trec + (t0 + k) * TC_REC;
+    r[0] = (tile_origin(fx, X0, twon) & 0xFFFF) | (tile_origin(fy, Y0, twon) << 16);
+    int ii = i + n / 2;
+    if (ii >= n) ii -= n;
+    r[1] = (p * n + ii) | ((i & 1) << 31);
 #pragma unroll
-  for (int d = 0; d < 2 * M + 1; d++) {
-    float w0 = etab[fx - M + d + n + M + EPAD] - x0;
-    float w1 = etab[fy - M + d + n + M + EPAD] - y0;
-    r[2 + d] = __float_as_int(__expf(geo.coeff1 * w0 * w0));
-    r[2 + 2 * M + 1 + d] = __float_as_int(__expf(geo.coeff1 * w1 * w1));
+    for (int d = 0; d < 2 * M + 1; d++) {
+      float w0 = etab[fx - M + d + n + M + EPAD] - x0;
+      float w1 = etab[fy - M + d + n + M + EPAD] - y0;
+      r[2 + d] = __float_as_int(__expf(geo.coeff1 * w0 * w0));
+      r[2 + 2 * M + 1 + d] = __float_as_int(__expf(geo.coeff1 * w1 * w1));
+    }
   }
 }
+
 // One smem stage per CTA and two CTAs per SM (2 x 256 TMEM columns = all 512):
 // one CTA builds its next chunk while the other's MMAs and loads are in flight.
-constexpr int TC_STAGES = 1;
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE + TC_STAGES * TCK * TC_REC * 4 + 64 + 1024;
+constexpr int TC_SMEM = TC_STAGE + TCK * TC_REC * 4 + 64 + 1024;
 constexpr uint32_t TC_IDESC = tc::idesc_f16_f32(128, TCN);
+constexpr int TC_RV4 = TCK * TC_REC / 4;   // int4 per chunk of records (320)
+constexpr int TC_VT = ZMAX * (TCK / 8);    // value threads: (pair, 8-sample group) = 128
 
 __global__ void absmax_kernel(const float2 *__restrict__ g, size_t total,
                               unsigned *__restrict__ out) {
@@ -514,28 +530,35 @@ __device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
   l = __float2half_rn(v - __half2float(h));
 }
 
+__device__ __forceinline__ uint32_t pack_h2(__half a, __half b) {
+  return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+
+// Tensor-core gridding of one tile and up to ZMAX slice pairs.  Per chunk of
+// TCK listed samples: the records (contiguous per tile, loaded as int4 one
+// chunk ahead into registers), the spectrum values of 16 pairs (one thread
+// per pair and 8-sample group, written as 16-byte rows of B), W zeroed and
+// the footprint weights scattered; then one thread issues the MMAs.  The
+// value indices run two chunks ahead so that the value loads of the next
+// chunk need no dependent load.
 __global__ void __launch_bounds__(TC_THREADS, 2)
     grid_tc(const float2 *__restrict__ G, float2 *__restrict__ grid,
-            const float2 *__restrict__ cs, const float *__restrict__ rtab,
-            const float *__restrict__ etab, const int *__restrict__ tile_order,
-            const long long *__restrict__ toffs, const int *__restrict__ tlist,
-            const int *__restrict__ recs, const unsigned *__restrict__ amax_bits, Geom geo,
+            const int *__restrict__ tile_order, const long long *__restrict__ toffs,
+            const int *__restrict__ trec, const unsigned *__restrict__ amax_bits, Geom geo,
             int *__restrict__ err) {
   using namespace tcb::tc;
   extern __shared__ uint8_t tsm_raw[];
   uint8_t *sm = tsm_raw + ((1024u - (smem_u32(tsm_raw) & 1023u)) & 1023u);
-  int *rec = reinterpret_cast<int *>(sm + TC_STAGES * TC_STAGE);   // [stages][TCK][TC_REC]
-  uint64_t *mma_done = reinterpret_cast<uint64_t *>(rec + TC_STAGES * TCK * TC_REC);
+  uint8_t *A = sm, *B = sm + TC_A;
+  int *R = reinterpret_cast<int *>(sm + TC_STAGE);   // [TCK][TC_REC]
+  uint64_t *mma_done = reinterpret_cast<uint64_t *>(R + TCK * TC_REC);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 2);
   const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
   const int zgroups = (geo.nz + ZMAX - 1) / ZMAX;
   const int tile = tile_order[blockIdx.x / zgroups];
   const int z0 = (blockIdx.x % zgroups) * ZMAX;
   const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
-  const int X0 = ix0 - n, Y0 = iy0 - n;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const float twonf = (float)(2 * n);
-  const int half = n / 2;
   // power-of-two scale that puts max |G| in [2^13, 2^14)
   const float amax = __uint_as_float(*amax_bits);
   int ex = 0;
@@ -544,7 +567,6 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 
   if (tid == 0) {
     mbar_init(&mma_done[0], 1);
-    mbar_init(&mma_done[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) tmem_alloc(tmem_slot, 256);
@@ -556,115 +578,95 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   const long long t0 = toffs[tile];
   const int S = (int)(toffs[tile + 1] - t0);
   const int nch = (S + TCK - 1) / TCK;
-  // Register prefetch of one chunk: this thread's record words (e = tid + j*TC_THREADS
-  // of TCK x TC_REC) and spectrum values (e = tid + j*TC_THREADS of TCK x ZMAX).
-  constexpr int NRW = (TCK * TC_REC + TC_THREADS - 1) / TC_THREADS;  // 3
-  constexpr int NGV = (TCK * ZMAX + TC_THREADS - 1) / TC_THREADS;    // 2
-  int pr[NRW], pr1[NRW];
-  float2 pg[NGV];
-  int pc[NGV];
-  auto prefetch = [&](int cc) {
+  const int4 *rec4 = reinterpret_cast<const int4 *>(trec + t0 * TC_REC);
+  // value thread: pair vz, samples 8 vg .. 8 vg + 7 of a chunk
+  const int vz = tid >> 3, vg = tid & 7;
+  const bool vthread = tid < TC_VT && z0 + vz < geo.nz;
+  const float2 *Gz = G + (size_t)(vthread ? z0 + vz : 0) * nproj * n;
+  int4 prec = make_int4(0, 0, 0, 0);   // this thread's int4 of the next chunk's records
+  int vi_next[8], vi_next2[8];         // value indices (with sign bit) one / two chunks ahead
+  float2 pv[8];                        // the next chunk's values
+  auto load_vidx = [&](int cc, int (&vi)[8]) {
 #pragma unroll
-    for (int j = 0; j < NRW; j++) {
-      const int e = tid + j * TC_THREADS;
-      pr[j] = 0;
-      pr1[j] = 0;
-      if (e < TCK * TC_REC) {
-        const int k = e / TC_REC, w = e % TC_REC;
-        const int idx = cc * TCK + k;
-        if (idx < S) {
-          const int sidx = tlist[t0 + idx];
-          if (w >= 2) {
-            pr[j] = recs[(size_t)sidx * TC_REC + w];
-          } else if (w == 0) {
-            pr[j] = recs[(size_t)sidx * TC_REC];
-            pr1[j] = recs[(size_t)sidx * TC_REC + 1];
-          } else {
-            pr[j] = sidx + 1;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < NGV; j++) {
-      const int e = tid + j * TC_THREADS;
-      pc[j] = 0;
-      pg[j] = make_float2(0.f, 0.f);
-      if (e < TCK * ZMAX) {
-        const int k = e % TCK, pz = e / TCK;
-        const int idx = cc * TCK + k;
-        if (idx < S && z0 + pz < geo.nz) {
-          const int sidx = tlist[t0 + idx];
-          const int pp = sidx / n, i = sidx % n;
-          int ii = i + half;
-          if (ii >= n) ii -= n;
-          pc[j] = 1 + (i & 1);
-          pg[j] = G[(size_t)(z0 + pz) * nproj * n + (size_t)pp * n + ii];
-        }
-      }
+    for (int j = 0; j < 8; j++) {
+      const int k = cc * TCK + vg * 8 + j;
+      vi[j] = (vthread && k < S) ? __ldg(trec + (t0 + k) * TC_REC + 1) : -1;
     }
   };
+  auto load_vals = [&](const int (&vi)[8]) {
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      pv[j] = vi[j] != -1 ? __ldg(Gz + (vi[j] & 0x7fffffff)) : make_float2(0.f, 0.f);
+  };
+  auto load_rec = [&](int cc) {  // int4 tid of chunk cc: record cc*TCK + tid/5
+    prec = make_int4(0, 0, 0, 0);
+    if (tid < TC_RV4 && cc * TCK + tid / (TC_REC / 4) < S)
+      prec = __ldg(rec4 + (size_t)cc * TC_RV4 + tid);
+  };
+  if (nch > 0) {
+    load_rec(0);
+    load_vidx(0, vi_next);
+    load_vals(vi_next);
+    load_vidx(1, vi_next2);
+  }
   bool ok = true;
-  if (nch > 0) prefetch(0);
   for (int c = 0; c < nch; c++) {
-    const int st = c % TC_STAGES;
-    uint8_t *A = sm + st * TC_STAGE, *B = A + TC_A;
-    int *R = rec + st * TCK * TC_REC;
-    // the MMAs that last read this stage (chunk c - TC_STAGES) must be done; one
-    // thread polls the mbarrier, the others wait at the block barrier
-    if (tid == 0 && c >= TC_STAGES && !mbar_wait(&mma_done[st], ((c / TC_STAGES) - 1) & 1))
-      ok = false;
+    const int cnt = min(TCK, S - c * TCK);
+    // the MMAs of chunk c - 1 read A and B: wait for them (one thread polls)
+    if (tid == 0 && c > 0 && !mbar_wait(&mma_done[0], (c - 1) & 1)) ok = false;
     ok = __syncthreads_and(ok);
     if (!ok) break;
-    // (1) records and (3) spectrum values of this chunk from the prefetch registers
+    // (1) records of this chunk, (2) values as fp16 hi/lo rows of B, (3) W = 0
+    if (tid < TC_RV4) reinterpret_cast<int4 *>(R)[tid] = prec;
+    if (tid < TC_VT) {
+      uint32_t rows[4][4];  // [re_hi, im_hi, re_lo, im_lo][8 samples as 4 half2]
 #pragma unroll
-    for (int j = 0; j < NRW; j++) {
-      const int e = tid + j * TC_THREADS;
-      if (e < TCK * TC_REC) {
-        const int w = e % TC_REC;
-        int v = pr[j];
-        if (w == 0) {
-          const int k = e / TC_REC;
-          v = (c * TCK + k < S) ? ((tile_origin(pr[j], X0, twon) & 0xFFFF) |
-                                   (tile_origin(pr1[j], Y0, twon) << 16))
-                                : 0;
+      for (int j = 0; j < 8; j += 2) {
+        __half h[2][4];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int vi = vi_next[j + q];
+          float re = 0.f, im = 0.f;
+          if (vi != -1) {
+            const float sg = ((vi < 0) ? -geo.scale : geo.scale) * gsc;
+            re = pv[j + q].x * sg;
+            im = pv[j + q].y * sg;
+          }
+          split_half(re, h[q][0], h[q][2]);
+          split_half(im, h[q][1], h[q][3]);
         }
-        R[e] = v;  // e == k * TC_REC + w
+#pragma unroll
+        for (int c4 = 0; c4 < 4; c4++) rows[c4][j / 2] = pack_h2(h[0][c4], h[1][c4]);
+      }
+#pragma unroll
+      for (int c4 = 0; c4 < 4; c4++) {
+        const int row = vz * 4 + c4;
+        *reinterpret_cast<uint4 *>(B + (row >> 3) * 1024 + (row & 7) * 128 +
+                                   (((vg ^ row) & 7) << 4)) =
+            make_uint4(rows[c4][0], rows[c4][1], rows[c4][2], rows[c4][3]);
       }
     }
-#pragma unroll
-    for (int j = 0; j < NGV; j++) {
-      const int e = tid + j * TC_THREADS;
-      if (e < TCK * ZMAX) {
-        const int k = e % TCK, pz = e / TCK;
-        __half rh = __float2half_rn(0.f), rl = rh, ih = rh, il = rh;
-        if (pc[j]) {
-          const float sg = ((pc[j] == 2) ? -geo.scale : geo.scale) * gsc;
-          split_half(pg[j].x * sg, rh, rl);
-          split_half(pg[j].y * sg, ih, il);
-        }
-        const int row = pz * 4;
-        *reinterpret_cast<__half *>(B + sw128_offset(row + 0, k)) = rh;
-        *reinterpret_cast<__half *>(B + sw128_offset(row + 1, k)) = ih;
-        *reinterpret_cast<__half *>(B + sw128_offset(row + 2, k)) = rl;
-        *reinterpret_cast<__half *>(B + sw128_offset(row + 3, k)) = il;
-      }
-    }
-    // (2) clear W (most entries are outside every footprint)
     {
-      uint4 zero = make_uint4(0, 0, 0, 0);
+      const uint4 zero = make_uint4(0, 0, 0, 0);
       uint4 *a4 = reinterpret_cast<uint4 *>(A);
+#pragma unroll
       for (int q = tid; q < TC_A / 16; q += TC_THREADS) a4[q] = zero;
     }
     __syncthreads();
-    // the next chunk's loads fly while this one is scattered and multiplied
-    if (c + 1 < nch) prefetch(c + 1);
-    // (4) scatter the footprint weights into W[cell][sample]: one thread per
-    // (sample, footprint row); consecutive threads take consecutive samples
+    // the next chunk's records and values (and the value indices after it) fly
+    // while this one is scattered and multiplied
+    if (c + 1 < nch) {
+      load_rec(c + 1);
+#pragma unroll
+      for (int j = 0; j < 8; j++) vi_next[j] = vi_next2[j];
+      load_vals(vi_next);
+      if (c + 2 < nch) load_vidx(c + 2, vi_next2);
+    }
+    // (4) footprint weights into W[cell][sample]: one thread per (sample, row)
     for (int e = tid; e < TCK * (2 * M + 1); e += TC_THREADS) {
       const int k = e % TCK, dy = e / TCK;
+      if (k >= cnt) continue;
       const int *r = R + k * TC_REC;
-      if (!r[1]) continue;
       const int o = r[0];
       const int ly = (o >> 16) + dy;
       if ((unsigned)ly >= (unsigned)TY) continue;
@@ -676,7 +678,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       for (int dx = 0; dx < 2 * M + 1; dx++) {
         const int lx = ox + dx;
         if ((unsigned)lx < (unsigned)TX) {
-          const int m = ly * TX + lx;  // row of W (cell); rows of one tile row share 8-row groups
+          const int m = ly * TX + lx;
           const float w = __int_as_float(r[2 + dx]) * wyv;
           *reinterpret_cast<__half *>(A + (m >> 3) * 1024 + (m & 7) * 128 +
                                       (((kchunk ^ m) & 7) << 4) + kcol) = __float2half_rn(w);
@@ -685,7 +687,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     }
     fence_proxy_async_smem();
     __syncthreads();
-    // (5) one thread issues the chunk's MMAs; the next chunk is built meanwhile
+    // (5) one thread issues the chunk's MMAs
     if (tid == 0) {
       tc_fence_after();
       const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
@@ -695,12 +697,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
         for (int kk = 0; kk < TCK / 16; kk++)
           mma_f16(tmem + g * TCN, sdesc(a0 + g * 16384 + kk * 32), sdesc(b0 + kk * 32),
                   TC_IDESC, (c > 0 || kk > 0) ? 1u : 0u);
-      mma_commit(&mma_done[st]);
+      mma_commit(&mma_done[0]);
     }
   }
-  if (tid == 0 && ok && nch > 0 &&
-      !mbar_wait(&mma_done[(nch - 1) % TC_STAGES], ((nch - 1) / TC_STAGES) & 1))
-    ok = false;
+  if (tid == 0 && ok && nch > 0 && !mbar_wait(&mma_done[0], (nch - 1) & 1)) ok = false;
   ok = __syncthreads_and(ok);
   tc_fence_after();
   // Epilogue: warp w reads TMEM lanes 32(w%4).. of M-group w/4 (16 warps, 4 groups).
@@ -1024,7 +1024,7 @@ struct tcb_fourierrec {
   bool out_f16 = false;       // fp16 output slices (set_output) with fp32 input
   bool spectrum_in = false;   // g already holds the projection FFT (set_input_spectrum)
   unsigned *amax = nullptr;   // max |G| bits for the tensor-core gridding scale
-  int *recs = nullptr;        // per-sample footprint records (tensor-core gridding)
+  int *trec = nullptr;        // per-(tile, sample) records (tensor-core gridding)
   int *tc_err = nullptr;      // set by a tensor-core gridding wait that timed out
   float2 *t1 = nullptr;  // first-pass output: [nz][2n][n] rows first, [nz][n][2n] columns first
   float2 *tw = nullptr;  // per-stage twiddle table of the length-2n transforms
@@ -1059,8 +1059,8 @@ void fr_release(tcb_fourierrec *h) {
   h->dtab = nullptr;
   cudaFree(h->amax);
   cudaFree(h->tc_err);
-  cudaFree(h->recs);
-  h->recs = nullptr;
+  cudaFree(h->trec);
+  h->trec = nullptr;
   h->t1 = h->tw = nullptr;
   h->amax = nullptr;
   h->tc_err = nullptr;
@@ -1119,8 +1119,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
                                                                                       h->amax);
     const unsigned zgroups = (unsigned)((h->nz + ZMAX - 1) / ZMAX);
     grid_tc<<<(unsigned)h->ntiles * zgroups, TC_THREADS, TC_SMEM, s>>>(
-        gc, h->grid, h->cs, h->rtab, h->etab, h->tile_order, h->toffs, h->tlist, h->recs, h->amax,
-        geo, h->tc_err);
+        gc, h->grid, h->tile_order, h->toffs, h->trec, h->amax, geo, h->tc_err);
     TCB_LAUNCH_CHECK();
     count_launch(2);
   } else {
@@ -1462,18 +1461,23 @@ extern "C" int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode) {
   TCB_CHECK_ARG(mode == TCB_GRID_FP32 || mode == TCB_GRID_TENSOR,
                 "tcb_fourierrec_set_gridding: unknown mode %d", mode);
   if (mode == TCB_GRID_TENSOR && !h->amax) {
-    const size_t nsamp = h->nproj * h->n;
+    TCB_CHECK_ARG(h->nproj * h->n < (size_t)INT32_MAX,
+                  "tcb_fourierrec_set_gridding: nproj * n too large for the tensor gridding");
+    long long total = 0;  // listed (tile, sample) entries
+    TCB_CUDA(cudaMemcpy(&total, h->toffs + h->ntiles, sizeof(long long),
+                        cudaMemcpyDeviceToHost));
     if (cudaMalloc(&h->amax, sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&h->tc_err, sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&h->recs, nsamp * TC_REC * sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&h->trec, ((size_t)total + 1) * TC_REC * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
-      set_error("tcb_fourierrec_set_gridding: out of device memory");
+      set_error("tcb_fourierrec_set_gridding: out of device memory (%lld records)", total);
       return TCB_ERR_OUT_OF_MEMORY;
     }
     TCB_CUDA(cudaMemset(h->tc_err, 0, sizeof(int)));
     TCB_CUDA(cudaFuncSetAttribute(grid_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   TC_SMEM));
-    sample_records<<<ceil_div(nsamp, 256), 256>>>(h->cs, h->rtab, h->etab, h->geo, h->recs);
+    tile_records<<<(unsigned)h->ntiles, 256>>>(h->cs, h->rtab, h->etab, h->toffs, h->tlist,
+                                               h->geo, h->trec);
     count_launch();
     TCB_CUDA(cudaDeviceSynchronize());
   }
