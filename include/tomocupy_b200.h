@@ -262,9 +262,9 @@ int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs);
 /* Gridding mode (no reference counterpart).  TCB_GRID_FP32: the fp32
  * register-accumulation gridding (default; the drop-in).  TCB_GRID_TENSOR:
  * mixed precision on the tensor cores -- footprint weights and the spectrum
- * values (hi/lo split, power-of-two scaled) in fp16, fp32 accumulation in
- * TMEM; used by the mixed-precision path.  status: 1 in *timed_out when a
- * tensor-core gridding wait gave up (synchronous). */
+ * values (power-of-two scaled) in fp16, fp32 accumulation in TMEM, 32 slice
+ * pairs per weight matrix; used by the mixed-precision path.  status: 1 in
+ * *timed_out when a tensor-core gridding wait gave up (synchronous). */
 #define TCB_GRID_FP32 0
 #define TCB_GRID_TENSOR 1
 int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode);

@@ -173,11 +173,12 @@ def test_fourierrec_own_fft_matches_cufft(cuda, monkeypatch, n, nproj, nz):
 
 
 @pytest.mark.parametrize("n,nproj,nz", [(128, 90, 2), (200, 120, 3), (512, 360, 16),
-                                        (256, 180, 20), (2048, 64, 8)])
+                                        (256, 180, 20), (2048, 64, 8), (256, 100, 40)])
 def test_fourierrec_tensor_gridding_vs_fp32(cuda, n, nproj, nz):
-    """Mixed-precision gridding (fp16 weights and hi/lo values on tcgen05, fp32
-    accumulation) against the fp32 gridding: partial tiles (n = 200), pair
-    counts that are not a multiple of 16, more than 16 pairs (two groups)."""
+    """Mixed-precision gridding (fp16 weights and values on tcgen05, fp32
+    accumulation, 32 slice pairs per CTA) against the fp32 gridding: partial
+    tiles (n = 200), pair counts that are not a multiple of 32, more than 32
+    pairs (two groups)."""
     from tomocupy_b200 import _lib, cfunc_fourierrec
     theta = torch.as_tensor(_theta(nproj, "random"), device=cuda)
     g = torch.randn((nz, nproj, n, 2), device=cuda) * 100.0
@@ -193,6 +194,7 @@ def test_fourierrec_tensor_gridding_vs_fp32(cuda, n, nproj, nz):
         op.free()
     assert torch.isfinite(out[_lib.GRID_TENSOR]).all()
     err = rel_l2(out[_lib.GRID_TENSOR], out[_lib.GRID_FP32])
+    print(f"tensor gridding n={n} nz={nz}: rel-L2 vs fp32 {err:.2e}")
     assert err < 1e-3, err
 
 

@@ -449,19 +449,20 @@ __global__ void __launch_bounds__(NTH, 2)
 // For one 32 x 16 tile and up to 16 slice pairs, gridding is the product
 //   D[cell, comp] = sum_s W[cell, s] * Gv[s, comp]
 // with W[cell, s] = wx_s[cell.x - ox_s] * wy_s[cell.y - oy_s] (zero outside
-// the sample's 9 x 9 footprint) and Gv the sample's spectrum values of the 16
+// the sample's 9 x 9 footprint) and Gv the sample's spectrum values of 32
 // pairs (re, im).  Per chunk of 64 listed samples the CTA writes W (512 x 64,
-// fp16) and Gv (64 x 64: 16 pairs x (re, im) x (hi, lo) fp16, scaled by a
-// power of two so every value is in fp16's normal range) into shared memory
+// fp16) and Gv (64 x 64: 32 pairs x (re, im) fp16, scaled by a power of two
+// that puts max |G| at 2^13..2^14) into shared memory
 // in the UMMA K-major 128-byte-swizzled layout, and one thread issues 4 M-groups
 // x 4 K-steps of tcgen05.mma (M = 128 cells, N = 64, K = 16) accumulating in
 // TMEM; while they run, the other CTA on the SM builds its chunk (one smem
-// stage per CTA, two CTAs per SM).  The epilogue sums hi + lo, undoes the
-// scale and stores like grid_blocks.  Weights and footprints are computed
+// stage per CTA, two CTAs per SM).  The epilogue undoes the scale and
+// stores like grid_blocks.  Weights and footprints are computed
 // exactly as grid_blocks computes them, once per geometry, into records laid
 // out in the order of the tile lists (tile_records).
 constexpr int TCK = 64;                       // samples per chunk (one K block)
-constexpr int TCN = 64;                       // 16 pairs x (re, im) x (hi, lo)
+constexpr int TCZ = 32;                       // slice pairs per tensor-gridding CTA
+constexpr int TCN = 2 * TCZ;                  // 32 pairs x (re, im)
 constexpr int TCM = TX * TY;                  // 512 cells
 constexpr int TC_A = TCM * TCK * 2;           // 64 KB
 constexpr int TC_B = TCN * TCK * 2;           // 8 KB
@@ -511,7 +512,7 @@ __global__ void tile_records(const float2 *__restrict__ cs, const float *__restr
 constexpr int TC_SMEM = TC_STAGE + TCK * TC_REC * 4 + 64 + 1024;
 constexpr uint32_t TC_IDESC = tc::idesc_f16_f32(128, TCN);
 constexpr int TC_RV4 = TCK * TC_REC / 4;   // int4 per chunk of records (320)
-constexpr int TC_VT = ZMAX * (TCK / 8);    // value threads: (pair, 8-sample group) = 128
+constexpr int TC_VT = TCZ * (TCK / 8);     // value threads: (pair, 8-sample group) = 256
 
 __global__ void absmax_kernel(const float2 *__restrict__ g, size_t total,
                               unsigned *__restrict__ out) {
@@ -525,18 +526,13 @@ __global__ void absmax_kernel(const float2 *__restrict__ g, size_t total,
   if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out, __float_as_uint(m));  // m >= 0: int order
 }
 
-__device__ __forceinline__ void split_half(float v, __half &h, __half &l) {
-  h = __float2half_rn(v);
-  l = __float2half_rn(v - __half2float(h));
-}
-
 __device__ __forceinline__ uint32_t pack_h2(__half a, __half b) {
   return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
 }
 
-// Tensor-core gridding of one tile and up to ZMAX slice pairs.  Per chunk of
+// Tensor-core gridding of one tile and up to TCZ slice pairs.  Per chunk of
 // TCK listed samples: the records (contiguous per tile, loaded as int4 one
-// chunk ahead into registers), the spectrum values of 16 pairs (one thread
+// chunk ahead into registers), the spectrum values of 32 pairs (one thread
 // per pair and 8-sample group, written as 16-byte rows of B), W zeroed and
 // the footprint weights scattered; then one thread issues the MMAs.  The
 // value indices run two chunks ahead so that the value loads of the next
@@ -554,9 +550,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   uint64_t *mma_done = reinterpret_cast<uint64_t *>(R + TCK * TC_REC);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 2);
   const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
-  const int zgroups = (geo.nz + ZMAX - 1) / ZMAX;
+  const int zgroups = (geo.nz + TCZ - 1) / TCZ;
   const int tile = tile_order[blockIdx.x / zgroups];
-  const int z0 = (blockIdx.x % zgroups) * ZMAX;
+  const int z0 = (blockIdx.x % zgroups) * TCZ;
   const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // power-of-two scale that puts max |G| in [2^13, 2^14)
@@ -616,13 +612,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     if (tid == 0 && c > 0 && !mbar_wait(&mma_done[0], (c - 1) & 1)) ok = false;
     ok = __syncthreads_and(ok);
     if (!ok) break;
-    // (1) records of this chunk, (2) values as fp16 hi/lo rows of B, (3) W = 0
+    // (1) records of this chunk, (2) values as fp16 rows of B, (3) W = 0
     if (tid < TC_RV4) reinterpret_cast<int4 *>(R)[tid] = prec;
     if (tid < TC_VT) {
-      uint32_t rows[4][4];  // [re_hi, im_hi, re_lo, im_lo][8 samples as 4 half2]
+      uint32_t rows[2][4];  // [re, im][8 samples as 4 half2]
 #pragma unroll
       for (int j = 0; j < 8; j += 2) {
-        __half h[2][4];
+        __half h[2][2];
 #pragma unroll
         for (int q = 0; q < 2; q++) {
           const int vi = vi_next[j + q];
@@ -632,18 +628,18 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
             re = pv[j + q].x * sg;
             im = pv[j + q].y * sg;
           }
-          split_half(re, h[q][0], h[q][2]);
-          split_half(im, h[q][1], h[q][3]);
+          h[q][0] = __float2half_rn(re);
+          h[q][1] = __float2half_rn(im);
         }
 #pragma unroll
-        for (int c4 = 0; c4 < 4; c4++) rows[c4][j / 2] = pack_h2(h[0][c4], h[1][c4]);
+        for (int c2 = 0; c2 < 2; c2++) rows[c2][j / 2] = pack_h2(h[0][c2], h[1][c2]);
       }
 #pragma unroll
-      for (int c4 = 0; c4 < 4; c4++) {
-        const int row = vz * 4 + c4;
+      for (int c2 = 0; c2 < 2; c2++) {
+        const int row = vz * 2 + c2;
         *reinterpret_cast<uint4 *>(B + (row >> 3) * 1024 + (row & 7) * 128 +
                                    (((vg ^ row) & 7) << 4)) =
-            make_uint4(rows[c4][0], rows[c4][1], rows[c4][2], rows[c4][3]);
+            make_uint4(rows[c2][0], rows[c2][1], rows[c2][2], rows[c2][3]);
       }
     }
     {
@@ -721,11 +717,11 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       }
       if (!ok || cx >= twon || cy >= twon) continue;
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const int pz = c0 / 4 + j;
+      for (int j = 0; j < 16; j++) {
+        const int pz = c0 / 2 + j;
         if (z0 + pz < geo.nz)
           grid[((size_t)(z0 + pz) * twon + cy) * twon + cx] =
-              make_float2((v[4 * j] + v[4 * j + 2]) * sgn, (v[4 * j + 1] + v[4 * j + 3]) * sgn);
+              make_float2(v[2 * j] * sgn, v[2 * j + 1] * sgn);
       }
     }
   }
@@ -1117,7 +1113,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     TCB_CUDA(cudaMemsetAsync(h->amax, 0, sizeof(unsigned), s));
     absmax_kernel<<<std::min<unsigned>(ceil_div(gtot, 256), 148u * 16u), 256, 0, s>>>(gc, gtot,
                                                                                       h->amax);
-    const unsigned zgroups = (unsigned)((h->nz + ZMAX - 1) / ZMAX);
+    const unsigned zgroups = (unsigned)((h->nz + TCZ - 1) / TCZ);
     grid_tc<<<(unsigned)h->ntiles * zgroups, TC_THREADS, TC_SMEM, s>>>(
         gc, h->grid, h->tile_order, h->toffs, h->trec, h->amax, geo, h->tc_err);
     TCB_LAUNCH_CHECK();
