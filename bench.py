@@ -335,7 +335,7 @@ def run_try(a, dev):
     outs = {}
     for prec in ("float32", "mixed"):
         tune = autotune(n, P, theta, center, shifts, data, d0, f0, fbp_filter="parzen",
-                        precision=prec, candidates=[(16, 8), (32, 8), (32, 16)], reps=1)
+                        precision=prec, candidates=[(32, 8), (32, 16), (64, 16)], reps=1)
         sw = TryCenterSweep(n, P, theta, center, shifts, "parzen", prec, tune["ncz"],
                             tune["pairs_per_block"], dev)
         sw.load(data, d0, f0)
@@ -631,6 +631,7 @@ def run_ours(a, ws, rank, local):
                                    f"filter, {a.algorithm}; ring removal "
                                    f"{'fw level 7 sigma 1 sym16' if a.ring_removal else 'off'}",
                        "n": a.n, "nproj": a.nproj, "nz": a.nz, "ncz": a.ncz,
+                       "e2e_ncz": a.e2e_ncz,
                        "precision": primary,
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "inputs (12.6 GB frames) larger than L2; no flush"},
@@ -662,12 +663,13 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank, precision=None, out_dtype
     osz = 2 if out_dtype == "float16" else 4
     full_bytes = data.numel() * 2 + a.nz * a.n * a.n * osz
     nz_e2e = a.nz if (avail > 3 * full_bytes * ws) else min(a.nz, a.e2e_slab)
-    nz_e2e -= nz_e2e % a.ncz
+    ncz = a.e2e_ncz  # the conveyor overlaps copies chunk by chunk: smaller chunks fill sooner
+    nz_e2e -= nz_e2e % ncz
     d_host = data[:, :nz_e2e].cpu().pin_memory()
     dk_host = dark[:, :nz_e2e].cpu().pin_memory()
     fl_host = flat[:, :nz_e2e].cpu().pin_memory()
     global_vars.reset(reconstruction_algorithm=a.algorithm, fbp_filter=a.filter,
-                      nsino_per_chunk=a.ncz, dtype=precision or a.precision, out_dtype=out_dtype,
+                      nsino_per_chunk=ncz, dtype=precision or a.precision, out_dtype=out_dtype,
                       **_ring_removal(a))
     reader = ArrayReader(d_host, dk_host, fl_host, theta=theta)
     writer = ArrayWriter(device="cpu", pin=True,
@@ -796,7 +798,9 @@ def main():
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--nproj", type=int, default=1500)
     ap.add_argument("--nz", type=int, default=2048)
-    ap.add_argument("--ncz", type=int, default=32)
+    ap.add_argument("--ncz", type=int, default=64)
+    ap.add_argument("--e2e-ncz", type=int, default=32,
+                    help="rows per chunk of the end-to-end (host buffer) leg")
     ap.add_argument("--algorithm", default="fourierrec", choices=["fourierrec", "lprec", "linerec"])
     ap.add_argument("--filter", default="shepp")
     ap.add_argument("--seed", type=int, default=0)

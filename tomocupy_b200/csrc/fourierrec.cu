@@ -52,7 +52,6 @@ constexpr int NRX = TX / RX, NRY = TY / RY;
 constexpr int NREG = NRX * NRY; // 16 blocks = 16 warps per tile
 constexpr int NTH = NREG * 32;  // 512 threads
 constexpr int SC = 256;         // samples staged per chunk
-constexpr int ZMAX = 16;        // slice pairs per CTA
 constexpr int SETUP_NT = 256;
 // Margin of the ell/(2n) table: __cosf/__sinf may exceed 1 in magnitude by an
 // ulp, which moves floor(2n*x0) one cell below -n.
@@ -854,8 +853,13 @@ __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16)) iff
 }
 
 // Rows-first order.  Pass 1 (rows): one row y of a pair's N x N grid per
-// block; the inverse FFT along x keeps x' in [n/2, 3n/2) in
-// t1[pair][y][x' - n/2] (N x n).  Only n of the N outputs are written.
+// block; the inverse FFT along x keeps x' in [n/2, 3n/2) and writes column
+// c = x' - n/2 to t1[pair][c / GW][y][c % GW] (GW = 16 columns: each row
+// writes whole 128-byte lines, and the columns that pass 2 reads lie in
+// 128-byte lines of one contiguous N x GW array).  Only n of the N outputs
+// are written.
+constexpr int T1_GW = 16;  // columns per group of the row-pass output (n >= 128)
+
 template <int N>
 __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
     ifft_rows_first(const float2 *__restrict__ grid, float2 *__restrict__ t1,
@@ -863,12 +867,13 @@ __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
   extern __shared__ float2 fsm[];
   constexpr int n = N / 2;
   const size_t row = blockIdx.x;  // pair * N + y
+  const int y = (int)(row % N);
   const float2 *src = grid + row * N;
-  float2 *dst = t1 + row * n;
+  float2 *dst = t1 + (row - y) * n + (size_t)y * T1_GW;  // pair base + row offset in a group
   auto in = [src](int e) { return __ldg(src + e); };
-  auto out = [dst](int o, float2 v) {
+  auto out = [&](int o, float2 v) {
     const unsigned x = (unsigned)(o - N / 4);
-    if (x < (unsigned)n) dst[x] = v;
+    if (x < (unsigned)n) dst[(size_t)(x / T1_GW) * N * T1_GW + x % T1_GW] = v;
   };
   fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
 }
@@ -888,10 +893,11 @@ __global__ void __launch_bounds__(1024) ifft_cols_deapod(const float2 *__restric
   const int c = threadIdx.x % cpc, tid = threadIdx.x / cpc;
   const int ncb = n / cpc;
   const int z = blockIdx.x / ncb, tx = (blockIdx.x % ncb) * cpc + c;
-  const float2 *src = t1 + (size_t)z * N * n + tx;
+  // column tx in its group of T1_GW columns (row stride T1_GW)
+  const float2 *src = t1 + (size_t)z * N * n + (size_t)(tx / T1_GW) * N * T1_GW + tx % T1_GW;
   const float4 X = __ldg(dtab + tx);
   const float mun2 = geo.mu * (n * n), nsign = (float)(1 - n % 4);
-  auto in = [src](int e) { return __ldg(src + (size_t)e * n); };
+  auto in = [src](int e) { return __ldg(src + (size_t)e * T1_GW); };
   auto out = [&](int o, float2 v) {
     const unsigned ty = (unsigned)(o - (N / 4 + 1));
     if (ty < (unsigned)n)

@@ -181,7 +181,7 @@ def autotune(n, nproj, theta, center, shifts, data, dark0=None, flat0=None, *,
              cache_file=None, device="cuda"):
     """Pick (ncz, pairs_per_block) with the fastest captured sweep for this geometry.
 
-    candidates: iterable of (ncz, pairs_per_block); default chunk sizes 8..32
+    candidates: iterable of (ncz, pairs_per_block); default chunk sizes 8..64
     with gridding depths 4..16 pairs.  Returns {"ncz", "pairs_per_block",
     "ms", "table"}; results are cached per geometry in-process and, when
     cache_file is given, in that JSON file.
@@ -195,7 +195,7 @@ def autotune(n, nproj, theta, center, shifts, data, dark0=None, flat0=None, *,
             _TUNED[key] = saved[key]
             return saved[key]
     if candidates is None:
-        candidates = [(ncz, zb) for ncz in (8, 16, 32) for zb in (4, 8, 16) if zb <= ncz // 2]
+        candidates = [(ncz, zb) for ncz in (8, 16, 32, 64) for zb in (4, 8, 16) if zb <= ncz // 2]
     table = []
     for ncz, zb in candidates:
         sw = TryCenterSweep(n, nproj, theta, center, shifts, fbp_filter, precision, ncz, zb,
