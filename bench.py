@@ -131,6 +131,7 @@ def stage_bytes(stage, n, nproj, ncz):
         "fft_filter": ncz * nproj * n * 4 + pairs * nproj * n * 8,
         "fr_ifft_rows": pairs * ((2 * n) ** 2 * 8 + 2 * n * n * 8),
         "fr_ifft_cols_deapod": pairs * (2 * n * n * 8 + 2 * n * n * 4),
+        "fr_gather_tc": pairs * (nproj * n * 8 + (2 * n) ** 2 * 8),
         "linerec": ncz * (nproj * n * 4 + n * n * 8),
         # tensor-core filter: FLOPs (3 split products of 2 n^2 per row), not bytes
         "tc_filter": 3 * 2 * ncz * nproj * n * n,
@@ -140,8 +141,13 @@ def stage_bytes(stage, n, nproj, ncz):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch from
 # the committed ncu captures, keyed by (stage, n, nproj, rows per chunk);
-# see profiles/fr_gather_grid_blocks_2048x1500_16pairs.md
-NCU_TRAFFIC = {("fr_gather", 2048, 1500, 32): 533.82e6 + 2104.92e6,
+# see profiles/launches_fourierrec_pipeline_2048x1500.md and
+# profiles/fr_gather_tc_grid_tc_2048x1500_32pairs.md
+NCU_TRAFFIC = {("fr_gather", 2048, 1500, 64): 1216.8e6 + 4259.3e6,
+               ("fft_filter", 2048, 1500, 64): 786.7e6 + 739.9e6,
+               ("fr_ifft_cols_deapod", 2048, 1500, 64): 2149.4e6 + 1043.0e6,
+               ("fr_ifft_rows", 2048, 1500, 64): 4295.0e6 + 2115.0e6,
+               ("fr_gather_tc", 2048, 1500, 64): 1705.8e6 + 4260.5e6,
                # profiles/tc_filter_tcf_gemm_2048x1500_32slices.md
                ("tc_filter", 2048, 1500, 32): 411.44e6 + 359.14e6}
 
@@ -693,7 +699,11 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank, precision=None, out_dtype
     d2h = nz_e2e * a.n * a.n * osz
     return {"value": round(ws * vox / (ms / 1e3) / 1e9, 2), "unit": "GUPS",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "rows": nz_e2e, "ms_per_step": round(ms, 2), "wall_ms_per_step": round(wall * 1e3, 2),
+            "rows": nz_e2e, "rows_per_chunk": ncz, "ms_per_step": round(ms, 2),
+            "wall_ms_per_step": round(wall * 1e3, 2),
+            # the bound of this leg: the host link, one direction each way
+            "d2h_gbs": round(d2h / (ms / 1e3) / 1e9, 1),
+            "h2d_gbs": round(h2d / (ms / 1e3) / 1e9, 1),
             "api": "GPURec.recon_all (pinned host frames -> pinned host volume)",
             "precision": precision or a.precision, "out_dtype": out_dtype}
 

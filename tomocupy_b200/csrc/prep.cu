@@ -6,6 +6,7 @@
 // Every CuPy elementwise step there is a separate kernel, so no multiply-add
 // is ever contracted; the explicit __f*_rn intrinsics below keep nvcc from
 // contracting either, which makes the fp32 results bit-identical.
+#include <algorithm>
 #include <cuda_fp16.h>
 
 #include <mutex>
@@ -118,12 +119,21 @@ __device__ __forceinline__ void split16(float v, __half &h, __half &l) {
   l = __float2half_rn(__fsub_rn(v, __half2float(h)));
 }
 
-// One CTA per output row (z, p); rows are enumerated z-major so consecutive
-// CTAs write consecutive output rows.  SPLIT writes the row as two fp16
-// planes (hi, lo) instead of fp32.
+// Output rows (z, p) enumerated z-major, a CTA taking rows blockIdx.x,
+// blockIdx.x + gridDim.x, ... (a row is 2 n bytes in and 4 n out: too short
+// for a CTA of its own).  SPLIT writes the row as two fp16 planes (hi, lo)
+// instead of fp32.
+template <typename T, bool SPLIT>
+__device__ __forceinline__ void prep_one_row(const PrepArgs &a, size_t row);
+
 template <typename T, bool SPLIT>
 __global__ void __launch_bounds__(256) prep_rows_kernel(PrepArgs a) {
-  size_t row = blockIdx.x;
+  const size_t rows = (size_t)a.nproj * a.nz;
+  for (size_t row = blockIdx.x; row < rows; row += gridDim.x) prep_one_row<T, SPLIT>(a, row);
+}
+
+template <typename T, bool SPLIT>
+__device__ __forceinline__ void prep_one_row(const PrepArgs &a, size_t row) {
   int z = (int)(row / a.nproj);
   int p = (int)(row % a.nproj);
   const T *src = (const T *)a.in + (size_t)p * a.in_pstride + (size_t)z * a.in_zstride;
@@ -190,6 +200,9 @@ __global__ void __launch_bounds__(256) prep_rows_kernel(PrepArgs a) {
     for (size_t x = xe + threadIdx.x; x < a.out_width; x += blockDim.x) dst[x] = right;
   }
 }
+
+// CTAs for `rows` output rows: 16 per SM of 148 (each loops over rows)
+inline unsigned prep_grid(size_t rows) { return (unsigned)std::min<size_t>(rows, 148 * 16); }
 
 }  // namespace
 }  // namespace tcb
@@ -259,9 +272,9 @@ extern "C" int tcb_prep_rows(float *out, const void *in, const float *dark0,
   StageTimer st("prep_rows", s);
   count_launch();
   switch (in_dtype) {
-    case TCB_U16: prep_rows_kernel<uint16_t, false><<<(unsigned)rows, 256, 0, s>>>(a); break;
-    case TCB_U8: prep_rows_kernel<uint8_t, false><<<(unsigned)rows, 256, 0, s>>>(a); break;
-    case TCB_F32: prep_rows_kernel<float, false><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_U16: prep_rows_kernel<uint16_t, false><<<prep_grid(rows), 256, 0, s>>>(a); break;
+    case TCB_U8: prep_rows_kernel<uint8_t, false><<<prep_grid(rows), 256, 0, s>>>(a); break;
+    case TCB_F32: prep_rows_kernel<float, false><<<prep_grid(rows), 256, 0, s>>>(a); break;
     default:
       set_error("tcb_prep_rows: unknown dtype %d", in_dtype);
       return TCB_ERR_INVALID_ARGUMENT;
@@ -295,9 +308,9 @@ extern "C" int tcb_prep_rows_split16(void *hi, void *lo, const void *in, const f
   StageTimer st("prep_rows", s);
   count_launch();
   switch (in_dtype) {
-    case TCB_U16: prep_rows_kernel<uint16_t, true><<<(unsigned)rows, 256, 0, s>>>(a); break;
-    case TCB_U8: prep_rows_kernel<uint8_t, true><<<(unsigned)rows, 256, 0, s>>>(a); break;
-    case TCB_F32: prep_rows_kernel<float, true><<<(unsigned)rows, 256, 0, s>>>(a); break;
+    case TCB_U16: prep_rows_kernel<uint16_t, true><<<prep_grid(rows), 256, 0, s>>>(a); break;
+    case TCB_U8: prep_rows_kernel<uint8_t, true><<<prep_grid(rows), 256, 0, s>>>(a); break;
+    case TCB_F32: prep_rows_kernel<float, true><<<prep_grid(rows), 256, 0, s>>>(a); break;
     default:
       set_error("tcb_prep_rows_split16: unknown dtype %d", in_dtype);
       return TCB_ERR_INVALID_ARGUMENT;
