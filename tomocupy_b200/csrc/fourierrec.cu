@@ -472,9 +472,17 @@ constexpr int TC_THREADS = 512;
 // arithmetic of grid_blocks, in the order of the tile lists:
 // [0] tile-local footprint origin (lx0 | ly0 << 16), [1] index of the
 // sample's spectrum value p*n + (i + n/2) % n with the odd-i sign in bit 31,
-// [2..10] x-weights, [11..19] y-weights.  80 bytes: five int4.
-constexpr int TC_REC = 2 + 2 * (2 * M + 1);
-static_assert(TC_REC * 4 == 80, "record = 5 int4");
+// [2..10] x-weights, [11..19] y-weights, [20..24] and [25..29] the byte
+// offsets in W of footprint column dx and row dy (16 bits each, two per
+// int; 0xFFFF outside the tile).  The sample sits at column k = (list
+// position) % 64 of its chunk, so its cell (lx, ly) is at
+// ly*4096 + (lx/8)*1024 + (lx%8)*128 + ((k/8 ^ lx) % 8)*16 + (k%8)*2: the
+// UMMA K-major 128-byte-swizzled layout of a 512 x 64 fp16 operand.
+// 128 bytes: eight int4.
+constexpr int TC_REC = 32;
+constexpr int TC_XO = 2 + 2 * (2 * M + 1);      // first int of the column offsets
+constexpr int TC_YO = TC_XO + (2 * M + 2) / 2;  // first int of the row offsets
+static_assert(TC_YO + (2 * M + 2) / 2 <= TC_REC, "record layout");
 
 __global__ void tile_records(const float2 *__restrict__ cs, const float *__restrict__ rtab,
                              const float *__restrict__ etab, const long long *__restrict__ toffs,
@@ -503,14 +511,34 @@ __global__ void tile_records(const float2 *__restrict__ cs, const float *__restr
       r[2 + d] = __float_as_int(__expf(geo.coeff1 * w0 * w0));
       r[2 + 2 * M + 1 + d] = __float_as_int(__expf(geo.coeff1 * w1 * w1));
     }
+    const int ox = tile_origin(fx, X0, twon), oy = tile_origin(fy, Y0, twon);
+    const int kc = (k % TCK) >> 3, kcol = (k & 7) << 1;
+    unsigned xo[2 * M + 2], yo[2 * M + 2];
+#pragma unroll
+    for (int d = 0; d < 2 * M + 2; d++) {
+      const int lx = ox + d, ly = oy + d;
+      xo[d] = (d < 2 * M + 1 && (unsigned)lx < (unsigned)TX)
+                  ? (unsigned)((lx >> 3) * 1024 + (lx & 7) * 128 + (((kc ^ lx) & 7) << 4) + kcol)
+                  : 0xFFFFu;
+      yo[d] = (d < 2 * M + 1 && (unsigned)ly < (unsigned)TY) ? (unsigned)(ly * 4096) : 0xFFFFu;
+    }
+#pragma unroll
+    for (int q = 0; q < (2 * M + 2) / 2; q++) {
+      r[TC_XO + q] = (int)(xo[2 * q] | (xo[2 * q + 1] << 16));
+      r[TC_YO + q] = (int)(yo[2 * q] | (yo[2 * q + 1] << 16));
+    }
+    r[TC_REC - 2] = r[TC_REC - 1] = 0;
   }
 }
 
 // One smem stage per CTA and two CTAs per SM (2 x 256 TMEM columns = all 512):
 // one CTA builds its next chunk while the other's MMAs and loads are in flight.
-constexpr int TC_SMEM = TC_STAGE + TCK * TC_REC * 4 + 64 + 1024;
+// records in shared memory field-major, R[field * TC_RS + k], so that the
+// lanes of a warp (consecutive k) read one field without bank conflicts
+constexpr int TC_RS = TCK + 1;
+constexpr int TC_SMEM = TC_STAGE + TC_REC * TC_RS * 4 + 64 + 1024;
 constexpr uint32_t TC_IDESC = tc::idesc_f16_f32(128, TCN);
-constexpr int TC_RV4 = TCK * TC_REC / 4;   // int4 per chunk of records (320)
+constexpr int TC_RV4 = TCK * TC_REC / 4;   // int4 per chunk of records (512)
 constexpr int TC_VT = TCZ * (TCK / 8);     // value threads: (pair, 8-sample group) = 256
 
 __global__ void absmax_kernel(const float2 *__restrict__ g, size_t total,
@@ -545,8 +573,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   extern __shared__ uint8_t tsm_raw[];
   uint8_t *sm = tsm_raw + ((1024u - (smem_u32(tsm_raw) & 1023u)) & 1023u);
   uint8_t *A = sm, *B = sm + TC_A;
-  int *R = reinterpret_cast<int *>(sm + TC_STAGE);   // [TCK][TC_REC]
-  uint64_t *mma_done = reinterpret_cast<uint64_t *>(R + TCK * TC_REC);
+  int *R = reinterpret_cast<int *>(sm + TC_STAGE);   // [TC_REC][TC_RS]
+  uint64_t *mma_done = reinterpret_cast<uint64_t *>(R + TC_REC * TC_RS);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 2);
   const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
   const int zgroups = (geo.nz + TCZ - 1) / TCZ;
@@ -612,7 +640,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     ok = __syncthreads_and(ok);
     if (!ok) break;
     // (1) records of this chunk, (2) values as fp16 rows of B, (3) W = 0
-    if (tid < TC_RV4) reinterpret_cast<int4 *>(R)[tid] = prec;
+    if (tid < TC_RV4) {
+      const int rk = tid / (TC_REC / 4), f0 = (tid % (TC_REC / 4)) * 4;
+      R[(f0 + 0) * TC_RS + rk] = prec.x;
+      R[(f0 + 1) * TC_RS + rk] = prec.y;
+      R[(f0 + 2) * TC_RS + rk] = prec.z;
+      R[(f0 + 3) * TC_RS + rk] = prec.w;
+    }
     if (tid < TC_VT) {
       uint32_t rows[2][4];  // [re, im][8 samples as 4 half2]
 #pragma unroll
@@ -657,26 +691,27 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       load_vals(vi_next);
       if (c + 2 < nch) load_vidx(c + 2, vi_next2);
     }
-    // (4) footprint weights into W[cell][sample]: one thread per (sample, row)
+    // (4) footprint weights into W[cell][sample]: one thread per (sample, row);
+    // cell addresses are the record's row offset + column offset
     for (int e = tid; e < TCK * (2 * M + 1); e += TC_THREADS) {
       const int k = e % TCK, dy = e / TCK;
       if (k >= cnt) continue;
-      const int *r = R + k * TC_REC;
-      const int o = r[0];
-      const int ly = (o >> 16) + dy;
-      if ((unsigned)ly >= (unsigned)TY) continue;
-      const float wyv = __int_as_float(r[2 + 2 * M + 1 + dy]);
-      const int ox = (int)(short)(o & 0xFFFF);
-      const uint32_t kcol = (uint32_t)((k & 7) << 1);
-      const int kchunk = k >> 3;
+      const int *r = R + k;  // field f at r[f * TC_RS]
+      const unsigned yo = ((unsigned)r[(TC_YO + dy / 2) * TC_RS] >> ((dy & 1) * 16)) & 0xFFFFu;
+      if (yo == 0xFFFFu) continue;
+      const float wyv = __int_as_float(r[(2 + 2 * M + 1 + dy) * TC_RS]);
+      uint8_t *Ay = A + yo;
 #pragma unroll
-      for (int dx = 0; dx < 2 * M + 1; dx++) {
-        const int lx = ox + dx;
-        if ((unsigned)lx < (unsigned)TX) {
-          const int m = ly * TX + lx;
-          const float w = __int_as_float(r[2 + dx]) * wyv;
-          *reinterpret_cast<__half *>(A + (m >> 3) * 1024 + (m & 7) * 128 +
-                                      (((kchunk ^ m) & 7) << 4) + kcol) = __float2half_rn(w);
+      for (int q = 0; q < (2 * M + 2) / 2; q++) {
+        const unsigned xx = (unsigned)r[(TC_XO + q) * TC_RS];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int dx = 2 * q + h;
+          const unsigned xo = (xx >> (16 * h)) & 0xFFFFu;
+          if (dx < 2 * M + 1 && xo != 0xFFFFu) {
+            const float w = __int_as_float(r[(2 + dx) * TC_RS]) * wyv;
+            *reinterpret_cast<__half *>(Ay + xo) = __float2half_rn(w);
+          }
         }
       }
     }
