@@ -691,29 +691,47 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
       load_vals(vi_next);
       if (c + 2 < nch) load_vidx(c + 2, vi_next2);
     }
-    // (4) footprint weights into W[cell][sample]: one thread per (sample, row);
-    // cell addresses are the record's row offset + column offset
-    for (int e = tid; e < TCK * (2 * M + 1); e += TC_THREADS) {
-      const int k = e % TCK, dy = e / TCK;
-      if (k >= cnt) continue;
+    // (4) footprint weights into W[cell][sample]; cell addresses are the
+    // record's row offset + column offset.  Rows 0..2M-1: one (sample, row)
+    // item per thread; row 2M: one cell per thread, so no thread does two
+    // rows.
+    static_assert(TCK * (2 * M) == TC_THREADS, "one (sample, row) item per thread");
+    auto row_off = [&](const int *r, int dy) {
+      return ((unsigned)r[(TC_YO + dy / 2) * TC_RS] >> ((dy & 1) * 16)) & 0xFFFFu;
+    };
+    {
+      const int k = tid % TCK, dy = tid / TCK;
       const int *r = R + k;  // field f at r[f * TC_RS]
-      const unsigned yo = ((unsigned)r[(TC_YO + dy / 2) * TC_RS] >> ((dy & 1) * 16)) & 0xFFFFu;
-      if (yo == 0xFFFFu) continue;
-      const float wyv = __int_as_float(r[(2 + 2 * M + 1 + dy) * TC_RS]);
-      uint8_t *Ay = A + yo;
+      const unsigned yo = k < cnt ? row_off(r, dy) : 0xFFFFu;
+      if (yo != 0xFFFFu) {
+        const float wyv = __int_as_float(r[(2 + 2 * M + 1 + dy) * TC_RS]);
+        uint8_t *Ay = A + yo;
 #pragma unroll
-      for (int q = 0; q < (2 * M + 2) / 2; q++) {
-        const unsigned xx = (unsigned)r[(TC_XO + q) * TC_RS];
+        for (int q = 0; q < (2 * M + 2) / 2; q++) {
+          const unsigned xx = (unsigned)r[(TC_XO + q) * TC_RS];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const int dx = 2 * q + h;
-          const unsigned xo = (xx >> (16 * h)) & 0xFFFFu;
-          if (dx < 2 * M + 1 && xo != 0xFFFFu) {
-            const float w = __int_as_float(r[(2 + dx) * TC_RS]) * wyv;
-            *reinterpret_cast<__half *>(Ay + xo) = __float2half_rn(w);
+          for (int h = 0; h < 2; h++) {
+            const int dx = 2 * q + h;
+            const unsigned xo = (xx >> (16 * h)) & 0xFFFFu;
+            if (dx < 2 * M + 1 && xo != 0xFFFFu) {
+              const float w = __int_as_float(r[(2 + dx) * TC_RS]) * wyv;
+              *reinterpret_cast<__half *>(Ay + xo) = __float2half_rn(w);
+            }
           }
         }
       }
+    }
+    for (int e = tid; e < TCK * (2 * M + 1); e += TC_THREADS) {
+      const int k = e % TCK, dx = e / TCK;
+      if (k >= cnt) continue;
+      const int *r = R + k;
+      const unsigned yo = row_off(r, 2 * M);
+      const unsigned xo =
+          ((unsigned)r[(TC_XO + dx / 2) * TC_RS] >> ((dx & 1) * 16)) & 0xFFFFu;
+      if (yo == 0xFFFFu || xo == 0xFFFFu) continue;
+      const float w = __int_as_float(r[(2 + dx) * TC_RS]) *
+                      __int_as_float(r[(2 + 2 * M + 1 + 2 * M) * TC_RS]);
+      *reinterpret_cast<__half *>(A + yo + xo) = __float2half_rn(w);
     }
     fence_proxy_async_smem();
     __syncthreads();
