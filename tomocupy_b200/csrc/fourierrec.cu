@@ -907,13 +907,15 @@ __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16)) iff
 
 // Rows-first order.  Pass 1 (rows): one row y of a pair's N x N grid per
 // block; the inverse FFT along x keeps x' in [n/2, 3n/2) and writes column
-// c = x' - n/2 to t1[pair][c / GW][y][c % GW] (GW = 16 columns: each row
-// writes whole 128-byte lines, and the columns that pass 2 reads lie in
-// 128-byte lines of one contiguous N x GW array).  Only n of the N outputs
-// are written.
-constexpr int T1_GW = 16;  // columns per group of the row-pass output (n >= 128)
+// c = x' - n/2 to t1[pair][c / GW][y][c % GW].  Only n of the N outputs are
+// written.  GW trades the two passes' access segments: a warp of pass 1
+// stores 32 consecutive columns as 32/GW segments of 8*GW bytes; a warp of
+// pass 2 (4 columns x 8 rows) loads 8 rows of 32 bytes at a row stride of
+// 8*GW bytes.  2n = 4096, 2048-slice volume (rows + columns pass): GW = 16
+// 35.5 + 44.5 ms, GW = 8 38.0 + 40.2 ms, GW = 4 41.0 + 38.0 ms.
+constexpr int T1_GW = 8;  // default columns per group of the row-pass output (n >= 128)
 
-template <int N>
+template <int N, int GW = T1_GW>
 __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
     ifft_rows_first(const float2 *__restrict__ grid, float2 *__restrict__ t1,
                     const float2 *__restrict__ tw) {
@@ -922,11 +924,11 @@ __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
   const size_t row = blockIdx.x;  // pair * N + y
   const int y = (int)(row % N);
   const float2 *src = grid + row * N;
-  float2 *dst = t1 + (row - y) * n + (size_t)y * T1_GW;  // pair base + row offset in a group
+  float2 *dst = t1 + (row - y) * n + (size_t)y * GW;  // pair base + row offset in a group
   auto in = [src](int e) { return __ldg(src + e); };
   auto out = [&](int o, float2 v) {
     const unsigned x = (unsigned)(o - N / 4);
-    if (x < (unsigned)n) dst[(size_t)(x / T1_GW) * N * T1_GW + x % T1_GW] = v;
+    if (x < (unsigned)n) dst[(size_t)(x / GW) * N * GW + x % GW] = v;
   };
   fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
 }
@@ -934,7 +936,7 @@ __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
 // Pass 2 (columns): CPC adjacent columns tx of t1 per block; the inverse
 // FFT along y keeps y' in [n/2 + 1, 3n/2 + 1) and applies deapodization and
 // the output layout (ty = y' - n/2 - 1).
-template <int N, typename OutT>
+template <int N, typename OutT, int GW = T1_GW>
 __global__ void __launch_bounds__(1024) ifft_cols_deapod(const float2 *__restrict__ t1,
                                                          OutT *__restrict__ f,
                                                          const float2 *__restrict__ tw,
@@ -947,10 +949,10 @@ __global__ void __launch_bounds__(1024) ifft_cols_deapod(const float2 *__restric
   const int ncb = n / cpc;
   const int z = blockIdx.x / ncb, tx = (blockIdx.x % ncb) * cpc + c;
   // column tx in its group of T1_GW columns (row stride T1_GW)
-  const float2 *src = t1 + (size_t)z * N * n + (size_t)(tx / T1_GW) * N * T1_GW + tx % T1_GW;
+  const float2 *src = t1 + (size_t)z * N * n + (size_t)(tx / GW) * N * GW + tx % GW;
   const float4 X = __ldg(dtab + tx);
   const float mun2 = geo.mu * (n * n), nsign = (float)(1 - n % 4);
-  auto in = [src](int e) { return __ldg(src + (size_t)e * T1_GW); };
+  auto in = [src](int e) { return __ldg(src + (size_t)e * GW); };
   auto out = [&](int o, float2 v) {
     const unsigned ty = (unsigned)(o - (N / 4 + 1));
     if (ty < (unsigned)n)
@@ -964,20 +966,50 @@ inline int cols_per_block(int N) { return std::min(16384 / N, 16); }
 inline size_t cols_smem(int N, int cpc) { return (size_t)cpc * (N + N / 16 + 4) * sizeof(float2); }
 inline size_t rows_smem(int N) { return (size_t)(N + N / 16) * sizeof(float2); }
 
+template <int N, int GW>
+cudaError_t rows_first_attrs(int csm) {
+  cudaError_t e = cudaFuncSetAttribute(ifft_rows_first<N, GW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)rows_smem(N));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_cols_deapod<N, float, GW>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_cols_deapod<N, __half, GW>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  return e;
+}
+
+// Rows pass, then columns pass with deapodization; t1 in groups of GW columns.
+template <int N, int GW>
+void rows_first_launch(const float2 *grid, float2 *t1, const float2 *tw, const float4 *dtab,
+                       void *f, bool half, const Geom &geo, int unpack, size_t nz, int cpc,
+                       cudaStream_t s) {
+  {
+    StageTimer st("fr_ifft_rows", s);
+    ifft_rows_first<N, GW><<<(unsigned)(N * nz), N / 16, rows_smem(N), s>>>(grid, t1, tw);
+    count_launch();
+  }
+  StageTimer st("fr_ifft_cols_deapod", s);
+  const unsigned blocks = (unsigned)((N / 2 / cpc) * nz);
+  const size_t sm = cols_smem(N, cpc);
+  if (half)
+    ifft_cols_deapod<N, __half, GW><<<blocks, cpc * (N / 16), sm, s>>>(
+        t1, (__half *)f, tw, dtab, geo, unpack, cpc);
+  else
+    ifft_cols_deapod<N, float, GW><<<blocks, cpc * (N / 16), sm, s>>>(
+        t1, (float *)f, tw, dtab, geo, unpack, cpc);
+  count_launch();
+}
+
 template <int N>
 cudaError_t own_fft_attrs() {
   const int csm = (int)cols_smem(N, cols_per_block(N));
   cudaError_t e = cudaFuncSetAttribute(ifft_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        csm);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ifft_cols_deapod<N, float>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ifft_cols_deapod<N, __half>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ifft_rows_first<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)rows_smem(N));
+  if (e == cudaSuccess) e = rows_first_attrs<N, 4>(csm);
+  if (e == cudaSuccess) e = rows_first_attrs<N, 8>(csm);
+  if (e == cudaSuccess) e = rows_first_attrs<N, 16>(csm);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(ifft_rows_deapod<N, float>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(N));
@@ -990,23 +1022,14 @@ cudaError_t own_fft_attrs() {
 template <int N>
 void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, const float4 *dtab,
                     void *f, bool half, const Geom &geo, int unpack, size_t nz, int cpc,
-                    bool rows_first, cudaStream_t s) {
+                    bool rows_first, int gw, cudaStream_t s) {
   if (rows_first) {
-    {
-      StageTimer st("fr_ifft_rows", s);
-      ifft_rows_first<N><<<(unsigned)(N * nz), N / 16, rows_smem(N), s>>>(grid, t1, tw);
-      count_launch();
-    }
-    StageTimer st("fr_ifft_cols_deapod", s);
-    const unsigned blocks = (unsigned)((N / 2 / cpc) * nz);
-    const size_t sm = cols_smem(N, cpc);
-    if (half)
-      ifft_cols_deapod<N, __half><<<blocks, cpc * (N / 16), sm, s>>>(t1, (__half *)f, tw, dtab,
-                                                                      geo, unpack, cpc);
+    if (gw == 4)
+      rows_first_launch<N, 4>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, s);
+    else if (gw == 16)
+      rows_first_launch<N, 16>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, s);
     else
-      ifft_cols_deapod<N, float><<<blocks, cpc * (N / 16), sm, s>>>(t1, (float *)f, tw, dtab,
-                                                                     geo, unpack, cpc);
-    count_launch();
+      rows_first_launch<N, 8>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, s);
     return;
   }
   {
@@ -1073,6 +1096,7 @@ struct tcb_fourierrec {
   // else 0.
   int own_n = 0;
   int own_cpc = 0;  // columns per block of the own column pass
+  int t1_gw = tcb::fr::T1_GW;  // columns per group of the row-pass output (4, 8 or 16)
   bool own_rows_first = true;  // rows pass first (columns pass fused with deapodization)
   int zblock = 0;  // pairs per gridding block (2/4/8/16; 0 = largest that fits nz)
   int grid_mode = 0;          // TCB_GRID_FP32 or TCB_GRID_TENSOR
@@ -1192,13 +1216,14 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     const bool half = out_half;
     const int cpc = h->own_cpc;
     const bool rf = h->own_rows_first;
+    const int gw = h->t1_gw;
     switch (h->own_n) {
-      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
-      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, s); break;
+      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
+      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
+      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
+      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
+      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
+      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
     }
     TCB_LAUNCH_CHECK();
     return TCB_OK;
@@ -1442,6 +1467,11 @@ extern "C" int tcb_fourierrec_create(tcb_fourierrec **out, size_t nproj, size_t 
     // cols_per_block (TCB_FOURIERREC_FFT_CPC tunes it)
     h->own_rows_first = !(fsel && strcmp(fsel, "own_cf") == 0);
     h->own_cpc = cols_per_block((int)N2);
+    // TCB_FOURIERREC_T1_GW=4/8/16 sets the row-pass output grouping
+    if (const char *c = getenv("TCB_FOURIERREC_T1_GW")) {
+      const int v = atoi(c);
+      if (v == 4 || v == 8 || v == 16) h->t1_gw = v;
+    }
     if (const char *c = getenv("TCB_FOURIERREC_FFT_CPC")) {
       const int v = atoi(c);
       if (v >= 1 && v <= h->own_cpc && (v & (v - 1)) == 0) h->own_cpc = v;
