@@ -544,6 +544,69 @@ def run_methods(a, data, dark, flat, theta, dev):
     return res
 
 
+def run_phase(a, dev, peaks, peaks_kind):
+    """Paganin phase retrieval of 2048 x 2048 projections (a.phase_proj of them,
+    frames resident) with production optics: 0.65 um pixels, 50 mm, 20 keV ->
+    4096 x 4096 padded transforms.  Algorithmic bytes: 8 per detector pixel
+    (float32 read + write); the padded chain's own traffic is in the stages."""
+    import torch
+    from oracle import np_tomo
+    from tomocupy_b200 import _lib
+    from tomocupy_b200.processing.retrieve_phase import PhaseFilter
+    n, P = a.n, a.phase_proj
+    ps, dist, en, alpha = 0.65e-4, 5.0, 20.0, 1e-3
+    g = torch.Generator(device=dev).manual_seed(a.seed)
+    x = 0.5 + 0.4 * torch.rand((P, n, n), device=dev, generator=g)
+    op = PhaseFilter(n, n, "paganin", ps, dist, en, alpha)
+    y = x.clone()
+    for _ in range(2):
+        op.apply(y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    e0.record()
+    for _ in range(reps):
+        op.apply(y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    _lib.profile_enable(True)
+    op.apply(y)
+    stages = _lib.profile_report()
+    _lib.profile_enable(False)
+    # parity of the first projection against the NumPy restatement
+    want = np_tomo.retrieve_phase(x[:1].cpu().numpy(), "paganin", ps, dist, en, alpha)
+    y1 = op.apply(x[:1].clone()).cpu().numpy()
+    rel = float(np.linalg.norm(y1 - want) / np.linalg.norm(want))
+    t0 = time.perf_counter()
+    np_tomo.retrieve_phase(x[:1].cpu().numpy(), "paganin", ps, dist, en, alpha)
+    cpu_s = time.perf_counter() - t0
+    alg = 8.0 * P * n * n
+    # the padded chain's least traffic per padded pixel: pad (write 4, read the
+    # image once), R2C (4 in, 4 out), multiply (8 B in + 8 out per half-spectrum
+    # entry = 8), C2R (4 + 4), crop (read and write the image): ~31 B
+    npad = float(n + 2 * op.py) * (n + 2 * op.pz)
+    chain = P * (npad * (4 + 8 + 8 + 8) + 3.0 * 4 * n * n)
+    res = {"workload": f"{P} projections {n}x{n} float32, paganin (0.65 um, 50 mm, 20 keV, "
+                       f"alpha 1e-3), padded {n + 2 * op.py}x{n + 2 * op.pz}",
+           "ms": round(ms, 2), "projections_per_s": round(P / (ms / 1e3), 1),
+           "unit": "projections/s", "batch": op.batch,
+           "achieved_gbs_algorithmic": round(alg / (ms / 1e3) / 1e9, 1),
+           "padded_chain_bytes": chain,
+           "achieved_gbs_padded_chain": round(chain / (ms / 1e3) / 1e9, 1),
+           "peak_gbs": peaks.get("hbm_gbs"), "peak_source": peaks_kind,
+           "stages_ms": {k: round(v["ms"], 2) for k, v in stages.items()},
+           "rel_l2_vs_numpy_oracle_first_projection": rel,
+           "cpu_baseline": {"value": round(1.0 / cpu_s, 3), "unit": "projections/s",
+                            "kind": "port", "cores": 1,
+                            "sample": f"1 projection {n}x{n} (NumPy complex64 fft2/ifft2 as "
+                                      f"the reference), {cpu_s:.1f} s"}}
+    op.free()
+    del x, y
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_ours(a, ws, rank, local):
     import torch
     from tomocupy_b200.global_vars import params
@@ -622,6 +685,9 @@ def run_ours(a, ws, rank, local):
     lamino = None
     if not a.no_lamino and ws == 1:
         lamino = run_lamino(a, dev)
+    phase = None
+    if not a.no_phase and ws == 1:
+        phase = run_phase(a, dev, peaks, peaks_kind)
 
     if rank == 0:
         tag = "fp32" if primary == "float32" else "mixed-precision"
@@ -650,6 +716,7 @@ def run_ours(a, ws, rank, local):
             "try_center": trycenter,
             "serving": serving,
             "lamino": lamino,
+            "phase_retrieval": phase,
         }
         print(json.dumps(line), flush=True)
 
@@ -828,6 +895,9 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--serve-ncz", type=int, default=16)
     ap.add_argument("--no-lamino", action="store_true", help="skip the laminography leg")
+    ap.add_argument("--no-phase", action="store_true", help="skip the phase-retrieval leg")
+    ap.add_argument("--phase-proj", type=int, default=64,
+                    help="projections in the phase-retrieval leg")
     ap.add_argument("--ring-removal", action="store_true",
                     help="main leg with Fourier-wavelet ring removal (level 7, sigma 1, sym16)")
     ap.add_argument("--no-methods", action="store_true",

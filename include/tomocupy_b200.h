@@ -140,6 +140,32 @@ int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t sstride, void
 int tcb_stripe_fw_destroy(tcb_stripe_fw *h);
 
 /* ------------------------------------------------------------------------
+ * Single-distance phase retrieval of projections.  Replaces paganin_filter
+ * (methods 'paganin', 'Gpaganin') and farago_filter
+ * (src/tomocupy/processing/retrieve_phase.py:57-145), called by
+ * ProcFunctions.proc_proj (src/tomocupy/processing/proc_functions.py:169-181).
+ * Units as in those functions: pixel_size and dist in cm, energy in keV,
+ * W in cm.  pads: the edge padding (rows py, columns pz, each side) that
+ * _calc_pad chooses (retrieve_phase.py:178-206); host only.
+ * create: batch = projections per transform batch; the filter is built on
+ * the host.  apply: in place on nproj projections [nproj, dy, dz] float32
+ * (the reference's data[m] = proj).  Not re-entrant across streams (the
+ * handle owns the padded batch and its spectra).
+ * ------------------------------------------------------------------------ */
+#define TCB_PHASE_PAGANIN 0
+#define TCB_PHASE_GPAGANIN 1
+#define TCB_PHASE_FARAGO 2
+typedef struct tcb_phase tcb_phase;
+int tcb_phase_pads(size_t dy, size_t dz, double pixel_size, double dist, double energy,
+                   int pad, size_t *py, size_t *pz);
+int tcb_phase_create(tcb_phase **out, size_t batch, size_t dy, size_t dz, int method,
+                     double pixel_size, double dist, double energy, double alpha, double db,
+                     double W, int pad);
+int tcb_phase_sizes(tcb_phase *h, size_t *py, size_t *pz);
+int tcb_phase_apply(tcb_phase *h, float *data, size_t nproj, void *stream);
+int tcb_phase_destroy(tcb_phase *h);
+
+/* ------------------------------------------------------------------------
  * FBP filter.  Replaces cfunc_filter (src/include/cfunc_filter.cuh:9-23,
  * src/cuda/cfunc_filter.i:9-21): g real [nz, nproj, n] filtered in place
  * with w complex [nz, n/2+1] (one spectrum per slice).

@@ -56,6 +56,90 @@ def minus_log(x):
 
 
 # --------------------------------------------------------------------------
+# phase retrieval (src/tomocupy/processing/retrieve_phase.py:57-305)
+# --------------------------------------------------------------------------
+_PR_PLANCK = 6.58211928e-19   # retrieve_phase.py:45-48
+_PR_LIGHT = 299792458e+2
+_PR_PI = 3.14159265359
+
+
+def pr_wavelength(energy):
+    """_wavelength (retrieve_phase.py:51-52), cm."""
+    return 2 * _PR_PI * _PR_PLANCK * _PR_LIGHT / energy
+
+
+def pr_pads(dy, dz, pixel_size, dist, energy, pad=True):
+    """(py, pz) of _calc_pad / _calc_pad_width (retrieve_phase.py:178-226)."""
+    if not pad:
+        return 0, 0
+    wl = pr_wavelength(energy)
+
+    def width(dim):
+        pad_pix = np.ceil(_PR_PI * wl * dist / pixel_size ** 2)
+        return int((pow(2, np.ceil(np.log2(dim + pad_pix))) - dim) * 0.5)
+    return width(dy), width(dz)
+
+
+def _pr_coord(pixel_size, num):
+    """_reciprocal_coord (retrieve_phase.py:285-305), float32."""
+    n = num - 1
+    rc = np.arange(-n, num, 2, dtype=np.float32)
+    rc *= 0.5 / (n * pixel_size)
+    return rc
+
+
+def pr_filter(method, ny, nz, pixel_size, dist, energy, alpha=1e-3, db=1000, W=2e-4):
+    """The fftshifted filter of paganin_filter / farago_filter
+    (retrieve_phase.py:85-93, 119-121, 209-258), float32 like the reference."""
+    wl = pr_wavelength(energy)
+    if method == "Gpaganin":
+        ix = np.cos(_pr_coord(pixel_size, ny) * 2 * _PR_PI * pixel_size)
+        iy = np.cos(_pr_coord(pixel_size, nz) * 2 * _PR_PI * pixel_size)
+        a, b = np.meshgrid(iy, ix)
+        kf = a + b
+        aph = db * (dist * wl) / (4 * _PR_PI)
+        f = 1 / (1.0 - (2 * aph / (W ** 2)) * (kf - 2))
+    else:
+        ix = np.square(_pr_coord(pixel_size, ny))
+        iy = np.square(_pr_coord(pixel_size, nz))
+        a, b = np.meshgrid(iy, ix)
+        w2 = a + b
+        if method == "paganin":
+            f = 1 / (wl * dist * w2 / (4 * _PR_PI) + alpha)
+        elif method == "farago":
+            f = 1 / (np.cos(_PR_PI * wl * dist * w2) + db * np.sin(_PR_PI * wl * dist * w2))
+        else:
+            raise ValueError(method)
+    return np.fft.fftshift(f).astype(np.float32)
+
+
+def retrieve_phase(data, method, pixel_size=1e-4, dist=50, energy=20, alpha=1e-3, db=1000,
+                   W=2e-4, pad=True):
+    """paganin_filter / farago_filter on float32 projections [nproj, dy, dz]
+    (retrieve_phase.py:57-145): edge padding by slice assignment, complex64
+    fft2, the normalised filter, ifft2, real part, crop.  Returns a new array."""
+    data = np.array(data, dtype=np.float32)
+    nproj, dy, dz = data.shape
+    px, py = pr_pads(dy, dz, pixel_size, dist, energy, pad)
+    f = pr_filter(method, dy + 2 * px, dz + 2 * py, pixel_size, dist, energy, alpha, db, W)
+    nf = f / f.max()
+    prj = np.zeros((dy + 2 * px, dz + 2 * py), np.float32)
+    for m in range(nproj):
+        prj[px:dy + px, py:dz + py] = data[m]
+        prj[:px] = prj[px]
+        prj[-px:] = prj[-px - 1]        # px = 0: the whole array takes the last row
+        prj[:, :py] = prj[:, py][:, np.newaxis]
+        prj[:, -py:] = prj[:, -py - 1][:, np.newaxis]
+        fproj = np.fft.fft2(prj.astype(np.complex64)).astype(np.complex64)
+        fproj *= nf
+        proj = np.real(np.fft.ifft2(fproj)).astype(np.float32)
+        if pad:
+            proj = proj[px:dy + px, py:dz + py]
+        data[m] = proj
+    return data
+
+
+# --------------------------------------------------------------------------
 # filter (reconstruction/fbp_filter.py:60-118, backproj_functions.py:93-109)
 # --------------------------------------------------------------------------
 def wint(n, t):

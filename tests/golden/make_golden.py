@@ -7,7 +7,9 @@
             (src/tomocupy/reconstruction/fbp_filter.py:60-118)
           * Reader.init_sizes / init_sizes_try / init_sizes_lamino for a set
             of option combinations (src/tomocupy/dataio/reader.py:82-272)
-        -> filter_spectra.npz, sizes_cases.json
+          * paganin_filter / farago_filter (retrieve_phase.py:57-145)
+        -> filter_spectra.npz, sizes_cases.json, ..., phase_retrieval.npz
+        (--phase: phase_retrieval.npz only)
 
     python tests/golden/make_golden.py --gpu --out DIR
         Runs the reference's CUDA operators (oracle/_ref, built from the
@@ -195,6 +197,54 @@ def gen_cpu(ref: Path):
                                     dtype=np.float32)
     np.savez_compressed(HERE / "fw_stripe.npz", **fw)
     print("wrote filter_spectra.npz, sizes_cases.json, lprec_grids.npz and fw_stripe.npz")
+    gen_phase(ref)
+
+
+# Phase retrieval (retrieve_phase.py:57-145): (method, nproj, dy, dz,
+# pixel_size cm, dist cm, energy keV, alpha, delta/beta, W cm, seed).  The
+# dist = 0 case on a power-of-two image and the 31-column farago case get a
+# zero-wide edge padding on an axis, where the reference's prj[-0:] =
+# prj[-1] gives every entry along that axis the last entry's value.
+PHASE_CASES = [
+    ("paganin", 3, 24, 40, 0.65e-4, 5.0, 20.0, 1e-3, 1500.0, 2e-4, 1),
+    ("paganin", 2, 64, 96, 0.65e-4, 5.0, 20.0, 1e-3, 1500.0, 2e-4, 2),
+    ("Gpaganin", 2, 24, 40, 0.65e-4, 5.0, 20.0, 1e-3, 1500.0, 1.3e-4, 3),
+    ("farago", 2, 25, 30, 1e-4, 0.5, 25.0, 1e-3, 1000.0, 2e-4, 4),
+    ("farago", 1, 20, 31, 1e-4, 0.5, 25.0, 1e-3, 1000.0, 2e-4, 6),
+    ("paganin", 2, 16, 16, 1e-4, 0.0, 20.0, 1e-3, 1500.0, 2e-4, 5),
+]
+
+
+def phase_input(nproj, dy, dz, seed):
+    """Seeded transmission-like projections in (0.2, 1): smooth field plus noise."""
+    import scipy.ndimage as ndi
+    rng = np.random.default_rng(seed)
+    base = ndi.gaussian_filter(rng.standard_normal((nproj, dy, dz)), (0, 3, 3))
+    base = base / (np.abs(base).max() + 1e-12)
+    x = 0.6 + 0.3 * base + 0.02 * rng.standard_normal((nproj, dy, dz))
+    return np.clip(x, 0.2, 1.0).astype(np.float32)
+
+
+def gen_phase(ref: Path):
+    """Runs paganin_filter / farago_filter from the reference's own source with
+    NumPy for CuPy -> phase_retrieval.npz."""
+    if "cupy" not in sys.modules:
+        _install_stubs()
+    sys.modules["cupy.fft"] = np.fft  # `from cupy.fft import fft2, ifft2`
+    rp = _load(ref / "src/tomocupy/processing/retrieve_phase.py", "ref_retrieve_phase")
+    out = {}
+    for i, (meth, nproj, dy, dz, ps, dist, en, alpha, db, W, seed) in enumerate(PHASE_CASES):
+        data = phase_input(nproj, dy, dz, seed)
+        out[f"in_{i}"] = data
+        if meth == "farago":
+            res = rp.farago_filter(data.copy(), ps, dist, en, db, meth)
+        else:
+            res = rp.paganin_filter(data.copy(), ps, dist, en, alpha, meth, db, W)
+        out[f"out_{i}"] = np.asarray(res, dtype=np.float32)
+        py, pz, _ = rp._calc_pad(data, ps, dist, en, True)
+        out[f"pads_{i}"] = np.array([py, pz], dtype=np.int64)
+    np.savez_compressed(HERE / "phase_retrieval.npz", **out)
+    print("wrote phase_retrieval.npz")
 
 
 # (nproj, nz, ni, level, sigma, wavelet, seed)
@@ -263,10 +313,13 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--cpu", action="store_true")
     ap.add_argument("--gpu", action="store_true")
+    ap.add_argument("--phase", action="store_true", help="only phase_retrieval.npz")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
     if a.cpu:
         gen_cpu(Path(a.ref))
+    elif a.phase:
+        gen_phase(Path(a.ref))
     if a.gpu:
         gen_gpu(Path(a.out))

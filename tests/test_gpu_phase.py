@@ -1,0 +1,120 @@
+"""GPU parity of the native phase retrieval (tcb_phase_*, through
+tomocupy_b200.processing.retrieve_phase) against fixtures made by the
+reference's own paganin_filter / farago_filter (NumPy for CuPy, complex64
+transforms) and against the NumPy restatement on larger, production-like
+geometries.  The native chain is R2C -> even part of the filter -> C2R in
+float32 (cuFFT), the reference's a complex64 fft2 -> filter -> ifft2 -> real
+part: equal in exact arithmetic, so the tolerance is float32 transform
+rounding, rel-L2 <= 1e-5."""
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ROOT, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    from make_golden import PHASE_CASES
+    return PHASE_CASES
+
+
+def _run(data, meth, ps, dist, en, alpha, db, W, **kw):
+    from tomocupy_b200.processing.retrieve_phase import PhaseFilter
+    op = PhaseFilter(data.shape[1], data.shape[2], meth, ps, dist, en, alpha, db, W, **kw)
+    out = op.apply(data)
+    torch.cuda.synchronize()
+    op.free()
+    return out
+
+
+@pytest.mark.parametrize("i", range(6))
+def test_phase_matches_reference_fixture(cuda, i):
+    g = np.load(ROOT / "tests" / "golden" / "phase_retrieval.npz")
+    meth, nproj, dy, dz, ps, dist, en, alpha, db, W, seed = _cases()[i]
+    data = torch.as_tensor(g[f"in_{i}"], device=cuda).contiguous()
+    out = _run(data, meth, ps, dist, en, alpha, db, W)
+    assert out.data_ptr() == data.data_ptr()          # in place, like data[m] = proj
+    want = g[f"out_{i}"]
+    err = rel_l2(out.cpu().numpy(), want)
+    assert err < 1e-5, (i, meth, err)
+
+
+@pytest.mark.parametrize("meth,shape,ps,dist,en", [
+    ("paganin", (3, 300, 412), 0.65e-4, 5.0, 20.0),     # production optics, odd pads
+    ("Gpaganin", (2, 256, 256), 0.65e-4, 5.0, 20.0),
+    ("farago", (2, 200, 333), 1e-4, 0.5, 25.0),
+])
+def test_phase_matches_oracle_larger(cuda, meth, shape, ps, dist, en):
+    from oracle import np_tomo
+    _cases()
+    from make_golden import phase_input
+    x = phase_input(*shape, seed=7)
+    want = np_tomo.retrieve_phase(x, meth, ps, dist, en, 1e-3, 1500.0, 1.3e-4)
+    got = _run(torch.as_tensor(x, device=cuda), meth, ps, dist, en, 1e-3, 1500.0, 1.3e-4)
+    err = rel_l2(got.cpu().numpy(), want)
+    assert err < 1e-5, (meth, err)
+
+
+def test_phase_batches_are_independent(cuda):
+    """5 projections through batches of 2 (a partial last batch running the
+    full-batch plan) equal one batch of 5, and a projection's result does not
+    depend on its neighbours."""
+    _cases()
+    from make_golden import phase_input
+    x = torch.as_tensor(phase_input(5, 48, 64, seed=9), device=cuda)
+    args = ("paganin", 0.65e-4, 5.0, 20.0, 1e-3, 1500.0, 2e-4)
+    a = _run(x.clone(), *args, batch=2)
+    b = _run(x.clone(), *args, batch=5)
+    c = _run(x[3:4].clone(), *args, batch=1)
+    assert rel_l2(a.cpu(), b.cpu()) < 1e-6
+    assert rel_l2(c[0].cpu(), b[3].cpu()) < 1e-6
+
+
+def test_phase_rejects_bad_input(cuda):
+    from tomocupy_b200.processing.retrieve_phase import PhaseFilter, paganin_filter
+    op = PhaseFilter(16, 24, "paganin", 1e-4, 5.0, 20.0)
+    with pytest.raises(ValueError):
+        op.apply(torch.zeros((2, 16, 25), device=cuda))
+    with pytest.raises(ValueError):
+        op.apply(torch.zeros((2, 16, 24), device=cuda, dtype=torch.float64))
+    op.free()
+    with pytest.raises(ValueError):
+        paganin_filter(torch.zeros((1, 8, 8), device=cuda), method="farago")
+
+
+def test_step_driver_with_phase_retrieval(cuda):
+    """GPURecSteps with Paganin phase retrieval (dark/flat -> phase -> -log ->
+    filter -> fourierrec) against the same chain with the NumPy restatement's
+    phase retrieval feeding the library's own reconstruction."""
+    from oracle import np_tomo
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    from tomocupy_b200.rec_steps import GPURecSteps
+    nproj, nz, n = 90, 16, 128
+    data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=4)
+    opts = dict(reconstruction_algorithm="fourierrec", nsino_per_chunk=8,
+                retrieve_phase_method="paganin", pixel_size=0.65, propagation_distance=50.0,
+                energy=20.0, retrieve_phase_alpha=1e-3)
+    global_vars.reset(**opts)
+    w = ArrayWriter(device="cuda")
+    got = GPURecSteps(ArrayReader(data, dark, flat, theta=theta), w).recon_steps_all()
+    got = w.rec.cpu().numpy() if got is None else got.cpu().numpy()
+    # the same chain with the NumPy phase retrieval in the middle
+    pre = np_tomo.darkflat(data.numpy(), dark.numpy(), flat.numpy())
+    pre = np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3)
+    pre = np_tomo.minus_log(pre)
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=8)
+    w2 = ArrayWriter(device="cuda")
+    rec = GPURec(ArrayReader(data, dark, flat, theta=theta), w2)
+    want = rec.recon_preprocessed(torch.as_tensor(pre, device=cuda)).cpu().numpy()
+    err = rel_l2(got, want)
+    assert np.isfinite(got).all() and err < 1e-4, err
+    global_vars.reset(**dict(opts, reconstruction_type="full"))
+    with pytest.raises(NotImplementedError):
+        GPURec(ArrayReader(data, dark, flat, theta=theta), ArrayWriter(device="cuda")).recon_all()

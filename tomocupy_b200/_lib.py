@@ -29,6 +29,10 @@ GRID_TENSOR = 1
 TCF_OUT_ROWS = 0
 TCF_OUT_PAIRS = 1
 
+TCB_PHASE_PAGANIN = 0
+TCB_PHASE_GPAGANIN = 1
+TCB_PHASE_FARAGO = 2
+
 FFF_OUT_ROWS = 0
 FFF_OUT_PAIRS = 1
 FFF_OUT_SPECTRUM = 2
@@ -51,7 +55,7 @@ class TcbError(RuntimeError):
         super().__init__(f"{func} -> {STATUS_NAMES.get(status, status)}: {msg}")
 
 
-vp, sz, f32, i32, u32 = C.c_void_p, C.c_size_t, C.c_float, C.c_int, C.c_uint
+vp, sz, f32, i32, u32, f64 = C.c_void_p, C.c_size_t, C.c_float, C.c_int, C.c_uint, C.c_double
 
 # name -> argtypes (every function returns int)
 SIGNATURES: dict[str, list] = {
@@ -80,6 +84,11 @@ SIGNATURES: dict[str, list] = {
     "tcb_fftfilter_apply": [vp, vp, sz, sz, sz, sz, vp, i32, sz, vp],
     "tcb_fftfilter_destroy": [vp],
     "tcb_prep_rows_split16": [vp, vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, u32, vp],
+    "tcb_phase_pads": [sz, sz, f64, f64, f64, i32, C.POINTER(sz), C.POINTER(sz)],
+    "tcb_phase_create": [C.POINTER(vp), sz, sz, sz, i32, f64, f64, f64, f64, f64, f64, i32],
+    "tcb_phase_sizes": [vp, C.POINTER(sz), C.POINTER(sz)],
+    "tcb_phase_apply": [vp, vp, sz, vp],
+    "tcb_phase_destroy": [vp],
     "tcb_fourierrec_create": [C.POINTER(vp), sz, sz, sz, vp, i32],
     "tcb_fourierrec_backprojection": [vp, vp, vp, vp],
     "tcb_fourierrec_backprojection_slices": [vp, vp, vp, vp],

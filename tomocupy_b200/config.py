@@ -44,7 +44,14 @@ DEFAULTS = {
     "fw_filter": "sym16",
     "fw_level": 7,
     "fw_pad": True,
-    "retrieve_phase_method": "none",
+    "retrieve_phase_method": "none",        # 'none' | 'paganin' | 'Gpaganin' | 'farago'
+    "energy": 20.0,                         # keV
+    "propagation_distance": 0.0,            # mm
+    "pixel_size": 0.0,                      # microns
+    "retrieve_phase_alpha": 0.0,
+    "retrieve_phase_delta_beta": 1500.0,
+    "retrieve_phase_W": 2e-4,               # microns
+    "retrieve_phase_pad": 1,
     "rotate_proj_angle": 0.0,
     "beam_hardening_method": "none",
     # laminography

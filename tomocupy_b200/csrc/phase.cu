@@ -1,0 +1,318 @@
+// Single-distance phase retrieval of projections: Paganin, generalised
+// Paganin and Farago filters (src/tomocupy/processing/retrieve_phase.py).
+//
+// The reference, per projection (_retrieve_phase, retrieve_phase.py:129-145):
+// edge-pad the dy x dz image to Ny x Nz, complex fft2, multiply by the
+// normalised real filter, ifft2, real part, crop.  Here:
+//  * The filter F is real, so for a real image p,
+//    real(ifft2(fft2(p) * F)) = ifft2(fft2(p) * Fe) with Fe(k) = (F(k) +
+//    F(-k)) / 2 (the odd part of F maps the Hermitian spectrum of p to an
+//    anti-Hermitian one, whose inverse transform is purely imaginary).  The
+//    chain is therefore an R2C transform, a multiply by the half spectrum of
+//    Fe (with the 1/(Ny Nz) normalisation folded in) and a C2R transform:
+//    half the transform work and half the spectrum bytes of the reference's
+//    C2C pair.  cuFFT runs the 2D transforms, batched over projections.
+//  * Padding is index clamping in one kernel (the reference's four slice
+//    assignments), cropping is a second kernel.
+//  * The filter is built once per geometry on the host with the reference's
+//    float32 operation order (_reciprocal_grid, _paganin_filter_factor,
+//    _farago_filter_factor, _paganin_filter_factorG, fftshift, / max).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+struct tcb_phase {
+  size_t batch, dy, dz;  // projections per transform batch, image rows x columns
+  size_t py, pz;         // padding of rows / columns (each side)
+  size_t Ny, Nz;         // padded sizes
+  cufftHandle fwd = 0, inv = 0;
+  float *real = nullptr;   // [batch, Ny, Nz] padded images / filtered images
+  float2 *spec = nullptr;  // [batch, Ny, Nz/2+1] spectra
+  float *fe = nullptr;     // [Ny, Nz/2+1] even part of the normalised filter / (Ny Nz)
+};
+
+namespace tcb {
+namespace {
+
+// Constants of retrieve_phase.py:45-48.
+constexpr double PR_PLANCK = 6.58211928e-19;    // [keV*s]
+constexpr double PR_LIGHT = 299792458e+2;        // [cm/s]
+constexpr double PR_PI = 3.14159265359;
+
+double wavelength(double energy) { return 2 * PR_PI * PR_PLANCK * PR_LIGHT / energy; }
+
+// _calc_pad_width (retrieve_phase.py:224-226), float64 like the reference.
+size_t pad_width(size_t dim, double pixel_size, double wl, double dist) {
+  const double pad_pix = std::ceil(PR_PI * wl * dist / (pixel_size * pixel_size));
+  const double p2 = std::pow(2.0, std::ceil(std::log2((double)dim + pad_pix)));
+  return (size_t)(long long)((p2 - (double)dim) * 0.5);
+}
+
+// _reciprocal_coord (retrieve_phase.py:285-305): float32 arange(-n, N, 2) *
+// float32(0.5 / (n * pixel_size)), n = N - 1.
+std::vector<float> reciprocal_coord(double pixel_size, size_t num) {
+  const long long n = (long long)num - 1;
+  const float s = (float)(0.5 / ((double)n * pixel_size));
+  std::vector<float> rc(num);
+  for (size_t i = 0; i < num; i++) rc[i] = (float)(-n + 2 * (long long)i) * s;
+  return rc;
+}
+
+// The reference's filter on the Ny x Nz grid (rows x columns), float32,
+// before fftshift.
+std::vector<float> filter_factor(int method, size_t Ny, size_t Nz, double pixel_size,
+                                 double dist, double energy, double alpha, double db,
+                                 double W) {
+  const double wl = wavelength(energy);
+  std::vector<float> f(Ny * Nz);
+  if (method == TCB_PHASE_GPAGANIN) {
+    // _reciprocal_gridG (retrieve_phase.py:261-282): cos(rc * 2 * PI * ps)
+    // per axis, summed; _paganin_filter_factorG (:214-221)
+    std::vector<float> cx = reciprocal_coord(pixel_size, Ny), cy = reciprocal_coord(pixel_size, Nz);
+    const float two = 2.0f, pi = (float)PR_PI, ps = (float)pixel_size;
+    for (auto &v : cx) v = std::cos(((v * two) * pi) * ps);
+    for (auto &v : cy) v = std::cos(((v * two) * pi) * ps);
+    const double aph = db * (dist * wl) / (4 * PR_PI);
+    const float c = (float)(2 * aph / (W * W));
+    for (size_t i = 0; i < Ny; i++)
+      for (size_t j = 0; j < Nz; j++) {
+        const float kf = cy[j] + cx[i];
+        f[i * Nz + j] = 1.0f / (1.0f - c * (kf - 2.0f));
+      }
+    return f;
+  }
+  // _reciprocal_grid (retrieve_phase.py:229-258): squared coordinates,
+  // meshgrid(indy, indx) summed as indy[j] + indx[i]
+  std::vector<float> ix = reciprocal_coord(pixel_size, Ny), iy = reciprocal_coord(pixel_size, Nz);
+  for (auto &v : ix) v = v * v;
+  for (auto &v : iy) v = v * v;
+  if (method == TCB_PHASE_PAGANIN) {
+    // 1 / (wavelength * dist * w2 / (4 * PI) + alpha) (:209-210)
+    const float a = (float)(wl * dist), d = (float)(4 * PR_PI), al = (float)alpha;
+    for (size_t i = 0; i < Ny; i++)
+      for (size_t j = 0; j < Nz; j++) {
+        const float w2 = iy[j] + ix[i];
+        f[i * Nz + j] = 1.0f / (a * w2 / d + al);
+      }
+  } else {
+    // 1 / (cos(PI*wl*dist*w2) + db*sin(PI*wl*dist*w2)) (:212-213)
+    const float a = (float)(PR_PI * wl * dist), b = (float)db;
+    for (size_t i = 0; i < Ny; i++)
+      for (size_t j = 0; j < Nz; j++) {
+        const float t = a * (iy[j] + ix[i]);
+        f[i * Nz + j] = 1.0f / (std::cos(t) + b * std::sin(t));
+      }
+  }
+  return f;
+}
+
+// Index of padded position i on an axis with padding p and data length d:
+// the reference's edge replication, prj[:p] = prj[p] and prj[-p:] =
+// prj[-p-1] (retrieve_phase.py:138-141).  With p = 0 the second assignment
+// is prj[0:] = prj[-1], which sets the whole axis to its last entry; kept.
+__device__ __forceinline__ int pad_src(int i, int p, int d) {
+  if (p == 0) return d - 1;
+  return min(max(i - p, 0), d - 1);
+}
+
+__global__ void phase_pad(float *__restrict__ out, const float *__restrict__ in, int dy, int dz,
+                          int py, int pz, int Ny, int Nz) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  const size_t b = blockIdx.z;
+  if (j >= Nz) return;
+  const int si = pad_src(i, py, dy), sj = pad_src(j, pz, dz);
+  out[(b * Ny + i) * Nz + j] = __ldg(in + (b * dy + si) * dz + sj);
+}
+
+__global__ void phase_mul(float2 *__restrict__ spec, const float *__restrict__ fe, size_t plane,
+                          size_t total) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const float w = __ldg(fe + t % plane);
+  float2 v = spec[t];
+  v.x *= w;
+  v.y *= w;
+  spec[t] = v;
+}
+
+// Crop (retrieve_phase.py:143-144); with p = 0 nothing is cropped on that axis.
+__global__ void phase_crop(float *__restrict__ out, const float *__restrict__ in, int dy, int dz,
+                           int py, int pz, int Ny, int Nz) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  const size_t b = blockIdx.z;
+  if (j >= dz) return;
+  out[(b * dy + i) * dz + j] = in[(b * Ny + i + py) * Nz + j + pz];
+}
+
+void phase_release(tcb_phase *h) {
+  if (h->fwd) cufftDestroy(h->fwd);
+  if (h->inv) cufftDestroy(h->inv);
+  cudaFree(h->real);
+  cudaFree(h->spec);
+  cudaFree(h->fe);
+  h->fwd = h->inv = 0;
+  h->real = h->fe = nullptr;
+  h->spec = nullptr;
+}
+
+}  // namespace
+}  // namespace tcb
+
+using namespace tcb;
+
+extern "C" int tcb_phase_pads(size_t dy, size_t dz, double pixel_size, double dist,
+                              double energy, int pad, size_t *py, size_t *pz) {
+  TCB_CHECK_ARG(py && pz, "tcb_phase_pads: null output");
+  TCB_CHECK_ARG(dy >= 1 && dz >= 1, "tcb_phase_pads: empty image %zu x %zu", dy, dz);
+  TCB_CHECK_ARG(pixel_size > 0 && energy > 0 && dist >= 0,
+                "tcb_phase_pads: pixel_size and energy must be > 0, dist >= 0");
+  *py = *pz = 0;
+  if (pad) {
+    const double wl = wavelength(energy);
+    *py = pad_width(dy, pixel_size, wl, dist);
+    *pz = pad_width(dz, pixel_size, wl, dist);
+  }
+  return TCB_OK;
+}
+
+extern "C" int tcb_phase_create(tcb_phase **out, size_t batch, size_t dy, size_t dz, int method,
+                                double pixel_size, double dist, double energy, double alpha,
+                                double db, double W, int pad) {
+  TCB_CHECK_ARG(out, "tcb_phase_create: null out");
+  *out = nullptr;
+  TCB_CHECK_ARG(method == TCB_PHASE_PAGANIN || method == TCB_PHASE_GPAGANIN ||
+                    method == TCB_PHASE_FARAGO,
+                "tcb_phase_create: unknown method %d", method);
+  TCB_CHECK_ARG(batch >= 1 && batch <= 65535, "tcb_phase_create: batch must be in [1, 65535]");
+  TCB_CHECK_ARG(method != TCB_PHASE_GPAGANIN || W > 0, "tcb_phase_create: W must be > 0");
+  size_t py = 0, pz = 0;
+  int st = tcb_phase_pads(dy, dz, pixel_size, dist, energy, pad, &py, &pz);
+  if (st != TCB_OK) return st;
+  const size_t Ny = dy + 2 * py, Nz = dz + 2 * pz, Nc = Nz / 2 + 1;
+  TCB_CHECK_ARG(Ny <= 65535 && Nz < (1u << 30) && Ny * Nz < (1ull << 31),
+                "tcb_phase_create: padded image %zu x %zu too large", Ny, Nz);
+  // the normalised filter, fftshifted, then its even part over the half spectrum
+  std::vector<float> f = filter_factor(method, Ny, Nz, pixel_size, dist, energy, alpha, db, W);
+  float fmax = -INFINITY;
+  std::vector<float> sh(Ny * Nz);
+  for (size_t i = 0; i < Ny; i++)
+    for (size_t j = 0; j < Nz; j++) {
+      // fftshift: output[i][j] = input[(i + Ny/2) % Ny][(j + Nz/2) % Nz]... with the
+      // reference's convention (numpy fftshift shifts by floor(N/2))
+      const float v = f[((i + Ny - Ny / 2) % Ny) * Nz + (j + Nz - Nz / 2) % Nz];
+      sh[i * Nz + j] = v;
+      fmax = std::max(fmax, v);
+    }
+  TCB_CHECK_ARG(std::isfinite(fmax) && fmax != 0.f,
+                "tcb_phase_create: filter maximum %g is not finite and nonzero", (double)fmax);
+  const float inv_n = (float)(1.0 / ((double)Ny * (double)Nz));
+  std::vector<float> fe(Ny * Nc);
+  for (size_t i = 0; i < Ny; i++)
+    for (size_t j = 0; j < Nc; j++) {
+      const float a = sh[i * Nz + j] / fmax;
+      const float b = sh[((Ny - i) % Ny) * Nz + (Nz - j) % Nz] / fmax;
+      fe[i * Nc + j] = 0.5f * (a + b) * inv_n;
+    }
+
+  tcb_phase *h = new tcb_phase();
+  h->batch = batch;
+  h->dy = dy;
+  h->dz = dz;
+  h->py = py;
+  h->pz = pz;
+  h->Ny = Ny;
+  h->Nz = Nz;
+  auto fail = [&](int code) {
+    phase_release(h);
+    delete h;
+    return code;
+  };
+  if (cudaMalloc(&h->real, batch * Ny * Nz * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->spec, batch * Ny * Nc * sizeof(float2)) != cudaSuccess ||
+      cudaMalloc(&h->fe, Ny * Nc * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("tcb_phase_create: out of device memory (batch %zu of %zu x %zu)", batch, Ny, Nz);
+    return fail(TCB_ERR_OUT_OF_MEMORY);
+  }
+  cudaError_t e = cudaMemcpy(h->fe, fe.data(), fe.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    set_error("tcb_phase_create: cudaMemcpy failed: %s", cudaGetErrorString(e));
+    return fail(TCB_ERR_CUDA);
+  }
+  int dims[2] = {(int)Ny, (int)Nz};
+  cufftResult r = cufftPlanMany(&h->fwd, 2, dims, nullptr, 1, (int)(Ny * Nz), nullptr, 1,
+                                (int)(Ny * Nc), CUFFT_R2C, (int)batch);
+  if (r == CUFFT_SUCCESS)
+    r = cufftPlanMany(&h->inv, 2, dims, nullptr, 1, (int)(Ny * Nc), nullptr, 1, (int)(Ny * Nz),
+                      CUFFT_C2R, (int)batch);
+  if (r != CUFFT_SUCCESS) {
+    set_error("tcb_phase_create: cufftPlanMany failed: %d", (int)r);
+    return fail(r == CUFFT_ALLOC_FAILED ? TCB_ERR_OUT_OF_MEMORY : TCB_ERR_CUFFT);
+  }
+  *out = h;
+  return TCB_OK;
+}
+
+extern "C" int tcb_phase_sizes(tcb_phase *h, size_t *py, size_t *pz) {
+  TCB_CHECK_ARG(h && py && pz, "tcb_phase_sizes: null pointer");
+  *py = h->py;
+  *pz = h->pz;
+  return TCB_OK;
+}
+
+extern "C" int tcb_phase_apply(tcb_phase *h, float *data, size_t nproj, void *stream) {
+  TCB_CHECK_ARG(h, "tcb_phase_apply: null handle");
+  TCB_CHECK_ARG(h->real, "tcb_phase_apply: handle was freed");
+  TCB_CHECK_ARG(data || nproj == 0, "tcb_phase_apply: null data");
+  cudaStream_t s = (cudaStream_t)stream;
+  TCB_CUFFT(cufftSetStream(h->fwd, s));
+  TCB_CUFFT(cufftSetStream(h->inv, s));
+  const size_t Nc = h->Nz / 2 + 1, plane = h->Ny * Nc;
+  for (size_t p0 = 0; p0 < nproj; p0 += h->batch) {
+    const size_t b = std::min(h->batch, nproj - p0);
+    float *d = data + p0 * h->dy * h->dz;
+    {
+      StageTimer t("phase_pad", s);
+      phase_pad<<<dim3(ceil_div(h->Nz, 256), (unsigned)h->Ny, (unsigned)b), 256, 0, s>>>(
+          h->real, d, (int)h->dy, (int)h->dz, (int)h->py, (int)h->pz, (int)h->Ny, (int)h->Nz);
+      TCB_LAUNCH_CHECK();
+      count_launch();
+    }
+    // a partial last batch runs the full-batch plan on stale padded images
+    // beyond b; only the first b are cropped back
+    {
+      StageTimer t("phase_r2c", s);
+      TCB_CUFFT(cufftExecR2C(h->fwd, h->real, (cufftComplex *)h->spec));
+    }
+    {
+      StageTimer t("phase_mul", s);
+      const size_t total = b * plane;
+      phase_mul<<<ceil_div(total, 256), 256, 0, s>>>(h->spec, h->fe, plane, total);
+      TCB_LAUNCH_CHECK();
+      count_launch();
+    }
+    {
+      StageTimer t("phase_c2r", s);
+      TCB_CUFFT(cufftExecC2R(h->inv, (cufftComplex *)h->spec, h->real));
+    }
+    {
+      StageTimer t("phase_crop", s);
+      phase_crop<<<dim3(ceil_div(h->dz, 256), (unsigned)h->dy, (unsigned)b), 256, 0, s>>>(
+          d, h->real, (int)h->dy, (int)h->dz, (int)h->py, (int)h->pz, (int)h->Ny, (int)h->Nz);
+      TCB_LAUNCH_CHECK();
+      count_launch();
+    }
+  }
+  return TCB_OK;
+}
+
+extern "C" int tcb_phase_destroy(tcb_phase *h) {
+  if (!h) return TCB_OK;
+  phase_release(h);
+  delete h;
+  return TCB_OK;
+}

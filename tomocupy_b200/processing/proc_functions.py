@@ -88,6 +88,31 @@ def prep_rows_split16(hi, lo, data, dark0=None, flat0=None, flat1=None, *, darkf
     return hi, lo
 
 
+PHASE_METHODS = ("paganin", "Gpaganin", "farago")
+
+
+def retrieve_phase(data):
+    """The phase-retrieval step of proc_proj (proc_functions.py:169-181), in
+    place on float32 projections [nproj, dy, dz] on the device, with the
+    reference's unit conversions (pixel_size um -> cm, propagation_distance
+    mm -> cm, W um -> cm).  'FourierFilter', a config choice that the
+    reference's proc_proj never matches (it tests for 'FF'), does nothing
+    there and does nothing here."""
+    method = args.retrieve_phase_method
+    if method in ("none", "FourierFilter"):
+        return data
+    if method not in PHASE_METHODS:
+        raise NotImplementedError(f"retrieve_phase_method={method!r}")
+    from . import retrieve_phase as rp
+    data = data.contiguous()
+    ps, dist = args.pixel_size * 1e-4, args.propagation_distance / 10
+    if method == "farago":
+        return rp.farago_filter(data, ps, dist, args.energy, args.retrieve_phase_delta_beta,
+                                method)
+    return rp.paganin_filter(data, ps, dist, args.energy, args.retrieve_phase_alpha, method,
+                             args.retrieve_phase_delta_beta, args.retrieve_phase_W * 1e-4)
+
+
 class ProcFunctions:
     def __init__(self):
         if args.beam_hardening_method != "none":
@@ -133,9 +158,10 @@ class ProcFunctions:
         return out
 
     def proc_proj(self, data, st=None, end=None, res=None):
-        """Processing of a projection chunk: -log (other steps are out of scope)."""
-        if args.retrieve_phase_method != "none":
-            raise NotImplementedError("phase retrieval is not part of tomocupy_b200")
+        """Processing of a projection chunk (proc_functions.py:163-196): phase
+        retrieval, then -log (projection rotation and beam hardening are out of
+        scope)."""
+        data = retrieve_phase(data)
         if args.rotate_proj_angle != 0:
             raise NotImplementedError("projection rotation is not part of tomocupy_b200")
         if args.file_type == "double_fov":

@@ -19,7 +19,7 @@ import torch
 
 from .global_vars import args, params
 from .pipeline import SinoPipeline, copy2d_rows
-from .processing.proc_functions import darkflat_stats
+from .processing.proc_functions import PHASE_METHODS, darkflat_stats
 
 
 def _supported():
@@ -31,6 +31,13 @@ def _supported():
     if args.dtype not in ("float32", "mixed"):
         raise NotImplementedError(
             "the fused driver runs the float32 drop-in path or the 'mixed' tensor-core path")
+
+
+def _no_phase(where):
+    if args.retrieve_phase_method in PHASE_METHODS:
+        raise NotImplementedError(
+            f"{where}: phase retrieval filters whole projections; run GPURecSteps "
+            "(the reference applies it to the rows of each sinogram chunk here)")
 
 
 class GPURec:
@@ -75,8 +82,30 @@ class GPURec:
         return darkflat_stats(dark, flat, args.bright_ratio, False, stream)
 
     # ------------------------------------------------------------------ full
+    def recon_preprocessed(self, data):
+        """Reconstruct every slice from pre-processed float32 projections
+        [nproj, nz, n] on the device (the step driver after proc_sino and
+        proc_proj: filter and backprojection only); results go to cl_writer."""
+        ncz, n, nz = params.ncz, params.n, params.nz
+        assert data.dtype == torch.float32 and tuple(data.shape) == (params.nproj, nz, n)
+        pipe = SinoPipeline(n, params.nproj, ncz, params.theta, params.center, args.fbp_filter,
+                            args.reconstruction_algorithm, minus_log=False, device=self.device,
+                            stripe=None, precision=self.precision, out_dtype=args.out_dtype,
+                            mixed_filter=args.mixed_filter)
+        rec_out = self.cl_writer.allocate(nz, n)
+        out = torch.empty((ncz, n, n), dtype=pipe.out_dtype, device=self.device)
+        for k in range(params.nzchunk):
+            z0, lz = k * ncz, int(params.lzchunk[k])
+            if lz < ncz:
+                pipe.clear_rows(lz)
+            pipe.reconstruct(out, data[:, z0:z0 + lz])
+            rec_out[z0:z0 + lz].copy_(out[:lz])
+        torch.cuda.synchronize(self.device)
+        return rec_out
+
     def recon_all(self):
         """Reconstruct every slice; results go to ``cl_writer`` (host or device)."""
+        _no_phase("GPURec.recon_all")
         data, dark, flat = self.cl_reader.frames()
         ncz, n, nz, nproj = params.ncz, params.n, params.nz, params.nproj
         dev = self.device
@@ -146,6 +175,7 @@ class GPURec:
         The sweep over all centres is one CUDA graph (TryCenterSweep), recorded
         once and replayed for each requested slice.
         """
+        _no_phase("GPURec.recon_try")
         from .trycenter import TryCenterSweep
         if args.reconstruction_algorithm != "fourierrec" or args.remove_stripe_method != "none":
             raise NotImplementedError("try-centre sweeps run fourierrec without ring removal")

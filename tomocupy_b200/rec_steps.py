@@ -27,7 +27,7 @@ import torch
 
 from .global_vars import args, params
 from .pipeline import SinoPipeline
-from .processing.proc_functions import darkflat_stats, prep_rows
+from .processing.proc_functions import PHASE_METHODS, darkflat_stats, prep_rows, retrieve_phase
 from .reconstruction.backproj_functions import phase_weights, rfftfreq32
 from .reconstruction.fbp_filter import calc_filter
 
@@ -55,7 +55,11 @@ class GPURecSteps:
         nproj, nz, n = data.shape
         out = torch.empty((nproj, nz, n), dtype=torch.float32, device=dev)
         fw = args.remove_stripe_method == "fw"
-        prep_rows(out, data, d0, f0, darkflat=True, minus_log=(args.minus_log == "True") and not fw,
+        phase = args.retrieve_phase_method in PHASE_METHODS
+        # -log comes last: after ring removal (proc_sino) and phase retrieval (proc_proj)
+        late_log = fw or phase
+        prep_rows(out, data, d0, f0, darkflat=True,
+                  minus_log=(args.minus_log == "True") and not late_log,
                   out_zstride=n, out_pstride=nz * n)
         if fw:
             from .processing.remove_stripe import remove_stripe_fw
@@ -64,11 +68,13 @@ class GPURecSteps:
                 out[:, z0:z0 + ncz] = remove_stripe_fw(out[:, z0:z0 + ncz].contiguous(),
                                                        args.fw_sigma, args.fw_filter,
                                                        args.fw_level)
-            if args.minus_log == "True":
-                prep_rows(out, out, darkflat=False, minus_log=True, out_zstride=n,
-                          out_pstride=nz * n)
         elif args.remove_stripe_method != "none":
             raise NotImplementedError(f"remove_stripe_method={args.remove_stripe_method!r}")
+        if phase:
+            retrieve_phase(out)
+        if late_log and args.minus_log == "True":
+            prep_rows(out, out, darkflat=False, minus_log=True, out_zstride=n,
+                      out_pstride=nz * n)
         return out
 
     # ------------------------------------------------------------------ driver
@@ -85,6 +91,12 @@ class GPURecSteps:
     def _tomo(self):
         from .rec import GPURec
         rec = GPURec(self.cl_reader, self.cl_writer, device=self.device)
+        if args.retrieve_phase_method in PHASE_METHODS:
+            # phase retrieval needs whole projections: pre-process the
+            # resident dataset (proc_sino + proc_proj), then backproject
+            if args.reconstruction_type != "full":
+                raise NotImplementedError("phase retrieval with try-centre sweeps")
+            return rec.recon_preprocessed(self.preprocessed())
         if args.reconstruction_type == "full":
             return rec.recon_all()
         return rec.recon_try()
