@@ -139,6 +139,26 @@ int tcb_stripe_fw_create(tcb_stripe_fw **out, size_t nproj, size_t nz, size_t ni
 int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t sstride, void *stream);
 int tcb_stripe_fw_destroy(tcb_stripe_fw *h);
 
+/* Titarenko ring removal.  Replaces remove_stripe_ti
+ * (src/tomocupy/processing/remove_stripe.py:296-307), called by
+ * ProcFunctions.proc_sino for remove_stripe_method 'ti'
+ * (src/tomocupy/processing/proc_functions.py:154-156).  mask: the column
+ * range [m0, m1) that the reference's mask[:, n//2 - ms//2 : n//2 + ms//2]
+ * selects (ms = mask_size * n, Python slice rules; host only; the reference
+ * slices with a float when mask_size is a float, which NumPy and CuPy
+ * reject, so only integer mask sizes run there).  n must be even (for odd n
+ * the reference's irfft returns n - 1 samples and its add fails).
+ * apply_sino: in place on
+ * sino[z * zstride + p * pstride + x] (nz slices, nproj angles, n columns).
+ * ------------------------------------------------------------------------ */
+typedef struct tcb_stripe_ti tcb_stripe_ti;
+int tcb_stripe_ti_mask(size_t n, double mask_size, long long *m0, long long *m1);
+int tcb_stripe_ti_create(tcb_stripe_ti **out, size_t nproj, size_t nz, size_t n, double beta,
+                         double mask_size);
+int tcb_stripe_ti_apply_sino(tcb_stripe_ti *h, float *sino, size_t zstride, size_t pstride,
+                             void *stream);
+int tcb_stripe_ti_destroy(tcb_stripe_ti *h);
+
 /* ------------------------------------------------------------------------
  * Single-distance phase retrieval of projections.  Replaces paganin_filter
  * (methods 'paganin', 'Gpaganin') and farago_filter

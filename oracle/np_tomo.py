@@ -56,6 +56,29 @@ def minus_log(x):
 
 
 # --------------------------------------------------------------------------
+# Titarenko ring removal (src/tomocupy/processing/remove_stripe.py:296-307)
+# --------------------------------------------------------------------------
+def remove_stripe_ti(data, beta, mask_size):
+    """remove_stripe_ti on float32 [nproj, nz, n] (returns a new array): float32
+    column means over angles minus column 0, convolution with
+    gamma = beta * ((1-beta)/(1+beta))**|k| (gamma[0] -= 1) through
+    rfft / irfft (complex64 times complex128, as CuPy types them), added to
+    every angle inside mask[:, n//2 - ms//2 : n//2 + ms//2], ms = mask_size*n."""
+    data = np.array(data, dtype=np.float32)
+    n = data.shape[-1]
+    gamma = beta * ((1 - beta) / (1 + beta)) ** np.abs(np.fft.fftfreq(n) * n)
+    gamma[0] -= 1
+    v = np.mean(data, axis=0, dtype=np.float32)
+    v = v - v[:, 0:1]
+    v = np.fft.irfft(np.fft.rfft(v).astype(np.complex64) * np.fft.rfft(gamma))
+    mask = np.zeros(v.shape, dtype=v.dtype)
+    ms = mask_size * mask.shape[1]
+    mask[:, mask.shape[1] // 2 - int(ms // 2):mask.shape[1] // 2 + int(ms // 2)] = 1
+    data[:] += v * mask
+    return data
+
+
+# --------------------------------------------------------------------------
 # phase retrieval (src/tomocupy/processing/retrieve_phase.py:57-305)
 # --------------------------------------------------------------------------
 _PR_PLANCK = 6.58211928e-19   # retrieve_phase.py:45-48

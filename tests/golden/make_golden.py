@@ -9,7 +9,8 @@
             of option combinations (src/tomocupy/dataio/reader.py:82-272)
           * paganin_filter / farago_filter (retrieve_phase.py:57-145)
         -> filter_spectra.npz, sizes_cases.json, ..., phase_retrieval.npz
-        (--phase: phase_retrieval.npz only)
+          * remove_stripe_ti (remove_stripe.py:296-307) -> ti_stripe.npz
+        (--phase / --ti: only those two)
 
     python tests/golden/make_golden.py --gpu --out DIR
         Runs the reference's CUDA operators (oracle/_ref, built from the
@@ -198,6 +199,7 @@ def gen_cpu(ref: Path):
     np.savez_compressed(HERE / "fw_stripe.npz", **fw)
     print("wrote filter_spectra.npz, sizes_cases.json, lprec_grids.npz and fw_stripe.npz")
     gen_phase(ref)
+    gen_ti(ref)
 
 
 # Phase retrieval (retrieve_phase.py:57-145): (method, nproj, dy, dz,
@@ -213,6 +215,50 @@ PHASE_CASES = [
     ("farago", 1, 20, 31, 1e-4, 0.5, 25.0, 1e-3, 1000.0, 2e-4, 6),
     ("paganin", 2, 16, 16, 1e-4, 0.0, 20.0, 1e-3, 1500.0, 2e-4, 5),
 ]
+
+
+# Titarenko ring removal (remove_stripe.py:296-307): (nproj, nz, ni, beta,
+# mask_size, seed).  Integer mask sizes only: the reference slices with
+# mask_size * n, which NumPy and CuPy reject when it is a float; mask 2
+# gives a negative slice start, i.e. the last n/2 columns.  Even widths
+# only: for odd n the reference's irfft returns n - 1 samples and the add
+# fails to broadcast.
+TI_CASES = [
+    (90, 4, 64, 0.022, 1, 1),
+    (60, 3, 100, 0.05, 2, 2),
+    (120, 2, 256, 0.022, 1, 3),
+    (30, 2, 48, 0.022, 0, 4),
+]
+
+
+def ti_input(nproj, nz, ni, seed):
+    """Seeded flat-normalised sinograms with column gain stripes."""
+    rng = np.random.default_rng(seed)
+    x = 0.7 + 0.1 * rng.random((nproj, nz, ni))
+    gains = 1.0 + 0.03 * rng.standard_normal(ni) * (rng.random(ni) < 0.2)
+    return (x * gains).astype(np.float32)
+
+
+def gen_ti(ref: Path):
+    """Runs remove_stripe_ti from the reference's own source with NumPy for
+    CuPy -> ti_stripe.npz."""
+    if "cupy" not in sys.modules:
+        _install_stubs()
+    for name in ("pywt", "cupyx", "cupyx.scipy", "cupyx.scipy.ndimage"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    nd = sys.modules["cupyx.scipy.ndimage"]
+    for f in ("median_filter", "binary_dilation", "uniform_filter1d"):
+        if not hasattr(nd, f):
+            setattr(nd, f, None)
+    rs = _load(ref / "src/tomocupy/processing/remove_stripe.py", "ref_remove_stripe_ti")
+    out = {}
+    for i, (nproj, nz, ni, beta, mask, seed) in enumerate(TI_CASES):
+        data = ti_input(nproj, nz, ni, seed)
+        out[f"in_{i}"] = data
+        out[f"out_{i}"] = np.asarray(rs.remove_stripe_ti(data.copy(), beta, mask),
+                                     dtype=np.float32)
+    np.savez_compressed(HERE / "ti_stripe.npz", **out)
+    print("wrote ti_stripe.npz")
 
 
 def phase_input(nproj, dy, dz, seed):
@@ -314,12 +360,16 @@ if __name__ == "__main__":
     ap.add_argument("--cpu", action="store_true")
     ap.add_argument("--gpu", action="store_true")
     ap.add_argument("--phase", action="store_true", help="only phase_retrieval.npz")
+    ap.add_argument("--ti", action="store_true", help="only ti_stripe.npz")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
     if a.cpu:
         gen_cpu(Path(a.ref))
-    elif a.phase:
-        gen_phase(Path(a.ref))
+    else:
+        if a.phase:
+            gen_phase(Path(a.ref))
+        if a.ti:
+            gen_ti(Path(a.ref))
     if a.gpu:
         gen_gpu(Path(a.out))

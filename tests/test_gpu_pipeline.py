@@ -50,7 +50,12 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
         d = np_tomo.darkflat(np.asarray(data[:, z0:z0 + ncz]), np.asarray(dark[:, z0:z0 + ncz]),
                              np.asarray(flat[:, z0:z0 + ncz]))
         d = torch.as_tensor(np.ascontiguousarray(d), device=dev)
-        if stripe is not None:
+        if stripe is not None and stripe[0] == "ti":
+            # Titarenko's method (checked on its own against the reference's
+            # remove_stripe_ti in tests/test_gpu_stripe.py)
+            from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
+            d = remove_stripe_ti(d.contiguous(), stripe[1], stripe[2])
+        elif stripe is not None:
             # proc_sino: ring removal on the dark/flat corrected frames (checked on
             # its own against the reference's remove_stripe_fw), then proc_proj: -log
             from tomocupy_b200.processing.remove_stripe import remove_stripe_fw
@@ -129,6 +134,24 @@ def test_c1_fw_ring_removal_pipeline(cuda, ref, c1):
     GPURec(reader, writer).recon_all()
     theirs = reference_chain(ref, d, dk, fl, theta, ncz=8, stripe=(1.0, "sym16", 7))
     err = rel_l2(writer.rec, theirs)
+    assert err < 1e-5, err
+
+
+def test_c1_ti_ring_removal_pipeline(cuda, ref, c1):
+    """dark/flat -> Titarenko ring removal -> -log -> filter -> fourierrec, with a
+    partial last chunk (12 rows in chunks of 8)."""
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    data, dark, flat, theta, _ = c1
+    d, dk, fl = data[:, :12], dark[:, :12], flat[:, :12]
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=8,
+                      remove_stripe_method="ti", ti_beta=0.022, ti_mask=1)
+    writer = ArrayWriter(device="cpu", pin=True)
+    GPURec(ArrayReader(d, dk, fl, theta=theta, pin=True), writer).recon_all()
+    theirs = reference_chain(ref, d[:, :8], dk[:, :8], fl[:, :8], theta, ncz=8,
+                             stripe=("ti", 0.022, 1))
+    err = rel_l2(writer.rec[:8], theirs)
     assert err < 1e-5, err
 
 

@@ -4,6 +4,8 @@ filter banks come from tomocupy_b200.processing.wavelets because PyWavelets
 is not available, see tests/golden/make_golden.py).  The wavelet stages use
 the reference's float32 operation order; the band FFTs differ (cuFFT float32
 here, NumPy float64 in the fixture), hence rel-L2 <= 1e-5."""
+import sys
+
 import numpy as np
 import pytest
 import torch
@@ -67,3 +69,47 @@ def test_fw_removes_stripes(cuda):
     before = np.abs(np.diff(data.cpu().numpy().mean(0), axis=-1)).max()
     after = np.abs(np.diff(out.mean(0), axis=-1)).max()
     assert after < 0.5 * before
+
+
+def _ti_cases():
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    from make_golden import TI_CASES
+    return TI_CASES
+
+
+@pytest.mark.parametrize("i", range(4))
+def test_ti_matches_reference_fixture(cuda, i):
+    """Titarenko ring removal against the reference's own remove_stripe_ti
+    (NumPy for CuPy): float32 column means (double accumulation here), the
+    gamma convolution in float64, the add rounded once to float32."""
+    from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
+    g = np.load(ROOT / "tests" / "golden" / "ti_stripe.npz")
+    nproj, nz, n, beta, mask, seed = _ti_cases()[i]
+    data = torch.as_tensor(g[f"in_{i}"], device=cuda)
+    out = remove_stripe_ti(data, beta, mask)
+    torch.cuda.synchronize()
+    assert out.data_ptr() == data.data_ptr()
+    want = g[f"out_{i}"]
+    assert rel_l2(out.cpu().numpy(), want) < 1e-6
+    assert float(np.abs(out.cpu().numpy() - want).max()) < 1e-6
+
+
+def test_ti_float_mask_and_larger_size(cuda):
+    """A float mask size (which the reference's slicing rejects) selects the
+    same centred columns as the oracle's integer-cast slice; 2048 columns."""
+    from oracle import np_tomo
+    from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    from make_golden import ti_input
+    x = ti_input(300, 3, 2048, seed=11)
+    want = np_tomo.remove_stripe_ti(x, 0.022, 0.5)
+    got = remove_stripe_ti(torch.as_tensor(x, device=cuda), 0.022, 0.5).cpu().numpy()
+    assert rel_l2(got, want) < 1e-6
+    assert np.array_equal(got[:, :, :512], x[:, :, :512])   # outside the mask: untouched
+
+
+def test_ti_rejects_odd_width(cuda):
+    from tomocupy_b200 import _lib
+    from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
+    with pytest.raises(_lib.TcbError):
+        remove_stripe_ti(torch.ones((4, 2, 101), device=cuda), 0.022, 1)

@@ -84,6 +84,10 @@ SIGNATURES: dict[str, list] = {
     "tcb_fftfilter_apply": [vp, vp, sz, sz, sz, sz, vp, i32, sz, vp],
     "tcb_fftfilter_destroy": [vp],
     "tcb_prep_rows_split16": [vp, vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, u32, vp],
+    "tcb_stripe_ti_mask": [sz, f64, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "tcb_stripe_ti_create": [C.POINTER(vp), sz, sz, sz, f64, f64],
+    "tcb_stripe_ti_apply_sino": [vp, vp, sz, sz, vp],
+    "tcb_stripe_ti_destroy": [vp],
     "tcb_phase_pads": [sz, sz, f64, f64, f64, i32, C.POINTER(sz), C.POINTER(sz)],
     "tcb_phase_create": [C.POINTER(vp), sz, sz, sz, i32, f64, f64, f64, f64, f64, f64, i32],
     "tcb_phase_sizes": [vp, C.POINTER(sz), C.POINTER(sz)],

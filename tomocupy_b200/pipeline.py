@@ -105,14 +105,19 @@ class SinoPipeline:
             self.rows = torch.empty((self.ncz, self.nproj, self.ne), dtype=torch.float32,
                                     device=self.device)
             self.filter = cfunc_filter.cfunc_filter(self.nproj, self.ncz, self.ne)
-        # optional Fourier-wavelet ring removal between dark/flat and -log
-        # (ProcFunctions.proc_sino, proc_functions.py:140-160): stripe is
-        # (sigma, wavelet, level)
+        # optional ring removal between dark/flat and -log (ProcFunctions.proc_sino,
+        # proc_functions.py:140-160): stripe is ("ti", beta, mask_size) for
+        # Titarenko's method, else (sigma, wavelet, level) for the
+        # Fourier-wavelet method; both work in place on sinograms in self.sino
         self.fw = None
-        if stripe is not None:
+        if stripe is not None and stripe[0] == "ti":
+            from .processing.remove_stripe import StripeTI
+            self.fw = StripeTI(self.nproj, self.ncz, self.n, stripe[1], stripe[2])
+        elif stripe is not None:
             from .processing.remove_stripe import StripeFW
             sigma, wname, level = stripe
             self.fw = StripeFW(self.nproj, self.ncz, self.n, sigma, wname, level)
+        if self.fw is not None:
             self.sino = torch.zeros((self.ncz, self.fw.nproj_pad, self.n), dtype=torch.float32,
                                     device=self.device)
         if algorithm == "fourierrec":

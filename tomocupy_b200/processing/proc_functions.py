@@ -149,6 +149,9 @@ class ProcFunctions:
             from . import remove_stripe
             out = remove_stripe.remove_stripe_fw(out, args.fw_sigma, args.fw_filter,
                                                  args.fw_level)
+        elif args.remove_stripe_method == "ti":
+            from . import remove_stripe
+            out = remove_stripe.remove_stripe_ti(out, args.ti_beta, args.ti_mask)
         elif args.remove_stripe_method != "none":
             raise NotImplementedError(
                 f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")

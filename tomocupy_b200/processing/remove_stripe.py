@@ -1,4 +1,5 @@
-"""Fourier-wavelet ring removal (``remove_stripe_fw``) over the native operator.
+"""Fourier-wavelet (``remove_stripe_fw``) and Titarenko (``remove_stripe_ti``)
+ring removal over the native operators.
 
 Same function signature and result layout as the reference
 (src/tomocupy/processing/remove_stripe.py:253-293): data [nproj, nz, ni]
@@ -62,3 +63,52 @@ def remove_stripe_fw(data, sigma, wname, level):
     out = torch.empty((nproj, nz, ni), dtype=data.dtype, device=data.device)
     out.copy_(sino[:, op.poff:op.poff + nproj].permute(1, 0, 2))
     return out
+
+
+# --------------------------------------------------------------------------
+# Titarenko ring removal (remove_stripe.py:296-307)
+# --------------------------------------------------------------------------
+def ti_mask(n: int, mask_size: float) -> tuple[int, int]:
+    """Column range [m0, m1) of the reference's
+    mask[:, n//2 - ms//2 : n//2 + ms//2], ms = mask_size * n (Python slice
+    rules; the reference only runs with an integer mask_size, since NumPy and
+    CuPy reject float slice bounds)."""
+    a, b = C.c_longlong(), C.c_longlong()
+    _lib.call("tcb_stripe_ti_mask", int(n), float(mask_size), C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+class StripeTI(NativeHandle):
+    """Titarenko ring removal for a fixed chunk shape, in place on sinograms
+    [nz, nproj, ni] (any slice / angle strides with contiguous rows)."""
+    _destroy = "tcb_stripe_ti_destroy"
+
+    def __init__(self, nproj, nz, ni, beta=0.022, mask_size=1):
+        self._set(_lib.create("tcb_stripe_ti_create", int(nproj), int(nz), int(ni), float(beta),
+                              float(mask_size)))
+        self.nproj, self.nz, self.ni = int(nproj), int(nz), int(ni)
+        # the pipeline's stripe-operator interface (no angle padding)
+        self.nproj_pad, self.poff = self.nproj, 0
+
+    def apply_sino(self, sino, stream=None):
+        """In place on sino [nz, >= nproj, ni] float32, angle rows 0..nproj-1."""
+        assert sino.dtype == torch.float32 and sino.stride(2) == 1 and sino.shape[0] == self.nz
+        _lib.call("tcb_stripe_ti_apply_sino", self._live(), sino.data_ptr(), sino.stride(0),
+                  sino.stride(1), _lib.stream_ptr(stream))
+        return sino
+
+
+@functools.lru_cache(maxsize=8)
+def _ti_operator(nproj, nz, ni, beta, mask_size, device_index):
+    return StripeTI(nproj, nz, ni, beta, mask_size)
+
+
+def remove_stripe_ti(data, beta, mask_size):
+    """Remove stripes with Titarenko's method: data [nproj, nz, ni] float32 on
+    the device, corrected in place and returned (like the reference)."""
+    nproj, nz, ni = data.shape
+    if data.dtype != torch.float32:
+        raise ValueError("remove_stripe_ti: float32 data")
+    op = _ti_operator(nproj, nz, ni, float(beta), float(mask_size), data.device.index or 0)
+    op.apply_sino(data.permute(1, 0, 2))   # [nz, nproj, ni] view: strides (ni, nz*ni, 1)
+    return data

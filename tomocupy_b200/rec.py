@@ -23,7 +23,7 @@ from .processing.proc_functions import PHASE_METHODS, darkflat_stats
 
 
 def _supported():
-    if args.remove_stripe_method not in ("none", "fw"):
+    if args.remove_stripe_method not in ("none", "fw", "ti"):
         raise NotImplementedError(
             f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
     if args.file_type != "standard" or args.binning != 0:
@@ -65,6 +65,8 @@ class GPURec:
             stripe = None
             if args.remove_stripe_method == "fw":
                 stripe = (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
+            elif args.remove_stripe_method == "ti":
+                stripe = ("ti", float(args.ti_beta), float(args.ti_mask))
             self._pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                       params.center, args.fbp_filter,
                                       args.reconstruction_algorithm,

@@ -54,14 +54,20 @@ class GPURecSteps:
         d0, f0, _ = darkflat_stats(dark, flat, args.bright_ratio)
         nproj, nz, n = data.shape
         out = torch.empty((nproj, nz, n), dtype=torch.float32, device=dev)
-        fw = args.remove_stripe_method == "fw"
+        stripe = args.remove_stripe_method in ("fw", "ti")
         phase = args.retrieve_phase_method in PHASE_METHODS
         # -log comes last: after ring removal (proc_sino) and phase retrieval (proc_proj)
-        late_log = fw or phase
+        late_log = stripe or phase
         prep_rows(out, data, d0, f0, darkflat=True,
                   minus_log=(args.minus_log == "True") and not late_log,
                   out_zstride=n, out_pstride=nz * n)
-        if fw:
+        if args.remove_stripe_method == "ti":
+            from .processing.remove_stripe import remove_stripe_ti
+            ncz = params.ncz
+            for z0 in range(0, nz, ncz):
+                part = out[:, z0:z0 + ncz].contiguous()
+                out[:, z0:z0 + ncz] = remove_stripe_ti(part, args.ti_beta, args.ti_mask)
+        elif stripe:
             from .processing.remove_stripe import remove_stripe_fw
             ncz = params.ncz
             for z0 in range(0, nz, ncz):
