@@ -505,8 +505,9 @@ def run_lamino(a, dev):
 def run_methods(a, data, dark, flat, theta, dev):
     """The rest of the production configuration, fp32 drop-in path, frames resident:
     fourierrec with Fourier-wavelet ring removal (level 7, sigma 1, sym16) and with
-    Titarenko ring removal (beta 0.022, full mask) on the whole volume, and lprec /
-    linerec on a bounded slab of rows."""
+    Titarenko ring removal (beta 0.022, full mask) and with outlier removal
+    (dezinger width 3, threshold 5000) on the whole volume, and lprec / linerec on
+    a bounded slab of rows."""
     import torch
     from tomocupy_b200 import _lib, global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
@@ -518,6 +519,8 @@ def run_methods(a, data, dark, flat, theta, dev):
                                                          fw_filter="sym16", fw_level=7)),
             ("fourierrec+ti", "fourierrec", a.nz, dict(remove_stripe_method="ti", ti_beta=0.022,
                                                          ti_mask=1)),
+            ("fourierrec+dezinger", "fourierrec", a.nz, dict(dezinger=3,
+                                                              dezinger_threshold=5000)),
             ("lprec", "lprec", min(a.nz, a.slab_rows), {}),
             ("linerec", "linerec", min(a.nz, a.slab_rows), {})]
     for name, alg, rows, extra in legs:

@@ -124,6 +124,18 @@ int tcb_prep_noalloc(float *out, const void *data, const void *dark, const void 
                      size_t out_pstride, size_t out_poff, size_t out_xoff,
                      size_t out_width, unsigned flags, void *stream);
 
+/* Outlier (zinger) removal.  Replaces ProcFunctions.remove_outliers
+ * (src/tomocupy/processing/proc_functions.py:96-107), which proc_sino applies
+ * to the projections, darks and flats of a chunk before dark/flat correction
+ * (proc_functions.py:146-148): out = where(in > f and in - f > threshold, f,
+ * in) with f = median_filter(in, [width, 1, width]) (mode 'reflect') over
+ * frames [nframes, nz, n] of type in_dtype (frame and row strides of the
+ * input in elements; out is contiguous with in's type).  Out of place.
+ * width in [1, 11]. */
+int tcb_dezinger(void *out, const void *in, int in_dtype, size_t nframes, size_t nz, size_t n,
+                 size_t in_fstride, size_t in_zstride, int width, double threshold,
+                 void *stream);
+
 /* ------------------------------------------------------------------------
  * Fourier-wavelet ring removal.  Replaces remove_stripe_fw with DWTForward /
  * DWTInverse / afb1d / sfb1d (src/tomocupy/processing/remove_stripe.py:51-293).

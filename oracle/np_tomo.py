@@ -47,6 +47,17 @@ def darkflat_linear(data, dark, flat, bright_ratio=1.0):
     return ((data.astype(np.float32) - dark0) / f).astype(np.float32)
 
 
+def dezinger(data, width, threshold):
+    """ProcFunctions.remove_outliers (proc_functions.py:96-107): median over
+    [width, 1, width] (scipy.ndimage.median_filter, mode 'reflect', the same
+    rank filter as cupyx's), pixels more than threshold above it replaced.
+    Returns a new array of data's type."""
+    import scipy.ndimage as ndi
+    data = np.array(data)
+    f = ndi.median_filter(data, [width, 1, width])
+    return np.where(np.logical_and(data > f, (data - f) > threshold), f, data)
+
+
 def minus_log(x):
     """where(x<=0 -> 1), -log, nan_to_num(nan=6, posinf=0, neginf=0)."""
     x = np.where(x <= 0, np.float32(1.0), x).astype(np.float32)

@@ -10,7 +10,8 @@
           * paganin_filter / farago_filter (retrieve_phase.py:57-145)
         -> filter_spectra.npz, sizes_cases.json, ..., phase_retrieval.npz
           * remove_stripe_ti (remove_stripe.py:296-307) -> ti_stripe.npz
-        (--phase / --ti: only those two)
+          * ProcFunctions.remove_outliers (proc_functions.py:96-107) -> dezinger.npz
+        (--phase / --ti / --dezinger: only those)
 
     python tests/golden/make_golden.py --gpu --out DIR
         Runs the reference's CUDA operators (oracle/_ref, built from the
@@ -200,6 +201,7 @@ def gen_cpu(ref: Path):
     print("wrote filter_spectra.npz, sizes_cases.json, lprec_grids.npz and fw_stripe.npz")
     gen_phase(ref)
     gen_ti(ref)
+    gen_dezinger(ref)
 
 
 # Phase retrieval (retrieve_phase.py:57-145): (method, nproj, dy, dz,
@@ -259,6 +261,60 @@ def gen_ti(ref: Path):
                                      dtype=np.float32)
     np.savez_compressed(HERE / "ti_stripe.npz", **out)
     print("wrote ti_stripe.npz")
+
+
+# Outlier removal, ProcFunctions.remove_outliers (proc_functions.py:96-107):
+# (dtype, nframes, nz, n, width, threshold, seed).  Widths 4 (an even window,
+# upper median) and 5 on 3 frames (reflections beyond the first) included.
+DEZINGER_CASES = [
+    ("uint16", 20, 3, 40, 3, 500, 1),
+    ("uint16", 12, 2, 33, 4, 300, 2),
+    ("uint16", 10, 2, 64, 5, 1000, 3),
+    ("uint16", 3, 2, 16, 5, 100, 4),
+    ("float32", 15, 2, 30, 3, 0.05, 5),
+]
+
+
+def dezinger_input(dtype, nframes, nz, n, seed):
+    """Seeded frames with sparse positive spikes (zingers)."""
+    rng = np.random.default_rng(seed)
+    if dtype == "uint16":
+        x = rng.normal(10000, 300, (nframes, nz, n))
+        x += (rng.random(x.shape) < 0.02) * rng.uniform(200, 20000, x.shape)
+        return np.clip(x, 0, 65535).astype(np.uint16)
+    x = rng.normal(0.7, 0.01, (nframes, nz, n))
+    x += (rng.random(x.shape) < 0.02) * rng.uniform(0.01, 0.5, x.shape)
+    return x.astype(np.float32)
+
+
+def gen_dezinger(ref: Path):
+    """Runs ProcFunctions.remove_outliers from the reference's own source with
+    NumPy for CuPy and scipy.ndimage for cupyx.scipy.ndimage -> dezinger.npz."""
+    import scipy.ndimage as ndi
+    gv = sys.modules["tomocupy.global_vars"] if "cupy" in sys.modules else _install_stubs()
+    sys.modules["cupy.fft"] = np.fft
+    for name in ("cupyx", "cupyx.scipy"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    nd = types.ModuleType("cupyx.scipy.ndimage")
+    nd.median_filter = ndi.median_filter
+    sys.modules["cupyx.scipy.ndimage"] = nd
+    sys.modules["cupyx.scipy"].ndimage = nd
+    proc = types.ModuleType("tomocupy.processing")
+    proc.__path__ = []
+    proc.retrieve_phase = types.ModuleType("tomocupy.processing.retrieve_phase")
+    proc.remove_stripe = types.ModuleType("tomocupy.processing.remove_stripe")
+    sys.modules["tomocupy.processing"] = proc
+    pf = _load(ref / "src/tomocupy/processing/proc_functions.py", "ref_proc_functions")
+    gv = sys.modules["tomocupy.global_vars"]
+    obj = pf.ProcFunctions.__new__(pf.ProcFunctions)
+    out = {}
+    for i, (dt, nf, nz, n, w, thr, seed) in enumerate(DEZINGER_CASES):
+        data = dezinger_input(dt, nf, nz, n, seed)
+        gv.args.dezinger, gv.args.dezinger_threshold = w, thr
+        out[f"in_{i}"] = data
+        out[f"out_{i}"] = np.asarray(obj.remove_outliers(data.copy()))
+    np.savez_compressed(HERE / "dezinger.npz", **out)
+    print("wrote dezinger.npz")
 
 
 def phase_input(nproj, dy, dz, seed):
@@ -361,6 +417,7 @@ if __name__ == "__main__":
     ap.add_argument("--gpu", action="store_true")
     ap.add_argument("--phase", action="store_true", help="only phase_retrieval.npz")
     ap.add_argument("--ti", action="store_true", help="only ti_stripe.npz")
+    ap.add_argument("--dezinger", action="store_true", help="only dezinger.npz")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
@@ -371,5 +428,7 @@ if __name__ == "__main__":
             gen_phase(Path(a.ref))
         if a.ti:
             gen_ti(Path(a.ref))
+        if a.dezinger:
+            gen_dezinger(Path(a.ref))
     if a.gpu:
         gen_gpu(Path(a.out))

@@ -41,6 +41,7 @@ import numpy as np
 import torch
 
 from . import _lib, cfunc_filter, cfunc_fourierrec, cfunc_linerec
+from .processing.proc_functions import dezinger as _dezinger
 from .processing.proc_functions import in_dtype_code, prep_rows, prep_rows_split16
 from .reconstruction.backproj_functions import phase_weights, rfftfreq32
 from .reconstruction import fftfilter as _fff
@@ -50,7 +51,7 @@ from .reconstruction.fbp_filter import calc_filter
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
                  algorithm="fourierrec", minus_log=True, device="cuda", stripe=None,
-                 precision="float32", out_dtype="float32", mixed_filter="fft"):
+                 precision="float32", out_dtype="float32", mixed_filter="fft", dezinger=None):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if precision not in ("float32", "mixed"):
@@ -72,6 +73,11 @@ class SinoPipeline:
         self.center = float(center) + (0.5 if algorithm == "lprec" else 0.0)
         self.algorithm = algorithm
         self.minus_log = minus_log
+        # outlier removal of the frames of each chunk (proc_sino's
+        # remove_outliers): (width, threshold) or None; frames go through a
+        # chunk-sized scratch stack
+        self.dezinger = dezinger
+        self._zbuf = None
         self.ne = 4 * self.n
         self.pad = self.ne // 2 - self.n // 2
         self.theta = torch.as_tensor(np.asarray(theta, dtype=np.float32), device=self.device)
@@ -161,6 +167,13 @@ class SinoPipeline:
         """Fill the padded filter rows from a [nproj, nz, n] frame (or float) stack view."""
         nz = data.shape[1]
         assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.n
+        if self.dezinger is not None:
+            if self._zbuf is None or self._zbuf.dtype != data.dtype:
+                self._zbuf = torch.empty((self.nproj, self.ncz, self.n), dtype=data.dtype,
+                                         device=self.device)
+            # a contiguous [nproj, nz, n] view of the scratch (partial chunks too)
+            zb = self._zbuf.view(-1)[:self.nproj * nz * self.n].view(self.nproj, nz, self.n)
+            data = _dezinger(data, *self.dezinger, out=zb, stream=stream)
         d0 = dark0[z_lo:z_lo + nz] if dark0 is not None else None
         f0 = flat0[z_lo:z_lo + nz] if flat0 is not None else None
         if self.fw is not None:

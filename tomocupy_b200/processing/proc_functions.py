@@ -3,10 +3,12 @@
 ``ProcFunctions`` mirrors the reference class
 (src/tomocupy/processing/proc_functions.py:47-198) for the hot-path steps:
 ``darkflat_correction`` and ``minus_log`` run as native kernels with the
-reference's float32 operation order (bit-identical results).  The other
-steps of that file (dezinger, phase retrieval, rotation, beam hardening,
-double-FOV padding) are outside this package's scope and raise
-``NotImplementedError`` when enabled, instead of silently doing nothing.
+reference's float32 operation order (bit-identical results), and so do
+``remove_outliers`` (dezinger: a [w, 1, w] median, bit-identical on integer
+frames) and the phase-retrieval step of ``proc_proj``.  The other steps of
+that file (rotation, beam hardening, double-FOV padding) are outside this
+package's scope and raise ``NotImplementedError`` when enabled, instead of
+silently doing nothing.
 """
 from __future__ import annotations
 
@@ -23,6 +25,30 @@ def in_dtype_code(t: torch.Tensor) -> int:
         return _DT[t.dtype]
     except KeyError:
         raise TypeError(f"unsupported frame dtype {t.dtype}; expected uint16, uint8 or float32")
+
+
+def dezinger(frames: torch.Tensor, width: int, threshold: float, out=None,
+             stream=None) -> torch.Tensor:
+    """remove_outliers of frames [k, nz, n] (proc_functions.py:96-107) into a new
+    contiguous tensor (or ``out``): median over width frames x width columns of a
+    row, mode 'reflect', replacing pixels more than ``threshold`` above it.  The
+    input may be a view whose rows are contiguous."""
+    k, nz, n = frames.shape
+    if frames.stride(2) != 1:
+        raise ValueError("dezinger: rows must be contiguous")
+    if out is None:
+        out = torch.empty((k, nz, n), dtype=frames.dtype, device=frames.device)
+    assert out.is_contiguous() and out.shape == frames.shape and out.dtype == frames.dtype
+    _lib.call("tcb_dezinger", _lib.ptr(out), _lib.ptr(frames), in_dtype_code(frames), k, nz, n,
+              frames.stride(0), frames.stride(1), int(width), float(threshold),
+              _lib.stream_ptr(stream))
+    return out
+
+
+def dezinger_args():
+    """(width, threshold) when args.dezinger enables outlier removal, else None."""
+    w = int(args.dezinger)
+    return (w, float(args.dezinger_threshold)) if w > 0 else None
 
 
 def darkflat_stats(dark: torch.Tensor, flat: torch.Tensor, bright_ratio: float = 1.0,
@@ -137,13 +163,17 @@ class ProcFunctions:
         return data
 
     def remove_outliers(self, data):
-        if int(args.dezinger) > 0:
-            raise NotImplementedError("dezinger is not part of tomocupy_b200")
+        """In place, like the reference's data[:] = remove_outliers(data)."""
+        dz = dezinger_args()
+        if dz is not None:
+            data.copy_(dezinger(data, *dz))
         return data
 
     def proc_sino(self, data, dark, flat, res=None):
         """Processing of a sinogram chunk: dark/flat correction and ring removal."""
         data = self.remove_outliers(data)
+        dark = self.remove_outliers(dark)
+        flat = self.remove_outliers(flat)
         out = self.darkflat_correction(data, dark, flat)
         if args.remove_stripe_method == "fw":
             from . import remove_stripe

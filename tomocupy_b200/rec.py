@@ -19,7 +19,7 @@ import torch
 
 from .global_vars import args, params
 from .pipeline import SinoPipeline, copy2d_rows
-from .processing.proc_functions import PHASE_METHODS, darkflat_stats
+from .processing.proc_functions import PHASE_METHODS, darkflat_stats, dezinger, dezinger_args
 
 
 def _supported():
@@ -73,7 +73,8 @@ class GPURec:
                                       minus_log=args.minus_log == "True", device=self.device,
                                       stripe=stripe, precision=self.precision,
                                       out_dtype=args.out_dtype,
-                                      mixed_filter=args.mixed_filter)
+                                      mixed_filter=args.mixed_filter,
+                                      dezinger=dezinger_args())
         return self._pipe
 
     # ------------------------------------------------------------------ helpers
@@ -81,6 +82,10 @@ class GPURec:
         flat_linear = args.flat_linear == "True"
         if flat_linear:
             raise NotImplementedError("flat_linear in the fused driver")
+        dz = dezinger_args()
+        if dz is not None:   # proc_sino cleans darks and flats too (proc_functions.py:146-148)
+            dark = dezinger(dark, *dz, stream=stream)
+            flat = dezinger(flat, *dz, stream=stream)
         return darkflat_stats(dark, flat, args.bright_ratio, False, stream)
 
     # ------------------------------------------------------------------ full
@@ -193,6 +198,8 @@ class GPURec:
         for id_slice in params.id_slices:
             z = int(id_slice)
             row = data[:, z:z + 1].to(dev)
+            if dezinger_args() is not None:
+                row = dezinger(row, *dezinger_args())
             d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
             sw.load(row, d0, f0)
             if sw.graph is None:

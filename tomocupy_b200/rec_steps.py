@@ -27,7 +27,8 @@ import torch
 
 from .global_vars import args, params
 from .pipeline import SinoPipeline
-from .processing.proc_functions import PHASE_METHODS, darkflat_stats, prep_rows, retrieve_phase
+from .processing.proc_functions import (PHASE_METHODS, darkflat_stats, dezinger, dezinger_args,
+                                        prep_rows, retrieve_phase)
 from .reconstruction.backproj_functions import phase_weights, rfftfreq32
 from .reconstruction.fbp_filter import calc_filter
 
@@ -51,6 +52,9 @@ class GPURecSteps:
         data, dark, flat = data.to(dev), dark.to(dev), flat.to(dev)
         if args.pre_processing != "True":
             return data.to(torch.float32)
+        dz = dezinger_args()
+        if dz is not None:   # remove_outliers of data, darks and flats (proc_sino)
+            data, dark, flat = dezinger(data, *dz), dezinger(dark, *dz), dezinger(flat, *dz)
         d0, f0, _ = darkflat_stats(dark, flat, args.bright_ratio)
         nproj, nz, n = data.shape
         out = torch.empty((nproj, nz, n), dtype=torch.float32, device=dev)
