@@ -124,6 +124,17 @@ int tcb_prep_noalloc(float *out, const void *data, const void *dark, const void 
                      size_t out_pstride, size_t out_poff, size_t out_xoff,
                      size_t out_width, unsigned flags, void *stream);
 
+/* Double-field-of-view padding.  Replaces ProcFunctions.pad360
+ * (src/tomocupy/processing/proc_functions.py:109-124), applied by proc_proj
+ * after -log when file_type is 'double_fov' (proc_functions.py:190-193).
+ * weights: the smooth transition v of length w into v (host, float64).
+ * rows: in place on nrows rows whose first ni floats hold the samples (row
+ * stride row_stride >= 2 ni): optional flip, the last w samples times v
+ * (device, float64), zeros in [ni, 2 ni). */
+int tcb_pad360_weights(double *v, size_t w);
+int tcb_pad360_rows(float *rows, size_t nrows, size_t ni, size_t row_stride, int flip,
+                    const double *v, size_t w, void *stream);
+
 /* Outlier (zinger) removal.  Replaces ProcFunctions.remove_outliers
  * (src/tomocupy/processing/proc_functions.py:96-107), which proc_sino applies
  * to the projections, darks and flats of a chunk before dark/flat correction

@@ -58,6 +58,22 @@ def dezinger(data, width, threshold):
     return np.where(np.logical_and(data > f, (data - f) > threshold), f, data)
 
 
+def pad360(data, centeri, ni, center):
+    """ProcFunctions.pad360 (proc_functions.py:109-124) on float32
+    [nproj, nz, ni]: flip when centeri < ni // 2, the last w = max(1,
+    int(2 (ni - center))) columns times the float64 transition
+    v**5 (126 - 420 v + 540 v**2 - 315 v**3 + 70 v**4), v = linspace(1, 0, w,
+    endpoint=False), then zeros up to 2 ni columns.  Returns a new array."""
+    data = np.array(data, dtype=np.float32)
+    if centeri < ni // 2:
+        data[:] = data[:, :, ::-1]
+    w = max(1, int(2 * (ni - center)))
+    v = np.linspace(1, 0, w, endpoint=False)
+    v = v ** 5 * (126 - 420 * v + 540 * v ** 2 - 315 * v ** 3 + 70 * v ** 4)
+    data[:, :, -w:] *= v
+    return np.pad(data, ((0, 0), (0, 0), (0, data.shape[-1])), "constant")
+
+
 def minus_log(x):
     """where(x<=0 -> 1), -log, nan_to_num(nan=6, posinf=0, neginf=0)."""
     x = np.where(x <= 0, np.float32(1.0), x).astype(np.float32)

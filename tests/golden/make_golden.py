@@ -11,7 +11,8 @@
         -> filter_spectra.npz, sizes_cases.json, ..., phase_retrieval.npz
           * remove_stripe_ti (remove_stripe.py:296-307) -> ti_stripe.npz
           * ProcFunctions.remove_outliers (proc_functions.py:96-107) -> dezinger.npz
-        (--phase / --ti / --dezinger: only those)
+          * ProcFunctions.pad360 (proc_functions.py:109-124) -> pad360.npz
+        (--phase / --ti / --dezinger / --pad360: only those)
 
     python tests/golden/make_golden.py --gpu --out DIR
         Runs the reference's CUDA operators (oracle/_ref, built from the
@@ -202,6 +203,7 @@ def gen_cpu(ref: Path):
     gen_phase(ref)
     gen_ti(ref)
     gen_dezinger(ref)
+    gen_pad360(ref)
 
 
 # Phase retrieval (retrieve_phase.py:57-145): (method, nproj, dy, dz,
@@ -275,6 +277,55 @@ DEZINGER_CASES = [
 ]
 
 
+# Double-FOV padding, ProcFunctions.pad360 (proc_functions.py:109-124):
+# (nproj, nz, ni, centeri, seed); center as Reader.init_sizes sets it for a
+# double_fov scan (reader.py:143-149).
+PAD360_CASES = [
+    (5, 2, 64, 58.0, 1),     # axis on the right: no flip, w = 12
+    (4, 3, 50, 6.5, 2),      # axis on the left: flip, w = 13
+    (3, 1, 33, 30.25, 3),    # odd width, fractional centre
+]
+
+
+def gen_pad360(ref: Path):
+    """Runs ProcFunctions.pad360 from the reference's own source with NumPy for
+    CuPy -> pad360.npz."""
+    if "cupy" not in sys.modules:
+        _install_stubs()
+    _proc_stubs()
+    pf = _load(ref / "src/tomocupy/processing/proc_functions.py", "ref_proc_functions_360")
+    gv = sys.modules["tomocupy.global_vars"]
+    obj = pf.ProcFunctions.__new__(pf.ProcFunctions)
+    out = {}
+    for i, (nproj, nz, ni, centeri, seed) in enumerate(PAD360_CASES):
+        rng = np.random.default_rng(seed)
+        data = rng.random((nproj, nz, ni)).astype(np.float32)
+        center = ni - centeri if centeri < ni // 2 else centeri
+        gv.params.centeri, gv.params.ni, gv.params.center = centeri, ni, center
+        pf.params = gv.params
+        out[f"in_{i}"] = data
+        out[f"out_{i}"] = np.asarray(obj.pad360(data.copy()), dtype=np.float32)
+    np.savez_compressed(HERE / "pad360.npz", **out)
+    print("wrote pad360.npz")
+
+
+def _proc_stubs():
+    """Modules that src/tomocupy/processing/proc_functions.py imports."""
+    import scipy.ndimage as ndi
+    sys.modules["cupy.fft"] = np.fft
+    for name in ("cupyx", "cupyx.scipy"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    nd = types.ModuleType("cupyx.scipy.ndimage")
+    nd.median_filter = ndi.median_filter
+    sys.modules["cupyx.scipy.ndimage"] = nd
+    sys.modules["cupyx.scipy"].ndimage = nd
+    proc = types.ModuleType("tomocupy.processing")
+    proc.__path__ = []
+    proc.retrieve_phase = types.ModuleType("tomocupy.processing.retrieve_phase")
+    proc.remove_stripe = types.ModuleType("tomocupy.processing.remove_stripe")
+    sys.modules["tomocupy.processing"] = proc
+
+
 def dezinger_input(dtype, nframes, nz, n, seed):
     """Seeded frames with sparse positive spikes (zingers)."""
     rng = np.random.default_rng(seed)
@@ -290,20 +341,9 @@ def dezinger_input(dtype, nframes, nz, n, seed):
 def gen_dezinger(ref: Path):
     """Runs ProcFunctions.remove_outliers from the reference's own source with
     NumPy for CuPy and scipy.ndimage for cupyx.scipy.ndimage -> dezinger.npz."""
-    import scipy.ndimage as ndi
-    gv = sys.modules["tomocupy.global_vars"] if "cupy" in sys.modules else _install_stubs()
-    sys.modules["cupy.fft"] = np.fft
-    for name in ("cupyx", "cupyx.scipy"):
-        sys.modules.setdefault(name, types.ModuleType(name))
-    nd = types.ModuleType("cupyx.scipy.ndimage")
-    nd.median_filter = ndi.median_filter
-    sys.modules["cupyx.scipy.ndimage"] = nd
-    sys.modules["cupyx.scipy"].ndimage = nd
-    proc = types.ModuleType("tomocupy.processing")
-    proc.__path__ = []
-    proc.retrieve_phase = types.ModuleType("tomocupy.processing.retrieve_phase")
-    proc.remove_stripe = types.ModuleType("tomocupy.processing.remove_stripe")
-    sys.modules["tomocupy.processing"] = proc
+    if "cupy" not in sys.modules:
+        _install_stubs()
+    _proc_stubs()
     pf = _load(ref / "src/tomocupy/processing/proc_functions.py", "ref_proc_functions")
     gv = sys.modules["tomocupy.global_vars"]
     obj = pf.ProcFunctions.__new__(pf.ProcFunctions)
@@ -418,6 +458,7 @@ if __name__ == "__main__":
     ap.add_argument("--phase", action="store_true", help="only phase_retrieval.npz")
     ap.add_argument("--ti", action="store_true", help="only ti_stripe.npz")
     ap.add_argument("--dezinger", action="store_true", help="only dezinger.npz")
+    ap.add_argument("--pad360", action="store_true", help="only pad360.npz")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
@@ -430,5 +471,7 @@ if __name__ == "__main__":
             gen_ti(Path(a.ref))
         if a.dezinger:
             gen_dezinger(Path(a.ref))
+        if a.pad360:
+            gen_pad360(Path(a.ref))
     if a.gpu:
         gen_gpu(Path(a.out))

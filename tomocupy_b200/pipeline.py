@@ -51,7 +51,8 @@ from .reconstruction.fbp_filter import calc_filter
 class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
                  algorithm="fourierrec", minus_log=True, device="cuda", stripe=None,
-                 precision="float32", out_dtype="float32", mixed_filter="fft", dezinger=None):
+                 precision="float32", out_dtype="float32", mixed_filter="fft", dezinger=None,
+                 ni=None, pad360=None):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if precision not in ("float32", "mixed"):
@@ -78,6 +79,20 @@ class SinoPipeline:
         # chunk-sized scratch stack
         self.dezinger = dezinger
         self._zbuf = None
+        # double field of view (proc_proj's pad360 after -log): frames of ni
+        # columns reconstructed at n = 2 ni; pad360 = (flip, w)
+        self.ni = int(ni) if ni is not None else self.n
+        self.pad360 = None
+        if pad360 is not None:
+            import ctypes as C
+            flip, w = bool(pad360[0]), int(pad360[1])
+            if self.ni * 2 != self.n or not 1 <= w <= self.ni:
+                raise ValueError(f"pad360: n={self.n} must be 2*ni={2 * self.ni}, 1 <= w <= ni")
+            v = np.empty(w, dtype=np.float64)
+            _lib.call("tcb_pad360_weights", v.ctypes.data_as(C.c_void_p), w)
+            self.pad360 = (flip, w, torch.as_tensor(v, device=self.device))
+        elif self.ni != self.n:
+            raise ValueError("input width differs from n without double-FOV padding")
         self.ne = 4 * self.n
         self.pad = self.ne // 2 - self.n // 2
         self.theta = torch.as_tensor(np.asarray(theta, dtype=np.float32), device=self.device)
@@ -166,7 +181,10 @@ class SinoPipeline:
     def load_rows(self, data, dark0=None, flat0=None, z_lo=0, stream=None):
         """Fill the padded filter rows from a [nproj, nz, n] frame (or float) stack view."""
         nz = data.shape[1]
-        assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.n
+        assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.ni
+        if self.pad360 is not None and (self.fw is not None or not self.fused):
+            raise NotImplementedError("double-FOV padding: fused fp32 filter without ring "
+                                      "removal only")
         if self.dezinger is not None:
             if self._zbuf is None or self._zbuf.dtype != data.dtype:
                 self._zbuf = torch.empty((self.nproj, self.ncz, self.n), dtype=data.dtype,
@@ -208,6 +226,10 @@ class SinoPipeline:
             prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                       minus_log=self.minus_log, out_zstride=self.nproj * self.n,
                       out_pstride=self.n, stream=stream)
+            if self.pad360 is not None:
+                flip, w, v = self.pad360
+                _lib.call("tcb_pad360_rows", self.rows.data_ptr(), nz * self.nproj, self.ni,
+                          self.n, int(flip), v.data_ptr(), w, _lib.stream_ptr(stream))
             return
         prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                   minus_log=self.minus_log, out_zstride=self.nproj * self.ne,

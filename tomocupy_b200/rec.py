@@ -26,11 +26,19 @@ def _supported():
     if args.remove_stripe_method not in ("none", "fw", "ti"):
         raise NotImplementedError(
             f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
-    if args.file_type != "standard" or args.binning != 0:
-        raise NotImplementedError("double_fov / binning are not part of tomocupy_b200")
+    if args.file_type not in ("standard", "double_fov") or args.binning != 0:
+        raise NotImplementedError("binning is not part of tomocupy_b200")
     if args.dtype not in ("float32", "mixed"):
         raise NotImplementedError(
             "the fused driver runs the float32 drop-in path or the 'mixed' tensor-core path")
+
+
+def _pad360_args():
+    """(flip, w) of pad360 (proc_functions.py:109-124) for a double-FOV scan, else None."""
+    if args.file_type != "double_fov":
+        return None
+    flip = params.centeri < params.ni // 2
+    return flip, max(1, int(2 * (params.ni - params.center)))
 
 
 def _no_phase(where):
@@ -74,7 +82,8 @@ class GPURec:
                                       stripe=stripe, precision=self.precision,
                                       out_dtype=args.out_dtype,
                                       mixed_filter=args.mixed_filter,
-                                      dezinger=dezinger_args())
+                                      dezinger=dezinger_args(), ni=params.ni,
+                                      pad360=_pad360_args())
         return self._pipe
 
     # ------------------------------------------------------------------ helpers
@@ -131,7 +140,8 @@ class GPURec:
             dark0, flat0, _ = self._stats(dark_d, flat_d, s2)
         host_in = data.device.type == "cpu"
         host_out = rec_out.device.type == "cpu"
-        dbuf = [torch.empty((nproj, ncz, n), dtype=data.dtype, device=dev) for _ in range(2)]
+        dbuf = [torch.empty((nproj, ncz, data.shape[2]), dtype=data.dtype, device=dev)
+                for _ in range(2)]
         odt = self.pipe.out_dtype
         if rec_out.dtype != odt:
             raise ValueError(f"writer dtype {rec_out.dtype} != output dtype {odt} (args.out_dtype)")
@@ -182,6 +192,8 @@ class GPURec:
         The sweep over all centres is one CUDA graph (TryCenterSweep), recorded
         once and replayed for each requested slice.
         """
+        if args.file_type == "double_fov":
+            raise NotImplementedError("try-centre sweeps of double-FOV scans")
         _no_phase("GPURec.recon_try")
         from .trycenter import TryCenterSweep
         if args.reconstruction_algorithm != "fourierrec" or args.remove_stripe_method != "none":
