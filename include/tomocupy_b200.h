@@ -124,6 +124,15 @@ int tcb_prep_noalloc(float *out, const void *data, const void *dark, const void 
                      size_t out_pstride, size_t out_poff, size_t out_xoff,
                      size_t out_width, unsigned flags, void *stream);
 
+/* Binning.  Replaces utils.downsample (src/tomocupy/utils.py:157-167) as the
+ * reader applies it to chunks of projections, darks and flats
+ * (src/tomocupy/dataio/reader.py:335-356): out float32 [nframes, nz, n] =
+ * sums of 2^binning x 2^binning blocks of in (frames of nz * 2^binning rows of
+ * n * 2^binning samples, frame and row strides in elements), columns then
+ * rows as pairwise float32 trees, the reference's order.  binning in [1, 4]. */
+int tcb_downsample(float *out, const void *in, int in_dtype, size_t nframes, size_t nz, size_t n,
+                   size_t in_fstride, size_t in_zstride, int binning, void *stream);
+
 /* Double-field-of-view padding.  Replaces ProcFunctions.pad360
  * (src/tomocupy/processing/proc_functions.py:109-124), applied by proc_proj
  * after -log when file_type is 'double_fov' (proc_functions.py:190-193).

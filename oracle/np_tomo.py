@@ -58,6 +58,17 @@ def dezinger(data, width, threshold):
     return np.where(np.logical_and(data > f, (data - f) > threshold), f, data)
 
 
+def downsample(data, binning):
+    """utils.downsample (utils.py:157-167) on float32 frames: b times the sum of
+    even and odd columns, then b times the sum of even and odd rows."""
+    data = np.asarray(data, dtype=np.float32)
+    for _ in range(binning):
+        data = data[:, :, ::2] + data[:, :, 1::2]
+    for _ in range(binning):
+        data = data[:, ::2] + data[:, 1::2]
+    return data
+
+
 def pad360(data, centeri, ni, center):
     """ProcFunctions.pad360 (proc_functions.py:109-124) on float32
     [nproj, nz, ni]: flip when centeri < ni // 2, the last w = max(1,

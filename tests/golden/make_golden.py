@@ -12,7 +12,8 @@
           * remove_stripe_ti (remove_stripe.py:296-307) -> ti_stripe.npz
           * ProcFunctions.remove_outliers (proc_functions.py:96-107) -> dezinger.npz
           * ProcFunctions.pad360 (proc_functions.py:109-124) -> pad360.npz
-        (--phase / --ti / --dezinger / --pad360: only those)
+          * utils.downsample (utils.py:157-167) -> downsample.npz
+        (--phase / --ti / --dezinger / --pad360 / --downsample: only those)
 
     python tests/golden/make_golden.py --gpu --out DIR
         Runs the reference's CUDA operators (oracle/_ref, built from the
@@ -204,6 +205,7 @@ def gen_cpu(ref: Path):
     gen_ti(ref)
     gen_dezinger(ref)
     gen_pad360(ref)
+    gen_downsample(ref)
 
 
 # Phase retrieval (retrieve_phase.py:57-145): (method, nproj, dy, dz,
@@ -275,6 +277,45 @@ DEZINGER_CASES = [
     ("uint16", 3, 2, 16, 5, 100, 4),
     ("float32", 15, 2, 30, 3, 0.05, 5),
 ]
+
+
+# Binning, utils.downsample (utils.py:157-167) on float32 frames (the reader
+# converts to float32 before binning): (nframes, rows, columns, binning,
+# integer-valued, seed).
+DOWNSAMPLE_CASES = [
+    (3, 8, 16, 1, True, 1),
+    (2, 8, 16, 2, False, 2),
+    (2, 16, 24, 3, False, 3),
+    (4, 6, 10, 1, False, 4),
+]
+
+
+def gen_downsample(ref: Path):
+    """Runs utils.downsample from the reference's own source (NumPy for CuPy,
+    a numexpr stand-in that evaluates 'x + y' with NumPy) -> downsample.npz."""
+    import inspect
+    if "cupy" not in sys.modules:
+        _install_stubs()
+    ne = types.ModuleType("numexpr")
+
+    def evaluate(expr):
+        f = inspect.currentframe().f_back
+        return eval(expr, {}, dict(f.f_locals))
+    ne.evaluate = evaluate
+    sys.modules["numexpr"] = ne
+    sys.modules.setdefault("tifffile", types.ModuleType("tifffile"))
+    ut = _load(ref / "src/tomocupy/utils.py", "ref_utils")
+    out = {}
+    for i, (k, zr, nr, b, integer, seed) in enumerate(DOWNSAMPLE_CASES):
+        rng = np.random.default_rng(seed)
+        if integer:
+            x = rng.integers(0, 65536, (k, zr, nr)).astype(np.float32)
+        else:
+            x = (rng.random((k, zr, nr)) * 1000).astype(np.float32)
+        out[f"in_{i}"] = x
+        out[f"out_{i}"] = np.asarray(ut.downsample(x, b), dtype=np.float32)
+    np.savez_compressed(HERE / "downsample.npz", **out)
+    print("wrote downsample.npz")
 
 
 # Double-FOV padding, ProcFunctions.pad360 (proc_functions.py:109-124):
@@ -459,6 +500,7 @@ if __name__ == "__main__":
     ap.add_argument("--ti", action="store_true", help="only ti_stripe.npz")
     ap.add_argument("--dezinger", action="store_true", help="only dezinger.npz")
     ap.add_argument("--pad360", action="store_true", help="only pad360.npz")
+    ap.add_argument("--downsample", action="store_true", help="only downsample.npz")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
@@ -473,5 +515,7 @@ if __name__ == "__main__":
             gen_dezinger(Path(a.ref))
         if a.pad360:
             gen_pad360(Path(a.ref))
+        if a.downsample:
+            gen_downsample(Path(a.ref))
     if a.gpu:
         gen_gpu(Path(a.out))

@@ -84,6 +84,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_fftfilter_apply": [vp, vp, sz, sz, sz, sz, vp, i32, sz, vp],
     "tcb_fftfilter_destroy": [vp],
     "tcb_prep_rows_split16": [vp, vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, i32, sz, sz, u32, vp],
+    "tcb_downsample": [vp, vp, i32, sz, sz, sz, sz, sz, i32, vp],
     "tcb_pad360_weights": [vp, sz],
     "tcb_pad360_rows": [vp, sz, sz, sz, i32, vp, sz, vp],
     "tcb_dezinger": [vp, vp, i32, sz, sz, sz, sz, sz, i32, f64, vp],

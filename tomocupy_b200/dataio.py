@@ -22,6 +22,24 @@ def _as_tensor(x):
     return torch.from_numpy(np.ascontiguousarray(x))
 
 
+def _binned(frames, b, slab=64):
+    """float32 binning of [k, nz * 2^b, n * 2^b] frames on the GPU."""
+    from .processing.proc_functions import downsample
+    dev = frames.device if frames.is_cuda else torch.device("cuda")
+    k, zr, nr = frames.shape
+    nz, n = zr >> b, nr >> b
+    out = torch.empty((k, nz, n), dtype=torch.float32, device=dev)
+    for z0 in range(0, nz, slab):
+        z1 = min(nz, z0 + slab)
+        part = frames[:, z0 << b:z1 << b]
+        if not part.is_cuda:
+            part = part.to(dev)
+        elif part.stride(2) != 1:
+            part = part.contiguous()
+        out[:, z0:z1] = downsample(part, b)
+    return out
+
+
 class ArrayReader:
     """Projections [nproj, nz, ni], darks [ndark, nz, ni], flats [nflat, nz, ni]."""
 
@@ -42,17 +60,24 @@ class ArrayReader:
         _sizes.setup(self.sizes, self.theta_all, args, params)
 
     def frames(self):
-        """(data, dark, flat) restricted to the selected projections and columns."""
+        """(data, dark, flat) restricted to the selected projections and columns;
+        with binning b > 0 the float32 2^b x 2^b block sums of those frames, as
+        the reference's reader produces them (dataio/reader.py:335-356), on
+        the GPU (host frames are binned slab by slab there)."""
         ids = params.ids_proj
         if isinstance(ids, (list, tuple)) and len(ids) == 2:
             sel = slice(ids[0], ids[1])
         else:
             sel = torch.as_tensor(np.asarray(ids))
+        b = int(args.binning)
         c0 = args.start_column if args.dtype != "float16" else params.st_n
-        c1 = c0 + params.ni
-        r0, r1 = args.start_row, args.start_row + params.nz
-        return (self.data[sel, r0:r1, c0:c1], self.dark[:, r0:r1, c0:c1],
-                self.flat[:, r0:r1, c0:c1])
+        c1 = c0 + params.ni * 2 ** b
+        r0, r1 = args.start_row, args.start_row + params.nz * 2 ** b
+        raw = (self.data[sel, r0:r1, c0:c1], self.dark[:, r0:r1, c0:c1],
+               self.flat[:, r0:r1, c0:c1])
+        if b == 0:
+            return raw
+        return tuple(_binned(t, b) for t in raw)
 
 
 class ArrayWriter:

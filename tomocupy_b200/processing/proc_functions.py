@@ -45,6 +45,23 @@ def dezinger(frames: torch.Tensor, width: int, threshold: float, out=None,
     return out
 
 
+def downsample(frames: torch.Tensor, binning: int, out=None, stream=None) -> torch.Tensor:
+    """utils.downsample (src/tomocupy/utils.py:157-167) of float32-converted
+    frames [k, nz * 2^b, n * 2^b] (device; any dtype of uint8 / uint16 /
+    float32, rows contiguous) -> float32 [k, nz, n] block sums, columns then
+    rows as pairwise trees."""
+    k, zr, nr = frames.shape
+    b = int(binning)
+    nz, n = zr >> b, nr >> b
+    if frames.stride(2) != 1:
+        raise ValueError("downsample: rows must be contiguous")
+    if out is None:
+        out = torch.empty((k, nz, n), dtype=torch.float32, device=frames.device)
+    _lib.call("tcb_downsample", _lib.ptr(out), _lib.ptr(frames), in_dtype_code(frames), k, nz, n,
+              frames.stride(0), frames.stride(1), b, _lib.stream_ptr(stream))
+    return out
+
+
 def dezinger_args():
     """(width, threshold) when args.dezinger enables outlier removal, else None."""
     w = int(args.dezinger)

@@ -26,8 +26,10 @@ def _supported():
     if args.remove_stripe_method not in ("none", "fw", "ti"):
         raise NotImplementedError(
             f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
-    if args.file_type not in ("standard", "double_fov") or args.binning != 0:
-        raise NotImplementedError("binning is not part of tomocupy_b200")
+    if args.file_type not in ("standard", "double_fov"):
+        raise NotImplementedError(f"file_type={args.file_type!r}")
+    if not 0 <= int(args.binning) <= 4:
+        raise NotImplementedError("binning above 4")
     if args.dtype not in ("float32", "mixed"):
         raise NotImplementedError(
             "the fused driver runs the float32 drop-in path or the 'mixed' tensor-core path")

@@ -38,8 +38,8 @@ class GPURecSteps:
         self.device = torch.device(device)
         self.cl_reader = cl_reader
         self.cl_writer = cl_writer
-        if args.file_type != "standard" or args.binning != 0:
-            raise NotImplementedError("double_fov / binning are not part of tomocupy_b200")
+        if args.file_type != "standard":
+            raise NotImplementedError("double_fov scans run in GPURec.recon_all")
         if args.dtype != "float32":
             raise NotImplementedError("the step driver runs the float32 path")
 
