@@ -117,35 +117,60 @@ __device__ __forceinline__ int pad_src(int i, int p, int d) {
   return min(max(i - p, 0), d - 1);
 }
 
+// PR_ROWS rows per thread: the loads of one thread are independent, so
+// each thread keeps PR_ROWS requests in flight (one row per thread left
+// the kernel latency-bound at ~1.8 TB/s); every warp access stays a run of
+// 32 consecutive floats.
+constexpr int PR_ROWS = 4;
+
 __global__ void phase_pad(float *__restrict__ out, const float *__restrict__ in, int dy, int dz,
                           int py, int pz, int Ny, int Nz) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y;
+  const int i0 = blockIdx.y * PR_ROWS;
   const size_t b = blockIdx.z;
   if (j >= Nz) return;
-  const int si = pad_src(i, py, dy), sj = pad_src(j, pz, dz);
-  out[(b * Ny + i) * Nz + j] = __ldg(in + (b * dy + si) * dz + sj);
+  const int sj = pad_src(j, pz, dz);
+  float v[PR_ROWS];
+#pragma unroll
+  for (int r = 0; r < PR_ROWS; r++)
+    if (i0 + r < Ny) v[r] = __ldg(in + (b * dy + pad_src(i0 + r, py, dy)) * dz + sj);
+#pragma unroll
+  for (int r = 0; r < PR_ROWS; r++)
+    if (i0 + r < Ny) out[(b * Ny + i0 + r) * Nz + j] = v[r];
 }
 
-__global__ void phase_mul(float2 *__restrict__ spec, const float *__restrict__ fe, size_t plane,
-                          size_t total) {
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  const float w = __ldg(fe + t % plane);
-  float2 v = spec[t];
-  v.x *= w;
-  v.y *= w;
-  spec[t] = v;
+// one row of the half spectrum per block row, PR_ROWS projections of the
+// batch per thread (the filter entry is loaded once for all of them)
+__global__ void phase_mul(float2 *__restrict__ spec, const float *__restrict__ fe, int nc,
+                          size_t plane, int nb) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  const size_t e = (size_t)blockIdx.y * nc + k;  // entry within a spectrum
+  const float w = __ldg(fe + e);
+  const int b0 = blockIdx.z * PR_ROWS;
+  float2 v[PR_ROWS];
+#pragma unroll
+  for (int r = 0; r < PR_ROWS; r++)
+    if (b0 + r < nb) v[r] = spec[(size_t)(b0 + r) * plane + e];
+#pragma unroll
+  for (int r = 0; r < PR_ROWS; r++)
+    if (b0 + r < nb) spec[(size_t)(b0 + r) * plane + e] = make_float2(v[r].x * w, v[r].y * w);
 }
 
 // Crop (retrieve_phase.py:143-144); with p = 0 nothing is cropped on that axis.
 __global__ void phase_crop(float *__restrict__ out, const float *__restrict__ in, int dy, int dz,
                            int py, int pz, int Ny, int Nz) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y;
+  const int i0 = blockIdx.y * PR_ROWS;
   const size_t b = blockIdx.z;
   if (j >= dz) return;
-  out[(b * dy + i) * dz + j] = in[(b * Ny + i + py) * Nz + j + pz];
+  float v[PR_ROWS];
+#pragma unroll
+  for (int r = 0; r < PR_ROWS; r++)
+    if (i0 + r < dy) v[r] = in[(b * Ny + i0 + r + py) * Nz + j + pz];
+#pragma unroll
+  for (int r = 0; r < PR_ROWS; r++)
+    if (i0 + r < dy) out[(b * dy + i0 + r) * dz + j] = v[r];
 }
 
 void phase_release(tcb_phase *h) {
@@ -277,7 +302,7 @@ extern "C" int tcb_phase_apply(tcb_phase *h, float *data, size_t nproj, void *st
     float *d = data + p0 * h->dy * h->dz;
     {
       StageTimer t("phase_pad", s);
-      phase_pad<<<dim3(ceil_div(h->Nz, 256), (unsigned)h->Ny, (unsigned)b), 256, 0, s>>>(
+      phase_pad<<<dim3(ceil_div(h->Nz, 256), ceil_div(h->Ny, PR_ROWS), (unsigned)b), 256, 0, s>>>(
           h->real, d, (int)h->dy, (int)h->dz, (int)h->py, (int)h->pz, (int)h->Ny, (int)h->Nz);
       TCB_LAUNCH_CHECK();
       count_launch();
@@ -290,8 +315,8 @@ extern "C" int tcb_phase_apply(tcb_phase *h, float *data, size_t nproj, void *st
     }
     {
       StageTimer t("phase_mul", s);
-      const size_t total = b * plane;
-      phase_mul<<<ceil_div(total, 256), 256, 0, s>>>(h->spec, h->fe, plane, total);
+      phase_mul<<<dim3(ceil_div(Nc, 256), (unsigned)h->Ny, ceil_div(b, PR_ROWS)), 256, 0, s>>>(
+          h->spec, h->fe, (int)Nc, plane, (int)b);
       TCB_LAUNCH_CHECK();
       count_launch();
     }
@@ -301,7 +326,7 @@ extern "C" int tcb_phase_apply(tcb_phase *h, float *data, size_t nproj, void *st
     }
     {
       StageTimer t("phase_crop", s);
-      phase_crop<<<dim3(ceil_div(h->dz, 256), (unsigned)h->dy, (unsigned)b), 256, 0, s>>>(
+      phase_crop<<<dim3(ceil_div(h->dz, 256), ceil_div(h->dy, PR_ROWS), (unsigned)b), 256, 0, s>>>(
           d, h->real, (int)h->dy, (int)h->dz, (int)h->py, (int)h->pz, (int)h->Ny, (int)h->Nz);
       TCB_LAUNCH_CHECK();
       count_launch();
