@@ -374,6 +374,9 @@ int tcb_linerec_backprojection_try(tcb_linerec *h, void *f, const void *g,
 int tcb_linerec_backprojection_try_lamino(tcb_linerec *h, void *f, const void *g,
                                           const float *theta, const float *phi,
                                           int sz, void *stream);
+/* status (no reference counterpart): 1 in *timed_out when a TMA wait of the
+ * float32 backprojection gave up (synchronous). */
+int tcb_linerec_status(tcb_linerec *h, int *timed_out);
 int tcb_linerec_destroy(tcb_linerec *h);
 
 /* ------------------------------------------------------------------------

@@ -111,6 +111,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_linerec_backprojection": [vp, vp, vp, vp, f32, i32, vp],
     "tcb_linerec_backprojection_try": [vp, vp, vp, vp, vp, f32, i32, vp],
     "tcb_linerec_backprojection_try_lamino": [vp, vp, vp, vp, vp, i32, vp],
+    "tcb_linerec_status": [vp, C.POINTER(i32)],
     "tcb_linerec_destroy": [vp],
     "tcb_lprec_create": [C.POINTER(vp), sz, sz, sz, sz, sz, i32],
     "tcb_lprec_setgrids": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, sz, sz],

@@ -42,6 +42,14 @@ class cfunc_linerec:
                   _lib.ptr(g_), _lib.ptr(theta_), _lib.ptr(phi_), int(sz),
                   _lib.stream_ptr(stream_))
 
+    def timed_out(self) -> bool:
+        """True when a TMA wait of the float32 backprojection gave up (synchronises;
+        not in the reference)."""
+        import ctypes as C
+        v = C.c_int(0)
+        _lib.call("tcb_linerec_status", self._live(), C.byref(v))
+        return bool(v.value)
+
     def free(self):
         if getattr(self, "_h", None) is not None:
             _lib.call("tcb_linerec_destroy", self._h)

@@ -12,14 +12,21 @@
 // bit-identical) instead of by every thread for every angle; each thread
 // accumulates in fp32 registers (also in the FLOAT16 variant, whose caller
 // buffers are fp16); reads of the sinogram go through the read-only path.
+#include <cuda.h>
 #include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
+#include <mutex>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 struct tcb_linerec {
   size_t nproj, nz, n, ncproj, ncz;
   int precision;
   bool freed = false;
+  int *err = nullptr;  // set by a TMA wait of backproject_full_tma that gave up
 };
 
 namespace tcb {
@@ -205,6 +212,180 @@ __global__ void __launch_bounds__(BX *BY)
   }
 }
 
+// FULL mode, float32, the same voxels, expressions and values as
+// backproject_full_zs, with the per-angle sinogram boxes staged by TMA:
+// a 3D tensor map over the sinogram (n, nproj, nz) and one box of TUW
+// samples x 1 angle x VR rows per angle, its first sample rounded down to a
+// multiple of 4 (16 bytes, the TMA alignment of the innermost coordinate;
+// TUW = 48 + 4 keeps the window), zero-filled outside the sinogram.  Two
+// stages of TAC angles: one thread issues the next chunk's TMA loads (one
+// mbarrier per stage) while the CTA sums the current chunk, so the staging
+// costs the CTA no load instructions and overlaps the arithmetic.  Every
+// wait is bounded; a wait that gives up sets *err and the CTA stops.
+constexpr int TUW = 52, TAC = 16;  // 16 angles per stage: 41 KB, 5 CTAs per SM
+constexpr int TBOX = 1280;  // bytes per angle slot: TUW * VR * 4 = 1248, 128-byte aligned
+constexpr int TSTAGE = TAC * TBOX;
+constexpr int TSMEM = 2 * TSTAGE + 128;
+static_assert(TUW * VR * 4 <= TBOX && TBOX % 128 == 0 && (TUW * 4) % 16 == 0, "TMA box");
+
+__global__ void __launch_bounds__(BX *BY)
+    backproject_full_tma(float *__restrict__ f, const float *__restrict__ data,
+                         const __grid_constant__ CUtensorMap map,
+                         const float *__restrict__ theta, float phi, float c, int sz, int ncz,
+                         int n, int nz, int nproj, int *__restrict__ err) {
+  using namespace tcb::tc;
+  extern __shared__ uint8_t lr_raw[];
+  uint8_t *sm = lr_raw + ((128u - (smem_u32(lr_raw) & 127u)) & 127u);
+  __shared__ float s_c[2][TAC], s_s[2][TAC];
+  __shared__ int s_u0[2][TAC];
+  __shared__ uint64_t bar[2];
+  const int tx = blockIdx.x * BX + threadIdx.x;
+  const int ty = blockIdx.y * BY + threadIdx.y;
+  const int tz0 = blockIdx.z * ZS;
+  const bool active = tx < n && ty < n;
+  const float cphi = __cosf(phi);
+  const float sphi = __sinf(phi);
+  float acc[ZS];
+#pragma unroll
+  for (int s = 0; s < ZS; s++) acc[s] = 0.f;
+  const int tid = threadIdx.y * BX + threadIdx.x;
+  const int x0 = blockIdx.x * BX - n / 2, y0 = blockIdx.y * BY - n / 2;
+  const int v0 = tz0 + sz - 1;  // first sinogram row of every box
+  const int nch = (nproj + TAC - 1) / TAC;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // rotation terms and box origins of chunk cc into stage st
+  auto prep = [&](int cc, int st) {
+    const int t0 = cc * TAC, cnt = min(TAC, nproj - t0);
+    if (tid < cnt) {
+      const float th = theta[t0 + tid];
+      const float ct = __cosf(th), stt = __sinf(th);
+      s_c[st][tid] = ct;
+      s_s[st][tid] = stt;
+      const float umin = fminf(fminf(ct * x0 + stt * y0, ct * (x0 + BX - 1) + stt * y0),
+                               fminf(ct * x0 + stt * (y0 + BY - 1),
+                                     ct * (x0 + BX - 1) + stt * (y0 + BY - 1))) +
+                         n / 2;
+      s_u0[st][tid] = ((int)floorf(umin) - 1) & ~3;  // down to a multiple of 4
+    }
+  };
+  auto issue = [&](int cc, int st) {  // one thread
+    const int t0 = cc * TAC, cnt = min(TAC, nproj - t0);
+    mbar_expect_tx(&bar[st], (uint32_t)(cnt * TUW * VR * 4));
+    for (int a = 0; a < cnt; a++)
+      tma_load_3d(sm + st * TSTAGE + a * TBOX, &map, &bar[st], s_u0[st][a], t0 + a, v0);
+  };
+  prep(0, 0);
+  __syncthreads();
+  if (tid == 0) issue(0, 0);
+  bool ok = true;
+  int waited = 0;  // chunks whose stage barrier completed
+  for (int cc = 0; cc < nch; cc++) {
+    const int st = cc & 1;
+    const int t0 = cc * TAC, cnt = min(TAC, nproj - t0);
+    if (cc + 1 < nch) prep(cc + 1, st ^ 1);
+    __syncthreads();
+    if (tid == 0 && cc + 1 < nch) issue(cc + 1, st ^ 1);
+    ok = __syncthreads_and(mbar_wait(&bar[st], (cc >> 1) & 1));
+    if (!ok) break;
+    waited = cc + 1;
+    if (active) {
+      for (int k = 0; k < cnt; k++) {
+        const int t = t0 + k;
+        float ctheta = s_c[st][k];
+        float stheta = s_s[st][k];
+        float R0 = ctheta, R1 = stheta;
+        float R3 = stheta * cphi, R4 = -ctheta * cphi, R5 = sphi;
+        float u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2;
+        int ur = (int)(u - 1e-5f);
+        if (!((ur >= 0) & (ur < n - 1))) continue;
+        u = u - ur;
+        const int bu = ur - s_u0[st][k];
+        const bool uin = (bu >= 0) & (bu < TUW - 1);
+        const float *bx = reinterpret_cast<const float *>(sm + st * TSTAGE + k * TBOX);
+#pragma unroll
+        for (int s = 0; s < ZS; s++) {
+          const int tz = tz0 + s;
+          const int zz = tz + sz - nz / 2;
+          float v = R3 * (tx - n / 2) + R4 * (ty - n / 2) + R5 * zz + nz / 2;
+          int vr = (int)(v - 1e-5f);
+          if ((tz < ncz) & (vr >= 0) & (vr < nz - 1)) {
+            v = v - vr;
+            const int bv = vr - v0;
+            float x00, x01, x10, x11;
+            if (uin & (bv >= 0) & (bv < VR - 1)) {
+              x00 = bx[bv * TUW + bu];
+              x01 = bx[bv * TUW + bu + 1];
+              x10 = bx[(bv + 1) * TUW + bu];
+              x11 = bx[(bv + 1) * TUW + bu + 1];
+            } else {
+              const float *d0 = data + ur + (size_t)t * n + (size_t)vr * n * nproj;
+              const float *d1 = d0 + (size_t)n * nproj;
+              x00 = d0[0];
+              x01 = d0[1];
+              x10 = d1[0];
+              x11 = d1[1];
+            }
+            acc[s] += x00 * ((1 - u) * (1 - v)) + x01 * ((0 + u) * (1 - v)) +
+                      x10 * ((1 - u) * (0 + v)) + x11 * ((0 + u) * (0 + v));
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage st and its tables are refilled for chunk cc + 2
+  }
+  if (!ok) {
+    // a wait gave up: report it, then wait (bounded) for the copies still in
+    // flight (chunks waited .. waited + 1) before the CTA's smem goes away
+    if (tid == 0) {
+      atomicOr(err, 1);
+      for (int cc = waited; cc < min(nch, waited + 2); cc++) mbar_wait(&bar[cc & 1], (cc >> 1) & 1);
+    }
+    __syncthreads();
+    return;
+  }
+  if (!active) return;
+#pragma unroll
+  for (int s = 0; s < ZS; s++) {
+    const int tz = tz0 + s;
+    if (tz >= ncz) break;
+    float *o = f + tx + (size_t)(n - ty - 1) * n + (size_t)tz * n * n;
+    *o = *o + acc[s] * c;
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 lr_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// The sinogram stack [nz][nproj][n] float32 as a TMA map with one
+// TUW x 1 x VR box per angle; false when the layout does not allow it.
+bool sino_map(CUtensorMap *m, const float *data, size_t n, size_t nproj, size_t nz) {
+  auto fn = lr_encode_fn();
+  if (!fn || n % 4 || ((uintptr_t)data & 15) || n < TUW) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)nproj, (cuuint64_t)nz};
+  cuuint64_t strides[2] = {(cuuint64_t)(n * 4), (cuuint64_t)(n * nproj * 4)};
+  cuuint32_t box[3] = {(cuuint32_t)TUW, 1, (cuuint32_t)VR};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(data), dims, strides, box,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename T>
 int launch(tcb_linerec *h, int mode, void *f, const void *g, const float *theta,
            float phi, const float *phi_v, const float *sh, int sz, cudaStream_t s) {
@@ -216,6 +397,16 @@ int launch(tcb_linerec *h, int mode, void *f, const void *g, const float *theta,
   switch (mode) {
     case FULL: {
       dim3 grz(ceil_div(h->n, BX), ceil_div(h->n, BY), ceil_div(h->ncz, ZS));
+      CUtensorMap map;
+      // TCB_LINEREC_TMA=0 keeps the plain staging (for comparisons)
+      const char *tsel = getenv("TCB_LINEREC_TMA");
+      const bool tma_on = !(tsel && tsel[0] == '0');
+      if (sizeof(T) == 4 && tma_on && h->err &&
+          sino_map(&map, (const float *)g, h->n, h->ncproj, h->nz)) {
+        backproject_full_tma<<<grz, blk, TSMEM, s>>>((float *)f, (const float *)g, map, theta,
+                                                     phi, c, sz, ncz, n, nz, np, h->err);
+        break;
+      }
       backproject_full_zs<T><<<grz, blk, 0, s>>>((T *)f, (const T *)g, theta, phi, c, sz, ncz,
                                                   n, nz, np);
       break;
@@ -265,7 +456,25 @@ extern "C" int tcb_linerec_create(tcb_linerec **out, size_t nproj, size_t nz, si
   h->ncproj = ncproj;
   h->ncz = ncz;
   h->precision = precision;
+  // the TMA-staged float32 kernel needs its dynamic shared memory and an
+  // error flag; without them the plain kernel runs
+  if (precision == TCB_FLOAT32 &&
+      cudaFuncSetAttribute(lr::backproject_full_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           lr::TSMEM) == cudaSuccess &&
+      cudaMalloc(&h->err, sizeof(int)) == cudaSuccess &&
+      cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess) {
+    cudaFree(h->err);
+    h->err = nullptr;
+  }
+  cudaGetLastError();
   *out = h;
+  return TCB_OK;
+}
+
+extern "C" int tcb_linerec_status(tcb_linerec *h, int *timed_out) {
+  TCB_CHECK_ARG(h && timed_out, "tcb_linerec_status: null pointer");
+  *timed_out = 0;
+  if (h->err) TCB_CUDA(cudaMemcpy(timed_out, h->err, sizeof(int), cudaMemcpyDeviceToHost));
   return TCB_OK;
 }
 
@@ -290,6 +499,7 @@ extern "C" int tcb_linerec_backprojection_try_lamino(tcb_linerec *h, void *f,
 
 extern "C" int tcb_linerec_destroy(tcb_linerec *h) {
   if (!h) return TCB_OK;
+  cudaFree(h->err);
   delete h;
   return TCB_OK;
 }
