@@ -491,8 +491,14 @@ def run_lamino(a, dev):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / 2
+        from tomocupy_b200 import _lib
+        _lib.profile_enable(True)
+        bp.rec_lam(data)
+        stages = _lib.profile_report()
+        _lib.profile_enable(False)
         key = "fp32" if dtype == "float32" else "fp16_storage"
-        res[key] = {"ms": round(ms, 2), "value": round(vox / (ms / 1e3) / 1e9, 2)}
+        res[key] = {"ms": round(ms, 2), "value": round(vox / (ms / 1e3) / 1e9, 2),
+                    "stages_ms": {k: round(v["ms"], 2) for k, v in stages.items()}}
         outs[key] = out
         del bp
     d = (outs["fp16_storage"].double() - outs["fp32"].double()).norm()
