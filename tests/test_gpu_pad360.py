@@ -81,3 +81,48 @@ def test_double_fov_reconstruction_matches_reference_chain(cuda, ref, axis):
     rec.backprojection(theirs, d)
     err = rel_l2(ours, theirs.cpu())
     assert err < 1e-5, err
+
+
+def test_double_fov_try_sweep_matches_reference_chain(cuda, ref):
+    """Try-centre sweep of a double-FOV scan (axis on the left: the shifts are
+    inverted as Reader.init_sizes_try does) against dark/flat -> -log ->
+    pad360 (restated) -> the reference's filter at each shift and its
+    fourierrec."""
+    from oracle import np_tomo
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.rec import GPURec
+    nproj, nz, ni = 180, 4, 128
+    theta = np.linspace(0, 2 * np.pi, nproj, endpoint=False).astype(np.float32)
+    data, dark, flat, _, _ = synthetic.make_dataset(nproj, nz, ni, seed=8, theta=theta)
+    global_vars.reset(reconstruction_algorithm="fourierrec", reconstruction_type="try",
+                      nsino_per_chunk=4, nsino="0.5", center_search_width=2.0,
+                      center_search_step=1.0, file_type="double_fov", rotation_axis=9.5)
+    w = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(data, dark, flat, theta=theta), w).recon_try()
+    zs, n, center = int(params.id_slices[0]), params.n, params.center
+    shifts = np.asarray(params.shift_array, dtype=np.float32)
+    assert n == 2 * ni and len(w.tries) == len(shifts)
+    pre = np_tomo.minus_log(np_tomo.darkflat(data[:, zs:zs + 1].numpy(),
+                                             dark[:, zs:zs + 1].numpy(),
+                                             flat[:, zs:zs + 1].numpy()))
+    pad = np_tomo.pad360(pre, params.centeri, ni, center)        # [nproj, 1, 2 ni]
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, "parzen"), device=cuda)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=cuda)
+    filt = ref.RefFilter(ne, nproj, 4)
+    rec = ref.RefFourierRec(n, nproj, 4, torch.as_tensor(theta, device=cuda))
+    rows = torch.as_tensor(np.ascontiguousarray(pad.transpose(1, 0, 2)), device=cuda)
+    for k in range(0, len(shifts), 4):
+        cnt = min(4, len(shifts) - k)
+        sht = torch.zeros(4, device=cuda)
+        sht[:cnt] = torch.as_tensor(shifts[k:k + cnt], device=cuda)
+        d = rows.expand(4, -1, -1).contiguous()
+        d = ref.ref_fbp_filter_center(filt, d, wf, t, center, sht, n, ne)
+        theirs = torch.zeros((4, n, n), device=cuda)
+        rec.backprojection(theirs, d)
+        for kk in range(cnt):
+            ours = w.tries[(zs, float(params.save_centers[k + kk]))].cpu()
+            err = rel_l2(ours, theirs[kk].cpu())
+            assert err < 1e-4, (k + kk, err)

@@ -194,8 +194,6 @@ class GPURec:
         The sweep over all centres is one CUDA graph (TryCenterSweep), recorded
         once and replayed for each requested slice.
         """
-        if args.file_type == "double_fov":
-            raise NotImplementedError("try-centre sweeps of double-FOV scans")
         _no_phase("GPURec.recon_try")
         from .trycenter import TryCenterSweep
         if args.reconstruction_algorithm != "fourierrec" or args.remove_stripe_method != "none":
@@ -207,7 +205,8 @@ class GPURec:
                                         params.shift_array, args.fbp_filter, self.precision,
                                         params.ncz, device=dev,
                                         minus_log=args.minus_log == "True",
-                                        mixed_filter=args.mixed_filter)
+                                        mixed_filter=args.mixed_filter, ni=params.ni,
+                                        pad360=_pad360_args())
         sw = self.sweep
         for id_slice in params.id_slices:
             z = int(id_slice)
