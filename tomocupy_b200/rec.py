@@ -35,6 +35,15 @@ def _supported():
             "the fused driver runs the float32 drop-in path or the 'mixed' tensor-core path")
 
 
+def _stripe_args():
+    """The pipeline's ring-removal argument for remove_stripe_method, else None."""
+    if args.remove_stripe_method == "fw":
+        return (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
+    if args.remove_stripe_method == "ti":
+        return ("ti", float(args.ti_beta), float(args.ti_mask))
+    return None
+
+
 def _pad360_args():
     """(flip, w) of pad360 (proc_functions.py:109-124) for a double-FOV scan, else None."""
     if args.file_type != "double_fov":
@@ -72,11 +81,7 @@ class GPURec:
     def pipe(self) -> SinoPipeline:
         """The chunk pipeline (built on first use; try-centre sweeps do not need it)."""
         if self._pipe is None:
-            stripe = None
-            if args.remove_stripe_method == "fw":
-                stripe = (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
-            elif args.remove_stripe_method == "ti":
-                stripe = ("ti", float(args.ti_beta), float(args.ti_mask))
+            stripe = _stripe_args()
             self._pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                       params.center, args.fbp_filter,
                                       args.reconstruction_algorithm,
@@ -196,8 +201,8 @@ class GPURec:
         """
         _no_phase("GPURec.recon_try")
         from .trycenter import TryCenterSweep
-        if args.reconstruction_algorithm != "fourierrec" or args.remove_stripe_method != "none":
-            raise NotImplementedError("try-centre sweeps run fourierrec without ring removal")
+        if args.reconstruction_algorithm != "fourierrec":
+            raise NotImplementedError("try-centre sweeps run fourierrec")
         data, dark, flat = self.cl_reader.frames()
         dev = self.device
         if self.sweep is None:
@@ -206,7 +211,7 @@ class GPURec:
                                         params.ncz, device=dev,
                                         minus_log=args.minus_log == "True",
                                         mixed_filter=args.mixed_filter, ni=params.ni,
-                                        pad360=_pad360_args())
+                                        pad360=_pad360_args(), stripe=_stripe_args())
         sw = self.sweep
         for id_slice in params.id_slices:
             z = int(id_slice)

@@ -56,7 +56,7 @@ class TryCenterSweep:
 
     def __init__(self, n, nproj, theta, center, shifts, fbp_filter="parzen",
                  precision="float32", ncz=32, pairs_per_block=0, device="cuda",
-                 minus_log=True, mixed_filter="fft", ni=None, pad360=None):
+                 minus_log=True, mixed_filter="fft", ni=None, pad360=None, stripe=None):
         self.device = torch.device(device)
         self.n, self.nproj, self.ncz = int(n), int(nproj), int(ncz)
         self.precision = precision
@@ -64,11 +64,12 @@ class TryCenterSweep:
         self.S = self.shifts.size
         self.sht = chunk_shifts(self.shifts, self.ncz)
         self.nchunks = self.sht.shape[0]
-        # ni / pad360: a double-FOV scan (frames of ni columns, pad360 after -log)
+        # ni / pad360: a double-FOV scan (frames of ni columns, pad360 after -log);
+        # stripe: ring removal of the slice (SinoPipeline's stripe argument)
         self.pipe = SinoPipeline(self.n, self.nproj, self.ncz, theta, center, fbp_filter,
                                  "fourierrec", minus_log=minus_log, device=self.device,
-                                 precision=precision, mixed_filter=mixed_filter, ni=ni,
-                                 pad360=pad360)
+                                 stripe=stripe, precision=precision, mixed_filter=mixed_filter,
+                                 ni=ni, pad360=pad360)
         if pairs_per_block:
             self.pipe.fr.set_pairs_per_block(pairs_per_block)
         self.pairs_per_block = int(pairs_per_block)
