@@ -208,6 +208,34 @@ def test_recon_try_matches_reference(cuda, ref, c1):
             assert err < 1e-5, (k + kk, err)
 
 
+@pytest.mark.parametrize("algorithm", ["lprec", "linerec"])
+def test_recon_try_lprec_linerec_match_reference(cuda, ref, c1, algorithm):
+    """Try-centre reconstruction with the other backprojectors (the reference's
+    recon_try runs whichever reconstruction_algorithm is set)."""
+    from tomocupy_b200 import global_vars
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.rec import GPURec
+    data, dark, flat, theta, _ = c1
+    global_vars.reset(reconstruction_type="try", reconstruction_algorithm=algorithm,
+                      center_search_width=2.0, center_search_step=0.5, nsino="0.5",
+                      nsino_per_chunk=4)
+    writer = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(data, dark, flat, theta=theta), writer).recon_try()
+    zs, shifts = int(params.id_slices[0]), params.shift_array
+    assert len(writer.tries) == len(shifts)
+    sl, dk, fl = (t[:, zs:zs + 1].repeat(1, 4, 1) for t in (data, dark, flat))
+    for k in range(0, len(shifts), 4):
+        sht = torch.zeros(4, device="cuda")
+        cnt = min(4, len(shifts) - k)
+        sht[:cnt] = torch.as_tensor(shifts[k:k + cnt], device="cuda")
+        theirs = reference_chain(ref, sl, dk, fl, theta, algorithm=algorithm, ncz=4, sht=sht)
+        for kk in range(cnt):
+            ours = writer.tries[(zs, float(params.save_centers[k + kk]))].cpu()
+            err = rel_l2(ours, theirs[kk])
+            assert err < 1e-5, (algorithm, k + kk, err)
+
+
 @pytest.mark.parametrize("stripe", [("ti", 0.022, 1), (1.0, "sym16", 3)])
 def test_recon_try_with_ring_removal_matches_reference(cuda, ref, c1, stripe):
     """Try-centre sweep with ring removal of the slice (proc_sino inside the

@@ -202,7 +202,7 @@ class GPURec:
         _no_phase("GPURec.recon_try")
         from .trycenter import TryCenterSweep
         if args.reconstruction_algorithm != "fourierrec":
-            raise NotImplementedError("try-centre sweeps run fourierrec")
+            return self._recon_try_chunks()
         data, dark, flat = self.cl_reader.frames()
         dev = self.device
         if self.sweep is None:
@@ -225,6 +225,34 @@ class GPURec:
             out = sw.run()
             for k in range(sw.S):
                 self.cl_writer.write_data_try(out[k], params.save_centers[k], id_slice)
+        torch.cuda.synchronize(dev)
+
+    def _recon_try_chunks(self):
+        """Try-centre reconstruction with lprec or linerec, as the reference's
+        recon_try does it (rec.py:210-275): the pre-processed slice tiled ncz
+        times, each copy filtered with its own centre shift, one backprojection
+        per chunk of ncz shifts."""
+        data, dark, flat = self.cl_reader.frames()
+        dev, ncz, n = self.device, params.ncz, params.n
+        pipe = self.pipe
+        shifts = np.asarray(params.shift_array, dtype=np.float32)
+        out = torch.empty((ncz, n, n), dtype=pipe.out_dtype, device=dev)
+        for id_slice in params.id_slices:
+            z = int(id_slice)
+            row = data[:, z:z + 1].to(dev)
+            if dezinger_args() is not None:
+                row = dezinger(row, *dezinger_args())
+            d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
+            for k0 in range(0, shifts.size, ncz):
+                cnt = min(ncz, shifts.size - k0)
+                sht = np.zeros(ncz, dtype=np.float32)
+                sht[:cnt] = shifts[k0:k0 + cnt]
+                pipe.load_rows(row, d0, f0, 0)
+                pipe.replicate_first_row()
+                pipe.filter_and_backproject(out, sht)
+                for kk in range(cnt):
+                    self.cl_writer.write_data_try(out[kk], params.save_centers[k0 + kk],
+                                                  id_slice)
         torch.cuda.synchronize(dev)
 
     # ------------------------------------------------------------------ device
