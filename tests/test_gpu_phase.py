@@ -115,6 +115,40 @@ def test_step_driver_with_phase_retrieval(cuda):
     want = rec.recon_preprocessed(torch.as_tensor(pre, device=cuda)).cpu().numpy()
     err = rel_l2(got, want)
     assert np.isfinite(got).all() and err < 1e-4, err
-    global_vars.reset(**dict(opts, reconstruction_type="full"))
+    global_vars.reset(**opts)
     with pytest.raises(NotImplementedError):
-        GPURec(ArrayReader(data, dark, flat, theta=theta), ArrayWriter(device="cuda")).recon_all()
+        GPURec(ArrayReader(data, dark, flat, theta=theta), ArrayWriter(device="cuda")).recon_try()
+
+
+def test_recon_all_phase_retrieval_per_chunk_matches_reference(cuda, ref):
+    """GPURec.recon_all with Paganin phase retrieval applies it to each
+    sinogram chunk's projections (rows of the chunk as the image height), as
+    the reference's recon_all does (rec.py:170-173): against dark/flat ->
+    restated paganin_filter per chunk -> -log -> the reference's CUDA filter
+    and fourierrec."""
+    from oracle import np_tomo
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    nproj, nz, n, ncz = 90, 16, 128, 8
+    data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=12)
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=ncz,
+                      retrieve_phase_method="paganin", pixel_size=0.65,
+                      propagation_distance=50.0, energy=20.0, retrieve_phase_alpha=1e-3)
+    w = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(data, dark, flat, theta=theta), w).recon_all()
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, "parzen"), device=cuda)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=cuda)
+    filt = ref.RefFilter(ne, nproj, ncz)
+    rec = ref.RefFourierRec(n, nproj, ncz, torch.as_tensor(theta, device=cuda))
+    for z0 in range(0, nz, ncz):
+        sl = slice(z0, z0 + ncz)
+        pre = np_tomo.darkflat(data[:, sl].numpy(), dark[:, sl].numpy(), flat[:, sl].numpy())
+        pre = np_tomo.minus_log(np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3))
+        d = torch.as_tensor(np.ascontiguousarray(pre.transpose(1, 0, 2)), device=cuda)
+        d = ref.ref_fbp_filter_center(filt, d, wf, t, n / 2, torch.zeros(ncz, device=cuda), n, ne)
+        theirs = torch.zeros((ncz, n, n), device=cuda)
+        rec.backprojection(theirs, d)
+        err = rel_l2(w.rec[sl].cpu(), theirs.cpu())
+        assert err < 1e-4, (z0, err)

@@ -19,7 +19,8 @@ import torch
 
 from .global_vars import args, params
 from .pipeline import SinoPipeline, copy2d_rows
-from .processing.proc_functions import PHASE_METHODS, darkflat_stats, dezinger, dezinger_args
+from .processing.proc_functions import (PHASE_METHODS, darkflat_stats, dezinger, dezinger_args,
+                                        prep_rows, retrieve_phase)
 
 
 def _supported():
@@ -128,7 +129,10 @@ class GPURec:
 
     def recon_all(self):
         """Reconstruct every slice; results go to ``cl_writer`` (host or device)."""
-        _no_phase("GPURec.recon_all")
+        phase = args.retrieve_phase_method in PHASE_METHODS
+        if phase and (args.remove_stripe_method != "none" or args.file_type == "double_fov"):
+            raise NotImplementedError("phase retrieval in GPURec.recon_all with ring removal or "
+                                      "double-FOV padding")
         data, dark, flat = self.cl_reader.frames()
         ncz, n, nz, nproj = params.ncz, params.n, params.nz, params.nproj
         dev = self.device
@@ -177,7 +181,13 @@ class GPURec:
                 if k >= 2 and host_out:
                     s2.wait_event(d2h_done[b])
                 out = rbuf[b] if (host_out or lz < ncz) else rec_out[z0:z0 + ncz]
-                self.pipe.reconstruct(out, src, dark0, flat0, z_lo=z0, stream=s2)
+                if lz < ncz:  # rows of the previous chunk must not pair with this one's
+                    self.pipe.clear_rows(lz, s2)
+                if phase:
+                    self.pipe.reconstruct(out, self._phase_chunk(src, dark0, flat0, z0, s2),
+                                          None, None, z_lo=z0, stream=s2)
+                else:
+                    self.pipe.reconstruct(out, src, dark0, flat0, z_lo=z0, stream=s2)
                 if not host_out and lz < ncz:
                     rec_out[z0:z0 + lz].copy_(out[:lz])
                 comp_done[b].record(s2)
@@ -226,6 +236,23 @@ class GPURec:
             for k in range(sw.S):
                 self.cl_writer.write_data_try(out[k], params.save_centers[k], id_slice)
         torch.cuda.synchronize(dev)
+
+    def _phase_chunk(self, src, dark0, flat0, z0, stream):
+        """proc_sino + proc_proj's phase step on one sinogram chunk, as the
+        reference's recon_all runs them (rec.py:170-173): dark/flat, then phase
+        retrieval of the chunk's projections (its rows are the image height);
+        -log follows in the pipeline."""
+        nproj, lz, n = src.shape
+        buf = getattr(self, "_phase_buf", None)
+        if buf is None or buf.numel() < nproj * lz * n:
+            buf = self._phase_buf = torch.empty(nproj * params.ncz * n, dtype=torch.float32,
+                                                device=self.device)
+        tmp = buf[:nproj * lz * n].view(nproj, lz, n)
+        prep_rows(tmp, src, dark0[z0:z0 + lz], flat0[z0:z0 + lz], darkflat=True,
+                  minus_log=False, out_zstride=n, out_pstride=lz * n, stream=stream)
+        with torch.cuda.stream(stream):
+            retrieve_phase(tmp)
+        return tmp
 
     def _recon_try_chunks(self):
         """Try-centre reconstruction with lprec or linerec, as the reference's
