@@ -38,8 +38,10 @@ class GPURecSteps:
         self.device = torch.device(device)
         self.cl_reader = cl_reader
         self.cl_writer = cl_writer
-        if args.file_type != "standard":
-            raise NotImplementedError("double_fov scans run in GPURec.recon_all")
+        if args.file_type not in ("standard", "double_fov"):
+            raise NotImplementedError(f"file_type={args.file_type!r}")
+        if args.file_type == "double_fov" and args.lamino_angle != 0:
+            raise NotImplementedError("double-FOV laminography")
         if args.dtype != "float32":
             raise NotImplementedError("the step driver runs the float32 path")
 
@@ -85,7 +87,26 @@ class GPURecSteps:
         if late_log and args.minus_log == "True":
             prep_rows(out, out, darkflat=False, minus_log=True, out_zstride=n,
                       out_pstride=nz * n)
+        if args.file_type == "double_fov":
+            out = self._pad360(out)
         return out
+
+    def _pad360(self, out):
+        """proc_proj's pad360 (proc_functions.py:109-124, 190-193) of every
+        projection row: [nproj, nz, ni] -> [nproj, nz, 2 ni]."""
+        import ctypes as C
+        from . import _lib
+        from .rec import _pad360_args
+        nproj, nz, ni = out.shape
+        flip, w = _pad360_args()
+        v = np.empty(w, dtype=np.float64)
+        _lib.call("tcb_pad360_weights", v.ctypes.data_as(C.c_void_p), w)
+        vd = torch.as_tensor(v, device=self.device)
+        padded = torch.empty((nproj, nz, 2 * ni), dtype=torch.float32, device=self.device)
+        padded[:, :, :ni] = out
+        _lib.call("tcb_pad360_rows", padded.data_ptr(), nproj * nz, ni, 2 * ni, int(flip),
+                  vd.data_ptr(), w, _lib.stream_ptr(None))
+        return padded
 
     # ------------------------------------------------------------------ driver
     def recon_steps_all(self):
@@ -101,11 +122,13 @@ class GPURecSteps:
     def _tomo(self):
         from .rec import GPURec
         rec = GPURec(self.cl_reader, self.cl_writer, device=self.device)
-        if args.retrieve_phase_method in PHASE_METHODS:
-            # phase retrieval needs whole projections: pre-process the
-            # resident dataset (proc_sino + proc_proj), then backproject
+        if args.retrieve_phase_method in PHASE_METHODS or args.file_type == "double_fov":
+            # phase retrieval needs whole projections, double-FOV padding
+            # follows it: pre-process the resident dataset (proc_sino +
+            # proc_proj), then backproject
             if args.reconstruction_type != "full":
-                raise NotImplementedError("phase retrieval with try-centre sweeps")
+                raise NotImplementedError("phase retrieval or double-FOV padding with "
+                                          "try-centre sweeps in the step driver")
             return rec.recon_preprocessed(self.preprocessed())
         if args.reconstruction_type == "full":
             return rec.recon_all()
