@@ -152,3 +152,40 @@ def test_recon_all_phase_retrieval_per_chunk_matches_reference(cuda, ref):
         rec.backprojection(theirs, d)
         err = rel_l2(w.rec[sl].cpu(), theirs.cpu())
         assert err < 1e-4, (z0, err)
+
+
+def test_recon_all_ring_removal_then_phase_matches_reference(cuda, ref):
+    """recon_all with Titarenko ring removal and Paganin phase retrieval: per
+    chunk dark/flat -> ring removal -> phase retrieval -> -log (proc_sino then
+    proc_proj), against the same order with the restated phase retrieval
+    (the ring removal itself is checked against the reference's
+    remove_stripe_ti in tests/test_gpu_stripe.py)."""
+    from oracle import np_tomo
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
+    from tomocupy_b200.rec import GPURec
+    nproj, nz, n, ncz = 90, 16, 128, 8
+    data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=13, stripes=6)
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=ncz,
+                      remove_stripe_method="ti", ti_beta=0.022, ti_mask=1,
+                      retrieve_phase_method="paganin", pixel_size=0.65,
+                      propagation_distance=50.0, energy=20.0, retrieve_phase_alpha=1e-3)
+    w = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(data, dark, flat, theta=theta), w).recon_all()
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, "parzen"), device=cuda)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=cuda)
+    filt = ref.RefFilter(ne, nproj, ncz)
+    rec = ref.RefFourierRec(n, nproj, ncz, torch.as_tensor(theta, device=cuda))
+    for z0 in range(0, nz, ncz):
+        sl = slice(z0, z0 + ncz)
+        pre = np_tomo.darkflat(data[:, sl].numpy(), dark[:, sl].numpy(), flat[:, sl].numpy())
+        pre = remove_stripe_ti(torch.as_tensor(pre, device=cuda), 0.022, 1).cpu().numpy()
+        pre = np_tomo.minus_log(np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3))
+        d = torch.as_tensor(np.ascontiguousarray(pre.transpose(1, 0, 2)), device=cuda)
+        d = ref.ref_fbp_filter_center(filt, d, wf, t, n / 2, torch.zeros(ncz, device=cuda), n, ne)
+        theirs = torch.zeros((ncz, n, n), device=cuda)
+        rec.backprojection(theirs, d)
+        err = rel_l2(w.rec[sl].cpu(), theirs.cpu())
+        assert err < 1e-4, (z0, err)

@@ -82,7 +82,9 @@ class GPURec:
     def pipe(self) -> SinoPipeline:
         """The chunk pipeline (built on first use; try-centre sweeps do not need it)."""
         if self._pipe is None:
-            stripe = _stripe_args()
+            # with phase retrieval the chunk's ring removal runs before it
+            # (_phase_chunk), not in the pipeline
+            stripe = None if args.retrieve_phase_method in PHASE_METHODS else _stripe_args()
             self._pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                       params.center, args.fbp_filter,
                                       args.reconstruction_algorithm,
@@ -130,9 +132,6 @@ class GPURec:
     def recon_all(self):
         """Reconstruct every slice; results go to ``cl_writer`` (host or device)."""
         phase = args.retrieve_phase_method in PHASE_METHODS
-        if phase and (args.remove_stripe_method != "none" or args.file_type == "double_fov"):
-            raise NotImplementedError("phase retrieval in GPURec.recon_all with ring removal or "
-                                      "double-FOV padding")
         data, dark, flat = self.cl_reader.frames()
         ncz, n, nz, nproj = params.ncz, params.n, params.nz, params.nproj
         dev = self.device
@@ -239,9 +238,10 @@ class GPURec:
 
     def _phase_chunk(self, src, dark0, flat0, z0, stream):
         """proc_sino + proc_proj's phase step on one sinogram chunk, as the
-        reference's recon_all runs them (rec.py:170-173): dark/flat, then phase
-        retrieval of the chunk's projections (its rows are the image height);
-        -log follows in the pipeline."""
+        reference's recon_all runs them (rec.py:170-173): dark/flat, ring
+        removal, then phase retrieval of the chunk's projections (its rows are
+        the image height); -log (and double-FOV padding) follow in the
+        pipeline."""
         nproj, lz, n = src.shape
         buf = getattr(self, "_phase_buf", None)
         if buf is None or buf.numel() < nproj * lz * n:
@@ -251,6 +251,12 @@ class GPURec:
         prep_rows(tmp, src, dark0[z0:z0 + lz], flat0[z0:z0 + lz], darkflat=True,
                   minus_log=False, out_zstride=n, out_pstride=lz * n, stream=stream)
         with torch.cuda.stream(stream):
+            if args.remove_stripe_method == "fw":
+                from .processing.remove_stripe import remove_stripe_fw
+                tmp.copy_(remove_stripe_fw(tmp, args.fw_sigma, args.fw_filter, args.fw_level))
+            elif args.remove_stripe_method == "ti":
+                from .processing.remove_stripe import remove_stripe_ti
+                remove_stripe_ti(tmp, args.ti_beta, args.ti_mask)
             retrieve_phase(tmp)
         return tmp
 
