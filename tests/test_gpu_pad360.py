@@ -128,11 +128,14 @@ def test_double_fov_try_sweep_matches_reference_chain(cuda, ref):
             assert err < 1e-4, (k + kk, err)
 
 
-@pytest.mark.parametrize("axis", [118.0, 9.5])
-def test_step_driver_double_fov_matches_recon_all(cuda, axis):
+@pytest.mark.parametrize("axis,stripe", [(118.0, "none"), (9.5, "none"), (118.0, "fw"),
+                                         (9.5, "ti")])
+def test_step_driver_double_fov_matches_recon_all(cuda, axis, stripe):
     """GPURecSteps pads whole pre-processed projections (pad360 after -log) and
-    backprojects; GPURec.recon_all pads each chunk's filter rows.  Same
-    operations in the same order: the volumes agree to float32 rounding."""
+    backprojects; GPURec.recon_all pads each chunk's filter rows.  Ring
+    removal runs on the ni-wide sinograms before the padding in both
+    (proc_sino before proc_proj, proc_functions.py:140-195).  Same operations
+    in the same order: the volumes agree to float32 rounding."""
     from tomocupy_b200 import global_vars, synthetic
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
@@ -141,7 +144,8 @@ def test_step_driver_double_fov_matches_recon_all(cuda, axis):
     theta = np.linspace(0, 2 * np.pi, nproj, endpoint=False).astype(np.float32)
     data, dark, flat, _, _ = synthetic.make_dataset(nproj, nz, ni, seed=9, theta=theta)
     opts = dict(reconstruction_algorithm="fourierrec", nsino_per_chunk=4,
-                file_type="double_fov", rotation_axis=axis)
+                file_type="double_fov", rotation_axis=axis, remove_stripe_method=stripe,
+                fw_level=4)
     global_vars.reset(**opts)
     w1 = ArrayWriter(device="cuda")
     GPURec(ArrayReader(data, dark, flat, theta=theta), w1).recon_all()
@@ -151,4 +155,4 @@ def test_step_driver_double_fov_matches_recon_all(cuda, axis):
     GPURecSteps(ArrayReader(data, dark, flat, theta=theta), w2).recon_steps_all()
     b = w2.rec.cpu()
     assert a.shape == b.shape == (nz, 2 * ni, 2 * ni)
-    assert rel_l2(b, a) < 1e-6
+    assert rel_l2(b, a) < (1e-6 if stripe == "none" else 1e-5)

@@ -133,13 +133,14 @@ class SinoPipeline:
         self.fw = None
         if stripe is not None and stripe[0] == "ti":
             from .processing.remove_stripe import StripeTI
-            self.fw = StripeTI(self.nproj, self.ncz, self.n, stripe[1], stripe[2])
+            self.fw = StripeTI(self.nproj, self.ncz, self.ni, stripe[1], stripe[2])
         elif stripe is not None:
             from .processing.remove_stripe import StripeFW
             sigma, wname, level = stripe
-            self.fw = StripeFW(self.nproj, self.ncz, self.n, sigma, wname, level)
+            self.fw = StripeFW(self.nproj, self.ncz, self.ni, sigma, wname, level)
         if self.fw is not None:
-            self.sino = torch.zeros((self.ncz, self.fw.nproj_pad, self.n), dtype=torch.float32,
+            # ni-wide sinograms: double-FOV scans are padded after ring removal
+            self.sino = torch.zeros((self.ncz, self.fw.nproj_pad, self.ni), dtype=torch.float32,
                                     device=self.device)
         if algorithm == "fourierrec":
             self.fr = cfunc_fourierrec.cfunc_fourierrec(self.nproj, self.ncz // 2, self.n,
@@ -182,9 +183,8 @@ class SinoPipeline:
         """Fill the padded filter rows from a [nproj, nz, n] frame (or float) stack view."""
         nz = data.shape[1]
         assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.ni
-        if self.pad360 is not None and (self.fw is not None or not self.fused):
-            raise NotImplementedError("double-FOV padding: fused fp32 filter without ring "
-                                      "removal only")
+        if self.pad360 is not None and not self.fused:
+            raise NotImplementedError("double-FOV padding: fused fp32 filter only")
         if self.dezinger is not None:
             if self._zbuf is None or self._zbuf.dtype != data.dtype:
                 self._zbuf = torch.empty((self.nproj, self.ncz, self.n), dtype=data.dtype,
@@ -200,7 +200,7 @@ class SinoPipeline:
             with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
                 self.sino.zero_()
             prep_rows(self.sino, data, d0, f0, darkflat=dark0 is not None, minus_log=False,
-                      out_zstride=fw.nproj_pad * self.n, out_pstride=self.n,
+                      out_zstride=fw.nproj_pad * self.ni, out_pstride=self.ni,
                       out_poff=fw.poff, stream=stream)
             fw.apply_sino(self.sino, stream)
             src = self.sino[:nz, fw.poff:fw.poff + self.nproj].permute(1, 0, 2)
@@ -212,6 +212,7 @@ class SinoPipeline:
             if self.fused:
                 prep_rows(self.rows, src, darkflat=False, minus_log=self.minus_log,
                           out_zstride=self.nproj * self.n, out_pstride=self.n, stream=stream)
+                self._pad360_rows(nz, stream)
                 return
             prep_rows(self.rows, src, darkflat=False, minus_log=self.minus_log,
                       out_zstride=self.nproj * self.ne, out_pstride=self.ne, out_xoff=self.pad,
@@ -226,15 +227,20 @@ class SinoPipeline:
             prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                       minus_log=self.minus_log, out_zstride=self.nproj * self.n,
                       out_pstride=self.n, stream=stream)
-            if self.pad360 is not None:
-                flip, w, v = self.pad360
-                _lib.call("tcb_pad360_rows", self.rows.data_ptr(), nz * self.nproj, self.ni,
-                          self.n, int(flip), v.data_ptr(), w, _lib.stream_ptr(stream))
+            self._pad360_rows(nz, stream)
             return
         prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                   minus_log=self.minus_log, out_zstride=self.nproj * self.ne,
                   out_pstride=self.ne, out_xoff=self.pad, out_width=self.ne, edge_pad=True,
                   stream=stream)
+
+    def _pad360_rows(self, nz: int, stream=None) -> None:
+        """Double-FOV padding of the -log rows of nz slices, in place (ni -> 2 ni)."""
+        if self.pad360 is None:
+            return
+        flip, w, v = self.pad360
+        _lib.call("tcb_pad360_rows", self.rows.data_ptr(), nz * self.nproj, self.ni,
+                  self.n, int(flip), v.data_ptr(), w, _lib.stream_ptr(stream))
 
     def clear_rows(self, lz: int, stream=None) -> None:
         """Zero the filter input rows of slices [lz, ncz) (a partial chunk).
