@@ -144,6 +144,20 @@ int tcb_pad360_weights(double *v, size_t w);
 int tcb_pad360_rows(float *rows, size_t nrows, size_t ni, size_t row_stride, int flip,
                     const double *v, size_t w, void *stream);
 
+/* Projection rotation.  Replaces ProcFunctions.rotate_proj
+ * (src/tomocupy/processing/proc_functions.py:126-138), applied by proc_proj
+ * after phase retrieval and before -log when rotate_proj_angle != 0
+ * (proc_functions.py:181-183): ndimage.rotate(data, angle, reshape=False,
+ * order, axes=(2, 1), mode='nearest').  out[f] (frame stride out_fstride)
+ * gets in[f] (frame stride in_fstride; nz rows of n floats) sampled at
+ * iz = offz + oz c + ox s, ix = offx - oz s + ox c, clamped to the plane,
+ * with spline order 0 or 1, in float64 rounded to float32.  c, s: cosine
+ * and sine of the angle; offz, offx: the offset that keeps the plane centre
+ * fixed (both computed by the caller).  out and in must not overlap. */
+int tcb_rotate_proj(float *out, const float *in, size_t nframes, size_t nz, size_t n,
+                    size_t in_fstride, size_t out_fstride, double c, double s, double offz,
+                    double offx, int order, void *stream);
+
 /* Outlier (zinger) removal.  Replaces ProcFunctions.remove_outliers
  * (src/tomocupy/processing/proc_functions.py:96-107), which proc_sino applies
  * to the projections, darks and flats of a chunk before dark/flat correction

@@ -567,3 +567,61 @@ def rec_lam64(data, theta, center, lamino_angle, rh, wfilter):
     s2 = usfft2d_adj64(s1, theta, phi, detw)
     s3 = usfft1d_adj64(s2, phi, rh, deth)
     return np.ascontiguousarray(s3.transpose(1, 0, 2))
+
+
+# ---------------------------------------------------------------- rotation
+def rotate_params(angle, nz, n):
+    """(c, s, offz, offx) of ndimage.rotate(angle, axes=(2, 1), reshape=False)
+    on nz x n planes, as the reference's host code forms them
+    (src/tomocupy/processing/proc_functions.py:126-138 calls cupyx's rotate,
+    which builds the matrix from NumPy's deg2rad, cos and sin)."""
+    a = np.deg2rad(float(angle))
+    c, s = float(np.cos(a)), float(np.sin(a))
+    rot = np.array([[c, s], [-s, c]])
+    shape = np.array([nz, n], dtype=np.float64)
+    off = (shape - 1) / 2 - rot @ ((shape - 1) / 2)
+    return c, s, float(off[0]), float(off[1])
+
+
+def rotate_planes(data, c, s, offz, offx, order=1):
+    """The geometric transform of scipy.ndimage (its published algorithm,
+    restated for spline orders 0 and 1, mode 'nearest'): every output pixel
+    (oz, ox) of each [nz, n] plane of data [k, nz, n] samples the input at
+    iz = (offz + oz c) + ox s, ix = (offx + oz (-s)) + ox c, clamped to
+    [0, len - 1]; order 1 weights (1 - t, 1 - (1 - t)); terms v * wz * wx
+    summed from 0 in the order (z0,x0), (z0,x1), (z1,x0), (z1,x1); float64
+    rounded to float32 once."""
+    data = np.asarray(data, dtype=np.float32)
+    k, nz, n = data.shape
+    oz = np.arange(nz, dtype=np.float64)[:, None]
+    ox = np.arange(n, dtype=np.float64)[None, :]
+    iz = (offz + oz * c) + ox * s
+    ix = (offx + oz * (-s)) + ox * c
+    iz = np.clip(iz, 0.0, nz - 1.0)
+    ix = np.clip(ix, 0.0, n - 1.0)
+    d = data.astype(np.float64)
+    if order == 0:
+        z0 = np.minimum(np.floor(iz + 0.5).astype(np.int64), nz - 1)
+        x0 = np.minimum(np.floor(ix + 0.5).astype(np.int64), n - 1)
+        return d[:, z0, x0].astype(np.float32)
+    if order != 1:
+        raise NotImplementedError("spline orders 0 and 1")
+    fz, fx = np.floor(iz), np.floor(ix)
+    z0, x0 = fz.astype(np.int64), fx.astype(np.int64)
+    z1, x1 = np.minimum(z0 + 1, nz - 1), np.minimum(x0 + 1, n - 1)
+    wz0 = 1.0 - (iz - fz)
+    wz1 = 1.0 - wz0
+    wx0 = 1.0 - (ix - fx)
+    wx1 = 1.0 - wx0
+    v = np.zeros((k, nz, n), dtype=np.float64)
+    v = v + d[:, z0, x0] * wz0 * wx0
+    v = v + d[:, z0, x1] * wz0 * wx1
+    v = v + d[:, z1, x0] * wz1 * wx0
+    v = v + d[:, z1, x1] * wz1 * wx1
+    return v.astype(np.float32)
+
+
+def rotate_proj(data, angle, order=1):
+    """ProcFunctions.rotate_proj (proc_functions.py:126-138) of [nproj, nz, n]."""
+    _, nz, n = np.shape(data)
+    return rotate_planes(data, *rotate_params(angle, nz, n), order=order)

@@ -87,6 +87,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_downsample": [vp, vp, i32, sz, sz, sz, sz, sz, i32, vp],
     "tcb_pad360_weights": [vp, sz],
     "tcb_pad360_rows": [vp, sz, sz, sz, i32, vp, sz, vp],
+    "tcb_rotate_proj": [vp, vp, sz, sz, sz, sz, sz, f64, f64, f64, f64, i32, vp],
     "tcb_dezinger": [vp, vp, i32, sz, sz, sz, sz, sz, i32, f64, vp],
     "tcb_stripe_ti_mask": [sz, f64, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "tcb_stripe_ti_create": [C.POINTER(vp), sz, sz, sz, f64, f64],

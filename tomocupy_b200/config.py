@@ -55,6 +55,7 @@ DEFAULTS = {
     "retrieve_phase_W": 2e-4,               # microns
     "retrieve_phase_pad": 1,
     "rotate_proj_angle": 0.0,
+    "rotate_proj_order": 1,
     "beam_hardening_method": "none",
     # laminography
     "lamino_angle": 0.0,

@@ -5,13 +5,13 @@
 ``darkflat_correction`` and ``minus_log`` run as native kernels with the
 reference's float32 operation order (bit-identical results), and so do
 ``remove_outliers`` (dezinger: a [w, 1, w] median, bit-identical on integer
-frames) and the phase-retrieval step of ``proc_proj``.  The other steps of
-that file (rotation, beam hardening, double-FOV padding) are outside this
-package's scope and raise ``NotImplementedError`` when enabled, instead of
-silently doing nothing.
+frames) and the phase-retrieval, rotation and double-FOV padding steps of
+``proc_proj``.  Beam hardening is outside this package's scope and raises
+``NotImplementedError`` when enabled, instead of silently doing nothing.
 """
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 from .. import _lib
@@ -60,6 +60,63 @@ def downsample(frames: torch.Tensor, binning: int, out=None, stream=None) -> tor
     _lib.call("tcb_downsample", _lib.ptr(out), _lib.ptr(frames), in_dtype_code(frames), k, nz, n,
               frames.stride(0), frames.stride(1), b, _lib.stream_ptr(stream))
     return out
+
+
+def rotate_params(angle: float, nz: int, n: int):
+    """(c, s, offz, offx) of ndimage.rotate(angle, axes=(2, 1), reshape=False)
+    on planes of nz x n, computed as the reference's cupyx call does on the
+    host: NumPy float64 deg2rad, cos, sin, and the offset that maps the
+    rotated plane centre onto the input's."""
+    a = np.deg2rad(float(angle))
+    c, s = float(np.cos(a)), float(np.sin(a))
+    rot = np.array([[c, s], [-s, c]])
+    shape = np.array([nz, n], dtype=np.float64)
+    off = (shape - 1) / 2 - rot @ ((shape - 1) / 2)
+    return c, s, float(off[0]), float(off[1])
+
+
+def rotate_proj(data: torch.Tensor, angle: float, order: int = 1, out=None,
+                stream=None) -> torch.Tensor:
+    """ProcFunctions.rotate_proj (proc_functions.py:126-138): every projection
+    of float32 data [nproj, nz, n] (device, rows contiguous) rotated by angle
+    degrees about its centre, ndimage.rotate(reshape=False, order,
+    axes=(2, 1), mode='nearest'); spline orders 0 and 1.  Returns a new
+    tensor (or out, which must not overlap data)."""
+    nproj, nz, n = data.shape
+    if data.dtype != torch.float32 or data.stride(2) != 1 or data.stride(1) != n:
+        raise ValueError("rotate_proj: float32 frames with contiguous rows of n samples")
+    if int(order) not in (0, 1):
+        raise NotImplementedError(f"rotate_proj: spline order {order} (orders 0 and 1)")
+    if out is None:
+        out = torch.empty((nproj, nz, n), dtype=torch.float32, device=data.device)
+    c, s, offz, offx = rotate_params(angle, nz, n)
+    _lib.call("tcb_rotate_proj", _lib.ptr(out), _lib.ptr(data), nproj, nz, n, data.stride(0),
+              out.stride(0), c, s, offz, offx, int(order), _lib.stream_ptr(stream))
+    return out
+
+
+def pad360_args():
+    """(flip, w) of pad360 (proc_functions.py:109-124) for a double-FOV scan, else None."""
+    if args.file_type != "double_fov":
+        return None
+    flip = params.centeri < params.ni // 2
+    return flip, max(1, int(2 * (params.ni - params.center)))
+
+
+def pad360(data: torch.Tensor, flip: bool, w: int) -> torch.Tensor:
+    """ProcFunctions.pad360 (proc_functions.py:109-124): float32 [nproj, nz, ni]
+    -> [nproj, nz, 2 ni], each row optionally flipped, its last w samples
+    times the smooth transition, zero-padded."""
+    import ctypes as C
+    nproj, nz, ni = data.shape
+    v = np.empty(int(w), dtype=np.float64)
+    _lib.call("tcb_pad360_weights", v.ctypes.data_as(C.c_void_p), int(w))
+    vd = torch.as_tensor(v, device=data.device)
+    padded = torch.empty((nproj, nz, 2 * ni), dtype=torch.float32, device=data.device)
+    padded[:, :, :ni] = data
+    _lib.call("tcb_pad360_rows", padded.data_ptr(), nproj * nz, ni, 2 * ni, int(flip),
+              vd.data_ptr(), int(w), _lib.stream_ptr(None))
+    return padded
 
 
 def dezinger_args():
@@ -207,17 +264,27 @@ class ProcFunctions:
             return res
         return out
 
+    def rotate_proj(self, data, angle, order=2):
+        """In place, like the reference's data[:] = ndimage.rotate(...)."""
+        data.copy_(rotate_proj(data.contiguous(), angle, order))
+        return data
+
+    def pad360(self, data):
+        """[nproj, nz, ni] -> [nproj, nz, 2 ni] for a double-FOV scan."""
+        return pad360(data.contiguous(), *pad360_args())
+
     def proc_proj(self, data, st=None, end=None, res=None):
         """Processing of a projection chunk (proc_functions.py:163-196): phase
-        retrieval, then -log (projection rotation and beam hardening are out of
-        scope)."""
+        retrieval, rotation, -log, double-FOV padding (beam hardening is out
+        of scope)."""
         data = retrieve_phase(data)
-        if args.rotate_proj_angle != 0:
-            raise NotImplementedError("projection rotation is not part of tomocupy_b200")
-        if args.file_type == "double_fov":
-            raise NotImplementedError("double_fov padding is not part of tomocupy_b200")
+        if float(args.rotate_proj_angle) != 0:
+            data = self.rotate_proj(data.contiguous(), args.rotate_proj_angle,
+                                    args.rotate_proj_order)
         if args.minus_log == "True":
             data = self.minus_log(data.contiguous())
+        if args.file_type == "double_fov":
+            data = self.pad360(data)
         if res is not None:
             res[:] = data
             return res

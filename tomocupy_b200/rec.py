@@ -20,7 +20,7 @@ import torch
 from .global_vars import args, params
 from .pipeline import SinoPipeline, copy2d_rows
 from .processing.proc_functions import (PHASE_METHODS, darkflat_stats, dezinger, dezinger_args,
-                                        prep_rows, retrieve_phase)
+                                        pad360_args, prep_rows, retrieve_phase, rotate_proj)
 
 
 def _supported():
@@ -45,19 +45,25 @@ def _stripe_args():
     return None
 
 
-def _pad360_args():
-    """(flip, w) of pad360 (proc_functions.py:109-124) for a double-FOV scan, else None."""
-    if args.file_type != "double_fov":
-        return None
-    flip = params.centeri < params.ni // 2
-    return flip, max(1, int(2 * (params.ni - params.center)))
+_pad360_args = pad360_args
 
 
 def _no_phase(where):
-    if args.retrieve_phase_method in PHASE_METHODS:
+    if args.retrieve_phase_method in PHASE_METHODS or _rotate():
         raise NotImplementedError(
-            f"{where}: phase retrieval filters whole projections; run GPURecSteps "
-            "(the reference applies it to the rows of each sinogram chunk here)")
+            f"{where}: phase retrieval and projection rotation work on whole "
+            "projections; run GPURecSteps (the reference applies them to the rows of "
+            "each sinogram chunk here)")
+
+
+def _rotate():
+    return float(args.rotate_proj_angle) != 0
+
+
+def _proj_chunk_ops():
+    """proc_proj steps that recon_all runs on each chunk's projections (phase
+    retrieval, rotation) before the pipeline's -log."""
+    return args.retrieve_phase_method in PHASE_METHODS or _rotate()
 
 
 class GPURec:
@@ -84,7 +90,7 @@ class GPURec:
         if self._pipe is None:
             # with phase retrieval the chunk's ring removal runs before it
             # (_phase_chunk), not in the pipeline
-            stripe = None if args.retrieve_phase_method in PHASE_METHODS else _stripe_args()
+            stripe = None if _proj_chunk_ops() else _stripe_args()
             self._pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                       params.center, args.fbp_filter,
                                       args.reconstruction_algorithm,
@@ -131,7 +137,7 @@ class GPURec:
 
     def recon_all(self):
         """Reconstruct every slice; results go to ``cl_writer`` (host or device)."""
-        phase = args.retrieve_phase_method in PHASE_METHODS
+        phase = _proj_chunk_ops()
         data, dark, flat = self.cl_reader.frames()
         ncz, n, nz, nproj = params.ncz, params.n, params.nz, params.nproj
         dev = self.device
@@ -258,6 +264,25 @@ class GPURec:
                 from .processing.remove_stripe import remove_stripe_ti
                 remove_stripe_ti(tmp, args.ti_beta, args.ti_mask)
             retrieve_phase(tmp)
+        if _rotate():
+            # the reference rotates its chunk buffer of ncz rows: a partial
+            # chunk is rotated at that height with zero rows below it
+            rb = getattr(self, "_rot_buf", None)
+            if rb is None or rb.shape[1] != nproj * params.ncz * n:
+                rb = self._rot_buf = torch.empty((2, nproj * params.ncz * n),
+                                                 dtype=torch.float32, device=self.device)
+            rin = rb[0].view(nproj, params.ncz, n)
+            rout = rb[1].view(nproj, params.ncz, n)
+            if lz < params.ncz:
+                with torch.cuda.stream(stream):
+                    rin.zero_()
+                    rin[:, :lz].copy_(tmp)
+                src_rot = rin
+            else:
+                src_rot = tmp
+            rotate_proj(src_rot, args.rotate_proj_angle, args.rotate_proj_order, out=rout,
+                        stream=stream)
+            return rout[:, :lz]
         return tmp
 
     def _recon_try_chunks(self):

@@ -62,8 +62,10 @@ class GPURecSteps:
         out = torch.empty((nproj, nz, n), dtype=torch.float32, device=dev)
         stripe = args.remove_stripe_method in ("fw", "ti")
         phase = args.retrieve_phase_method in PHASE_METHODS
-        # -log comes last: after ring removal (proc_sino) and phase retrieval (proc_proj)
-        late_log = stripe or phase
+        rotate = float(args.rotate_proj_angle) != 0
+        # -log comes last: after ring removal (proc_sino), phase retrieval and
+        # rotation (proc_proj)
+        late_log = stripe or phase or rotate
         prep_rows(out, data, d0, f0, darkflat=True,
                   minus_log=(args.minus_log == "True") and not late_log,
                   out_zstride=n, out_pstride=nz * n)
@@ -84,6 +86,9 @@ class GPURecSteps:
             raise NotImplementedError(f"remove_stripe_method={args.remove_stripe_method!r}")
         if phase:
             retrieve_phase(out)
+        if rotate:
+            from .processing.proc_functions import rotate_proj
+            out = rotate_proj(out, args.rotate_proj_angle, args.rotate_proj_order)
         if late_log and args.minus_log == "True":
             prep_rows(out, out, darkflat=False, minus_log=True, out_zstride=n,
                       out_pstride=nz * n)
@@ -94,19 +99,8 @@ class GPURecSteps:
     def _pad360(self, out):
         """proc_proj's pad360 (proc_functions.py:109-124, 190-193) of every
         projection row: [nproj, nz, ni] -> [nproj, nz, 2 ni]."""
-        import ctypes as C
-        from . import _lib
-        from .rec import _pad360_args
-        nproj, nz, ni = out.shape
-        flip, w = _pad360_args()
-        v = np.empty(w, dtype=np.float64)
-        _lib.call("tcb_pad360_weights", v.ctypes.data_as(C.c_void_p), w)
-        vd = torch.as_tensor(v, device=self.device)
-        padded = torch.empty((nproj, nz, 2 * ni), dtype=torch.float32, device=self.device)
-        padded[:, :, :ni] = out
-        _lib.call("tcb_pad360_rows", padded.data_ptr(), nproj * nz, ni, 2 * ni, int(flip),
-                  vd.data_ptr(), w, _lib.stream_ptr(None))
-        return padded
+        from .processing.proc_functions import pad360, pad360_args
+        return pad360(out, *pad360_args())
 
     # ------------------------------------------------------------------ driver
     def recon_steps_all(self):
@@ -122,13 +116,14 @@ class GPURecSteps:
     def _tomo(self):
         from .rec import GPURec
         rec = GPURec(self.cl_reader, self.cl_writer, device=self.device)
-        if args.retrieve_phase_method in PHASE_METHODS or args.file_type == "double_fov":
-            # phase retrieval needs whole projections, double-FOV padding
-            # follows it: pre-process the resident dataset (proc_sino +
-            # proc_proj), then backproject
+        if (args.retrieve_phase_method in PHASE_METHODS or args.file_type == "double_fov"
+                or float(args.rotate_proj_angle) != 0):
+            # phase retrieval and rotation need whole projections, double-FOV
+            # padding follows them: pre-process the resident dataset
+            # (proc_sino + proc_proj), then backproject
             if args.reconstruction_type != "full":
-                raise NotImplementedError("phase retrieval or double-FOV padding with "
-                                          "try-centre sweeps in the step driver")
+                raise NotImplementedError("phase retrieval, rotation or double-FOV padding "
+                                          "with try-centre sweeps in the step driver")
             return rec.recon_preprocessed(self.preprocessed())
         if args.reconstruction_type == "full":
             return rec.recon_all()
