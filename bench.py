@@ -613,6 +613,34 @@ def run_phase(a, dev, peaks, peaks_kind):
                             "kind": "port", "cores": 1,
                             "sample": f"1 projection {n}x{n} (NumPy complex64 fft2/ifft2 as "
                                       f"the reference), {cpu_s:.1f} s"}}
+    # projection rotation (rotate_proj, order 1, 1 degree) of the same stack:
+    # 8 algorithmic bytes per pixel (float32 read + write), 1 GiB in and out
+    from tomocupy_b200.processing.proc_functions import rotate_proj
+    for _ in range(3):
+        rotate_proj(x, 1.0, 1, out=y)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        rotate_proj(x, 1.0, 1, out=y)
+    e1.record()
+    torch.cuda.synchronize()
+    rms = e0.elapsed_time(e1) / reps
+    want = np_tomo.rotate_proj(x[:1].cpu().numpy(), 1.0, 1)
+    exact = bool(np.array_equal(y[:1].cpu().numpy(), want))
+    t0 = time.perf_counter()
+    np_tomo.rotate_proj(x[:1].cpu().numpy(), 1.0, 1)
+    rcpu = time.perf_counter() - t0
+    ragb = alg / (rms / 1e3) / 1e9
+    res["rotate"] = {
+        "workload": f"{P} projections {n}x{n} float32, 1 degree, spline order 1, 'nearest'",
+        "ms": round(rms, 3), "projections_per_s": round(P / (rms / 1e3), 1),
+        "roofline": {"bound": "hbm", "achieved": round(ragb, 1), "peak": peaks.get("hbm_gbs"),
+                     "unit": "GB/s", "frac": round(ragb / peaks["hbm_gbs"], 3)
+                     if peaks.get("hbm_gbs") else None, "peak_source": peaks_kind},
+        "bit_exact_vs_numpy_oracle_first_projection": exact,
+        "cpu_baseline": {"value": round(1.0 / rcpu, 3), "unit": "projections/s",
+                         "kind": "port", "cores": 1,
+                         "sample": f"1 projection {n}x{n} (NumPy float64), {rcpu:.2f} s"}}
     op.free()
     del x, y
     torch.cuda.empty_cache()

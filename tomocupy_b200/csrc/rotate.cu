@@ -18,8 +18,12 @@
 // float32 once.  The caller passes c, s and the offsets so that the host
 // decides the trigonometry (the reference computes them with NumPy).
 //
-// One thread per output pixel, x fastest: for the small roll angles this
+// One thread per output pixel (x fastest) and a run of frames: the float64
+// coordinates and weights, the costly part, are formed once per pixel and
+// reused for every frame of the run; for the small roll angles this
 // corrects, a warp's four taps fall on two nearly contiguous row segments.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace tcb {
@@ -63,6 +67,7 @@ __global__ void __launch_bounds__(128) rotate_kernel(float *__restrict__ out,
     z1 = min(z0 + 1, nz - 1);
     x1 = min(x0 + 1, n - 1);
   }
+#pragma unroll 2
   for (size_t f = blockIdx.z; f < nframes; f += gridDim.z) {
     const float *p = in + f * in_fstride;
     double v;
@@ -97,7 +102,11 @@ extern "C" int tcb_rotate_proj(float *out, const float *in, size_t nframes, size
                 nz, n, in_fstride, out_fstride);
   cudaStream_t st = (cudaStream_t)stream;
   StageTimer t("rotate_proj", st);
-  const dim3 grid(ceil_div(n, 128), (unsigned)nz, (unsigned)std::min<size_t>(nframes, 65535));
+  // frame runs: as few grid layers as keep about 64 CTAs per SM busy
+  const size_t plane_ctas = (size_t)ceil_div(n, 128) * nz;
+  const size_t layers = std::min<size_t>(
+      {nframes, (size_t)65535, std::max<size_t>(1, ceil_div(148 * 64, plane_ctas))});
+  const dim3 grid(ceil_div(n, 128), (unsigned)nz, (unsigned)layers);
   if (order == 0)
     rotate_kernel<0><<<grid, 128, 0, st>>>(out, in, nframes, (int)nz, (int)n, in_fstride,
                                            out_fstride, c, s, offz, offx);
