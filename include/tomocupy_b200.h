@@ -57,6 +57,16 @@ int tcb_profile_enable(int on);
 int tcb_profile_report(char *buf, size_t len);
 int tcb_launch_count(uint64_t *out);
 
+/* Failure-detection check (no counterpart in the reference, whose kernels
+ * have no waits).  Runs the bounded mbarrier wait that the tensor-core and
+ * TMA kernels use (tcb_tcfilter_status, tcb_fourierrec_status and
+ * tcb_linerec_status report its expiry) on an mbarrier that nothing
+ * arrives on, with a budget of budget_cycles SM clock cycles: *timed_out
+ * is 1 when the wait gave up (always, by construction) and *waited_cycles
+ * how long it waited.  Synchronous on the stream; the context stays usable. */
+int tcb_check_bounded_wait(long long budget_cycles, int *timed_out, long long *waited_cycles,
+                           void *stream);
+
 /* Asynchronous 2D copy (host<->device or device<->device, direction inferred
  * from the pointers): height rows of width_bytes, with row pitches in bytes.
  * The chunk conveyor uses it to move [nproj, ncz, n] slabs of a
@@ -370,6 +380,14 @@ int tcb_fourierrec_set_output(tcb_fourierrec *h, int precision);
  * FFT is skipped.  FLOAT32 handles only. */
 int tcb_fourierrec_set_input_spectrum(tcb_fourierrec *h, int on);
 int tcb_fourierrec_status(tcb_fourierrec *h, int *timed_out);
+/* Sample positions (test hook for bit-exact indexing): x, y fp32 [nproj, n]
+ * are the polar sample coordinates that takexy computes
+ * (src/include/kernels_fourierrec.cuh:23-36, same layout), fx, fy int32
+ * [nproj, n] the floor(2n x), floor(2n y) that place each sample's 9 x 9
+ * footprint (kernels_fourierrec.cuh:84-85 adds -m), all as the gridding
+ * kernels of this handle compute them. */
+int tcb_fourierrec_sample_positions(tcb_fourierrec *h, float *x, float *y, int *fx, int *fy,
+                                    void *stream);
 int tcb_fourierrec_destroy(tcb_fourierrec *h);
 
 /* ------------------------------------------------------------------------
@@ -452,6 +470,12 @@ int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1, const float *
  * caller's and must outlive the calls. */
 int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision, const float *in_scale,
                             float *out_inv_scale);
+/* Sample positions (test hook for bit-exact indexing): x, y fp32
+ * [ntheta, deth, detw] as take_x computes them for chunk k and full height
+ * deth0 (src/include/kernels_usfft2d.cu:5-18, same layout), with the
+ * arithmetic of this handle's gridding kernel. */
+int tcb_usfft2d_sample_positions(tcb_usfft2d *h, float *x, float *y, const float *theta,
+                                 float phi, int k, int deth0, void *stream);
 int tcb_usfft2d_destroy(tcb_usfft2d *h);
 
 /* Replaces cfunc_usfft1d (src/include/cfunc_usfft1d.cuh:7-34,

@@ -117,6 +117,110 @@ def remove_stripe_ti(data, beta, mask_size):
 
 
 # --------------------------------------------------------------------------
+# Fourier-wavelet ring removal (src/tomocupy/processing/remove_stripe.py:51-293)
+# --------------------------------------------------------------------------
+def _fw_sym_index(m1, length, m2):
+    """Indices -m1 .. length+m2-1 folded into [0, length) by the half-sample
+    symmetric reflection of _reflect/_mypad (remove_stripe.py:51-88)."""
+    x = np.arange(-m1, length + m2)
+    period = 2 * length
+    r = np.mod(x, period)
+    return np.where(r >= length, period - 1 - r, r)
+
+
+def _fw_coeff_len(n, L):
+    """pywt.dwt_coeff_len(n, L, 'symmetric') = floor((n + L - 1) / 2)."""
+    return (n + L - 1) // 2
+
+
+def _fw_analysis(x, lo, hi, axis):
+    """afb1d (remove_stripe.py:90-126): symmetric pad, stride-2 correlation with
+    the time-reversed taps, tap by tap in float32 (product, then sum: no
+    fused multiply-add); returns (low, high) along ``axis`` (2 or 3)."""
+    L = lo.size
+    N = x.shape[axis]
+    out = _fw_coeff_len(N, L)
+    p = 2 * (out - 1) - N + L
+    x = np.take(x, _fw_sym_index(p // 2, N, (p + 1) // 2), axis=axis)
+
+    def tap(j):
+        sl = [slice(None)] * 4
+        sl[axis] = slice(j, j + 2 * out, 2)
+        return x[tuple(sl)]
+    a = lo[0] * tap(0)
+    b = hi[0] * tap(0)
+    for j in range(1, L):
+        s = tap(j)
+        a = a + lo[j] * s
+        b = b + hi[j] * s
+    return a.astype(np.float32), b.astype(np.float32)
+
+
+def _fw_synthesis(lo, hi, g0, g1, axis):
+    """sfb1d (remove_stripe.py:129-154): zero-initialised upsampled scatter of
+    g0[j]*lo + g1[j]*hi at offsets j, j+2, ... then the crop of L-2 samples on
+    each side, float32 throughout."""
+    L = g0.size
+    H = lo.shape[axis]
+    full = (H - 1) * 2 + L
+    shape = list(lo.shape)
+    shape[axis] = full
+    out = np.zeros(shape, dtype=np.float32)
+    for j in range(L):
+        sl = [slice(None)] * 4
+        sl[axis] = slice(j, j + 2 * H, 2)
+        out[tuple(sl)] += g0[j] * lo + g1[j] * hi
+    sl = [slice(None)] * 4
+    sl[axis] = slice(L - 2, full - (L - 2))
+    return out[tuple(sl)]
+
+
+def remove_stripe_fw(data, sigma, level, bank):
+    """remove_stripe_fw on float32 [nproj, nz, n] (returns a new array).
+
+    ``bank`` = (dec_lo, dec_hi, rec_lo, rec_hi) of the wavelet (PyWavelets'
+    filter-bank convention).  The sinogram stack is zero-padded along the
+    angles to nproj + nproj//8 (centred), decomposed ``level`` times (rows
+    along the detector first, then columns along the angles); at every level
+    the band that is high-pass along the detector and low-pass along the
+    angles is damped along the angles by 1 - exp(-y^2 / (2 sigma^2)) in the
+    rfft domain; then the inverse transform and the crop.  Same float32
+    operation order as the reference run with NumPy for CuPy."""
+    dec_lo, dec_hi, rec_lo, rec_hi = (np.asarray(b, dtype=np.float64) for b in bank)
+    h0 = dec_lo.astype(np.float32)[::-1].copy()
+    h1 = dec_hi.astype(np.float32)[::-1].copy()
+    g0 = rec_lo.astype(np.float32)
+    g1 = rec_hi.astype(np.float32)
+    data = np.asarray(data, dtype=np.float32)
+    nproj, nz, ni = data.shape
+    npad = nproj + nproj // 8
+    sli = np.zeros((nz, 1, npad, ni), dtype=np.float32)
+    sli[:, 0, (npad - nproj) // 2:(npad + nproj) // 2] = data.swapaxes(0, 1)
+    bands = []
+    for _ in range(level):
+        rlo, rhi = _fw_analysis(sli, h0, h1, axis=3)     # along the detector
+        ll, lh = _fw_analysis(rlo, h0, h1, axis=2)       # along the angles
+        hl, hh = _fw_analysis(rhi, h0, h1, axis=2)
+        # yh[:, 0, 0..2] = (low-row/high-col, high-row/low-col, high/high)
+        band = hl[:, 0]
+        my = band.shape[1]
+        spec = np.fft.rfft(band, axis=1)
+        yhat = np.fft.ifftshift((np.arange(-my, my, 2) + 1) / 2)[:my // 2 + 1]
+        spec *= (-np.expm1(-yhat ** 2 / (2 * sigma ** 2)))[:, None]
+        hl = np.fft.irfft(spec, my, axis=1).astype(np.float32)[:, None]
+        bands.append((lh, hl, hh))
+        sli = ll
+    for lh, hl, hh in bands[::-1]:
+        h, w = hl.shape[2], hl.shape[3]
+        sli = sli[:, :, :h, :w]
+        lo_hi = _fw_synthesis(np.concatenate([sli, hl], axis=1), np.concatenate([lh, hh], axis=1),
+                              g0, g1, axis=2)
+        sli = _fw_synthesis(lo_hi[:, :1], lo_hi[:, 1:], g0, g1, axis=3)
+    out = sli[:, 0, (npad - nproj) // 2:(npad + nproj) // 2, :ni]
+    return np.ascontiguousarray(out.swapaxes(0, 1)).astype(np.float32)
+
+
+# --------------------------------------------------------------------------
 # phase retrieval (src/tomocupy/processing/retrieve_phase.py:57-305)
 # --------------------------------------------------------------------------
 _PR_PLANCK = 6.58211928e-19   # retrieve_phase.py:45-48

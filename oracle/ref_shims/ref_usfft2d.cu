@@ -18,3 +18,15 @@ void ref_adj(void *h, size_t f, size_t g, size_t theta, float phi, int k, int de
 void ref_destroy(void *h) { delete static_cast<cfunc_usfft2d *>(h); }
 int ref_last_error(void) { return (int)cudaGetLastError(); }
 }
+
+// The reference's own take_x kernel (kernels_usfft2d.cu:5-18), launched with
+// the operator's launch shape (cfunc_usfft2d.cu:37-40) into the caller's
+// x, y [ntheta, deth, detw].
+extern "C" void ref_take_x(size_t x, size_t y, size_t theta, float phi, int k, int deth0,
+                           int detw, int deth, int ntheta, size_t stream) {
+  dim3 BS2d(16, 8, 8);
+  dim3 GS2d2(ceil(detw / (float)BS2d.x), ceil(deth / (float)BS2d.y),
+             ceil(ntheta / (float)BS2d.z));
+  take_x<<<GS2d2, BS2d, 0, (cudaStream_t)stream>>>((float *)x, (float *)y, (float *)theta, phi,
+                                                   k, deth0, detw, deth, ntheta);
+}

@@ -22,7 +22,8 @@ _libs: dict = {}
 vp, sz, f32, i32 = C.c_void_p, C.c_size_t, C.c_float, C.c_int
 
 _SIGS = {
-    "fourierrec": {"ref_create": ([sz, sz, sz, sz], vp), "ref_backprojection": ([vp, sz, sz, sz], None)},
+    "fourierrec": {"ref_create": ([sz, sz, sz, sz], vp), "ref_backprojection": ([vp, sz, sz, sz], None),
+                   "ref_takexy": ([sz, sz, sz, sz, sz, sz], None)},
     "filter": {"ref_create": ([sz, sz, sz], vp), "ref_filter": ([vp, sz, sz, sz], None)},
     "linerec": {"ref_create": ([sz, sz, sz, sz, sz], vp),
                 "ref_backprojection": ([vp, sz, sz, sz, f32, i32, sz], None),
@@ -34,7 +35,8 @@ _SIGS = {
     "usfft1d": {"ref_create": ([sz, sz, sz, sz], vp), "ref_fwd": ([vp, sz, sz, f32, sz], None),
                 "ref_adj": ([vp, sz, sz, f32, sz], None)},
     "usfft2d": {"ref_create": ([sz] * 6, vp), "ref_fwd": ([vp, sz, sz, sz, f32, i32, i32, sz], None),
-                "ref_adj": ([vp, sz, sz, sz, f32, i32, i32, sz], None)},
+                "ref_adj": ([vp, sz, sz, sz, f32, i32, i32, sz], None),
+                "ref_take_x": ([sz, sz, sz, f32, i32, i32, i32, i32, i32, sz], None)},
     "fft2d": {"ref_create": ([sz, sz, sz], vp), "ref_fwd": ([vp, sz, sz, sz], None)},
 }
 

@@ -128,9 +128,10 @@ def test_double_fov_try_sweep_matches_reference_chain(cuda, ref):
             assert err < 1e-4, (k + kk, err)
 
 
-@pytest.mark.parametrize("axis,stripe", [(118.0, "none"), (9.5, "none"), (118.0, "fw"),
-                                         (9.5, "ti")])
-def test_step_driver_double_fov_matches_recon_all(cuda, axis, stripe):
+@pytest.mark.parametrize("axis,stripe,dz", [(118.0, "none", 0), (9.5, "none", 0),
+                                            (118.0, "fw", 0), (9.5, "ti", 0),
+                                            (118.0, "none", 3), (9.5, "ti", 5)])
+def test_step_driver_double_fov_matches_recon_all(cuda, axis, stripe, dz):
     """GPURecSteps pads whole pre-processed projections (pad360 after -log) and
     backprojects; GPURec.recon_all pads each chunk's filter rows.  Ring
     removal runs on the ni-wide sinograms before the padding in both
@@ -143,9 +144,12 @@ def test_step_driver_double_fov_matches_recon_all(cuda, axis, stripe):
     nproj, nz, ni = 120, 8, 96
     theta = np.linspace(0, 2 * np.pi, nproj, endpoint=False).astype(np.float32)
     data, dark, flat, _, _ = synthetic.make_dataset(nproj, nz, ni, seed=9, theta=theta)
+    if dz:  # outlier removal runs on the ni-wide raw frames before the padding
+        data = data.clone()
+        data.view(-1)[torch.as_tensor(np.random.default_rng(2).integers(0, data.numel(), 200))] = 60000
     opts = dict(reconstruction_algorithm="fourierrec", nsino_per_chunk=4,
                 file_type="double_fov", rotation_axis=axis, remove_stripe_method=stripe,
-                fw_level=4)
+                fw_level=4, dezinger=dz)
     global_vars.reset(**opts)
     w1 = ArrayWriter(device="cuda")
     GPURec(ArrayReader(data, dark, flat, theta=theta), w1).recon_all()

@@ -120,6 +120,7 @@ FR_CASES = [
     (200, 120, 3, "random"),   # 2n not a multiple of the tile: partial tiles
     (256, 401, 1, "random"),
     (2048, 150, 2, "uniform"),  # 2n = 4096: the production FFT length
+    (2048, 1500, 4, "uniform"),  # the production geometry: 2048 columns x 1500 angles
     (4096, 64, 1, "random"),    # 2n = 8192: radix-16^3 x 2
 ]
 
@@ -214,19 +215,25 @@ def test_fourierrec_backprojection_slices_matches_dropin(cuda):
     assert rel_l2(fs[nz:].cpu(), fc[..., 1].cpu()) < 1e-6
 
 
-def test_fourierrec_deterministic(cuda):
-    from tomocupy_b200 import cfunc_fourierrec
-    n, nproj, nz = 256, 180, 2
+@pytest.mark.parametrize("n,nproj,nz", [(256, 180, 2), (512, 360, 40)])
+def test_fourierrec_deterministic(cuda, n, nproj, nz):
+    """Both gridding modes sum in a fixed order (registers or TMEM, no atomics)
+    and every other stage is a fixed sequence of operations: two runs are
+    bit-identical."""
+    from tomocupy_b200 import _lib, cfunc_fourierrec
     theta = torch.as_tensor(_theta(nproj), device=cuda)
-    op = cfunc_fourierrec.cfunc_fourierrec(nproj, nz, n, theta)
     g = torch.randn((nz, nproj, n, 2), device=cuda)
-    outs = []
-    for _ in range(2):
-        f = torch.empty((nz, n, n, 2), device=cuda)
-        op.backprojection(f, g.clone(), None)
-        outs.append(f.cpu())
-    # shared-memory atomics make the order vary only inside one tile: tiny diffs
-    assert rel_l2(outs[0], outs[1]) < 1e-6
+    for mode in (_lib.GRID_FP32, _lib.GRID_TENSOR):
+        op = cfunc_fourierrec.cfunc_fourierrec(nproj, nz, n, theta)
+        op.set_gridding(mode)
+        outs = []
+        for _ in range(2):
+            f = torch.empty((nz, n, n, 2), device=cuda)
+            op.backprojection(f, g.clone(), None)
+            outs.append(f.cpu())
+        assert not op.timed_out()
+        op.free()
+        assert torch.equal(outs[0], outs[1]), mode
 
 
 def test_fourierrec_fp16_vs_fp64(cuda):

@@ -158,12 +158,11 @@ def test_recon_all_ring_removal_then_phase_matches_reference(cuda, ref):
     """recon_all with Titarenko ring removal and Paganin phase retrieval: per
     chunk dark/flat -> ring removal -> phase retrieval -> -log (proc_sino then
     proc_proj), against the same order with the restated phase retrieval
-    (the ring removal itself is checked against the reference's
-    remove_stripe_ti in tests/test_gpu_stripe.py)."""
+    (the NumPy restatement of the ring removal reproduces the reference's
+    remove_stripe_ti fixtures bit for bit, tests/test_stripe_ti_cpu.py)."""
     from oracle import np_tomo
     from tomocupy_b200 import global_vars, synthetic
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
-    from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
     from tomocupy_b200.rec import GPURec
     nproj, nz, n, ncz = 90, 16, 128, 8
     data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=13, stripes=6)
@@ -181,8 +180,54 @@ def test_recon_all_ring_removal_then_phase_matches_reference(cuda, ref):
     for z0 in range(0, nz, ncz):
         sl = slice(z0, z0 + ncz)
         pre = np_tomo.darkflat(data[:, sl].numpy(), dark[:, sl].numpy(), flat[:, sl].numpy())
-        pre = remove_stripe_ti(torch.as_tensor(pre, device=cuda), 0.022, 1).cpu().numpy()
+        pre = np_tomo.remove_stripe_ti(pre, 0.022, 1)
         pre = np_tomo.minus_log(np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3))
+        d = torch.as_tensor(np.ascontiguousarray(pre.transpose(1, 0, 2)), device=cuda)
+        d = ref.ref_fbp_filter_center(filt, d, wf, t, n / 2, torch.zeros(ncz, device=cuda), n, ne)
+        theirs = torch.zeros((ncz, n, n), device=cuda)
+        rec.backprojection(theirs, d)
+        err = rel_l2(w.rec[sl].cpu(), theirs.cpu())
+        assert err < 1e-4, (z0, err)
+
+
+@pytest.mark.parametrize("rotate", [False, True])
+def test_recon_all_dezinger_then_phase_matches_reference(cuda, ref, rotate):
+    """recon_all with outlier removal and Paganin phase retrieval (and
+    projection rotation): the raw frames, darks and flats lose their outliers
+    before dark/flat correction (proc_sino, proc_functions.py:146-148), then
+    the chunk's phase retrieval and rotation, -log, filter, fourierrec.
+    Against the restated chain (oracle dezinger, dark/flat, Paganin, rotate)
+    feeding the reference's CUDA filter and fourierrec."""
+    from oracle import np_tomo
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    nproj, nz, n, ncz = 90, 16, 128, 8
+    data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=14)
+    rng = np.random.default_rng(3)
+    data = data.clone()
+    idx = rng.integers(0, data.numel(), 300)
+    data.view(-1)[torch.as_tensor(idx)] = 60000   # zingers
+    opts = dict(rotate_proj_angle=1.5, rotate_proj_order=1) if rotate else {}
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=ncz, dezinger=3,
+                      dezinger_threshold=5000, retrieve_phase_method="paganin",
+                      pixel_size=0.65, propagation_distance=50.0, energy=20.0,
+                      retrieve_phase_alpha=1e-3, **opts)
+    w = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(data, dark, flat, theta=theta), w).recon_all()
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, "parzen"), device=cuda)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=cuda)
+    filt = ref.RefFilter(ne, nproj, ncz)
+    rec = ref.RefFourierRec(n, nproj, ncz, torch.as_tensor(theta, device=cuda))
+    for z0 in range(0, nz, ncz):
+        sl = slice(z0, z0 + ncz)
+        raw, dk, fl = (np_tomo.dezinger(a[:, sl].numpy(), 3, 5000.0) for a in (data, dark, flat))
+        pre = np_tomo.darkflat(raw, dk, fl)
+        pre = np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3)
+        if rotate:
+            pre = np_tomo.rotate_proj(pre, 1.5, 1)
+        pre = np_tomo.minus_log(pre)
         d = torch.as_tensor(np.ascontiguousarray(pre.transpose(1, 0, 2)), device=cuda)
         d = ref.ref_fbp_filter_center(filt, d, wf, t, n / 2, torch.zeros(ncz, device=cuda), n, ne)
         theirs = torch.zeros((ncz, n, n), device=cuda)

@@ -49,17 +49,17 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
         # bit-exact with the native kernel), -log with the device logf
         d = np_tomo.darkflat(np.asarray(data[:, z0:z0 + ncz]), np.asarray(dark[:, z0:z0 + ncz]),
                              np.asarray(flat[:, z0:z0 + ncz]))
-        d = torch.as_tensor(np.ascontiguousarray(d), device=dev)
+        # proc_sino: ring removal on the dark/flat corrected frames with the
+        # NumPy restatements, which reproduce the reference's remove_stripe_ti
+        # and remove_stripe_fw fixtures bit for bit (tests/test_stripe_*_cpu.py);
+        # then proc_proj: -log
         if stripe is not None and stripe[0] == "ti":
-            # Titarenko's method (checked on its own against the reference's
-            # remove_stripe_ti in tests/test_gpu_stripe.py)
-            from tomocupy_b200.processing.remove_stripe import remove_stripe_ti
-            d = remove_stripe_ti(d.contiguous(), stripe[1], stripe[2])
+            d = np_tomo.remove_stripe_ti(d, stripe[1], stripe[2])
         elif stripe is not None:
-            # proc_sino: ring removal on the dark/flat corrected frames (checked on
-            # its own against the reference's remove_stripe_fw), then proc_proj: -log
-            from tomocupy_b200.processing.remove_stripe import remove_stripe_fw
-            d = remove_stripe_fw(d.contiguous(), *stripe)
+            from tomocupy_b200.processing import wavelets
+            sigma, wname, level = stripe
+            d = np_tomo.remove_stripe_fw(d, sigma, level, wavelets.filter_bank(wname))
+        d = torch.as_tensor(np.ascontiguousarray(d), device=dev)
         d = torch.where(d <= 0, torch.ones((), device=dev), d)
         d = torch.nan_to_num(-torch.log(d), nan=6.0, posinf=0.0, neginf=0.0)
         d = d.permute(1, 0, 2).contiguous()
@@ -332,3 +332,21 @@ def test_c1_mixed_fp16_output_vs_fp64_oracle(cuda, c1):
     assert e16 < 1e-3, e16
     # the fp16 rounding of the output is the only difference
     assert rel_l2(out16.float(), out32) < 5e-4
+
+
+def test_production_geometry_vs_fp64_oracle(cuda):
+    """2048 columns x 1500 angles (the production geometry), 4 rows = 2 slice
+    pairs: the fp32 path and the mixed-precision path against the FP64
+    oracle of the same algorithm (fp32 <= 1e-4, mixed <= 1e-3), and mixed
+    against fp32."""
+    from tomocupy_b200 import synthetic
+    n, nproj, nz = 2048, 1500, 4
+    d, dk, fl, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=5)
+    fp32 = run_ours(d, dk, fl, theta, ncz=nz, host=False).numpy()
+    mixed = run_ours(d, dk, fl, theta, ncz=nz, host=False, dtype="mixed").numpy()
+    want = _fp64_fourierrec(d, dk, fl, theta, n)
+    e32, emix = rel_l2(fp32, want), rel_l2(mixed, want)
+    print(f"2048x1500: fp32 vs FP64 {e32:.2e}, mixed vs FP64 {emix:.2e}, "
+          f"mixed vs fp32 {rel_l2(mixed, fp32):.2e}")
+    assert e32 < 1e-4, e32
+    assert emix < 1e-3, emix

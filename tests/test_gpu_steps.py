@@ -57,16 +57,27 @@ def test_steps_lamino_linerec_full_matches_reference(cuda, ref):
     assert err < 1e-5, err
 
 
-def test_steps_lamino_fourierrec_runs(cuda):
-    """recon_steps_all dispatches laminography + fourierrec to the Fourier chain."""
+def test_steps_lamino_fourierrec_matches_reference(cuda, ref):
+    """recon_steps_all dispatches laminography + fourierrec to the Fourier
+    chain: the reference's rec_lam (its operators behind the restated glue)
+    on the same dark/flat-corrected, -log projections."""
+    from oracle import np_tomo
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import args, params
     from tomocupy_b200.rec_steps import GPURecSteps
-    nproj, nz, n = 48, 64, 64
+    nproj, nz, n, tilt = 48, 64, 64, 30.0
     data, dark, flat, theta, _ = _data(nproj, nz, n)
     global_vars.reset(reconstruction_algorithm="fourierrec", reconstruction_type="full",
-                      lamino_angle=30.0, nsino_per_chunk=8, nproj_per_chunk=8,
+                      lamino_angle=tilt, nsino_per_chunk=8, nproj_per_chunk=8,
                       lamino_end_row=32)
     u = GPURecSteps(ArrayReader(data, dark, flat, theta=theta),
-                    ArrayWriter(device="cuda")).recon_steps_all()
+                    ArrayWriter(device="cuda")).recon_steps_all().cpu()
     assert tuple(u.shape) == (32, n, n) and torch.isfinite(u).all()
+    dev = torch.device("cuda")
+    d = ref.ref_darkflat_minus_log(data.to(dev), dark.to(dev), flat.to(dev))  # [P, nz, n]
+    wf = torch.as_tensor(np_tomo.calc_filter(4 * n, args.fbp_filter), device=dev)
+    theirs = ref.ref_rec_lam(d.contiguous(), torch.as_tensor(theta, device=dev), params.center,
+                             tilt, params.rh, wf, nthetac=8, dethc=8, n1c=8).cpu()
+    err = rel_l2(u, theirs)
+    assert err < 1e-5, err

@@ -61,6 +61,7 @@ vp, sz, f32, i32, u32, f64 = C.c_void_p, C.c_size_t, C.c_float, C.c_int, C.c_uin
 SIGNATURES: dict[str, list] = {
     "tcb_version": [],
     "tcb_copy2d": [vp, sz, vp, sz, sz, sz, vp],
+    "tcb_check_bounded_wait": [C.c_longlong, C.POINTER(i32), C.POINTER(C.c_longlong), vp],
     "tcb_profile_enable": [i32],
     "tcb_profile_report": [C.c_char_p, sz],
     "tcb_launch_count": [C.POINTER(C.c_uint64)],
@@ -105,6 +106,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_fourierrec_set_pairs_per_block": [vp, i32],
     "tcb_fourierrec_set_gridding": [vp, i32],
     "tcb_fourierrec_status": [vp, C.POINTER(i32)],
+    "tcb_fourierrec_sample_positions": [vp, vp, vp, vp, vp, vp],
     "tcb_fourierrec_set_output": [vp, i32],
     "tcb_fourierrec_set_input_spectrum": [vp, i32],
     "tcb_fourierrec_destroy": [vp],
@@ -125,6 +127,7 @@ SIGNATURES: dict[str, list] = {
     "tcb_usfft2d_adj": [vp, vp, vp, vp, f32, i32, i32, vp],
     "tcb_usfft2d_adj_rows": [vp, vp, vp, vp, f32, i32, i32, i32, vp],
     "tcb_usfft2d_set_storage": [vp, i32, vp, vp],
+    "tcb_usfft2d_sample_positions": [vp, vp, vp, vp, f32, i32, i32, vp],
     "tcb_usfft2d_destroy": [vp],
     "tcb_usfft1d_create": [C.POINTER(vp), sz, sz, sz, sz],
     "tcb_usfft1d_adj": [vp, vp, vp, f32, vp],

@@ -61,6 +61,21 @@ class cfunc_fourierrec:
         self._check()
         _lib.call("tcb_fourierrec_set_input_spectrum", self._h, int(bool(on)))
 
+    def sample_positions(self):
+        """(x, y, fx, fy) [nproj, n]: the polar sample coordinates (takexy's) and
+        the floor(2n x), floor(2n y) that place the footprints, as the gridding
+        kernels compute them (a test hook; not in the reference)."""
+        import torch
+        self._check()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        x = torch.empty((self._nproj, self._n), dtype=torch.float32, device=dev)
+        y = torch.empty_like(x)
+        fx = torch.empty((self._nproj, self._n), dtype=torch.int32, device=dev)
+        fy = torch.empty_like(fx)
+        _lib.call("tcb_fourierrec_sample_positions", self._h, x.data_ptr(), y.data_ptr(),
+                  fx.data_ptr(), fy.data_ptr(), _lib.stream_ptr(None))
+        return x, y, fx, fy
+
     def timed_out(self) -> bool:
         """True when a tensor-core gridding wait gave up (synchronises)."""
         import ctypes as C

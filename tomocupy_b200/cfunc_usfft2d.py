@@ -31,5 +31,12 @@ class cfunc_usfft2d(NativeHandle):
         fp16, with optional per-angle / per-row power-of-two scale arrays."""
         _lib.call("tcb_usfft2d_set_storage", self._live(), int(precision), _lib.ptr(in_scale), _lib.ptr(out_inv_scale))
 
+    def sample_positions(self, x, y, theta_, phi, k, deth0, stream_):
+        """x, y fp32 [ntheta, deth, detw] <- the sample positions take_x computes
+        for chunk k, as the gridding kernel computes them (a test hook; not in
+        the reference)."""
+        _lib.call("tcb_usfft2d_sample_positions", self._live(), _lib.ptr(x), _lib.ptr(y),
+                  _lib.ptr(theta_), float(phi), int(k), int(deth0), _lib.stream_ptr(stream_))
+
     def fwd(self, *a, **k):
         raise NotImplementedError("usfft2d forward is not on the reconstruction path")

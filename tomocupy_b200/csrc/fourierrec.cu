@@ -1523,6 +1523,37 @@ extern "C" int tcb_fourierrec_pack(tcb_fourierrec *h, void *g, const void *src,
   return TCB_OK;
 }
 
+// Sample positions and footprint origins exactly as the gridding kernels use
+// them (sample_pos), one per (angle p, radial index i), in takexy's layout
+// [p * n + i].
+__global__ void sample_positions_kernel(float *__restrict__ x, float *__restrict__ y,
+                                        int *__restrict__ fx, int *__restrict__ fy,
+                                        const float2 *__restrict__ cs,
+                                        const float *__restrict__ rtab, int n, int nproj) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)n * nproj) return;
+  float x0, y0;
+  int ox, oy;
+  sample_pos(cs, rtab, (int)(i / n), (int)(i % n), (float)(2 * n), x0, y0, ox, oy);
+  x[i] = x0;
+  y[i] = y0;
+  fx[i] = ox;
+  fy[i] = oy;
+}
+
+extern "C" int tcb_fourierrec_sample_positions(tcb_fourierrec *h, float *x, float *y, int *fx,
+                                               int *fy, void *stream) {
+  TCB_CHECK_ARG(h && x && y && fx && fy, "tcb_fourierrec_sample_positions: null pointer");
+  TCB_CHECK_ARG(h->grid, "tcb_fourierrec_sample_positions: handle was freed");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t total = h->n * h->nproj;
+  sample_positions_kernel<<<ceil_div(total, 256), 256, 0, s>>>(x, y, fx, fy, h->cs, h->rtab,
+                                                               (int)h->n, (int)h->nproj);
+  TCB_LAUNCH_CHECK();
+  count_launch();
+  return TCB_OK;
+}
+
 extern "C" int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs) {
   TCB_CHECK_ARG(h, "tcb_fourierrec_set_pairs_per_block: null handle");
   TCB_CHECK_ARG(pairs == 0 || pairs == 2 || pairs == 4 || pairs == 8 || pairs == 16,

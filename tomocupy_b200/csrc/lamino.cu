@@ -82,7 +82,6 @@ struct U2Geom {
   int ntheta, detw, deth;   // deth = rows of this call (slabs)
   int ntx, nty;             // tiles per axis
   int k, deth0;             // chunk index and full detector height (kv)
-  float cphi;
   float wscale;             // PI / sqrt(mu0 mu1 ntheta)
   float c0, c1;             // -PI^2/mu0, -PI^2/mu1
   // sample source
@@ -137,13 +136,14 @@ __device__ __forceinline__ void interval(float c, float a, float b, float &lo, f
   hi = fmaxf(u0, u1);
 }
 
-// Sample position as take_x computes it (kernels_usfft2d.cu:5-18).
-__device__ __forceinline__ void u2_pos(const U2Geom &g, float2 csa, int tx, int ty, float &x,
-                                       float &y) {
+// Sample position as take_x computes it (kernels_usfft2d.cu:5-18); cphi is
+// the device cosf(phi), as there (u2_tables stores it after the angles).
+__device__ __forceinline__ void u2_pos(const U2Geom &g, float cphi, float2 csa, int tx, int ty,
+                                       float &x, float &y) {
   float ku = (tx - g.detw / 2.0f) / g.detw;
   float kv = (ty + g.k * g.deth - g.deth0 / 2.0f) / g.deth0;
-  x = ku * csa.x + kv * csa.y * g.cphi;
-  y = ku * csa.y - kv * csa.x * g.cphi;
+  x = ku * csa.x + kv * csa.y * cphi;
+  y = ku * csa.y - kv * csa.x * cphi;
   x = (float)fmin(fmax((double)x, -0.5f + 1e-5), 0.5f - 1e-5);
   y = (float)fmin(fmax((double)y, -0.5f + 1e-5), 0.5f - 1e-5);
 }
@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(NT) u2_gather(const S *__restrict__ src,
   const bool edge_y = (Y0 <= -n1 + M1 + 2) || (Y0 + th - 1 >= n1 - 1 - M1 - 2);
   const float kv = (slab + geo.k * geo.deth - geo.deth0 / 2.0f) / geo.deth0;
   const int detw = geo.detw;
+  const float cphi = cs[geo.ntheta].x;
 
   for (int pc = 0; pc < geo.ntheta; pc += CHUNK) {
     int p = pc + threadIdx.x;
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(NT) u2_gather(const S *__restrict__ src,
     int nseg = 0, ncand = 0;
     if (p < geo.ntheta) {
       float2 csp = cs[p];
-      float ox = kv * csp.y * geo.cphi, oy = -kv * csp.x * geo.cphi;
+      float ox = kv * csp.y * cphi, oy = -kv * csp.x * cphi;
       for (int ky = ky_lo; ky <= ky_hi; ky++)
         for (int kx = kx_lo; kx <= kx_hi; kx++) {
           float lo = -3.0e38f, hi = 3.0e38f, l, h;
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(NT) u2_gather(const S *__restrict__ src,
       int img = a >> 20, ang = a & 0xFFFFF;
       int tx = sm.seg_i0[lo] + (j - sm.seg_start[lo]);
       float x0, y0;
-      u2_pos(geo, cs[ang], tx, slab, x0, y0);
+      u2_pos(geo, cphi, cs[ang], tx, slab, x0, y0);
       int b0 = (int)floorf(2 * n0 * x0) - M0;
       int b1 = (int)floorf(2 * n1 * y0) - M1;
       int kx = img % 3 - 1, ky = img / 3 - 1;
@@ -329,11 +330,14 @@ __global__ void __launch_bounds__(NT) u2_gather(const S *__restrict__ src,
   }
 }
 
+// cs[0, ntheta): cos/sin of the angles; cs[ntheta].x: cos(phi), all with the
+// device cosf/sinf that take_x calls (kernels_usfft2d.cu:14-15).
 __global__ void u2_tables(float2 *__restrict__ cs, float *__restrict__ ex, float *__restrict__ ey,
-                          const float *__restrict__ theta, int ntheta, int n0, int m0, int n1,
-                          int m1) {
+                          const float *__restrict__ theta, float phi, int ntheta, int n0, int m0,
+                          int n1, int m1) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < ntheta) cs[t] = make_float2(cosf(theta[t]), sinf(theta[t]));
+  if (t == 0) cs[ntheta] = make_float2(cosf(phi), 0.f);
   if (t < 2 * n0 + 2 * m0 + 1 + 2 * EPAD) ex[t] = (t - n0 - m0 - EPAD) / (float)(2 * n0);
   if (t < 2 * n1 + 2 * m1 + 1 + 2 * EPAD) ey[t] = (t - n1 - m1 - EPAD) / (float)(2 * n1);
 }
@@ -608,7 +612,7 @@ extern "C" int tcb_usfft2d_create(tcb_usfft2d **out, size_t n0_, size_t n1_, siz
     return code;
   };
   if (cudaMalloc(&h->grid, n2 * 4 * n0 * n1 * sizeof(float2)) != cudaSuccess ||
-      cudaMalloc(&h->cs, ntheta * sizeof(float2)) != cudaSuccess ||
+      cudaMalloc(&h->cs, (ntheta + 1) * sizeof(float2)) != cudaSuccess ||
       cudaMalloc(&h->ex, (2 * n0 + 2 * m0 + 1 + 2 * EPAD) * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&h->ey, (2 * n1 + 2 * m1 + 1 + 2 * EPAD) * sizeof(float)) != cudaSuccess)
     return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
@@ -630,14 +634,13 @@ static int u2_run(tcb_usfft2d *h, void *f, const void *g, const float *theta, fl
   geo.in_scale = h->storage == TCB_FLOAT16 ? h->in_scale : nullptr;
   geo.k = k;
   geo.deth0 = deth0;
-  geo.cphi = cosf(phi);
   geo.fused = fused;
   geo.row0 = row0;
   geo.deth_full = deth_full;
   int tab = (int)std::max<size_t>(h->geo.ntheta,
                                   2 * std::max(geo.n0, geo.n1) + 2 * 4 + 1 + 2 * EPAD);
-  u2_tables<<<ceil_div(tab, 256), 256, 0, s>>>(h->cs, h->ex, h->ey, theta, geo.ntheta, geo.n0,
-                                              geo.m0, geo.n1, geo.m1);
+  u2_tables<<<ceil_div(tab, 256), 256, 0, s>>>(h->cs, h->ex, h->ey, theta, phi, geo.ntheta,
+                                              geo.n0, geo.m0, geo.n1, geo.m1);
   TCB_LAUNCH_CHECK();
   count_launch();
   {
@@ -712,6 +715,44 @@ extern "C" int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1,
   int st = u2_run(&tmp, S2, S1, theta, phi, row0, deth_full, 1, row0,
                   deth_full, nrows, deth_full / 2 + 1, row0, (cudaStream_t)stream);
   return st;
+}
+
+// The sample positions that the gridding above uses, one per (angle, detector
+// row of the call, detector column), written in take_x's layout.
+__global__ void u2_positions(float *__restrict__ x, float *__restrict__ y,
+                             const float2 *__restrict__ cs, U2Geom geo) {
+  const size_t total = (size_t)geo.detw * geo.deth * geo.ntheta;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int tx = (int)(i % geo.detw);
+  const int ty = (int)((i / geo.detw) % geo.deth);
+  const int tz = (int)(i / ((size_t)geo.detw * geo.deth));
+  float xv, yv;
+  u2_pos(geo, cs[geo.ntheta].x, cs[tz], tx, ty, xv, yv);
+  x[i] = xv;
+  y[i] = yv;
+}
+
+extern "C" int tcb_usfft2d_sample_positions(tcb_usfft2d *h, float *x, float *y,
+                                            const float *theta, float phi, int k, int deth0,
+                                            void *stream) {
+  TCB_CHECK_ARG(h && h->grid, "tcb_usfft2d_sample_positions: null or freed handle");
+  TCB_CHECK_ARG(x && y && theta, "tcb_usfft2d_sample_positions: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  U2Geom geo = h->geo;
+  geo.k = k;
+  geo.deth0 = deth0;
+  int tab = (int)std::max<size_t>(h->geo.ntheta,
+                                  2 * std::max(geo.n0, geo.n1) + 2 * 4 + 1 + 2 * EPAD);
+  u2_tables<<<ceil_div(tab, 256), 256, 0, s>>>(h->cs, h->ex, h->ey, theta, phi, geo.ntheta,
+                                              geo.n0, geo.m0, geo.n1, geo.m1);
+  TCB_LAUNCH_CHECK();
+  count_launch();
+  const size_t total = (size_t)geo.detw * geo.deth * geo.ntheta;
+  u2_positions<<<ceil_div(total, 256), 256, 0, s>>>(x, y, h->cs, geo);
+  TCB_LAUNCH_CHECK();
+  count_launch();
+  return TCB_OK;
 }
 
 extern "C" int tcb_usfft2d_set_storage(tcb_usfft2d *h, int precision, const float *in_scale,

@@ -51,12 +51,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: false when the clock budget ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+// Bounded wait: false when the clock budget (in SM clock cycles) ran out.
+__device__ __forceinline__ bool mbar_wait_budget(uint64_t *b, uint32_t parity,
+                                                 long long budget) {
   long long t0 = clock64();
   while (!mbar_try_wait(b, parity))
-    if (clock64() - t0 > WAIT_CYCLES) return false;
+    if (clock64() - t0 > budget) return false;
   return true;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+  return mbar_wait_budget(b, parity, WAIT_CYCLES);
 }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,

@@ -187,10 +187,11 @@ class SinoPipeline:
             raise NotImplementedError("double-FOV padding: fused fp32 filter only")
         if self.dezinger is not None:
             if self._zbuf is None or self._zbuf.dtype != data.dtype:
-                self._zbuf = torch.empty((self.nproj, self.ncz, self.n), dtype=data.dtype,
+                self._zbuf = torch.empty((self.nproj, self.ncz, self.ni), dtype=data.dtype,
                                          device=self.device)
             # a contiguous [nproj, nz, n] view of the scratch (partial chunks too)
-            zb = self._zbuf.view(-1)[:self.nproj * nz * self.n].view(self.nproj, nz, self.n)
+            # frames arrive at the input width ni (double-FOV scans reconstruct at n = 2 ni)
+            zb = self._zbuf.view(-1)[:self.nproj * nz * self.ni].view(self.nproj, nz, self.ni)
             data = _dezinger(data, *self.dezinger, out=zb, stream=stream)
         d0 = dark0[z_lo:z_lo + nz] if dark0 is not None else None
         f0 = flat0[z_lo:z_lo + nz] if flat0 is not None else None

@@ -88,9 +88,10 @@ class GPURec:
     def pipe(self) -> SinoPipeline:
         """The chunk pipeline (built on first use; try-centre sweeps do not need it)."""
         if self._pipe is None:
-            # with phase retrieval the chunk's ring removal runs before it
-            # (_phase_chunk), not in the pipeline
-            stripe = None if _proj_chunk_ops() else _stripe_args()
+            # with phase retrieval or rotation the chunk's outlier removal and
+            # ring removal run before them (_phase_chunk), not in the pipeline
+            proj_ops = _proj_chunk_ops()
+            stripe = None if proj_ops else _stripe_args()
             self._pipe = SinoPipeline(params.n, params.nproj, params.ncz, params.theta,
                                       params.center, args.fbp_filter,
                                       args.reconstruction_algorithm,
@@ -98,7 +99,8 @@ class GPURec:
                                       stripe=stripe, precision=self.precision,
                                       out_dtype=args.out_dtype,
                                       mixed_filter=args.mixed_filter,
-                                      dezinger=dezinger_args(), ni=params.ni,
+                                      dezinger=None if proj_ops else dezinger_args(),
+                                      ni=params.ni,
                                       pad360=_pad360_args())
         return self._pipe
 
@@ -244,11 +246,18 @@ class GPURec:
 
     def _phase_chunk(self, src, dark0, flat0, z0, stream):
         """proc_sino + proc_proj's phase step on one sinogram chunk, as the
-        reference's recon_all runs them (rec.py:170-173): dark/flat, ring
-        removal, then phase retrieval of the chunk's projections (its rows are
-        the image height); -log (and double-FOV padding) follow in the
-        pipeline."""
+        reference's recon_all runs them (rec.py:170-173): outlier removal,
+        dark/flat, ring removal, then phase retrieval and rotation of the
+        chunk's projections (its rows are the image height); -log (and
+        double-FOV padding) follow in the pipeline."""
         nproj, lz, n = src.shape
+        dz = dezinger_args()
+        if dz is not None:  # proc_sino: outliers of the raw frames first (proc_functions.py:146-148)
+            zb = getattr(self, "_phase_zbuf", None)
+            if zb is None or zb.dtype != src.dtype or zb.numel() < nproj * lz * n:
+                zb = self._phase_zbuf = torch.empty(nproj * params.ncz * n, dtype=src.dtype,
+                                                    device=self.device)
+            src = dezinger(src, *dz, out=zb[:nproj * lz * n].view(nproj, lz, n), stream=stream)
         buf = getattr(self, "_phase_buf", None)
         if buf is None or buf.numel() < nproj * lz * n:
             buf = self._phase_buf = torch.empty(nproj * params.ncz * n, dtype=torch.float32,
