@@ -185,6 +185,18 @@ def make_data(a, device):
                                   block=32)
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (the `lscpu` "Model name" field, read from
+    /proc/cpuinfo so that no external tool is needed)."""
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.lower().startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(a, data_cpu, dark, flat, theta):
     """NumPy port on the host cores: one slice pair through prep + filter + fourierrec."""
     from oracle import np_tomo
@@ -199,6 +211,7 @@ def cpu_baseline(a, data_cpu, dark, flat, theta):
     secs = time.perf_counter() - t0
     gups = a.n * a.n * 2 * a.nproj / secs / 1e9
     return {"value": gups, "unit": "GUPS", "cores": np_tomo.WORKERS, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"1 slice pair of the {a.n}x{a.nproj} geometry (prep+filter+fourierrec, "
                       f"NumPy/scipy.fft float32, workers={np_tomo.WORKERS}), {secs:.1f} s",
             "seconds": secs}
@@ -382,16 +395,29 @@ def run_serving(a, dev):
     from tomocupy_b200 import synthetic
     from tomocupy_b200.serving import Request, Server, latency_summary, poisson_stream
     specs = poisson_stream(rate=a.serve_rate, count=a.serve_requests, seed=a.seed)
-    pool, outs = {}, {}
+    pool = {}
     for _, n, P, _, _ in specs:
         if (n, P) not in pool:
             d, dk, fl, th, _ = synthetic.make_dataset(P, 64, n, seed=a.seed, device=dev)
             pool[(n, P)] = (d.cpu().pin_memory(), dk.cpu().pin_memory(), fl.cpu().pin_memory(),
                             th)
             del d, dk, fl
-        for dt in (torch.float32, torch.float16):
-            if (n, dt) not in outs:
-                outs[(n, dt)] = torch.empty((64, n, n), dtype=dt, pin_memory=True)
+    # every request writes its own pinned host volume (sized for fp32, viewed as
+    # fp16 for mixed requests), so concurrent requests never copy into the same
+    # host memory; with too little host memory, a ring of buffers per width
+    # that is longer than the server's admission limit
+    need = sum(nz * n * n * 4 for _, n, _, nz, _ in specs)
+    own = need * 1.5 < _mem_available()
+    ring = {}
+    outs = []
+    for k, (_, n, _, nz, _) in enumerate(specs):
+        if own:
+            outs.append(torch.empty(nz * n * n * 4, dtype=torch.uint8, pin_memory=True))
+        else:
+            r = ring.setdefault(n, [])
+            if len(r) < 32:
+                r.append(torch.empty(64 * n * n * 4, dtype=torch.uint8, pin_memory=True))
+            outs.append(r[sum(1 for _, m, _, _, _ in specs[:k] if m == n) % 32])
 
     def make(precision=None):
         # mixed-precision requests return fp16 volumes, fp32 requests fp32
@@ -400,7 +426,8 @@ def run_serving(a, dev):
             d, dk, fl, th = pool[(n, P)]
             prec = precision or prec
             odt = "float16" if prec == "mixed" else "float32"
-            out = outs[(n, torch.float16 if odt == "float16" else torch.float32)][:nz]
+            dt = torch.float16 if odt == "float16" else torch.float32
+            out = outs[k].view(dt)[:nz * n * n].view(nz, n, n)
             reqs.append(Request(k, d[:, :nz], dk[:, :nz], fl[:, :nz], th, n / 2, prec, "parzen",
                                 arrival=t, out=out, out_dtype=odt))
         return reqs
@@ -409,7 +436,8 @@ def run_serving(a, dev):
                        "n in {512,1024,2048,4096}, nproj in {180,720,1500,3000}, nz U{1..64}, "
                        "fp32:mixed 1:1 (mixed requests return fp16 volumes), uint16 pinned host "
                        "frames -> pinned host volumes",
-           "hbm_budget_gb": a.serve_budget_gb}
+           "hbm_budget_gb": a.serve_budget_gb,
+           "output_buffers": "one per request" if own else "ring of 32 per width"}
     srv = Server(dev, hbm_budget=a.serve_budget_gb * 1e9, ncz=a.serve_ncz)
     srv.warm(make())
     srv.warm(make("float32"))
@@ -751,14 +779,82 @@ def run_ours(a, ws, rank, local):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": base,
             "clocks": clocks, "gpu_launches": launches,
             "stages_ms": {k: round(v["ms"] / a.steps, 3) for k, v in stages.items()},
-            other if other == "mixed" else "fp32": side,
+            other if other == "mixed" else "fp32": _compact(side),
             "methods": methods,
-            "try_center": trycenter,
-            "serving": serving,
-            "lamino": lamino,
-            "phase_retrieval": phase,
+            "try_center": _compact(trycenter),
+            "serving": _compact(serving),
+            "lamino": _compact(lamino),
+            "phase_retrieval": _compact(phase),
         }
+        line["summary"] = _summary(line, side, methods, trycenter, serving, lamino, phase)
+        # the full records of the side legs (autotune tables, per-stage times) go to
+        # stderr; the JSON line on stdout stays short and ends with the summary
+        log("detail: " + json.dumps({"mixed": side, "try_center": trycenter, "serving": serving,
+                                     "lamino": lamino, "phase_retrieval": phase}))
         print(json.dumps(line), flush=True)
+
+
+_VERBOSE = ("autotune", "stages_ms", "workload", "peak_source", "fp64_oracle",
+            "rel_l2_vs_fp64", "api", "sample")
+
+
+def _compact(d):
+    """A leg's record without its long descriptive fields (kept on stderr)."""
+    if not isinstance(d, dict):
+        return d
+    return {k: _compact(v) for k, v in d.items() if k not in _VERBOSE}
+
+
+def _summary(line, side, methods, trycenter, serving, lamino, phase):
+    """The figures of every leg in one short object at the end of the line."""
+    g = lambda d, *ks: _dig(d, ks)  # noqa: E731
+    return {
+        "fp32_gups": line["value"], "fp32_ms": line["ms_per_step"],
+        "e2e_gups": g(line, "e2e", "value"),
+        "roofline_kernel": g(line, "roofline", "kernel"),
+        "roofline_frac": g(line, "roofline", "frac"),
+        "mixed_gups": g(side, "value"), "mixed_ms": g(side, "ms_per_step"),
+        "mixed_speedup_vs_fp32": g(side, "mixed_speedup_vs_fp32"),
+        "mixed_rel_l2_vs_fp32": g(side, "rel_l2_vs_float32"),
+        "mixed_e2e_fp16_out_gups": g(side, "e2e_fp16_out", "value"),
+        "fw_gups": g(methods, "fourierrec+fw", "value"),
+        "fw_ms": g(methods, "fourierrec+fw", "ms"),
+        "ti_gups": g(methods, "fourierrec+ti", "value"),
+        "dezinger_gups": g(methods, "fourierrec+dezinger", "value"),
+        "lprec_gups": g(methods, "lprec", "value"),
+        "linerec_gups": g(methods, "linerec", "value"),
+        "try_fp32_ms": g(trycenter, "float32", "ms_per_sweep"),
+        "try_mixed_ms": g(trycenter, "mixed", "ms_per_sweep"),
+        "try_mixed_speedup": g(trycenter, "mixed_speedup_vs_fp32"),
+        "serve_p50_ms": g(serving, "continuous_batching", "p50_ms"),
+        "serve_p99_ms": g(serving, "continuous_batching", "p99_ms"),
+        "serve_single_p99_ms": g(serving, "single_request", "p99_ms"),
+        "serve_p99_over_single_p99": g(serving, "p99_over_single_p99"),
+        "lamino_fp32_ms": g(lamino, "fp32", "ms"),
+        "lamino_fp16_storage_ms": g(lamino, "fp16_storage", "ms"),
+        "phase_projections_per_s": g(phase, "projections_per_s"),
+        "fw_taps": "derived by spectral factorisation (PyWavelets absent): parity with "
+                   "PyWavelets' sym16 table unpinned",
+    }
+
+
+def _dig(d, keys):
+    for k in keys:
+        if not isinstance(d, dict) or k not in d:
+            return None
+        d = d[k]
+    return round(d, 4) if isinstance(d, float) else d
+
+
+def _mem_available() -> int:
+    """Host memory available to this process (bytes, /proc/meminfo)."""
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
 
 
 def run_e2e(a, data, dark, flat, theta, dev, ws, rank, precision=None, out_dtype="float32"):
@@ -766,13 +862,7 @@ def run_e2e(a, data, dark, flat, theta, dev, ws, rank, precision=None, out_dtype
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
-    avail = 0
-    try:
-        for ln in open("/proc/meminfo"):
-            if ln.startswith("MemAvailable:"):
-                avail = int(ln.split()[1]) * 1024
-    except OSError:
-        pass
+    avail = _mem_available()
     osz = 2 if out_dtype == "float16" else 4
     full_bytes = data.numel() * 2 + a.nz * a.n * a.n * osz
     nz_e2e = a.nz if (avail > 3 * full_bytes * ws) else min(a.nz, a.e2e_slab)
@@ -886,6 +976,7 @@ def run_reference(a, ws, rank, local):
                "value": round(float(a.lam_rh) * a.lam_n ** 2 * a.lam_nproj / (lms / 1e3) / 1e9, 2),
                "workload": "laminography, same as our lamino leg (reference CUDA operators)"}
         del ld
+    others = {} if a.no_methods else _reference_methods(a, data, dark, flat, theta, dev)
     line = {"impl": "reference",
             "metric": f"GUPS @{a.n}^2x{a.nproj} ({a.algorithm} fp32 pipeline, 1 GPU rate)",
             "value": round(value, 2), "unit": "GUPS", "n_gpus": 1, "steps": a.steps,
@@ -902,8 +993,71 @@ def run_reference(a, ws, rank, local):
                                        f"thread; the reference has no CPU implementation"},
             "e2e": {"value": round(value, 2), "unit": "GUPS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "lamino": lam}
+            "lamino": lam,
+            "summary": {"fourierrec_fp32_gups": round(value, 2), **others,
+                        "lamino_ms": lam["ms"] if lam else None}}
     print(json.dumps(line), flush=True)
+
+
+def _reference_methods(a, data, dark, flat, theta, dev):
+    """The reference's other operators on slabs of the same workload, each
+    timed once after one warm-up run: its -DHALF fourierrec build with its
+    fp16 filter (the reference's own fast path, the anchor of our mixed
+    precision), lprec and linerec.  Reported in GUPS (n^2 rows nproj / t)."""
+    import torch
+    from oracle import np_tomo, refglue
+    n, P = a.n, a.nproj
+    ne = 4 * n
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=dev)
+    th = torch.as_tensor(theta, device=dev)
+    res = {}
+    legs = [("fourierrec_fp16", 64, 8), ("lprec", 64, 8), ("linerec", 16, 8)]
+    for name, rows, ncz in legs:
+        rows = min(rows, data.shape[1])
+        center = n / 2
+        if name == "fourierrec_fp16":
+            filt = refglue.RefFilter(ne, P, ncz, "float16")
+            op = refglue.RefFourierRec(n, P, ncz, th, "float16")
+            wf = torch.as_tensor(np_tomo.calc_filter(ne, a.filter), device=dev)
+        elif name == "lprec":
+            from tomocupy_b200.reconstruction import lprec_grids as L
+            ntheta, nrho = L.lp_sizes(n, P)
+            filt = refglue.RefFilter(ne, P, ncz)
+            op = refglue.RefLpRec(n, P, ncz, vars(L.create_adj(L.create_gl(n, P, ntheta, nrho))))
+            wf = torch.as_tensor(np_tomo.calc_filter(ne, a.filter), device=dev)
+            center += 0.5
+        else:
+            filt = refglue.RefFilter(ne, P, ncz)
+            op = refglue.RefLineRec(th, P, P, ncz, ncz, n)
+            wf = torch.as_tensor(np_tomo.calc_filter(ne, a.filter), device=dev)
+        half = name == "fourierrec_fp16"
+        out = torch.zeros((ncz, n, n), dtype=torch.float16 if half else torch.float32,
+                          device=dev)
+
+        def step():
+            for z0 in range(0, rows, ncz):
+                d = refglue.ref_darkflat_minus_log(data[:, z0:z0 + ncz], dark[:, z0:z0 + ncz],
+                                                   flat[:, z0:z0 + ncz])
+                d = d.permute(1, 0, 2).contiguous()
+                if half:
+                    d = refglue.ref_fbp_filter_center(filt, d.half(), wf, t, center, 0.0, n,
+                                                      ne)
+                else:
+                    d = refglue.ref_fbp_filter_center(filt, d, wf, t, center, 0.0, n, ne)
+                op.backprojection(out, d)
+        step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name + "_gups"] = round(float(n) ** 2 * rows * P / (ms / 1e3) / 1e9, 2)
+        res[name + "_rows"] = rows
+        del op, filt, out
+        torch.cuda.empty_cache()
+    return res
 
 
 def main():

@@ -459,6 +459,13 @@ int tcb_usfft2d_adj(tcb_usfft2d *h, void *f, const void *g, const float *theta, 
  * of backproj_lamfourier_parallel.py:197-215 and the host copies). */
 int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1, const float *theta,
                          float phi, int row0, int nrows, int deth_full, void *stream);
+/* cfunc_usfft2d::fwd (src/cuda/cfunc_usfft2d.cu:53-70): g complex
+ * [2*ntheta, deth, detw/2+1] in adj's packed layout (detector frequencies
+ * above detw/2 mirrored into angle planes ntheta..) <- f complex [n1][n0][n2]
+ * (the layout adj writes), chunk index k, full detector height deth0.
+ * The adjoint of tcb_usfft2d_adj. */
+int tcb_usfft2d_fwd(tcb_usfft2d *h, void *g, const void *f, const float *theta, float phi,
+                    int k, int deth0, void *stream);
 /* fp16 storage (no reference counterpart; the reference's laminography path
  * is fp32 only): TCB_FLOAT16 makes the stage-1 spectrum input and the output
  * of adj/adj_rows complex fp16 (__half2) arrays; gridding, FFTs and
@@ -485,6 +492,12 @@ int tcb_usfft2d_destroy(tcb_usfft2d *h);
 typedef struct tcb_usfft1d tcb_usfft1d;
 int tcb_usfft1d_create(tcb_usfft1d **out, size_t n0, size_t n1, size_t n2, size_t deth);
 int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi, void *stream);
+/* cfunc_usfft1d::fwd (src/cuda/cfunc_usfft1d.cu:50-66): g complex
+ * [n1, deth/2+1, n2] <- f real [n1, n0(height), n2(width)].  Row t of g is
+ * computed from its own height z(t) for t <= deth/2 (the reference's kernel
+ * also runs rows t > deth/2, which race to overwrite row deth - t with an
+ * unconjugated value). */
+int tcb_usfft1d_fwd(tcb_usfft1d *h, void *g, const void *f, float phi, void *stream);
 /* fp16 storage of the input g (complex fp16); output and arithmetic fp32.
  * in_scale (device, [deth/2+1], or NULL): row r of g is multiplied by
  * in_scale[r] on load (the out_inv_scale rows written by usfft2d). */

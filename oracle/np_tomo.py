@@ -96,7 +96,23 @@ def minus_log(x):
 # --------------------------------------------------------------------------
 # Titarenko ring removal (src/tomocupy/processing/remove_stripe.py:296-307)
 # --------------------------------------------------------------------------
-def remove_stripe_ti(data, beta, mask_size):
+class NumpyFFT:
+    """The real FFTs the restatements call, as NumPy computes them (float32
+    in -> complex64 out, complex64 in -> float32 out, float64 as float64).
+    The reference calls cupy.fft, i.e. cuFFT, with the same types; a caller
+    may pass another provider with these two methods (e.g. cuFFT through
+    torch) to reproduce the reference's transforms more closely."""
+
+    @staticmethod
+    def rfft(a, axis=-1):
+        return np.fft.rfft(a, axis=axis)
+
+    @staticmethod
+    def irfft(a, n, axis=-1):
+        return np.fft.irfft(a, n, axis=axis)
+
+
+def remove_stripe_ti(data, beta, mask_size, fft=NumpyFFT):
     """remove_stripe_ti on float32 [nproj, nz, n] (returns a new array): float32
     column means over angles minus column 0, convolution with
     gamma = beta * ((1-beta)/(1+beta))**|k| (gamma[0] -= 1) through
@@ -108,7 +124,7 @@ def remove_stripe_ti(data, beta, mask_size):
     gamma[0] -= 1
     v = np.mean(data, axis=0, dtype=np.float32)
     v = v - v[:, 0:1]
-    v = np.fft.irfft(np.fft.rfft(v).astype(np.complex64) * np.fft.rfft(gamma))
+    v = fft.irfft(fft.rfft(v).astype(np.complex64) * fft.rfft(gamma), n)
     mask = np.zeros(v.shape, dtype=v.dtype)
     ms = mask_size * mask.shape[1]
     mask[:, mask.shape[1] // 2 - int(ms // 2):mask.shape[1] // 2 + int(ms // 2)] = 1
@@ -175,7 +191,7 @@ def _fw_synthesis(lo, hi, g0, g1, axis):
     return out[tuple(sl)]
 
 
-def remove_stripe_fw(data, sigma, level, bank):
+def remove_stripe_fw(data, sigma, level, bank, fft=NumpyFFT):
     """remove_stripe_fw on float32 [nproj, nz, n] (returns a new array).
 
     ``bank`` = (dec_lo, dec_hi, rec_lo, rec_hi) of the wavelet (PyWavelets'
@@ -204,10 +220,10 @@ def remove_stripe_fw(data, sigma, level, bank):
         # yh[:, 0, 0..2] = (low-row/high-col, high-row/low-col, high/high)
         band = hl[:, 0]
         my = band.shape[1]
-        spec = np.fft.rfft(band, axis=1)
+        spec = fft.rfft(band, axis=1)
         yhat = np.fft.ifftshift((np.arange(-my, my, 2) + 1) / 2)[:my // 2 + 1]
         spec *= (-np.expm1(-yhat ** 2 / (2 * sigma ** 2)))[:, None]
-        hl = np.fft.irfft(spec, my, axis=1).astype(np.float32)[:, None]
+        hl = fft.irfft(spec, my, axis=1).astype(np.float32)[:, None]
         bands.append((lh, hl, hh))
         sli = ll
     for lh, hl, hh in bands[::-1]:

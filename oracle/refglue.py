@@ -244,6 +244,10 @@ class RefUSFFT2D(_Handle):
         self.L.ref_adj(self.h, f.data_ptr(), g.data_ptr(), theta.data_ptr(), phi, k, deth0,
                        _s(stream))
 
+    def fwd(self, g, f, theta, phi, k, deth0, stream=None):
+        self.L.ref_fwd(self.h, g.data_ptr(), f.data_ptr(), theta.data_ptr(), phi, k, deth0,
+                       _s(stream))
+
 
 class RefUSFFT1D(_Handle):
     op = "usfft1d"
@@ -253,6 +257,9 @@ class RefUSFFT1D(_Handle):
 
     def adj(self, f, g, phi, stream=None):
         self.L.ref_adj(self.h, f.data_ptr(), g.data_ptr(), phi, _s(stream))
+
+    def fwd(self, g, f, phi, stream=None):
+        self.L.ref_fwd(self.h, g.data_ptr(), f.data_ptr(), phi, _s(stream))
 
 
 def ref_rec_lam(data, theta, center, lamino_angle, rh, wfilter, nthetac=8, dethc=8, n1c=8):

@@ -35,3 +35,24 @@ def ref():
     if not refglue.available():
         pytest.fail("oracle/_ref is not built: run `make -C oracle` (needs the reference sources)")
     return refglue
+
+
+class TorchCuFFT:
+    """Real FFTs through cuFFT (torch.fft on the GPU), the library that the
+    reference's cupy.fft calls, with NumPy's types (float32 <-> complex64,
+    float64 <-> complex128) and normalisation; a drop-in ``fft`` provider for
+    the oracle's ring-removal restatements."""
+
+    @staticmethod
+    def rfft(a, axis=-1):
+        import numpy as np
+        import torch
+        x = torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+        return torch.fft.rfft(x, dim=axis).cpu().numpy()
+
+    @staticmethod
+    def irfft(a, n, axis=-1):
+        import numpy as np
+        import torch
+        x = torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+        return torch.fft.irfft(x, n=n, dim=axis).cpu().numpy()

@@ -80,6 +80,47 @@ def test_usfft2d_rows_matches_packed_glue(cuda):
         assert err < 1e-6, (k, err)
 
 
+@pytest.mark.parametrize("k", [0, 2])
+def test_usfft2d_fwd_vs_reference(cuda, ref, k):
+    """cfunc_usfft2d.fwd: same packed output layout (mirrored upper detector
+    frequencies in angle planes ntheta..), rel-L2 <= 1e-5 (the reference
+    gathers with one exp per footprint cell, here a product of two)."""
+    from tomocupy_b200 import cfunc_usfft2d
+    n, ntheta, detw, dethc, deth0 = 128, 60, 128, 8, 128
+    theta = _theta(ntheta)
+    f = torch.randn((n, dethc, n), dtype=torch.complex64, device=cuda)
+    ga = torch.zeros((2 * ntheta, dethc, detw // 2 + 1), dtype=torch.complex64, device=cuda)
+    gb = torch.zeros_like(ga)
+    cfunc_usfft2d.cfunc_usfft2d(dethc, n, n, ntheta, detw, dethc).fwd(ga, f, theta, PHI, k,
+                                                                      deth0, None)
+    ref.RefUSFFT2D(dethc, n, n, ntheta, detw, dethc).fwd(gb, f.clone(), theta, PHI, k, deth0)
+    torch.cuda.synchronize()
+    err = rel_l2(torch.view_as_real(ga).cpu(), torch.view_as_real(gb).cpu())
+    assert err < 1e-5, err
+
+
+def test_usfft1d_fwd_vs_reference(cuda, ref):
+    """cfunc_usfft1d.fwd.  The reference's gather1d(direction 0) runs all deth
+    height samples and lets sample deth - t store its (conjugate) value into
+    row t unconjugated, racing with sample t; rows 0 and deth/2 have one
+    writer.  So: rows 0 and deth/2 as complex numbers, and every row's real
+    part and |imaginary part| (the same for g and conj(g)), rel-L2 <= 1e-5."""
+    from tomocupy_b200 import cfunc_usfft1d
+    rh, n1c, n, deth = 64, 4, 96, 128
+    f = torch.randn((n1c, rh, n), device=cuda)
+    ga = torch.zeros((n1c, deth // 2 + 1, n), dtype=torch.complex64, device=cuda)
+    gb = torch.zeros_like(ga)
+    cfunc_usfft1d.cfunc_usfft1d(rh, n1c, n, deth).fwd(ga, f, PHI, None)
+    ref.RefUSFFT1D(rh, n1c, n, deth).fwd(gb, f.clone(), PHI)
+    torch.cuda.synchronize()
+    a, b = ga.cpu(), gb.cpu()
+    for r in (0, deth // 2):
+        err = rel_l2(torch.view_as_real(a[:, r]), torch.view_as_real(b[:, r]))
+        assert err < 1e-5, (r, err)
+    assert rel_l2(a.real, b.real) < 1e-5
+    assert rel_l2(a.imag.abs(), b.imag.abs()) < 1e-5
+
+
 def test_usfft1d_adj_vs_reference(cuda, ref):
     from tomocupy_b200 import cfunc_usfft1d
     rh, n1c, n, deth = 64, 4, 96, 128

@@ -145,8 +145,9 @@ def test_step_driver_double_fov_matches_recon_all(cuda, axis, stripe, dz):
     theta = np.linspace(0, 2 * np.pi, nproj, endpoint=False).astype(np.float32)
     data, dark, flat, _, _ = synthetic.make_dataset(nproj, nz, ni, seed=9, theta=theta)
     if dz:  # outlier removal runs on the ni-wide raw frames before the padding
-        data = data.clone()
-        data.view(-1)[torch.as_tensor(np.random.default_rng(2).integers(0, data.numel(), 200))] = 60000
+        d32 = data.to(torch.int32)
+        d32.view(-1)[torch.as_tensor(np.random.default_rng(2).integers(0, data.numel(), 200))] = 60000
+        data = d32.to(torch.uint16)
     opts = dict(reconstruction_algorithm="fourierrec", nsino_per_chunk=4,
                 file_type="double_fov", rotation_axis=axis, remove_stripe_method=stripe,
                 fw_level=4, dezinger=dz)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import ROOT, rel_l2
+from conftest import TorchCuFFT, ROOT, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -180,7 +180,7 @@ def test_recon_all_ring_removal_then_phase_matches_reference(cuda, ref):
     for z0 in range(0, nz, ncz):
         sl = slice(z0, z0 + ncz)
         pre = np_tomo.darkflat(data[:, sl].numpy(), dark[:, sl].numpy(), flat[:, sl].numpy())
-        pre = np_tomo.remove_stripe_ti(pre, 0.022, 1)
+        pre = np_tomo.remove_stripe_ti(pre, 0.022, 1, fft=TorchCuFFT)
         pre = np_tomo.minus_log(np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3))
         d = torch.as_tensor(np.ascontiguousarray(pre.transpose(1, 0, 2)), device=cuda)
         d = ref.ref_fbp_filter_center(filt, d, wf, t, n / 2, torch.zeros(ncz, device=cuda), n, ne)
@@ -205,9 +205,9 @@ def test_recon_all_dezinger_then_phase_matches_reference(cuda, ref, rotate):
     nproj, nz, n, ncz = 90, 16, 128, 8
     data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=14)
     rng = np.random.default_rng(3)
-    data = data.clone()
-    idx = rng.integers(0, data.numel(), 300)
-    data.view(-1)[torch.as_tensor(idx)] = 60000   # zingers
+    d32 = data.to(torch.int32)
+    d32.view(-1)[torch.as_tensor(rng.integers(0, data.numel(), 300))] = 60000   # zingers
+    data = d32.to(torch.uint16)
     opts = dict(rotate_proj_angle=1.5, rotate_proj_order=1) if rotate else {}
     global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=ncz, dezinger=3,
                       dezinger_threshold=5000, retrieve_phase_method="paganin",
@@ -234,3 +234,51 @@ def test_recon_all_dezinger_then_phase_matches_reference(cuda, ref, rotate):
         rec.backprojection(theirs, d)
         err = rel_l2(w.rec[sl].cpu(), theirs.cpu())
         assert err < 1e-4, (z0, err)
+
+
+@pytest.mark.parametrize("algorithm", ["fourierrec", "linerec"])
+def test_recon_try_with_phase_and_rotation_matches_reference(cuda, ref, algorithm):
+    """recon_try with Paganin phase retrieval and projection rotation: the
+    reference's recon_try runs proc_sino and proc_proj on the one-row slice
+    (rec.py:224-225), so phase retrieval and rotation see images one row
+    high; then the slice is tiled and filtered per centre shift."""
+    from oracle import np_tomo
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.global_vars import params
+    from tomocupy_b200.rec import GPURec
+    nproj, nz, n, ncz = 90, 8, 128, 4
+    data, dark, flat, theta, _ = synthetic.make_dataset(nproj, nz, n, seed=15)
+    global_vars.reset(reconstruction_type="try", reconstruction_algorithm=algorithm,
+                      center_search_width=2.0, center_search_step=1.0, nsino="0.5",
+                      nsino_per_chunk=ncz, retrieve_phase_method="paganin", pixel_size=0.65,
+                      propagation_distance=50.0, energy=20.0, retrieve_phase_alpha=1e-3,
+                      rotate_proj_angle=1.5)
+    w = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(data, dark, flat, theta=theta), w).recon_try()
+    zs, shifts = int(params.id_slices[0]), params.shift_array
+    assert len(w.tries) == len(shifts)
+    sl = slice(zs, zs + 1)
+    pre = np_tomo.darkflat(data[:, sl].numpy(), dark[:, sl].numpy(), flat[:, sl].numpy())
+    pre = np_tomo.retrieve_phase(pre, "paganin", 0.65e-4, 5.0, 20.0, 1e-3)
+    pre = np_tomo.minus_log(np_tomo.rotate_proj(pre, 1.5, 1))
+    row = torch.as_tensor(np.ascontiguousarray(pre.transpose(1, 0, 2)), device=cuda)
+    ne = 4 * n
+    wf = torch.as_tensor(np_tomo.calc_filter(ne, "parzen"), device=cuda)
+    t = torch.as_tensor(np_tomo.rfftfreq32(ne), device=cuda)
+    filt = ref.RefFilter(ne, nproj, ncz)
+    th = torch.as_tensor(theta, device=cuda)
+    rec = (ref.RefFourierRec(n, nproj, ncz, th) if algorithm == "fourierrec"
+           else ref.RefLineRec(th, nproj, nproj, ncz, ncz, n))
+    for k in range(0, len(shifts), ncz):
+        cnt = min(ncz, len(shifts) - k)
+        sht = torch.zeros(ncz, device=cuda)
+        sht[:cnt] = torch.as_tensor(shifts[k:k + cnt], device=cuda)
+        d = ref.ref_fbp_filter_center(filt, row.repeat(ncz, 1, 1).contiguous(), wf, t, n / 2,
+                                      sht, n, ne)
+        theirs = torch.zeros((ncz, n, n), device=cuda)
+        rec.backprojection(theirs, d)
+        for kk in range(cnt):
+            ours = w.tries[(zs, float(params.save_centers[k + kk]))].cpu()
+            err = rel_l2(ours, theirs[kk].cpu())
+            assert err < 1e-4, (k + kk, err)

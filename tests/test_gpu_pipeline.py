@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import rel_l2
+from conftest import TorchCuFFT, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -22,8 +22,22 @@ def c1():
     return synthetic.make_dataset(NPROJ, NZ, N, seed=0)
 
 
+@pytest.fixture(scope="module")
+def c1_thin():
+    """The C1 geometry with a quarter of the densities (transmissions above
+    ~8 %, no zero counts) and stripes.  Ring removal adds a correction to
+    the normalised frames before -log; where a transmission is at or near
+    zero (the C1 phantom has ~32 k such values per 8 rows), a last-bit
+    difference between two float32 implementations of the correction moves
+    a value across where(x <= 0, 1) or into log's steep region and changes
+    the sinogram by O(1).  The ring-removal chains are compared on this
+    well-conditioned phantom."""
+    from tomocupy_b200 import synthetic
+    return synthetic.make_dataset(NPROJ, NZ, N, seed=0, density_max=0.005, stripes=6)
+
+
 def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
-                    fbp="parzen", center=None, sht=None, stripe=None):
+                    fbp="parzen", center=None, sht=None, stripe=None, flat_linear=False):
     from oracle import np_tomo
     dev = torch.device("cuda")
     P, nz, n = data.shape
@@ -47,18 +61,20 @@ def reference_chain(ref, data, dark, flat, theta, algorithm="fourierrec", ncz=8,
     for z0 in range(0, nz, ncz):
         # dark/flat in CuPy's float32 operation order (NumPy restatement,
         # bit-exact with the native kernel), -log with the device logf
-        d = np_tomo.darkflat(np.asarray(data[:, z0:z0 + ncz]), np.asarray(dark[:, z0:z0 + ncz]),
-                             np.asarray(flat[:, z0:z0 + ncz]))
+        norm = np_tomo.darkflat_linear if flat_linear else np_tomo.darkflat
+        d = norm(np.asarray(data[:, z0:z0 + ncz]), np.asarray(dark[:, z0:z0 + ncz]),
+                 np.asarray(flat[:, z0:z0 + ncz]))
         # proc_sino: ring removal on the dark/flat corrected frames with the
-        # NumPy restatements, which reproduce the reference's remove_stripe_ti
-        # and remove_stripe_fw fixtures bit for bit (tests/test_stripe_*_cpu.py);
-        # then proc_proj: -log
+        # oracle's restatements, which reproduce the reference's remove_stripe_ti
+        # and remove_stripe_fw fixtures bit for bit (tests/test_stripe_*_cpu.py),
+        # with their FFTs on cuFFT as cupy.fft runs them; then proc_proj: -log
         if stripe is not None and stripe[0] == "ti":
-            d = np_tomo.remove_stripe_ti(d, stripe[1], stripe[2])
+            d = np_tomo.remove_stripe_ti(d, stripe[1], stripe[2], fft=TorchCuFFT)
         elif stripe is not None:
             from tomocupy_b200.processing import wavelets
             sigma, wname, level = stripe
-            d = np_tomo.remove_stripe_fw(d, sigma, level, wavelets.filter_bank(wname))
+            d = np_tomo.remove_stripe_fw(d, sigma, level, wavelets.filter_bank(wname),
+                                         fft=TorchCuFFT)
         d = torch.as_tensor(np.ascontiguousarray(d), device=dev)
         d = torch.where(d <= 0, torch.ones((), device=dev), d)
         d = torch.nan_to_num(-torch.log(d), nan=6.0, posinf=0.0, neginf=0.0)
@@ -120,12 +136,12 @@ def test_c1_linerec_matches_reference(cuda, ref, c1):
     assert err < 1e-5, err
 
 
-def test_c1_fw_ring_removal_pipeline(cuda, ref, c1):
+def test_c1_fw_ring_removal_pipeline(cuda, ref, c1_thin):
     """dark/flat -> fw ring removal (level 7, sym16) -> -log -> filter -> fourierrec."""
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
-    data, dark, flat, theta, _ = c1
+    data, dark, flat, theta, _ = c1_thin
     d, dk, fl = data[:, :8], dark[:, :8], flat[:, :8]
     global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=8,
                       remove_stripe_method="fw", fw_sigma=1.0, fw_filter="sym16", fw_level=7)
@@ -137,13 +153,13 @@ def test_c1_fw_ring_removal_pipeline(cuda, ref, c1):
     assert err < 1e-5, err
 
 
-def test_c1_ti_ring_removal_pipeline(cuda, ref, c1):
+def test_c1_ti_ring_removal_pipeline(cuda, ref, c1_thin):
     """dark/flat -> Titarenko ring removal -> -log -> filter -> fourierrec, with a
     partial last chunk (12 rows in chunks of 8)."""
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.rec import GPURec
-    data, dark, flat, theta, _ = c1
+    data, dark, flat, theta, _ = c1_thin
     d, dk, fl = data[:, :12], dark[:, :12], flat[:, :12]
     global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=8,
                       remove_stripe_method="ti", ti_beta=0.022, ti_mask=1)
@@ -237,14 +253,14 @@ def test_recon_try_lprec_linerec_match_reference(cuda, ref, c1, algorithm):
 
 
 @pytest.mark.parametrize("stripe", [("ti", 0.022, 1), (1.0, "sym16", 3)])
-def test_recon_try_with_ring_removal_matches_reference(cuda, ref, c1, stripe):
+def test_recon_try_with_ring_removal_matches_reference(cuda, ref, c1_thin, stripe):
     """Try-centre sweep with ring removal of the slice (proc_sino inside the
     reference's recon_try, rec.py:224-226): Titarenko and Fourier-wavelet."""
     from tomocupy_b200 import global_vars
     from tomocupy_b200.dataio import ArrayReader, ArrayWriter
     from tomocupy_b200.global_vars import params
     from tomocupy_b200.rec import GPURec
-    data, dark, flat, theta, _ = c1
+    data, dark, flat, theta, _ = c1_thin
     opts = (dict(remove_stripe_method="ti", ti_beta=stripe[1], ti_mask=stripe[2])
             if stripe[0] == "ti" else
             dict(remove_stripe_method="fw", fw_sigma=stripe[0], fw_filter=stripe[1],
@@ -350,3 +366,21 @@ def test_production_geometry_vs_fp64_oracle(cuda):
           f"mixed vs fp32 {rel_l2(mixed, fp32):.2e}")
     assert e32 < 1e-4, e32
     assert emix < 1e-3, emix
+
+
+def test_c1_flat_linear_matches_reference(cuda, ref):
+    """flat_linear (proc_functions.py:62-66: flats blended linearly over the
+    angles from the means of the first and the last half) in the fused
+    driver, 8 flats, against the restated normalisation feeding the
+    reference's filter and fourierrec."""
+    from tomocupy_b200 import global_vars, synthetic
+    from tomocupy_b200.dataio import ArrayReader, ArrayWriter
+    from tomocupy_b200.rec import GPURec
+    d, dk, fl, theta, _ = synthetic.make_dataset(NPROJ, 8, N, seed=17, nflat=8)
+    global_vars.reset(reconstruction_algorithm="fourierrec", nsino_per_chunk=8,
+                      flat_linear="True")
+    w = ArrayWriter(device="cuda")
+    GPURec(ArrayReader(d, dk, fl, theta=theta), w).recon_all()
+    theirs = reference_chain(ref, d, dk, fl, theta, ncz=8, flat_linear=True)
+    err = rel_l2(w.rec.cpu(), theirs)
+    assert err < 1e-5, err

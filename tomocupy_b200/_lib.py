@@ -126,11 +126,13 @@ SIGNATURES: dict[str, list] = {
     "tcb_usfft2d_create": [C.POINTER(vp), sz, sz, sz, sz, sz, sz],
     "tcb_usfft2d_adj": [vp, vp, vp, vp, f32, i32, i32, vp],
     "tcb_usfft2d_adj_rows": [vp, vp, vp, vp, f32, i32, i32, i32, vp],
+    "tcb_usfft2d_fwd": [vp, vp, vp, vp, f32, i32, i32, vp],
     "tcb_usfft2d_set_storage": [vp, i32, vp, vp],
     "tcb_usfft2d_sample_positions": [vp, vp, vp, vp, f32, i32, i32, vp],
     "tcb_usfft2d_destroy": [vp],
     "tcb_usfft1d_create": [C.POINTER(vp), sz, sz, sz, sz],
     "tcb_usfft1d_adj": [vp, vp, vp, f32, vp],
+    "tcb_usfft1d_fwd": [vp, vp, vp, f32, vp],
     "tcb_usfft1d_set_storage": [vp, i32, vp],
     "tcb_usfft1d_destroy": [vp],
 }

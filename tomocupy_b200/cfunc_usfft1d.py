@@ -1,8 +1,6 @@
-"""Drop-in for ``tomocupy.cfunc_usfft1d`` (src/cuda/cfunc_usfft1d.i:9-18).
-
-Only the adjoint is used by the reconstruction path
-(LamFourierRec.usfft1d_adj); ``fwd`` raises NotImplementedError.
-"""
+"""Drop-in for ``tomocupy.cfunc_usfft1d`` (src/cuda/cfunc_usfft1d.i:9-18):
+``fwd`` and ``adj`` with the reference's argument order (the reconstruction
+path, LamFourierRec.usfft1d_adj, uses the adjoint)."""
 from __future__ import annotations
 
 from . import _lib
@@ -24,5 +22,7 @@ class cfunc_usfft1d(NativeHandle):
         fp16, with optional per-angle / per-row power-of-two scale arrays."""
         _lib.call("tcb_usfft1d_set_storage", self._live(), int(precision), _lib.ptr(in_scale))
 
-    def fwd(self, *a, **k):
-        raise NotImplementedError("usfft1d forward is not on the reconstruction path")
+    def fwd(self, g_, f_, phi, stream_):
+        """g [n1, deth/2+1, n2] complex <- f [n1, n0 (height), n2] real."""
+        _lib.call("tcb_usfft1d_fwd", self._live(), _lib.ptr(g_), _lib.ptr(f_), float(phi),
+                  _lib.stream_ptr(stream_))

@@ -1,8 +1,6 @@
-"""Drop-in for ``tomocupy.cfunc_usfft2d`` (src/cuda/cfunc_usfft2d.i:9-18).
-
-Only the adjoint is used by the reconstruction path
-(LamFourierRec.usfft2d_adj); ``fwd`` raises NotImplementedError.
-"""
+"""Drop-in for ``tomocupy.cfunc_usfft2d`` (src/cuda/cfunc_usfft2d.i:9-18):
+``fwd`` and ``adj`` with the reference's argument order (the reconstruction
+path, LamFourierRec.usfft2d_adj, uses the adjoint)."""
 from __future__ import annotations
 
 from . import _lib
@@ -38,5 +36,7 @@ class cfunc_usfft2d(NativeHandle):
         _lib.call("tcb_usfft2d_sample_positions", self._live(), _lib.ptr(x), _lib.ptr(y),
                   _lib.ptr(theta_), float(phi), int(k), int(deth0), _lib.stream_ptr(stream_))
 
-    def fwd(self, *a, **k):
-        raise NotImplementedError("usfft2d forward is not on the reconstruction path")
+    def fwd(self, g_, f_, theta_, phi, k, deth0, stream_):
+        """g [2*ntheta, deth, detw/2+1] complex <- f [n1, n2 slabs, n0] complex."""
+        _lib.call("tcb_usfft2d_fwd", self._live(), _lib.ptr(g_), _lib.ptr(f_), _lib.ptr(theta_),
+                  float(phi), int(k), int(deth0), _lib.stream_ptr(stream_))

@@ -137,13 +137,16 @@ __device__ __forceinline__ void interval(float c, float a, float b, float &lo, f
 }
 
 // Sample position as take_x computes it (kernels_usfft2d.cu:5-18); cphi is
-// the device cosf(phi), as there (u2_tables stores it after the angles).
+// the device cosf(phi), as there (u2_tables stores it after the angles).  The
+// roundings are written out as the reference build performs them,
+// x = fma(ku, cos t, (kv sin t) cos phi) and y = fma(-(kv cos t), cos phi,
+// ku sin t), so the positions are bit-identical to take_x's.
 __device__ __forceinline__ void u2_pos(const U2Geom &g, float cphi, float2 csa, int tx, int ty,
                                        float &x, float &y) {
   float ku = (tx - g.detw / 2.0f) / g.detw;
   float kv = (ty + g.k * g.deth - g.deth0 / 2.0f) / g.deth0;
-  x = ku * csa.x + kv * csa.y * cphi;
-  y = ku * csa.y - kv * csa.x * cphi;
+  x = __fmaf_rn(ku, csa.x, __fmul_rn(__fmul_rn(kv, csa.y), cphi));
+  y = __fmaf_rn(-__fmul_rn(kv, csa.x), cphi, __fmul_rn(ku, csa.y));
   x = (float)fmin(fmax((double)x, -0.5f + 1e-5), 0.5f - 1e-5);
   y = (float)fmin(fmax((double)y, -0.5f + 1e-5), 0.5f - 1e-5);
 }
@@ -475,6 +478,136 @@ __global__ void u1_deapod(const float2 *__restrict__ grid, float *__restrict__ f
   f[(size_t)tx + (size_t)tz * n0 + (size_t)ty * n0 * n2] = v / ker / (2 * n2);
 }
 
+// ------------------------------------------------------------------ forward operators
+// cfunc_usfft2d::fwd (cfunc_usfft2d.cu:53-70): divker2d(direction 0) with the
+// fftshift sign writes f [n1][n2 slabs][n0] / ker / (n0 n1) into the centre of
+// each slab's periodic [2n1][2n0] grid (every other cell zero, so the grid
+// needs no memset), a forward 2D FFT, then each sample gathers its 9 x 9
+// footprint (gather2d direction 0, the fftshift sign at read time).
+__global__ void u2f_load(float2 *__restrict__ grid, const float2 *__restrict__ f, U2Geom geo,
+                         int nslab) {
+  const int n0 = geo.n0, n1 = geo.n1;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y;
+  const int slab = blockIdx.z;
+  if (ix >= 2 * n0 || slab >= nslab) return;
+  const int tx = ix - n0 / 2, ty = n1 - 1 + n1 / 2 - iy;
+  float2 v = make_float2(0.f, 0.f);
+  if (tx >= 0 && tx < n0 && ty >= 0 && ty < n1) {
+    const float ker = __expf(-geo.mu0 * (tx - n0 / 2) * (tx - n0 / 2) -
+                             geo.mu1 * (ty - n1 / 2) * (ty - n1 / 2));
+    const float2 a = f[(size_t)tx + (size_t)slab * n0 + (size_t)ty * n0 * nslab];
+    const float nn = (float)(n0 * n1);
+    const float s = (float)(sgn_idx(ix + geo.m0) * sgn_idx(iy + geo.m1));
+    v = make_float2(a.x / ker / nn * s, a.y / ker / nn * s);
+  }
+  grid[(size_t)slab * (2 * n0) * (2 * n1) + (size_t)iy * (2 * n0) + ix] = v;
+}
+
+template <int M0, int M1>
+__global__ void u2f_gather(float2 *__restrict__ g, const float2 *__restrict__ grid,
+                           const float2 *__restrict__ cs, const float *__restrict__ ex,
+                           const float *__restrict__ ey, U2Geom geo) {
+  const int n0 = geo.n0, n1 = geo.n1, detw = geo.detw, deth = geo.deth;
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ty = blockIdx.y;   // detector row of this call = slab
+  const int tz = blockIdx.z;   // angle
+  if (tx >= detw) return;
+  float x0, y0;
+  u2_pos(geo, cs[geo.ntheta].x, cs[tz], tx, ty, x0, y0);
+  const int b0 = (int)floorf(2 * n0 * x0) - M0;
+  const int b1 = (int)floorf(2 * n1 * y0) - M1;
+  float k0[2 * M0 + 1], k1[2 * M1 + 1];
+#pragma unroll
+  for (int t = 0; t < 2 * M0 + 1; t++) {
+    const float w0 = ex[b0 + t + n0 + M0 + EPAD] - x0;
+    k0[t] = __expf(geo.c0 * (w0 * w0));
+  }
+#pragma unroll
+  for (int t = 0; t < 2 * M1 + 1; t++) {
+    const float w1 = ey[b1 + t + n1 + M1 + EPAD] - y0;
+    k1[t] = __expf(geo.c1 * (w1 * w1));
+  }
+  const float2 *gz = grid + (size_t)ty * (2 * n0) * (2 * n1);
+  float sr = 0.f, si = 0.f;
+#pragma unroll
+  for (int t1 = 0; t1 < 2 * M1 + 1; t1++) {
+    int iy = n1 + b1 + t1;                 // periodic cell of fdee2d row n1 + m1 + ell1
+    const int sy = sgn_idx(iy + M1);
+    iy = (iy % (2 * n1) + 2 * n1) % (2 * n1);
+#pragma unroll
+    for (int t0 = 0; t0 < 2 * M0 + 1; t0++) {
+      int ix = n0 + b0 + t0;
+      const float s = (float)(sy * sgn_idx(ix + M0));
+      ix = (ix % (2 * n0) + 2 * n0) % (2 * n0);
+      const float2 v = gz[(size_t)iy * (2 * n0) + ix];
+      const float w = k0[t0] * k1[t1] * geo.wscale * s;
+      sr += w * v.x;
+      si += w * v.y;
+    }
+  }
+  // gather2d's storage: the upper half of the detector frequencies (tx > detw/2)
+  // goes, mirrored, to angle planes ntheta.. (cfunc_usfft2d packing)
+  int txs = tx, tys = ty, tzs = tz;
+  if (tx > detw / 2) {
+    txs = detw - tx;
+    tys = deth - ty - 1;
+    tzs = tz + geo.ntheta;
+  }
+  g[(size_t)txs + (size_t)tys * (detw / 2 + 1) + (size_t)tzs * (detw / 2 + 1) * deth] =
+      make_float2(sr, si);
+}
+
+// cfunc_usfft1d::fwd (cfunc_usfft1d.cu:50-66): divker1d(direction 0) with the
+// fftshift sign into the periodic [2n2][n1][n0] grid (cells outside the n2
+// centred rows zero), a forward FFT along the 2n2 axis, then each height
+// sample gathers its 2m+1 cells (gather1d direction 0).
+__global__ void u1f_load(float2 *__restrict__ grid, const float *__restrict__ f, U1Geom geo) {
+  const int n0 = geo.n0, n1 = geo.n1, n2 = geo.n2;
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ty = blockIdx.y;
+  const int iz = blockIdx.z;  // 0 .. 2 n2 - 1
+  if (tx >= n0) return;
+  const int tz = iz - n2 / 2;
+  float v = 0.f;
+  if (tz >= 0 && tz < n2) {
+    const float ker = __expf(-geo.mu2 * (tz - n2 / 2) * (tz - n2 / 2));
+    v = f[(size_t)tx + (size_t)tz * n0 + (size_t)ty * n0 * n2] / ker / (2 * n2) *
+        (float)sgn_idx(iz + geo.m2);
+  }
+  grid[(size_t)tx + (size_t)ty * n0 + (size_t)iz * n0 * n1] = make_float2(v, 0.f);
+}
+
+// Rows t of g [n1][deth/2+1][n0] for t <= deth/2, each from its own height
+// z(t).  (The reference launches all deth rows and lets row deth - t write
+// its value into row t as well, unconjugated: a race whose winner decides
+// whether rows 0 < t < deth/2 hold g or conj(g); for real f the two differ
+// only in the sign of the imaginary part.  Here every row is written once.)
+__global__ void u1f_gather(float2 *__restrict__ g, const float2 *__restrict__ grid,
+                           const float *__restrict__ zt, const float *__restrict__ ez,
+                           U1Geom geo) {
+  const int n0 = geo.n0, n1 = geo.n1, n2 = geo.n2, M = geo.m2, deth = geo.deth;
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ty = blockIdx.y;
+  const int t = blockIdx.z;  // 0 .. deth/2
+  if (tx >= n0) return;
+  const float z0 = zt[t];
+  const int e0 = (int)floorf(2 * n2 * z0) - M;
+  float sr = 0.f, si = 0.f;
+  for (int i2 = 0; i2 < 2 * M + 1; i2++) {
+    const int ell = e0 + i2;
+    const float w2 = ez[ell + n2 + M + EPAD] - z0;
+    const float w = geo.wscale * __expf(geo.c2 * (w2 * w2));
+    int iz = n2 + ell;
+    const float s = (float)sgn_idx(iz + M);
+    iz = (iz % (2 * n2) + 2 * n2) % (2 * n2);
+    const float2 v = grid[(size_t)tx + (size_t)ty * n0 + (size_t)iz * n0 * n1];
+    sr += w * (v.x * s);
+    si += w * (v.y * s);
+  }
+  g[(size_t)tx + (size_t)t * n0 + (size_t)ty * n0 * (deth / 2 + 1)] = make_float2(sr, si);
+}
+
 }  // namespace lam
 }  // namespace tcb
 
@@ -717,6 +850,49 @@ extern "C" int tcb_usfft2d_adj_rows(tcb_usfft2d *h, void *S2, const void *S1,
   return st;
 }
 
+// cfunc_usfft2d::fwd: g complex [2*ntheta][deth][detw/2+1] (the packed layout
+// that adj reads) from f complex [n1][n2][n0], chunk index k.
+extern "C" int tcb_usfft2d_fwd(tcb_usfft2d *h, void *g, const void *f, const float *theta,
+                               float phi, int k, int deth0, void *stream) {
+  TCB_CHECK_ARG(h && h->grid, "tcb_usfft2d_fwd: null or freed handle");
+  TCB_CHECK_ARG(g && f && theta, "tcb_usfft2d_fwd: null pointer");
+  TCB_CHECK_ARG((size_t)h->geo.deth == h->n2, "tcb_usfft2d_fwd: deth must equal n2 slabs");
+  TCB_CHECK_ARG(h->geo.ntheta <= 65535 && h->geo.deth <= 65535 && 2 * h->geo.n1 <= 65535,
+                "tcb_usfft2d_fwd: grid too large");
+  cudaStream_t s = (cudaStream_t)stream;
+  U2Geom geo = h->geo;
+  geo.k = k;
+  geo.deth0 = deth0;
+  geo.fused = 0;
+  geo.in_scale = nullptr;
+  const int nslab = (int)h->n2;
+  int tab = (int)std::max<size_t>(h->geo.ntheta,
+                                  2 * std::max(geo.n0, geo.n1) + 2 * 4 + 1 + 2 * EPAD);
+  u2_tables<<<ceil_div(tab, 256), 256, 0, s>>>(h->cs, h->ex, h->ey, theta, phi, geo.ntheta,
+                                              geo.n0, geo.m0, geo.n1, geo.m1);
+  TCB_LAUNCH_CHECK();
+  {
+    StageTimer st("usfft2d_fwd_load", s);
+    u2f_load<<<dim3(ceil_div(2 * geo.n0, 256), 2 * geo.n1, nslab), 256, 0, s>>>(
+        h->grid, (const float2 *)f, geo, nslab);
+    TCB_LAUNCH_CHECK();
+  }
+  TCB_CUFFT(cufftSetStream(h->plan, s));
+  {
+    StageTimer st("usfft2d_fwd_fft", s);
+    TCB_CUFFT(cufftExecC2C(h->plan, (cufftComplex *)h->grid, (cufftComplex *)h->grid,
+                           CUFFT_FORWARD));
+  }
+  {
+    StageTimer st("usfft2d_fwd_gather", s);
+    u2f_gather<4, 4><<<dim3(ceil_div(geo.detw, 128), geo.deth, geo.ntheta), 128, 0, s>>>(
+        (float2 *)g, h->grid, h->cs, h->ex, h->ey, geo);
+    TCB_LAUNCH_CHECK();
+  }
+  count_launch(3);
+  return TCB_OK;
+}
+
 // The sample positions that the gridding above uses, one per (angle, detector
 // row of the call, detector column), written in take_x's layout.
 __global__ void u2_positions(float *__restrict__ x, float *__restrict__ y,
@@ -879,6 +1055,39 @@ extern "C" int tcb_usfft1d_adj(tcb_usfft1d *h, void *f, const void *g, float phi
     TCB_LAUNCH_CHECK();
     count_launch();
   }
+  return TCB_OK;
+}
+
+// cfunc_usfft1d::fwd: g complex [n1][deth/2+1][n0] from f real [n1][n2][n0].
+extern "C" int tcb_usfft1d_fwd(tcb_usfft1d *h, void *g, const void *f, float phi,
+                               void *stream) {
+  TCB_CHECK_ARG(h && h->grid, "tcb_usfft1d_fwd: null or freed handle");
+  TCB_CHECK_ARG(f && g, "tcb_usfft1d_fwd: null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const U1Geom &geo = h->geo;
+  TCB_CHECK_ARG(geo.deth / 2 + 1 <= 65535, "tcb_usfft1d_fwd: deth too large");
+  int tab = std::max(geo.deth, 2 * geo.n2 + 2 * geo.m2 + 1 + 2 * EPAD);
+  u1_tables<<<ceil_div(tab, 256), 256, 0, s>>>(h->zt, h->ez, phi, geo.deth, geo.n2, geo.m2);
+  TCB_LAUNCH_CHECK();
+  {
+    StageTimer st("usfft1d_fwd_load", s);
+    u1f_load<<<dim3(ceil_div(geo.n0, 128), geo.n1, 2 * geo.n2), 128, 0, s>>>(
+        h->grid, (const float *)f, geo);
+    TCB_LAUNCH_CHECK();
+  }
+  TCB_CUFFT(cufftSetStream(h->plan, s));
+  {
+    StageTimer st("usfft1d_fwd_fft", s);
+    TCB_CUFFT(cufftExecC2C(h->plan, (cufftComplex *)h->grid, (cufftComplex *)h->grid,
+                           CUFFT_FORWARD));
+  }
+  {
+    StageTimer st("usfft1d_fwd_gather", s);
+    u1f_gather<<<dim3(ceil_div(geo.n0, 128), geo.n1, geo.deth / 2 + 1), 128, 0, s>>>(
+        (float2 *)g, h->grid, h->zt, h->ez, geo);
+    TCB_LAUNCH_CHECK();
+  }
+  count_launch(3);
   return TCB_OK;
 }
 

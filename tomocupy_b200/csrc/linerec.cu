@@ -46,6 +46,27 @@ template <> __device__ __forceinline__ __half from_f32<__half>(float v) {
   return __float2half_rn(v);
 }
 
+// The reference kernel's arithmetic (kernels_linerec.cuh:23-40) with every
+// rounding written out, so that no compiler contraction can differ from the
+// reference build's: u = fma(R0, x, R1 y) + n/2,
+// v = fma(R5, z, fma(R3, x, R4 y)) + nz/2 (R3 = sin(t) cos(phi),
+// R4 = -cos(t) cos(phi)), and the bilinear sum
+// fma(d11, w11, fma(d10, w10, fma(d00, w00, d01 w01))) added to the
+// accumulator.  Bit-identical per angle to the reference build.
+__device__ __forceinline__ float lr_u(float R0, float R1, float x, float y, float h) {
+  return __fadd_rn(__fmaf_rn(R0, x, __fmul_rn(R1, y)), h);
+}
+__device__ __forceinline__ float lr_v(float R3, float R4, float R5, float x, float y, float z,
+                                      float hz) {
+  return __fadd_rn(__fmaf_rn(R5, z, __fmaf_rn(R3, x, __fmul_rn(R4, y))), hz);
+}
+__device__ __forceinline__ float lr_interp(float d00, float d01, float d10, float d11, float u,
+                                           float v) {
+  const float w00 = __fmul_rn(1 - u, 1 - v), w01 = __fmul_rn(u, 1 - v);
+  const float w10 = __fmul_rn(1 - u, v), w11 = __fmul_rn(u, v);
+  return __fmaf_rn(d11, w11, __fmaf_rn(d10, w10, __fmaf_rn(d00, w00, __fmul_rn(d01, w01))));
+}
+
 template <typename T, int MODE>
 __global__ void __launch_bounds__(BX *BY)
     backproject_kernel(T *__restrict__ f, const T *__restrict__ data,
@@ -79,13 +100,11 @@ __global__ void __launch_bounds__(BX *BY)
       float ctheta = s_c[k];
       float stheta = s_s[k];
       float R0 = ctheta, R1 = stheta;
-      float R3 = stheta * cphi, R4 = -ctheta * cphi, R5 = sphi;
-      float u, v;
-      if (MODE == TRY)
-        u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2 - shift;
-      else
-        u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2;
-      v = R3 * (tx - n / 2) + R4 * (ty - n / 2) + R5 * zz + nz / 2;
+      float R3 = __fmul_rn(stheta, cphi), R4 = __fmul_rn(-ctheta, cphi), R5 = sphi;
+      float u = lr_u(R0, R1, (float)(tx - n / 2), (float)(ty - n / 2), (float)(n / 2));
+      if (MODE == TRY) u = __fsub_rn(u, shift);
+      float v = lr_v(R3, R4, R5, (float)(tx - n / 2), (float)(ty - n / 2), (float)zz,
+                     (float)(nz / 2));
       int ur = (int)(u - 1e-5f);
       int vr = (int)(v - 1e-5f);
       if ((ur >= 0) & (ur < n - 1) & (vr >= 0) & (vr < nz - 1)) {
@@ -93,14 +112,13 @@ __global__ void __launch_bounds__(BX *BY)
         v = v - vr;
         const T *d0 = data + ur + (size_t)t * n + (size_t)vr * n * nproj;
         const T *d1 = d0 + (size_t)n * nproj;
-        f0 += ld(d0) * ((1 - u) * (1 - v)) + ld(d0 + 1) * ((0 + u) * (1 - v)) +
-              ld(d1) * ((1 - u) * (0 + v)) + ld(d1 + 1) * ((0 + u) * (0 + v));
+        f0 = __fadd_rn(f0, lr_interp(ld(d0), ld(d0 + 1), ld(d1), ld(d1 + 1), u, v));
       }
     }
   }
   if (!active) return;
   T *o = f + tx + (size_t)(n - ty - 1) * n + (size_t)tz * n * n;
-  *o = from_f32<T>(ld(o) + f0 * c);
+  *o = from_f32<T>(__fmaf_rn(f0, c, ld(o)));
 }
 
 // FULL mode, ZS consecutive slices per thread, sinogram footprints staged in
@@ -166,8 +184,8 @@ __global__ void __launch_bounds__(BX *BY)
       float ctheta = s_c[k];
       float stheta = s_s[k];
       float R0 = ctheta, R1 = stheta;
-      float R3 = stheta * cphi, R4 = -ctheta * cphi, R5 = sphi;
-      float u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2;
+      float R3 = __fmul_rn(stheta, cphi), R4 = __fmul_rn(-ctheta, cphi), R5 = sphi;
+      float u = lr_u(R0, R1, (float)(tx - n / 2), (float)(ty - n / 2), (float)(n / 2));
       int ur = (int)(u - 1e-5f);
       if (!((ur >= 0) & (ur < n - 1))) continue;
       u = u - ur;
@@ -177,7 +195,8 @@ __global__ void __launch_bounds__(BX *BY)
       for (int s = 0; s < ZS; s++) {
         const int tz = tz0 + s;
         const int zz = tz + sz - nz / 2;
-        float v = R3 * (tx - n / 2) + R4 * (ty - n / 2) + R5 * zz + nz / 2;
+        float v = lr_v(R3, R4, R5, (float)(tx - n / 2), (float)(ty - n / 2), (float)zz,
+                     (float)(nz / 2));
         int vr = (int)(v - 1e-5f);
         if ((tz < ncz) & (vr >= 0) & (vr < nz - 1)) {
           v = v - vr;
@@ -196,8 +215,7 @@ __global__ void __launch_bounds__(BX *BY)
             x10 = ld(d1);
             x11 = ld(d1 + 1);
           }
-          acc[s] += x00 * ((1 - u) * (1 - v)) + x01 * ((0 + u) * (1 - v)) +
-                    x10 * ((1 - u) * (0 + v)) + x11 * ((0 + u) * (0 + v));
+          acc[s] = __fadd_rn(acc[s], lr_interp(x00, x01, x10, x11, u, v));
         }
       }
     }
@@ -208,7 +226,7 @@ __global__ void __launch_bounds__(BX *BY)
     const int tz = tz0 + s;
     if (tz >= ncz) break;
     T *o = f + tx + (size_t)(n - ty - 1) * n + (size_t)tz * n * n;
-    *o = from_f32<T>(ld(o) + acc[s] * c);
+    *o = from_f32<T>(__fmaf_rn(acc[s], c, ld(o)));
   }
 }
 
@@ -298,8 +316,8 @@ __global__ void __launch_bounds__(BX *BY)
         float ctheta = s_c[st][k];
         float stheta = s_s[st][k];
         float R0 = ctheta, R1 = stheta;
-        float R3 = stheta * cphi, R4 = -ctheta * cphi, R5 = sphi;
-        float u = R0 * (tx - n / 2) + R1 * (ty - n / 2) + n / 2;
+        float R3 = __fmul_rn(stheta, cphi), R4 = __fmul_rn(-ctheta, cphi), R5 = sphi;
+        float u = lr_u(R0, R1, (float)(tx - n / 2), (float)(ty - n / 2), (float)(n / 2));
         int ur = (int)(u - 1e-5f);
         if (!((ur >= 0) & (ur < n - 1))) continue;
         u = u - ur;
@@ -310,7 +328,8 @@ __global__ void __launch_bounds__(BX *BY)
         for (int s = 0; s < ZS; s++) {
           const int tz = tz0 + s;
           const int zz = tz + sz - nz / 2;
-          float v = R3 * (tx - n / 2) + R4 * (ty - n / 2) + R5 * zz + nz / 2;
+          float v = lr_v(R3, R4, R5, (float)(tx - n / 2), (float)(ty - n / 2), (float)zz,
+                     (float)(nz / 2));
           int vr = (int)(v - 1e-5f);
           if ((tz < ncz) & (vr >= 0) & (vr < nz - 1)) {
             v = v - vr;
@@ -329,8 +348,7 @@ __global__ void __launch_bounds__(BX *BY)
               x10 = d1[0];
               x11 = d1[1];
             }
-            acc[s] += x00 * ((1 - u) * (1 - v)) + x01 * ((0 + u) * (1 - v)) +
-                      x10 * ((1 - u) * (0 + v)) + x11 * ((0 + u) * (0 + v));
+            acc[s] = __fadd_rn(acc[s], lr_interp(x00, x01, x10, x11, u, v));
           }
         }
       }
@@ -353,7 +371,7 @@ __global__ void __launch_bounds__(BX *BY)
     const int tz = tz0 + s;
     if (tz >= ncz) break;
     float *o = f + tx + (size_t)(n - ty - 1) * n + (size_t)tz * n * n;
-    *o = *o + acc[s] * c;
+    *o = __fmaf_rn(acc[s], c, *o);
   }
 }
 

@@ -7,11 +7,13 @@
 //           gamma[0] -= 1
 //   sino[z][p][x] += v[z][x] for x in the mask's column range.
 // The column means reduce over angles with one thread per (slice, column)
-// (coalesced along x, double accumulation in a fixed order); the
-// convolution is cuFFT D2Z / Z2D over the nz rows with the gamma spectrum
-// (float64, 1/n folded in) resident; the add is one pass over the chunk,
-// in double and rounded once to float32 like the reference's float32 +
-// float64 in-place add.
+// (coalesced along x, double accumulation in a fixed order, rounded to
+// float32); the convolution follows the reference's types: a float32 real
+// FFT of the float32 row (cuFFT R2C, as cupy.fft.rfft of a float32 array),
+// promoted to complex128 and multiplied by the float64 gamma spectrum (1/n
+// folded in, resident), then a float64 inverse (cuFFT Z2D); the add is one
+// pass over the chunk, in double and rounded once to float32 like the
+// reference's float32 + float64 in-place add.
 #include <cmath>
 #include <vector>
 
@@ -21,6 +23,8 @@ struct tcb_stripe_ti {
   size_t nproj, nz, n;
   long long m0, m1;  // masked column range [m0, m1)
   cufftHandle fwd = 0, inv = 0;
+  float *v32 = nullptr;         // [nz, n] float32 rows (mean minus column 0)
+  cufftComplex *V32 = nullptr;  // [nz, n/2+1] their float32 spectra
   double *v = nullptr;          // [nz, n]
   double2 *V = nullptr;         // [nz, n/2+1]
   double2 *G = nullptr;         // [n/2+1] rfft(gamma) / n
@@ -30,7 +34,7 @@ namespace tcb {
 namespace {
 
 // mean over angles minus the row's first mean: v[z][x] = float32(mean) - float32(mean_0)
-__global__ void ti_colmean(double *__restrict__ v, const float *__restrict__ sino, int nproj,
+__global__ void ti_colmean(float *__restrict__ v, const float *__restrict__ sino, int nproj,
                            int n, size_t zstride, size_t pstride) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y;
@@ -38,28 +42,30 @@ __global__ void ti_colmean(double *__restrict__ v, const float *__restrict__ sin
   const float *s = sino + (size_t)z * zstride + x;
   double acc = 0.0;
   for (int p = 0; p < nproj; p++) acc += (double)__ldg(s + (size_t)p * pstride);
-  v[(size_t)z * n + x] = (double)(float)(acc / nproj);
+  v[(size_t)z * n + x] = (float)(acc / nproj);
 }
 
-__global__ void ti_sub_first(double *__restrict__ v, int n) {
+__global__ void ti_sub_first(float *__restrict__ v, int n) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int z = blockIdx.y;
   // column 0 is only read here (ti_zero_first clears it afterwards)
   if (x >= n) return;
-  const double v0 = v[(size_t)z * n];
-  if (x > 0) v[(size_t)z * n + x] = (double)((float)v[(size_t)z * n + x] - (float)v0);
+  const float v0 = v[(size_t)z * n];
+  if (x > 0) v[(size_t)z * n + x] = v[(size_t)z * n + x] - v0;
 }
 
-__global__ void ti_zero_first(double *__restrict__ v, int n) {
-  v[(size_t)blockIdx.x * n] = 0.0;
+__global__ void ti_zero_first(float *__restrict__ v, int n) {
+  v[(size_t)blockIdx.x * n] = 0.f;
 }
 
-__global__ void ti_mul(double2 *__restrict__ V, const double2 *__restrict__ G, int nc,
-                       size_t total) {
+// complex64 spectrum promoted to complex128, times the float64 gamma spectrum
+__global__ void ti_mul(double2 *__restrict__ V, const cufftComplex *__restrict__ V32,
+                       const double2 *__restrict__ G, int nc, size_t total) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= total) return;
-  const double2 a = V[t], g = G[t % nc];
-  V[t] = make_double2(a.x * g.x - a.y * g.y, a.x * g.y + a.y * g.x);
+  const double ax = V32[t].x, ay = V32[t].y;
+  const double2 g = G[t % nc];
+  V[t] = make_double2(ax * g.x - ay * g.y, ax * g.y + ay * g.x);
 }
 
 __global__ void ti_add(float *__restrict__ sino, const double *__restrict__ v, int nproj, int n,
@@ -78,6 +84,10 @@ void ti_release(tcb_stripe_ti *h) {
   cudaFree(h->v);
   cudaFree(h->V);
   cudaFree(h->G);
+  cudaFree(h->v32);
+  cudaFree(h->V32);
+  h->v32 = nullptr;
+  h->V32 = nullptr;
   h->fwd = h->inv = 0;
   h->v = nullptr;
   h->V = h->G = nullptr;
@@ -150,7 +160,9 @@ extern "C" int tcb_stripe_ti_create(tcb_stripe_ti **out, size_t nproj, size_t nz
     delete h;
     return code;
   };
-  if (cudaMalloc(&h->v, nz * n * sizeof(double)) != cudaSuccess ||
+  if (cudaMalloc(&h->v32, nz * n * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->V32, nz * nc * sizeof(cufftComplex)) != cudaSuccess ||
+      cudaMalloc(&h->v, nz * n * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&h->V, nz * nc * sizeof(double2)) != cudaSuccess ||
       cudaMalloc(&h->G, nc * sizeof(double2)) != cudaSuccess) {
     cudaGetLastError();
@@ -163,7 +175,7 @@ extern "C" int tcb_stripe_ti_create(tcb_stripe_ti **out, size_t nproj, size_t nz
   }
   int len[1] = {(int)n};
   cufftResult r = cufftPlanMany(&h->fwd, 1, len, nullptr, 1, (int)n, nullptr, 1, (int)nc,
-                                CUFFT_D2Z, (int)nz);
+                                CUFFT_R2C, (int)nz);
   if (r == CUFFT_SUCCESS)
     r = cufftPlanMany(&h->inv, 1, len, nullptr, 1, (int)nc, nullptr, 1, (int)n, CUFFT_Z2D,
                       (int)nz);
@@ -190,16 +202,17 @@ extern "C" int tcb_stripe_ti_apply_sino(tcb_stripe_ti *h, float *sino, size_t zs
   const int n = (int)h->n, nz = (int)h->nz, np = (int)h->nproj;
   const size_t nc = h->n / 2 + 1;
   StageTimer t("stripe_ti", s);
-  ti_colmean<<<dim3(ceil_div(h->n, 256), nz), 256, 0, s>>>(h->v, sino, np, n, zstride, pstride);
+  ti_colmean<<<dim3(ceil_div(h->n, 256), nz), 256, 0, s>>>(h->v32, sino, np, n, zstride,
+                                                             pstride);
   TCB_LAUNCH_CHECK();
-  ti_sub_first<<<dim3(ceil_div(h->n, 256), nz), 256, 0, s>>>(h->v, n);
+  ti_sub_first<<<dim3(ceil_div(h->n, 256), nz), 256, 0, s>>>(h->v32, n);
   TCB_LAUNCH_CHECK();
-  ti_zero_first<<<nz, 1, 0, s>>>(h->v, n);
+  ti_zero_first<<<nz, 1, 0, s>>>(h->v32, n);
   TCB_LAUNCH_CHECK();
   TCB_CUFFT(cufftSetStream(h->fwd, s));
   TCB_CUFFT(cufftSetStream(h->inv, s));
-  TCB_CUFFT(cufftExecD2Z(h->fwd, h->v, (cufftDoubleComplex *)h->V));
-  ti_mul<<<ceil_div(h->nz * nc, 256), 256, 0, s>>>(h->V, h->G, (int)nc, h->nz * nc);
+  TCB_CUFFT(cufftExecR2C(h->fwd, h->v32, h->V32));
+  ti_mul<<<ceil_div(h->nz * nc, 256), 256, 0, s>>>(h->V, h->V32, h->G, (int)nc, h->nz * nc);
   TCB_LAUNCH_CHECK();
   TCB_CUFFT(cufftExecZ2D(h->inv, (cufftDoubleComplex *)h->V, h->v));
   if (h->m1 > h->m0) {

@@ -62,8 +62,6 @@ class SinoPipeline:
             raise NotImplementedError(f"SinoPipeline: mixed_filter {mixed_filter!r}")
         if out_dtype not in ("float32", "float16"):
             raise NotImplementedError(f"SinoPipeline: out_dtype {out_dtype!r}")
-        if out_dtype == "float16" and algorithm != "fourierrec":
-            raise NotImplementedError("fp16 output slices: fourierrec only")
         self.out_dtype = torch.float16 if out_dtype == "float16" else torch.float32
         if algorithm == "fourierrec" and ncz % 2:
             raise ValueError("fourierrec needs an even number of rows per chunk")
@@ -165,6 +163,11 @@ class SinoPipeline:
                                 device=self.device)
             self.crop = torch.empty((self.ncz, self.nproj, self.n), dtype=torch.float32,
                                     device=self.device)
+            # fp16 output slices (the reference's float16 path returns fp16
+            # volumes): lprec and linerec accumulate in fp32 here, then round
+            self.out32 = (torch.empty((self.ncz, self.n, self.n), dtype=torch.float32,
+                                      device=self.device)
+                          if self.out_dtype == torch.float16 else None)
 
     def weights(self, sht=None) -> torch.Tensor:
         """Per-slice filter spectra (cached for the zero shift)."""
@@ -179,8 +182,10 @@ class SinoPipeline:
         return torch.view_as_real(
             phase_weights(self.wfilter, self.t, self.center, sht, self.n)).contiguous()
 
-    def load_rows(self, data, dark0=None, flat0=None, z_lo=0, stream=None):
-        """Fill the padded filter rows from a [nproj, nz, n] frame (or float) stack view."""
+    def load_rows(self, data, dark0=None, flat0=None, z_lo=0, stream=None, flat1=None):
+        """Fill the padded filter rows from a [nproj, nz, n] frame (or float) stack view.
+        flat1: the second flat mean of flat_linear (the per-angle blend of
+        proc_functions.py:62-66), or None."""
         nz = data.shape[1]
         assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.ni
         if self.pad360 is not None and not self.fused:
@@ -195,6 +200,8 @@ class SinoPipeline:
             data = _dezinger(data, *self.dezinger, out=zb, stream=stream)
         d0 = dark0[z_lo:z_lo + nz] if dark0 is not None else None
         f0 = flat0[z_lo:z_lo + nz] if flat0 is not None else None
+        f1 = flat1[z_lo:z_lo + nz] if flat1 is not None else None
+        fl = dict(flat1=f1, flat_linear=f1 is not None)
         if self.fw is not None:
             fw = self.fw
             s = torch.cuda.current_stream() if stream is None else stream
@@ -202,7 +209,7 @@ class SinoPipeline:
                 self.sino.zero_()
             prep_rows(self.sino, data, d0, f0, darkflat=dark0 is not None, minus_log=False,
                       out_zstride=fw.nproj_pad * self.ni, out_pstride=self.ni,
-                      out_poff=fw.poff, stream=stream)
+                      out_poff=fw.poff, stream=stream, **fl)
             fw.apply_sino(self.sino, stream)
             src = self.sino[:nz, fw.poff:fw.poff + self.nproj].permute(1, 0, 2)
             if self.tensor_filter:
@@ -222,18 +229,18 @@ class SinoPipeline:
         if self.tensor_filter:
             prep_rows_split16(self.xhi, self.xlo, data, d0, f0, darkflat=dark0 is not None,
                               minus_log=self.minus_log, out_zstride=self.nproj * self.npl,
-                              out_pstride=self.npl, stream=stream)
+                              out_pstride=self.npl, stream=stream, **fl)
             return
         if self.fused:
             prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                       minus_log=self.minus_log, out_zstride=self.nproj * self.n,
-                      out_pstride=self.n, stream=stream)
+                      out_pstride=self.n, stream=stream, **fl)
             self._pad360_rows(nz, stream)
             return
         prep_rows(self.rows, data, d0, f0, darkflat=dark0 is not None,
                   minus_log=self.minus_log, out_zstride=self.nproj * self.ne,
                   out_pstride=self.ne, out_xoff=self.pad, out_width=self.ne, edge_pad=True,
-                  stream=stream)
+                  stream=stream, **fl)
 
     def _pad360_rows(self, nz: int, stream=None) -> None:
         """Double-FOV padding of the -log rows of nz slices, in place (ni -> 2 ni)."""
@@ -345,6 +352,15 @@ class SinoPipeline:
     def filter_and_backproject(self, out, sht=None, stream=None):
         """out [ncz, n, n] of self.out_dtype (contiguous) from the loaded rows."""
         assert out.dtype == self.out_dtype, (out.dtype, self.out_dtype)
+        if self.algorithm != "fourierrec" and out.dtype == torch.float16:
+            self._filter_and_backproject32(self.out32[:out.shape[0]], sht, stream)
+            s = torch.cuda.current_stream() if stream is None else stream
+            with torch.cuda.stream(s) if not isinstance(s, int) else _nullctx():
+                out.copy_(self.out32[:out.shape[0]])
+            return out
+        return self._filter_and_backproject32(out, sht, stream)
+
+    def _filter_and_backproject32(self, out, sht=None, stream=None):
         if self.tensor_filter:
             return self._filter_and_backproject_mixed(out, sht, stream)
         if self.fused:
@@ -365,8 +381,9 @@ class SinoPipeline:
                 self.lp.fslv.backprojection(out, self.crop, stream)
         return out
 
-    def reconstruct(self, out, data, dark0=None, flat0=None, z_lo=0, sht=None, stream=None):
-        self.load_rows(data, dark0, flat0, z_lo, stream)
+    def reconstruct(self, out, data, dark0=None, flat0=None, z_lo=0, sht=None, stream=None,
+                    flat1=None):
+        self.load_rows(data, dark0, flat0, z_lo, stream, flat1=flat1)
         return self.filter_and_backproject(out, sht, stream)
 
 

@@ -31,9 +31,8 @@ def _supported():
         raise NotImplementedError(f"file_type={args.file_type!r}")
     if not 0 <= int(args.binning) <= 4:
         raise NotImplementedError("binning above 4")
-    if args.dtype not in ("float32", "mixed"):
-        raise NotImplementedError(
-            "the fused driver runs the float32 drop-in path or the 'mixed' tensor-core path")
+    if args.dtype not in ("float32", "float16", "mixed"):
+        raise NotImplementedError(f"dtype={args.dtype!r}")
 
 
 def _stripe_args():
@@ -46,14 +45,6 @@ def _stripe_args():
 
 
 _pad360_args = pad360_args
-
-
-def _no_phase(where):
-    if args.retrieve_phase_method in PHASE_METHODS or _rotate():
-        raise NotImplementedError(
-            f"{where}: phase retrieval and projection rotation work on whole "
-            "projections; run GPURecSteps (the reference applies them to the rows of "
-            "each sinogram chunk here)")
 
 
 def _rotate():
@@ -82,7 +73,21 @@ class GPURec:
 
     @property
     def precision(self) -> str:
-        return "mixed" if args.dtype == "mixed" else "float32"
+        """'mixed' (fp16 weights and values on the tensor cores, fp32
+        accumulation) for dtype 'mixed' and, with fourierrec, for the
+        reference's dtype 'float16' (its cfunc_*fp16 operators grid in fp16);
+        'float32' otherwise."""
+        if args.dtype == "mixed":
+            return "mixed"
+        if args.dtype == "float16" and args.reconstruction_algorithm == "fourierrec":
+            return "mixed"
+        return "float32"
+
+    @staticmethod
+    def out_dtype() -> str:
+        """Output slices: float16 for the reference's dtype 'float16' (its
+        reconstruction arrays are float16), else args.out_dtype."""
+        return "float16" if args.dtype == "float16" else args.out_dtype
 
     @property
     def pipe(self) -> SinoPipeline:
@@ -97,7 +102,7 @@ class GPURec:
                                       args.reconstruction_algorithm,
                                       minus_log=args.minus_log == "True", device=self.device,
                                       stripe=stripe, precision=self.precision,
-                                      out_dtype=args.out_dtype,
+                                      out_dtype=self.out_dtype(),
                                       mixed_filter=args.mixed_filter,
                                       dezinger=None if proj_ops else dezinger_args(),
                                       ni=params.ni,
@@ -106,14 +111,13 @@ class GPURec:
 
     # ------------------------------------------------------------------ helpers
     def _stats(self, dark, flat, stream):
-        flat_linear = args.flat_linear == "True"
-        if flat_linear:
-            raise NotImplementedError("flat_linear in the fused driver")
+        """dark0, flat0 and (flat_linear) flat1 of darkflat_correction
+        (proc_functions.py:55-74), after outlier removal of the darks and flats."""
         dz = dezinger_args()
         if dz is not None:   # proc_sino cleans darks and flats too (proc_functions.py:146-148)
             dark = dezinger(dark, *dz, stream=stream)
             flat = dezinger(flat, *dz, stream=stream)
-        return darkflat_stats(dark, flat, args.bright_ratio, False, stream)
+        return darkflat_stats(dark, flat, args.bright_ratio, args.flat_linear == "True", stream)
 
     # ------------------------------------------------------------------ full
     def recon_preprocessed(self, data):
@@ -124,7 +128,7 @@ class GPURec:
         assert data.dtype == torch.float32 and tuple(data.shape) == (params.nproj, nz, n)
         pipe = SinoPipeline(n, params.nproj, ncz, params.theta, params.center, args.fbp_filter,
                             args.reconstruction_algorithm, minus_log=False, device=self.device,
-                            stripe=None, precision=self.precision, out_dtype=args.out_dtype,
+                            stripe=None, precision=self.precision, out_dtype=self.out_dtype(),
                             mixed_filter=args.mixed_filter)
         rec_out = self.cl_writer.allocate(nz, n)
         out = torch.empty((ncz, n, n), dtype=pipe.out_dtype, device=self.device)
@@ -155,7 +159,7 @@ class GPURec:
             flat_d = flat.to(dev, non_blocking=True)
         s2.wait_stream(s1)
         with torch.cuda.stream(s2):
-            dark0, flat0, _ = self._stats(dark_d, flat_d, s2)
+            dark0, flat0, flat1 = self._stats(dark_d, flat_d, s2)
         host_in = data.device.type == "cpu"
         host_out = rec_out.device.type == "cpu"
         dbuf = [torch.empty((nproj, ncz, data.shape[2]), dtype=data.dtype, device=dev)
@@ -191,10 +195,12 @@ class GPURec:
                 if lz < ncz:  # rows of the previous chunk must not pair with this one's
                     self.pipe.clear_rows(lz, s2)
                 if phase:
-                    self.pipe.reconstruct(out, self._phase_chunk(src, dark0, flat0, z0, s2),
+                    self.pipe.reconstruct(out, self._phase_chunk(src, dark0, flat0, z0, s2,
+                                                                 flat1),
                                           None, None, z_lo=z0, stream=s2)
                 else:
-                    self.pipe.reconstruct(out, src, dark0, flat0, z_lo=z0, stream=s2)
+                    self.pipe.reconstruct(out, src, dark0, flat0, z_lo=z0, stream=s2,
+                                          flat1=flat1)
                 if not host_out and lz < ncz:
                     rec_out[z0:z0 + lz].copy_(out[:lz])
                 comp_done[b].record(s2)
@@ -216,27 +222,34 @@ class GPURec:
         The sweep over all centres is one CUDA graph (TryCenterSweep), recorded
         once and replayed for each requested slice.
         """
-        _no_phase("GPURec.recon_try")
         from .trycenter import TryCenterSweep
         if args.reconstruction_algorithm != "fourierrec":
             return self._recon_try_chunks()
         data, dark, flat = self.cl_reader.frames()
         dev = self.device
+        proj_ops = _proj_chunk_ops()
         if self.sweep is None:
             self.sweep = TryCenterSweep(params.n, params.nproj, params.theta, params.center,
                                         params.shift_array, args.fbp_filter, self.precision,
                                         params.ncz, device=dev,
                                         minus_log=args.minus_log == "True",
                                         mixed_filter=args.mixed_filter, ni=params.ni,
-                                        pad360=_pad360_args(), stripe=_stripe_args())
+                                        pad360=_pad360_args(),
+                                        stripe=None if proj_ops else _stripe_args())
         sw = self.sweep
         for id_slice in params.id_slices:
             z = int(id_slice)
             row = data[:, z:z + 1].to(dev)
-            if dezinger_args() is not None:
-                row = dezinger(row, *dezinger_args())
-            d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
-            sw.load(row, d0, f0)
+            d0, f0, f1 = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
+            if proj_ops:
+                # proc_sino then proc_proj on the one-row slice, as the
+                # reference's recon_try does (rec.py:224-225): the image height
+                # of phase retrieval and rotation is 1
+                sw.load(self._phase_chunk(row, d0, f0, 0, None, f1, chunk_height=False))
+            else:
+                if dezinger_args() is not None:
+                    row = dezinger(row, *dezinger_args())
+                sw.load(row, d0, f0, f1)
             if sw.graph is None:
                 sw.capture()
             out = sw.run()
@@ -244,7 +257,7 @@ class GPURec:
                 self.cl_writer.write_data_try(out[k], params.save_centers[k], id_slice)
         torch.cuda.synchronize(dev)
 
-    def _phase_chunk(self, src, dark0, flat0, z0, stream):
+    def _phase_chunk(self, src, dark0, flat0, z0, stream, flat1=None, chunk_height=True):
         """proc_sino + proc_proj's phase step on one sinogram chunk, as the
         reference's recon_all runs them (rec.py:170-173): outlier removal,
         dark/flat, ring removal, then phase retrieval and rotation of the
@@ -263,8 +276,10 @@ class GPURec:
             buf = self._phase_buf = torch.empty(nproj * params.ncz * n, dtype=torch.float32,
                                                 device=self.device)
         tmp = buf[:nproj * lz * n].view(nproj, lz, n)
-        prep_rows(tmp, src, dark0[z0:z0 + lz], flat0[z0:z0 + lz], darkflat=True,
-                  minus_log=False, out_zstride=n, out_pstride=lz * n, stream=stream)
+        prep_rows(tmp, src, dark0[z0:z0 + lz], flat0[z0:z0 + lz],
+                  flat1[z0:z0 + lz] if flat1 is not None else None, darkflat=True,
+                  minus_log=False, flat_linear=flat1 is not None, out_zstride=n,
+                  out_pstride=lz * n, stream=stream)
         with torch.cuda.stream(stream):
             if args.remove_stripe_method == "fw":
                 from .processing.remove_stripe import remove_stripe_fw
@@ -273,6 +288,12 @@ class GPURec:
                 from .processing.remove_stripe import remove_stripe_ti
                 remove_stripe_ti(tmp, args.ti_beta, args.ti_mask)
             retrieve_phase(tmp)
+        if _rotate() and not chunk_height:
+            # a try-centre slice is rotated at its own height
+            out = torch.empty_like(tmp)
+            rotate_proj(tmp, args.rotate_proj_angle, args.rotate_proj_order, out=out,
+                        stream=stream)
+            return out
         if _rotate():
             # the reference rotates its chunk buffer of ncz rows: a partial
             # chunk is rotated at that height with zero rows below it
@@ -304,17 +325,21 @@ class GPURec:
         pipe = self.pipe
         shifts = np.asarray(params.shift_array, dtype=np.float32)
         out = torch.empty((ncz, n, n), dtype=pipe.out_dtype, device=dev)
+        proj_ops = _proj_chunk_ops()
         for id_slice in params.id_slices:
             z = int(id_slice)
             row = data[:, z:z + 1].to(dev)
-            if dezinger_args() is not None:
+            d0, f0, f1 = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
+            if proj_ops:   # proc_sino + proc_proj on the slice (rec.py:224-225)
+                row = self._phase_chunk(row, d0, f0, 0, None, f1, chunk_height=False)
+                d0 = f0 = f1 = None
+            elif dezinger_args() is not None:
                 row = dezinger(row, *dezinger_args())
-            d0, f0, _ = self._stats(dark[:, z:z + 1].to(dev), flat[:, z:z + 1].to(dev), None)
             for k0 in range(0, shifts.size, ncz):
                 cnt = min(ncz, shifts.size - k0)
                 sht = np.zeros(ncz, dtype=np.float32)
                 sht[:cnt] = shifts[k0:k0 + cnt]
-                pipe.load_rows(row, d0, f0, 0)
+                pipe.load_rows(row, d0, f0, 0, flat1=f1)
                 pipe.replicate_first_row()
                 pipe.filter_and_backproject(out, sht)
                 for kk in range(cnt):

@@ -42,8 +42,8 @@ class GPURecSteps:
             raise NotImplementedError(f"file_type={args.file_type!r}")
         if args.file_type == "double_fov" and args.lamino_angle != 0:
             raise NotImplementedError("double-FOV laminography")
-        if args.dtype != "float32":
-            raise NotImplementedError("the step driver runs the float32 path")
+        if args.dtype not in ("float32", "float16", "mixed"):
+            raise NotImplementedError(f"dtype={args.dtype!r}")
 
     # ------------------------------------------------------------ pre-processing
     def preprocessed(self):
@@ -110,6 +110,9 @@ class GPURecSteps:
         if args.reconstruction_algorithm == "fourierrec" and args.reconstruction_type == "full":
             from .reconstruction.backproj_lamfourier_parallel import BackprojLamFourierParallel
             u = BackprojLamFourierParallel(self.cl_writer, device=self.device).rec_lam(data)
+            if args.dtype == "float16":
+                u = self._out(u)
+                self.cl_writer.rec = u.to(self.cl_writer.device)
             return u
         return self._lamino_linerec(data)
 
@@ -122,12 +125,18 @@ class GPURecSteps:
             # padding follows them: pre-process the resident dataset
             # (proc_sino + proc_proj), then backproject
             if args.reconstruction_type != "full":
-                raise NotImplementedError("phase retrieval, rotation or double-FOV padding "
-                                          "with try-centre sweeps in the step driver")
+                return rec.recon_try()   # proc_sino + proc_proj of each slice
             return rec.recon_preprocessed(self.preprocessed())
         if args.reconstruction_type == "full":
             return rec.recon_all()
         return rec.recon_try()
+
+    @staticmethod
+    def _out(vol):
+        """The reference's dtype 'float16' returns float16 volumes."""
+        if args.dtype == "float16" and vol.dtype != torch.float16:
+            return vol.to(torch.float16)
+        return vol
 
     # ------------------------------------------------- laminography with linerec
     def _filtered_projections(self, data):
@@ -164,7 +173,7 @@ class GPURecSteps:
         g = self._filtered_projections(data)
         theta = torch.as_tensor(np.asarray(params.theta, dtype=np.float32), device=dev)
         ncz = params.ncz
-        lr = LineRec(theta, nproj, nproj, nz, ncz, n, args.dtype)
+        lr = LineRec(theta, nproj, nproj, nz, ncz, n, "float32")  # filtered rows are fp32
         if args.reconstruction_type == "full":
             rh = params.rh
             vol = torch.zeros((rh, n, n), dtype=torch.float32, device=dev)
@@ -174,6 +183,7 @@ class GPURecSteps:
                 lr.backprojection(f, g, None, theta, args.lamino_angle,
                                   r0 + args.lamino_start_row)
                 vol[r0:r0 + ncz] = f[:min(ncz, rh - r0)]
+            vol = self._out(vol)
             self.cl_writer.rec = vol
             return vol
         results = {}

@@ -77,7 +77,7 @@ class BackprojLamFourierParallel:
         nthetac, deth, detw = self.nthetac, self.deth, self.detw
         w = self._weights(nthetac)
         # fp16 storage of the two stage arrays (fp32 arithmetic) in mixed precision
-        half = args.dtype == "mixed"
+        half = args.dtype in ("mixed", "float16")  # fp16 storage of the stage arrays
         sdt = torch.float16 if half else torch.float32
         prec = _lib.TCB_FLOAT16 if half else _lib.TCB_FLOAT32
         nrow = deth // 2 + 1

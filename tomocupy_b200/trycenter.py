@@ -94,10 +94,11 @@ class TryCenterSweep:
         self._stream = torch.cuda.Stream(self.device)
 
     # ------------------------------------------------------------------ data
-    def load(self, data, dark0=None, flat0=None):
-        """Normalise one slice of frames (data [nproj, 1, n] on the device) into the rows."""
+    def load(self, data, dark0=None, flat0=None, flat1=None):
+        """Normalise one slice of frames (data [nproj, 1, n] on the device) into the
+        rows (flat1: the second flat mean of flat_linear, or None)."""
         with torch.cuda.stream(self._stream):
-            self.pipe.load_rows(data, dark0, flat0, 0, self._stream)
+            self.pipe.load_rows(data, dark0, flat0, 0, self._stream, flat1=flat1)
             self.pipe.replicate_first_row()
             if not self.pipe.tensor_filter and not self.pipe.fused:
                 # same buffer on every load: a captured graph reads it
