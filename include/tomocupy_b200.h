@@ -365,10 +365,21 @@ int tcb_fourierrec_set_pairs_per_block(tcb_fourierrec *h, int pairs);
  * register-accumulation gridding (default; the drop-in).  TCB_GRID_TENSOR:
  * mixed precision on the tensor cores -- footprint weights and the spectrum
  * values (power-of-two scaled) in fp16, fp32 accumulation in TMEM, 32 slice
- * pairs per weight matrix; used by the mixed-precision path.  status: 1 in
- * *timed_out when a tensor-core gridding wait gave up (synchronous). */
+ * pairs per weight matrix; used by the mixed-precision path.
+ * TCB_GRID_TENSOR_FP32: the fp32 drop-in on the tensor cores -- the weights of
+ * 16 x 16-cell tiles and chunks of 64 samples precomputed once (split fp16
+ * hi/lo images, about 64 KB per chunk: 9 GB at 2048 x 1500) and streamed by
+ * bulk copies, the spectrum split into fp16 hi/lo rows per call and
+ * gathered by cp.async, W_hi V_hi + W_lo V_hi + W_hi V_lo accumulated in fp32
+ * in TMEM (within 1e-5 of the reference).  TCB_GRID_TENSOR_STREAM: the same
+ * with fp16 weights and values only (mixed precision, half the tables).
+ * Both return TCB_ERR_OUT_OF_MEMORY when the tables do not fit (the handle
+ * keeps its previous mode).  status: 1 in *timed_out when a tensor-core
+ * gridding wait gave up (synchronous). */
 #define TCB_GRID_FP32 0
 #define TCB_GRID_TENSOR 1
+#define TCB_GRID_TENSOR_FP32 2
+#define TCB_GRID_TENSOR_STREAM 3
 int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode);
 /* Output precision (no reference counterpart): TCB_FLOAT16 writes the
  * reconstructed slices in fp16 while the input g stays fp32 (a FLOAT16 handle

@@ -133,6 +133,122 @@ def remove_stripe_ti(data, beta, mask_size, fft=NumpyFFT):
 
 
 # --------------------------------------------------------------------------
+# Vo's all-stripe removal (src/tomocupy/processing/remove_stripe.py:311-498)
+# --------------------------------------------------------------------------
+def _vo_detect(listfact, snr):
+    """_detect_stripe_batch (remove_stripe.py:346-370) on [nz, ni] float32: per
+    row, a least-squares line through the middle of the descending sort
+    (dropping a quarter at each end), a noise level from its ends, and the
+    columns beyond snr/2 noise levels above the line's start or below its
+    end (only when the row's extreme passes snr)."""
+    nz, num = listfact.shape
+    srt = np.sort(listfact, axis=1)[:, ::-1]
+    xl = np.arange(num, dtype=np.float32)
+    nd = int(0.25 * num)
+    x = xl[nd:-nd - 1]
+    y = srt[:, nd:-nd - 1]
+    n = x.size
+    xm = float(x.mean())
+    ym = y.mean(axis=1)
+    sxy = (y * x).sum(axis=1) - n * ym * xm
+    sxx = float((x ** 2).sum() - n * xm ** 2)
+    slope = sxy / sxx
+    icpt = ym - slope * xm
+    numt1 = icpt + slope * xl[-1]
+    noise = np.clip(np.abs(numt1 - icpt), 1e-6, None)
+    val1 = np.abs(srt[:, 0] - icpt) / noise
+    val2 = np.abs(srt[:, -1] - numt1) / noise
+    mask = np.zeros((nz, num), dtype=np.float32)
+    upper = (icpt + noise * snr * 0.5)[:, None]
+    lower = (numt1 - noise * snr * 0.5)[:, None]
+    mask = np.where((val1 >= snr)[:, None] & (listfact > upper), 1.0, mask)
+    mask = np.where((val2 >= snr)[:, None] & (listfact <= lower), 1.0, mask)
+    return mask
+
+
+def _vo_dilate(mask):
+    """binary_dilation with a (1, 3) structure, one iteration: a column is set
+    when it or a neighbour along the detector is set."""
+    import scipy.ndimage as ndi
+    return ndi.binary_dilation(mask, iterations=1,
+                               structure=np.ones((1, 3), dtype=bool)).astype(mask.dtype)
+
+
+def _vo_sort_t(tomo):
+    """The reference's sort along the angles: on the [ni, nz, nproj] transpose,
+    a stable argsort and the sorted values (C-contiguous in that order)."""
+    t = np.transpose(tomo, (2, 1, 0))
+    ids = np.argsort(t, axis=2, kind="stable")
+    return np.take_along_axis(t, ids, axis=2), ids
+
+
+def _vo_unsort_t(vals_t, ids):
+    """Inverse of _vo_sort_t on [ni, nz, nproj] values, back to [nproj, nz, ni]."""
+    inv = np.empty_like(ids)
+    np.put_along_axis(inv, ids, np.broadcast_to(np.arange(ids.shape[2], dtype=ids.dtype),
+                                                ids.shape), axis=2)
+    return np.transpose(np.take_along_axis(vals_t, inv, axis=2), (2, 1, 0))
+
+
+def _vo_large(tomo, snr, size, drop_ratio=0.1):
+    """_rs_large3 (remove_stripe.py:388-424) on [nproj, nz, ni], with the
+    reference's array layouts (the float32 means reduce in the same order)."""
+    import scipy.ndimage as ndi
+    drop_ratio = max(min(drop_ratio, 0.8), 0)
+    nproj = tomo.shape[0]
+    ndrop = int(0.5 * drop_ratio * nproj)
+    srt_t, ids = _vo_sort_t(tomo)
+    srt = np.transpose(srt_t, (2, 1, 0))
+    smooth = ndi.median_filter(srt, (1, 1, size))
+    list1 = np.mean(srt[ndrop:nproj - ndrop], axis=0)
+    list2 = np.mean(smooth[ndrop:nproj - ndrop], axis=0)
+    fact = list1 / list2
+    mask = _vo_dilate(_vo_detect(fact, snr))
+    tomo = tomo / fact[None]
+    corr = _vo_unsort_t(np.transpose(smooth, (2, 1, 0)), ids)
+    np.copyto(tomo, corr, where=(mask[None] > 0.0))
+    return tomo
+
+
+def _vo_dead(tomo, snr, size):
+    """_rs_dead3 (remove_stripe.py:427-454) on [nproj, nz, ni]: columns whose
+    total variation along the angles stands out are replaced by linear
+    interpolation between their unmasked neighbours, then _rs_large3."""
+    import scipy.ndimage as ndi
+    tomo = np.array(tomo, dtype=np.float32)
+    nz = tomo.shape[1]
+    smooth = ndi.uniform_filter1d(tomo, 10, axis=0)
+    diff = np.sum(np.abs(tomo - smooth), axis=0)
+    bck = ndi.median_filter(diff, (1, size))
+    fact = diff / bck
+    mask = _vo_dilate(_vo_detect(fact, snr))
+    mask[:, 0:2] = 0.0
+    mask[:, -2:] = 0.0
+    for m in range(nz):
+        good = np.where(mask[m] < 1.0)[0]
+        miss = np.where(mask[m] > 0.0)[0]
+        if len(miss) > 0:
+            matz = tomo[:, m, good]
+            ids = np.searchsorted(good, miss)
+            tomo[:, m, miss] = (matz[:, ids - 1] + (miss - good[ids - 1]) *
+                                (matz[:, ids] - matz[:, ids - 1]) / (good[ids] - good[ids - 1]))
+    return _vo_large(tomo, snr, size)
+
+
+def remove_all_stripe(tomo, snr=3, la_size=61, sm_size=21, dim=1):
+    """remove_all_stripe (remove_stripe.py:457-498) on float32 [nproj, nz, ni]:
+    dead and large stripes (_rs_dead3, window la_size), then small-to-medium
+    stripes by a median of the angle-sorted values along the detector
+    (_rs_sort3, window sm_size; dim 2 adds the window along the angles).
+    Sorts along the angles are stable (CuPy's argsort is)."""
+    import scipy.ndimage as ndi
+    tomo = _vo_dead(tomo, snr, la_size)
+    srt_t, ids = _vo_sort_t(tomo)
+    srt_t = ndi.median_filter(srt_t, (sm_size, 1, 1) if dim == 1 else (sm_size, 1, sm_size))
+    return _vo_unsort_t(srt_t, ids)
+
+
+# --------------------------------------------------------------------------
 # Fourier-wavelet ring removal (src/tomocupy/processing/remove_stripe.py:51-293)
 # --------------------------------------------------------------------------
 def _fw_sym_index(m1, length, m2):

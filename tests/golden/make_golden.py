@@ -13,7 +13,8 @@
           * ProcFunctions.remove_outliers (proc_functions.py:96-107) -> dezinger.npz
           * ProcFunctions.pad360 (proc_functions.py:109-124) -> pad360.npz
           * utils.downsample (utils.py:157-167) -> downsample.npz
-        (--phase / --ti / --dezinger / --pad360 / --downsample: only those)
+          * remove_all_stripe (remove_stripe.py:311-498) -> vo_stripe.npz
+        (--phase / --ti / --dezinger / --pad360 / --downsample / --vo: only those)
 
     python tests/golden/make_golden.py --gpu --out DIR
         Runs the reference's CUDA operators (oracle/_ref, built from the
@@ -267,6 +268,56 @@ def gen_ti(ref: Path):
     print("wrote ti_stripe.npz")
 
 
+# Vo's all-stripe removal, remove_all_stripe (remove_stripe.py:311-498):
+# (nproj, nz, ni, snr, la_size, sm_size, seed).  Inputs have no repeated
+# values inside a column (continuous noise; the dead column is constant up
+# to 1e-6 noise), so every sort along the angles is unique: the fixtures do
+# not depend on how an argsort orders ties (NumPy's default here, a stable
+# sort in CuPy and in the library).
+VO_CASES = [(90, 2, 64, 3.0, 21, 11, 1), (120, 3, 96, 3.0, 31, 11, 2),
+            (64, 1, 80, 2.5, 11, 5, 3)]
+
+
+def vo_input(nproj, nz, ni, seed):
+    """Normalised sinogram-like data with partial, full and dead stripes,
+    float32 [nproj, nz, ni], no ties along the angles."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(-1, 1, ni)
+    ang = np.linspace(0, 1, nproj)[:, None, None]
+    base = 0.6 + 0.3 * np.exp(-4 * (x[None, None, :] - 0.3 * np.sin(6 * ang)) ** 2)
+    gain = 1 + 0.08 * rng.standard_normal(ni) * (rng.uniform(size=ni) < 0.15)
+    data = base * gain[None, None, :] + 0.01 * rng.standard_normal((nproj, nz, ni))
+    dead = rng.integers(4, ni - 4)
+    data[:, :, dead] = 0.05 + 1e-6 * rng.standard_normal((nproj, nz))
+    part = rng.integers(4, ni - 4)
+    data[nproj // 3:, :, part] *= 1.15
+    return data.astype(np.float32)
+
+
+def gen_vo(ref: Path):
+    """Runs remove_all_stripe from the reference's own source with NumPy for
+    CuPy and scipy.ndimage for cupyx.scipy.ndimage -> vo_stripe.npz."""
+    import scipy.ndimage as ndi
+    if "cupy" not in sys.modules:
+        _install_stubs()
+    sys.modules.setdefault("pywt", types.ModuleType("pywt"))
+    cx = types.ModuleType("cupyx")
+    cxs = types.ModuleType("cupyx.scipy")
+    cxn = types.ModuleType("cupyx.scipy.ndimage")
+    for f in ("median_filter", "binary_dilation", "uniform_filter1d"):
+        setattr(cxn, f, getattr(ndi, f))
+    sys.modules.update({"cupyx": cx, "cupyx.scipy": cxs, "cupyx.scipy.ndimage": cxn})
+    rs = _load(ref / "src/tomocupy/processing/remove_stripe.py", "ref_remove_stripe_vo")
+    out = {}
+    for i, (nproj, nz, ni, snr, la, sm, seed) in enumerate(VO_CASES):
+        data = vo_input(nproj, nz, ni, seed)
+        out[f"in_{i}"] = data
+        out[f"out_{i}"] = np.asarray(rs.remove_all_stripe(data.copy(), snr, la, sm),
+                                     dtype=np.float32)
+    np.savez_compressed(HERE / "vo_stripe.npz", **out)
+    print("wrote vo_stripe.npz")
+
+
 # Outlier removal, ProcFunctions.remove_outliers (proc_functions.py:96-107):
 # (dtype, nframes, nz, n, width, threshold, seed).  Widths 4 (an even window,
 # upper median) and 5 on 3 frames (reflections beyond the first) included.
@@ -501,6 +552,7 @@ if __name__ == "__main__":
     ap.add_argument("--dezinger", action="store_true", help="only dezinger.npz")
     ap.add_argument("--pad360", action="store_true", help="only pad360.npz")
     ap.add_argument("--downsample", action="store_true", help="only downsample.npz")
+    ap.add_argument("--vo", action="store_true", help="only vo_stripe.npz")
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
@@ -517,5 +569,7 @@ if __name__ == "__main__":
             gen_pad360(Path(a.ref))
         if a.downsample:
             gen_downsample(Path(a.ref))
+        if a.vo:
+            gen_vo(Path(a.ref))
     if a.gpu:
         gen_gpu(Path(a.out))

@@ -73,14 +73,14 @@ def test_usfft2d_sample_positions_bit_exact(cuda, ref, lamino_deg, k):
     assert torch.equal(y.cpu(), yr.cpu())
 
 
-@pytest.mark.parametrize("lamino_deg", [0.0, 20.0])
+@pytest.mark.parametrize("lamino_deg", [0.0, 20.0, -35.0])
 @pytest.mark.parametrize("nproj", [1, 60])
 def test_linerec_bit_identical_to_reference(cuda, ref, lamino_deg, nproj):
     """One angle (every special angle on its own) and 60 angles: the detector
     indices, weights and per-voxel sums equal the reference build's bit for
     bit (the kernels write out the reference's roundings)."""
     from tomocupy_b200.reconstruction.linerec import LineRec
-    n, nz, ncz, sz = 256, 8, 4, 2
+    n, nz, ncz, sz = 256, 24, 4, 7   # slice offsets z = tz + sz - nz/2 in [-5, -2]
     g = torch.Generator(device="cpu").manual_seed(3)
     if nproj == 1:
         cases = [np.float32([t]) for t in (0.0, np.pi / 4, np.pi / 2, 3 * np.pi / 4,

@@ -25,6 +25,8 @@ PREP_EDGE_PAD = 8
 
 GRID_FP32 = 0
 GRID_TENSOR = 1
+GRID_TENSOR_FP32 = 2
+GRID_TENSOR_STREAM = 3
 
 TCF_OUT_ROWS = 0
 TCF_OUT_PAIRS = 1
@@ -36,6 +38,8 @@ TCB_PHASE_FARAGO = 2
 FFF_OUT_ROWS = 0
 FFF_OUT_PAIRS = 1
 FFF_OUT_SPECTRUM = 2
+
+TCB_ERR_OUT_OF_MEMORY = 4
 
 STATUS_NAMES = {
     0: "TCB_OK", 1: "TCB_ERR_INVALID_ARGUMENT", 2: "TCB_ERR_CUDA", 3: "TCB_ERR_CUFFT",

@@ -161,6 +161,8 @@ __device__ __forceinline__ bool local_range(int f, int origin, int width, int tw
 // ---- per-geometry sample lists ------------------------------------------
 // pass 0: count the samples whose footprint reaches each tile;
 // pass 1: write them (packed p*n+i) in angle-then-radius order.
+// Tiles of TXT x TYT cells (ntx = ceil(2n / TXT) per row).
+template <int TXT, int TYT>
 __global__ void __launch_bounds__(SETUP_NT)
     list_tile_samples(const float2 *__restrict__ cs, const float *__restrict__ rtab, Geom geo,
                       int pass, int *__restrict__ counts, const long long *__restrict__ offs,
@@ -168,8 +170,9 @@ __global__ void __launch_bounds__(SETUP_NT)
   __shared__ int warp_tot[SETUP_NT / 32];
   const int n = geo.n, twon = geo.twon, nproj = geo.nproj;
   const int tile = blockIdx.x;
-  const int ix0 = (tile % geo.ntx) * TX, iy0 = (tile / geo.ntx) * TY;
-  const int tw = min(TX, twon - ix0), th = min(TY, twon - iy0);
+  const int ntx = (twon + TXT - 1) / TXT;
+  const int ix0 = (tile % ntx) * TXT, iy0 = (tile / ntx) * TYT;
+  const int tw = min(TXT, twon - ix0), th = min(TYT, twon - iy0);
   const int X0 = ix0 - n, Y0 = iy0 - n;
   const float twonf = (float)(2 * n);
   int kx_lo = 1, kx_hi = -1, ky_lo = 1, ky_hi = -1;
@@ -786,6 +789,366 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
   }
 }
 
+// ---- gridding on the tensor cores with streamed weights ------------------------
+// The same product D[cell, comp] = sum_s W[cell, s] V[s, comp] per grid tile,
+// with every operand moved by copy engines instead of built by threads:
+//  * W depends on the geometry only.  For 16 x 16-cell tiles (M = 256 cells,
+//    two UMMA M-groups of 128) and chunks of 64 listed samples it is computed
+//    once, with the fp32 gridding's arithmetic, scaled by 2^12 and by the
+//    sample's fftshift sign, split into fp16 hi = fp16(w) and lo = fp16(w - hi),
+//    and stored as the 32 KB shared-memory image of a K-major 128-byte-swizzled
+//    operand (wimg_build).  A chunk's hi (and lo) image is one bulk copy.
+//  * V holds the spectrum values of up to 64 slice pairs (N = 128 columns:
+//    re, im per pair) of the chunk's 64 samples.  g16_split writes the
+//    spectrum once per call as fp16 hi/lo rows [sample][comp] (pair-innermost,
+//    power-of-two scaled so that max |G| is in [2^13, 2^14)); each sample's
+//    256-byte row is gathered with cp.async into an MN-major 128-byte-swizzled
+//    operand, so no thread converts or transposes a value.
+//  * fp32 mode: W_hi V_hi + W_lo V_hi + W_hi V_lo (the lo x lo term, 2^-22
+//    relative, is dropped) accumulated in fp32 in TMEM; mixed mode: W_hi V_hi.
+// Two stages: the next chunk's bulk copy and gathers fly while the tensor
+// cores multiply the current one.  Waits are bounded (error flag).
+constexpr int SW_TX = 16, SW_TY = 16;          // cells per tile
+constexpr int SW_M = SW_TX * SW_TY;            // 256 cells = 2 M-groups
+constexpr int SW_K = 64;                       // samples per chunk
+constexpr int SW_WIMG = SW_M * SW_K * 2;       // 32 KB: one fp16 image
+constexpr int SW_THREADS = 256;
+constexpr float SW_WSCALE = 4096.f;            // W is stored times 2^12
+
+// Shared-memory byte offset of V element (sample k, comp c) in an MN-major
+// 128-byte-swizzled operand of N comps: MN atoms of 64 comps 8192 bytes
+// apart, K atoms of 8 samples 1024 bytes apart, 16-byte chunk (c % 64) / 8
+// of row k % 8 at chunk position ((c % 64) / 8) ^ (k % 8).
+__device__ __forceinline__ uint32_t mn_sw128_offset(int k, int c) {
+  return (uint32_t)((c >> 6) * 8192 + (k >> 3) * 1024 + (k & 7) * 128 +
+                    ((((c & 63) >> 3) ^ k) & 7) * 16 + (c & 7) * 2);
+}
+
+// MN-major, 128-byte swizzle: LBO = stride of MN atoms (lbo bytes), SBO =
+// stride of K atoms (1024).  With a single MN atom (N = 64) lbo is 1024 too,
+// so the descriptor addresses the same bytes whichever stride the MN atoms
+// would take.
+__device__ __forceinline__ uint64_t sdesc_mn(uint32_t saddr, uint32_t lbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)(lbo >> 4) << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+// One CTA per chunk: the chunk's W images (hi, and lo when wlo != null) and
+// the spectrum row (with bit 31 clear) of each of its 64 samples (-1 = none).
+__global__ void __launch_bounds__(SW_THREADS)
+    wimg_build(const float2 *__restrict__ cs, const float *__restrict__ rtab,
+               const float *__restrict__ etab, const long long *__restrict__ toffs,
+               const int *__restrict__ tlist, const int2 *__restrict__ chunk_of,
+               int ntx, Geom geo, uint4 *__restrict__ whi, uint4 *__restrict__ wlo,
+               int *__restrict__ vidx) {
+  extern __shared__ __align__(16) uint8_t wsm[];
+  uint8_t *ihi = wsm, *ilo = wsm + SW_WIMG;
+  __shared__ int s_org[SW_K];              // tile-local origin lx | ly << 16
+  __shared__ float s_w[SW_K][2][2 * M + 1];  // x and y weights
+  __shared__ float s_sg[SW_K];             // 2^12 times the fftshift sign of the sample
+  const int c = blockIdx.x;
+  const int2 co = chunk_of[c];             // (tile, first list position)
+  const int tile = co.x, k0 = co.y;
+  const int n = geo.n, twon = geo.twon;
+  const int ix0 = (tile % ntx) * SW_TX, iy0 = (tile / ntx) * SW_TY;
+  const int X0 = ix0 - n, Y0 = iy0 - n;
+  const long long t0 = toffs[tile];
+  const int S = (int)(toffs[tile + 1] - t0);
+  const int nimg = wlo ? 2 : 1;
+  for (int e = threadIdx.x; e < nimg * SW_WIMG / 16; e += SW_THREADS)
+    reinterpret_cast<uint4 *>(wsm)[e] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x < SW_K) {
+    const int k = threadIdx.x;
+    int row = -1;
+    if (k0 + k < S) {
+      const int sidx = tlist[t0 + k0 + k];
+      const int p = sidx / n, i = sidx % n;
+      float x0, y0;
+      int fx, fy;
+      sample_pos(cs, rtab, p, i, (float)(2 * n), x0, y0, fx, fy);
+      s_org[k] = (tile_origin(fx, X0, twon) & 0xFFFF) | (tile_origin(fy, Y0, twon) << 16);
+      s_sg[k] = (i & 1) ? -SW_WSCALE : SW_WSCALE;
+      // the weights as the fp32 gridding computes them (grid_blocks)
+#pragma unroll
+      for (int d = 0; d < 2 * M + 1; d++) {
+        float w0 = etab[fx - M + d + n + M + EPAD] - x0;
+        float w1 = etab[fy - M + d + n + M + EPAD] - y0;
+        s_w[k][0][d] = __expf(geo.coeff1 * w0 * w0);
+        s_w[k][1][d] = __expf(geo.coeff1 * w1 * w1);
+      }
+      int ii = i + n / 2;
+      if (ii >= n) ii -= n;
+      row = p * n + ii;
+    } else {
+      s_org[k] = 0x7FFF7FFF;  // outside every tile: no weights
+    }
+    vidx[(size_t)c * SW_K + k] = row;
+  }
+  __syncthreads();
+  // 64 samples x 81 footprint cells: hi (and lo) of each weight in its cell's row
+  for (int e = threadIdx.x; e < SW_K * (2 * M + 1) * (2 * M + 1); e += SW_THREADS) {
+    const int k = e % SW_K, d = e / SW_K;
+    const int dx = d % (2 * M + 1), dy = d / (2 * M + 1);
+    const int o = s_org[k];
+    if (o == 0x7FFF7FFF) continue;
+    const int lx = (int)(short)(o & 0xFFFF) + dx, ly = (o >> 16) + dy;
+    if (lx < 0 || lx >= SW_TX || ly < 0 || ly >= SW_TY) continue;
+    // the product as grid_blocks forms it, then the exact power-of-two scale and sign
+    const float w = (s_w[k][0][dx] * s_w[k][1][dy]) * s_sg[k];
+    const __half h = __float2half_rn(w);
+    const uint32_t off = tc::sw128_offset(ly * SW_TX + lx, k);
+    *reinterpret_cast<__half *>(ihi + off) = h;
+    if (wlo) *reinterpret_cast<__half *>(ilo + off) = __float2half_rn(w - __half2float(h));
+  }
+  __syncthreads();
+  uint4 *dh = whi + (size_t)c * (SW_WIMG / 16);
+  for (int e = threadIdx.x; e < SW_WIMG / 16; e += SW_THREADS) {
+    dh[e] = reinterpret_cast<const uint4 *>(ihi)[e];
+    if (wlo) wlo[(size_t)c * (SW_WIMG / 16) + e] = reinterpret_cast<const uint4 *>(ilo)[e];
+  }
+}
+
+// Spectrum rows for the streamed-weight gridding: pairs [zp0, zp0 + NN/2) of
+// G [nz][rows] (complex) as fp16 rows [rows][NN] (pair-innermost re, im),
+// hi = fp16(g * gsc) and (lo != null) lo = fp16(g * gsc - hi); absent pairs
+// are zero.  A block moves 32 rows: coalesced reads per pair, 16-byte row
+// writes.
+template <int NN>
+__global__ void __launch_bounds__(256)
+    g16_split(const float2 *__restrict__ G, __half *__restrict__ hi, __half *__restrict__ lo,
+              const unsigned *__restrict__ amax_bits, size_t rows, int nz, int zp0) {
+  constexpr int ZP = NN / 2;
+  __shared__ float2 t[32][ZP + 1];
+  const size_t r0 = (size_t)blockIdx.x * 32;
+  const float amax = __uint_as_float(*amax_bits);
+  int ex = 0;
+  if (amax > 0.f) frexpf(amax, &ex);
+  const float gsc = ldexpf(1.f, 14 - ex);
+  for (int e = threadIdx.x; e < 32 * ZP; e += 256) {
+    const int rr = e % 32, z = e / 32;
+    float2 v = make_float2(0.f, 0.f);
+    if (r0 + rr < rows && zp0 + z < nz) v = G[(size_t)(zp0 + z) * rows + r0 + rr];
+    t[rr][z] = make_float2(v.x * gsc, v.y * gsc);
+  }
+  __syncthreads();
+  // each thread writes 8 comps (16 bytes) of one row
+  for (int e = threadIdx.x; e < 32 * (NN / 8); e += 256) {
+    const int rr = e / (NN / 8), q = e % (NN / 8);
+    if (r0 + rr >= rows) continue;
+    __half h[8], l[8];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float2 v = t[rr][q * 4 + j];
+      h[2 * j] = __float2half_rn(v.x);
+      h[2 * j + 1] = __float2half_rn(v.y);
+      l[2 * j] = __float2half_rn(v.x - __half2float(h[2 * j]));
+      l[2 * j + 1] = __float2half_rn(v.y - __half2float(h[2 * j + 1]));
+    }
+    const size_t o = (r0 + rr) * NN + (size_t)q * 8;
+    *reinterpret_cast<uint4 *>(hi + o) = *reinterpret_cast<const uint4 *>(h);
+    if (lo) *reinterpret_cast<uint4 *>(lo + o) = *reinterpret_cast<const uint4 *>(l);
+  }
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+      : "memory");
+}
+
+template <int NN, bool SPLIT>
+struct SwCfg {
+  static constexpr int WB = SPLIT ? 2 * SW_WIMG : SW_WIMG;   // W bytes per stage
+  static constexpr int VB = SW_K * NN * 2;                   // one V operand
+  static constexpr int STAGE = WB + (SPLIT ? 2 : 1) * VB;
+  static constexpr int SMEM = 2 * STAGE + 1024 + 64;
+  static constexpr uint32_t TMEM_COLS = 2 * NN;               // two M-groups
+};
+
+// One CTA per (16 x 16 tile, group of NN/2 slice pairs).
+template <int NN, bool SPLIT>
+__global__ void __launch_bounds__(SW_THREADS, 1)
+    grid_sw(const uint4 *__restrict__ whi, const uint4 *__restrict__ wlo,
+            const int *__restrict__ vidx, const int2 *__restrict__ tile_chunks,
+            const int *__restrict__ tile_order, const __half *__restrict__ ghi,
+            const __half *__restrict__ glo, const unsigned *__restrict__ amax_bits,
+            float2 *__restrict__ grid, Geom geo, int ntx, size_t rows, int zg_first,
+            int *__restrict__ err) {
+  using namespace tcb::tc;
+  using Cfg = SwCfg<NN, SPLIT>;
+  extern __shared__ uint8_t swsm_raw[];
+  uint8_t *sm = swsm_raw + ((1024u - (smem_u32(swsm_raw) & 1023u)) & 1023u);
+  uint64_t *wfull = reinterpret_cast<uint64_t *>(sm + 2 * Cfg::STAGE);
+  uint64_t *mdone = wfull + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 2);
+  const int twon = geo.twon;
+  const int tile = tile_order[blockIdx.x];
+  const int zg = zg_first + blockIdx.y;           // pair group of this launch
+  const int z0 = zg * (NN / 2);
+  const int ix0 = (tile % ntx) * SW_TX, iy0 = (tile / ntx) * SW_TY;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int2 tc_ = tile_chunks[tile];             // (first chunk, chunks)
+  const int c0 = tc_.x, nch = tc_.y;
+  const __half *gh = ghi + (size_t)blockIdx.y * rows * NN;
+  const __half *gl = SPLIT ? glo + (size_t)blockIdx.y * rows * NN : nullptr;
+
+  if (tid == 0) {
+    mbar_init(&wfull[0], 1);
+    mbar_init(&wfull[1], 1);
+    mbar_init(&mdone[0], 1);
+    mbar_init(&mdone[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  // loads of chunk cc into stage st: W by one bulk copy per image, V rows by cp.async
+  auto issue = [&](int cc, int st) {
+    uint8_t *S = sm + st * Cfg::STAGE;
+    if (tid == 0) {
+      mbar_expect_tx(&wfull[st], (uint32_t)Cfg::WB);
+      bulk_g2s(smem_u32(S), whi + (size_t)(c0 + cc) * (SW_WIMG / 16), SW_WIMG, &wfull[st]);
+      if (SPLIT)
+        bulk_g2s(smem_u32(S + SW_WIMG), wlo + (size_t)(c0 + cc) * (SW_WIMG / 16), SW_WIMG,
+                 &wfull[st]);
+    }
+    const int *vi = vidx + (size_t)(c0 + cc) * SW_K;
+    const uint32_t vb = smem_u32(S + Cfg::WB);
+    constexpr int PIECES = SW_K * (NN / 8);   // 16-byte pieces per operand
+    for (int e = tid; e < PIECES; e += SW_THREADS) {
+      const int k = e / (NN / 8), q = e % (NN / 8);
+      const int row = __ldg(vi + k);
+      const size_t so = (size_t)(row < 0 ? 0 : row) * NN + (size_t)q * 8;
+      const uint32_t d = mn_sw128_offset(k, q * 8);
+      cp_async16(vb + d, gh + so, row < 0 ? 0 : 16);
+      if (SPLIT) cp_async16(vb + Cfg::VB + d, gl + so, row < 0 ? 0 : 16);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  bool ok = true;
+  int issued = 0, consumed = 0;  // chunks whose W copy was issued / arrived (thread 0)
+  if (nch > 0) {
+    issue(0, 0);
+    issued = 1;
+  }
+  for (int c = 0; c < nch; c++) {
+    const int st = c & 1;
+    if (c + 1 < nch) {
+      // stage st^1 was read by the MMAs of chunk c - 1
+      if (c >= 1) {
+        if (tid == 0 && !mbar_wait(&mdone[st ^ 1], ((c - 1) >> 1) & 1)) ok = false;
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+      }
+      issue(c + 1, st ^ 1);
+      issued = c + 2;
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      if (!mbar_wait(&wfull[st], (c >> 1) & 1)) {
+        ok = false;
+      } else {
+        consumed = c + 1;
+        tc_fence_after();
+        uint8_t *S = sm + st * Cfg::STAGE;
+        const uint32_t a_hi = smem_u32(S), a_lo = a_hi + SW_WIMG;
+        const uint32_t b_hi = smem_u32(S + Cfg::WB), b_lo = b_hi + Cfg::VB;
+        constexpr uint32_t idesc = idesc_f16_f32(128, NN) | (1u << 16);  // B MN-major
+#pragma unroll
+        for (int g = 0; g < 2; g++) {
+          const uint32_t d = tmem + (uint32_t)(g * NN);
+#pragma unroll
+          for (int kk = 0; kk < SW_K / 16; kk++) {
+            const uint32_t acc0 = (c > 0 || kk > 0) ? 1u : 0u;
+            constexpr uint32_t lbo = NN > 64 ? 8192u : 1024u;
+            const uint64_t bh = sdesc_mn(b_hi + kk * 2048, lbo);
+            mma_f16(d, sdesc(a_hi + g * 16384 + kk * 32), bh, idesc, acc0);
+            if (SPLIT) {
+              mma_f16(d, sdesc(a_lo + g * 16384 + kk * 32), bh, idesc, 1u);
+              mma_f16(d, sdesc(a_hi + g * 16384 + kk * 32), sdesc_mn(b_lo + kk * 2048, lbo),
+                      idesc, 1u);
+            }
+          }
+        }
+        mma_commit(&mdone[st]);
+      }
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+  }
+  // all MMAs (and so all reads of shared memory) done before the epilogue
+  if (nch > 0) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if (tid == 0 && ok && !mbar_wait(&mdone[(nch - 1) & 1], ((nch - 1) >> 1) & 1)) ok = false;
+    if (tid == 0 && !ok) {
+      // a wait gave up: let the copies still in flight land (bounded) and the
+      // last committed MMAs finish before the CTA releases its memory
+      for (int cc = consumed; cc < issued; cc++) mbar_wait(&wfull[cc & 1], (cc >> 1) & 1);
+      if (consumed > 0) mbar_wait(&mdone[(consumed - 1) & 1], ((consumed - 1) >> 1) & 1);
+    }
+    ok = __syncthreads_and(ok);
+  }
+  tc_fence_after();
+  // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. of M-group w / 4.
+  {
+    const int g = warp >> 2, q = warp & 3;
+    const int m = g * 128 + q * 32 + lane;
+    const int cx = ix0 + (m % SW_TX), cy = iy0 + (m / SW_TX);
+    const float amax = __uint_as_float(*amax_bits);
+    int ex = 0;
+    if (amax > 0.f) frexpf(amax, &ex);
+    const float unsc = ldexpf(1.f, ex - 14) / SW_WSCALE;
+    const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
+    const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
+    for (int cb = 0; cb < NN; cb += 32) {
+      float v[32];
+      if (nch > 0) {
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * NN + cb), v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) v[j] = 0.f;
+      }
+      if (!ok || cx >= twon || cy >= twon) continue;
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int pz = z0 + cb / 2 + j;
+        if (pz < geo.nz)
+          grid[((size_t)pz * twon + cy) * twon + cx] =
+              make_float2(v[2 * j] * sgn, v[2 * j + 1] * sgn);
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicOr(err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, Cfg::TMEM_COLS);
+  }
+}
+
 // Deapodization of output pixel (tx, ty) from the inverse-FFT value at grid
 // index (tx + n/2, ty + 1 + n/2): the post-FFT fftshift sign, divphi
 // (exp(mu n^2 (dx^2 + dy^2)) / nproj with dx = tx/n - 0.5, and the
@@ -1110,6 +1473,18 @@ struct tcb_fourierrec {
   float4 *dtab = nullptr;  // [n] deapodization terms (deapod_terms)
   int ntiles = 0;
   size_t list_bytes = 0;
+  // streamed-weight tensor-core gridding (16 x 16 tiles, chunks of 64 samples)
+  int sw_nn = 0;                   // comps per CTA (64 or 128); 0 = not built
+  int sw_ntx = 0, sw_ntiles = 0, sw_zgroups = 0;
+  long long sw_chunks = 0;
+  bool sw_lo = false;              // lo images present (fp32 mode)
+  long long *sw_toffs = nullptr;
+  int *sw_tlist = nullptr;
+  int2 *sw_tile_chunks = nullptr;  // per tile: first chunk, chunk count
+  int *sw_order = nullptr;         // tiles centre-first
+  uint4 *sw_whi = nullptr, *sw_wlo = nullptr;
+  int *sw_vidx = nullptr;
+  __half *sw_ghi = nullptr, *sw_glo = nullptr;
 };
 
 using namespace tcb;
@@ -1140,6 +1515,23 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->tc_err);
   cudaFree(h->trec);
   h->trec = nullptr;
+  cudaFree(h->sw_toffs);
+  cudaFree(h->sw_tlist);
+  cudaFree(h->sw_tile_chunks);
+  cudaFree(h->sw_order);
+  cudaFree(h->sw_whi);
+  cudaFree(h->sw_wlo);
+  cudaFree(h->sw_vidx);
+  cudaFree(h->sw_ghi);
+  cudaFree(h->sw_glo);
+  h->sw_toffs = nullptr;
+  h->sw_tlist = nullptr;
+  h->sw_tile_chunks = nullptr;
+  h->sw_order = nullptr;
+  h->sw_whi = h->sw_wlo = nullptr;
+  h->sw_vidx = nullptr;
+  h->sw_ghi = h->sw_glo = nullptr;
+  h->sw_nn = 0;
   h->t1 = h->tw = nullptr;
   h->amax = nullptr;
   h->tc_err = nullptr;
@@ -1190,7 +1582,42 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     StageTimer st("fr_fft1d", s);
     TCB_CUFFT(cufftExecC2C(h->plan1d, (cufftComplex *)gc, (cufftComplex *)gc, CUFFT_FORWARD));
   }
-  if (h->grid_mode == TCB_GRID_TENSOR) {
+  if (h->grid_mode == TCB_GRID_TENSOR_FP32 || h->grid_mode == TCB_GRID_TENSOR_STREAM) {
+    const size_t gtot = h->nz * h->nproj * h->n;
+    const size_t rows = h->nproj * h->n;
+    {
+      StageTimer st("fr_split16", s);
+      TCB_CUDA(cudaMemsetAsync(h->amax, 0, sizeof(unsigned), s));
+      absmax_kernel<<<std::min<unsigned>(ceil_div(gtot, 256), 148u * 16u), 256, 0, s>>>(
+          gc, gtot, h->amax);
+      for (int zg = 0; zg < h->sw_zgroups; zg++) {
+        const size_t off = (size_t)zg * rows * h->sw_nn;
+        __half *lo = h->sw_lo ? h->sw_glo + off : nullptr;
+        if (h->sw_nn == 128)
+          g16_split<128><<<ceil_div(rows, 32), 256, 0, s>>>(gc, h->sw_ghi + off, lo, h->amax,
+                                                            rows, (int)h->nz, zg * 64);
+        else
+          g16_split<64><<<ceil_div(rows, 32), 256, 0, s>>>(gc, h->sw_ghi + off, lo, h->amax,
+                                                           rows, (int)h->nz, zg * 32);
+      }
+      TCB_LAUNCH_CHECK();
+      count_launch(1 + h->sw_zgroups);
+    }
+    StageTimer st("fr_gather_sw", s);
+    const dim3 grd((unsigned)h->sw_ntiles, (unsigned)h->sw_zgroups);
+#define FR_SW(NN_, SPLIT_)                                                                 \
+  grid_sw<NN_, SPLIT_><<<grd, SW_THREADS, SwCfg<NN_, SPLIT_>::SMEM, s>>>(                  \
+      h->sw_whi, h->sw_wlo, h->sw_vidx, h->sw_tile_chunks, h->sw_order, h->sw_ghi,          \
+      h->sw_glo, h->amax, h->grid, geo, h->sw_ntx, rows, 0, h->tc_err)
+    if (h->sw_nn == 128) {
+      if (h->sw_lo) FR_SW(128, true); else FR_SW(128, false);
+    } else {
+      if (h->sw_lo) FR_SW(64, true); else FR_SW(64, false);
+    }
+#undef FR_SW
+    TCB_LAUNCH_CHECK();
+    count_launch();
+  } else if (h->grid_mode == TCB_GRID_TENSOR) {
     StageTimer st("fr_gather_tc", s);
     const size_t gtot = h->nz * h->nproj * h->n;
     TCB_CUDA(cudaMemsetAsync(h->amax, 0, sizeof(unsigned), s));
@@ -1279,14 +1706,16 @@ int build_lists(tcb_fourierrec *h) {
   int st = TCB_OK;
   long long ntot = 0, nbtot = 0;
   do {
-    list_tile_samples<<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 0, counts, nullptr, nullptr);
+    list_tile_samples<TX, TY><<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 0, counts, nullptr,
+                                                nullptr);
     if (cudaGetLastError() != cudaSuccess) { st = TCB_ERR_CUDA; break; }
     if ((st = scan_counts(counts, h->toffs, nt, ntot)) != TCB_OK) break;
     if (cudaMalloc(&h->tlist, std::max<long long>(ntot, 1) * sizeof(int)) != cudaSuccess) {
       st = TCB_ERR_OUT_OF_MEMORY;
       break;
     }
-    list_tile_samples<<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 1, nullptr, h->toffs, h->tlist);
+    list_tile_samples<TX, TY><<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 1, nullptr, h->toffs,
+                                                h->tlist);
     list_block_samples<<<nt, NTH>>>(h->cs, h->rtab, geo, h->toffs, h->tlist, 0, counts,
                                     nullptr, nullptr);
     if (cudaGetLastError() != cudaSuccess) { st = TCB_ERR_CUDA; break; }
@@ -1309,6 +1738,127 @@ int build_lists(tcb_fourierrec *h) {
   if (st == TCB_ERR_CUDA && tcb_last_error()[0] == 0) set_error("fourierrec: list kernel failed");
   h->list_bytes = (size_t)(ntot + nbtot) * sizeof(int);
   return st;
+}
+
+// Streamed-weight gridding tables: sample lists of 16 x 16 tiles, their chunks
+// of 64, the weight images (hi, and lo for fp32) and the spectrum rows of
+// every chunk, tiles centre-first; and the per-call fp16 spectrum buffers.
+int sw_build(tcb_fourierrec *h, bool with_lo) {
+  const Geom &geo = h->geo;
+  const int ntx = (geo.twon + SW_TX - 1) / SW_TX, nty = (geo.twon + SW_TY - 1) / SW_TY;
+  const int nt = ntx * nty;
+  const int nn = h->nz > 32 ? 128 : 64;
+  const int zgroups = (int)((h->nz + nn / 2 - 1) / (nn / 2));
+  const size_t rows = h->nproj * h->n;
+  int *counts = nullptr;
+  int2 *chunk_of = nullptr;
+  auto oom = [&](const char *what) {
+    cudaGetLastError();
+    cudaFree(counts);
+    cudaFree(chunk_of);
+    set_error("tcb_fourierrec_set_gridding: out of device memory (%s)", what);
+    return TCB_ERR_OUT_OF_MEMORY;
+  };
+  if (!h->sw_toffs) {
+    if (cudaMalloc(&counts, (size_t)nt * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h->sw_toffs, ((size_t)nt + 1) * sizeof(long long)) != cudaSuccess)
+      return oom("tile offsets");
+    list_tile_samples<SW_TX, SW_TY><<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 0, counts, nullptr,
+                                                      nullptr);
+    TCB_CUDA(cudaGetLastError());
+    long long total = 0;
+    int st = scan_counts(counts, h->sw_toffs, nt, total);
+    cudaFree(counts);
+    counts = nullptr;
+    if (st != TCB_OK) return st;
+    if (cudaMalloc(&h->sw_tlist, std::max<long long>(total, 1) * sizeof(int)) != cudaSuccess)
+      return oom("tile lists");
+    list_tile_samples<SW_TX, SW_TY><<<nt, SETUP_NT>>>(h->cs, h->rtab, geo, 1, nullptr,
+                                                      h->sw_toffs, h->sw_tlist);
+    TCB_CUDA(cudaGetLastError());
+  }
+  // chunks of 64 listed samples per tile
+  std::vector<long long> toffs(nt + 1);
+  TCB_CUDA(cudaMemcpy(toffs.data(), h->sw_toffs, (nt + 1) * sizeof(long long),
+                      cudaMemcpyDeviceToHost));
+  std::vector<int2> tch(nt);
+  std::vector<int2> cof;
+  for (int t = 0; t < nt; t++) {
+    const long long S = toffs[t + 1] - toffs[t];
+    const int nc = (int)((S + SW_K - 1) / SW_K);
+    tch[t] = make_int2((int)cof.size(), nc);
+    for (int j = 0; j < nc; j++) cof.push_back(make_int2(t, j * SW_K));
+  }
+  const long long C = (long long)cof.size();
+  TCB_CHECK_ARG(C < (1ll << 31), "tcb_fourierrec_set_gridding: too many chunks");
+  if (!h->sw_tile_chunks &&
+      cudaMalloc(&h->sw_tile_chunks, (size_t)nt * sizeof(int2)) != cudaSuccess)
+    return oom("chunk table");
+  TCB_CUDA(cudaMemcpy(h->sw_tile_chunks, tch.data(), nt * sizeof(int2), cudaMemcpyHostToDevice));
+  // tiles centre-first (the sample density peaks at the origin)
+  std::vector<int> order(nt);
+  std::vector<float> dist(nt);
+  for (int t = 0; t < nt; t++) {
+    order[t] = t;
+    const float cx = (t % ntx) * SW_TX + 0.5f * SW_TX - (float)geo.n;
+    const float cy = (t / ntx) * SW_TY + 0.5f * SW_TY - (float)geo.n;
+    dist[t] = cx * cx + cy * cy;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dist[a] < dist[b]; });
+  if (!h->sw_order && cudaMalloc(&h->sw_order, (size_t)nt * sizeof(int)) != cudaSuccess)
+    return oom("tile order");
+  TCB_CUDA(cudaMemcpy(h->sw_order, order.data(), nt * sizeof(int), cudaMemcpyHostToDevice));
+  // weight images and spectrum rows
+  const size_t img = (size_t)SW_WIMG;
+  if (cudaMalloc(&chunk_of, std::max<long long>(C, 1) * sizeof(int2)) != cudaSuccess)
+    return oom("chunk map");
+  if (cudaMalloc(&h->sw_whi, std::max<long long>(C, 1) * img) != cudaSuccess ||
+      (with_lo && cudaMalloc(&h->sw_wlo, std::max<long long>(C, 1) * img) != cudaSuccess))
+    return oom("weight images");
+  if (!h->sw_vidx &&
+      cudaMalloc(&h->sw_vidx, std::max<long long>(C, 1) * SW_K * sizeof(int)) != cudaSuccess)
+    return oom("spectrum rows");
+  if (!h->sw_ghi) {
+    const size_t gb = (size_t)zgroups * rows * nn * sizeof(__half);
+    if (cudaMalloc(&h->sw_ghi, gb) != cudaSuccess) return oom("fp16 spectrum");
+  }
+  if (with_lo && !h->sw_glo) {
+    const size_t gb = (size_t)zgroups * rows * nn * sizeof(__half);
+    if (cudaMalloc(&h->sw_glo, gb) != cudaSuccess) return oom("fp16 spectrum");
+  }
+  TCB_CUDA(cudaMemcpy(chunk_of, cof.data(), C * sizeof(int2), cudaMemcpyHostToDevice));
+  const int wsm = (with_lo ? 2 : 1) * SW_WIMG;
+  TCB_CUDA(cudaFuncSetAttribute(wimg_build, cudaFuncAttributeMaxDynamicSharedMemorySize, wsm));
+  for (long long c0 = 0; c0 < C; c0 += 1 << 30) {
+    const unsigned nb = (unsigned)std::min<long long>(C - c0, 1 << 30);
+    wimg_build<<<nb, SW_THREADS, wsm>>>(h->cs, h->rtab, h->etab, h->sw_toffs, h->sw_tlist,
+                                        chunk_of + c0, ntx, geo,
+                                        h->sw_whi + (size_t)c0 * (img / 16),
+                                        with_lo ? h->sw_wlo + (size_t)c0 * (img / 16) : nullptr,
+                                        h->sw_vidx + (size_t)c0 * SW_K);
+  }
+  count_launch(2);
+  cudaError_t e = cudaDeviceSynchronize();
+  cudaFree(chunk_of);
+  if (e != cudaSuccess) {
+    set_error("tcb_fourierrec_set_gridding: weight tables failed: %s", cudaGetErrorString(e));
+    return TCB_ERR_CUDA;
+  }
+  TCB_CUDA(cudaFuncSetAttribute(grid_sw<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SwCfg<128, true>::SMEM));
+  TCB_CUDA(cudaFuncSetAttribute(grid_sw<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SwCfg<128, false>::SMEM));
+  TCB_CUDA(cudaFuncSetAttribute(grid_sw<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SwCfg<64, true>::SMEM));
+  TCB_CUDA(cudaFuncSetAttribute(grid_sw<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SwCfg<64, false>::SMEM));
+  h->sw_nn = nn;
+  h->sw_ntx = ntx;
+  h->sw_ntiles = nt;
+  h->sw_zgroups = zgroups;
+  h->sw_chunks = C;
+  h->sw_lo = with_lo;
+  return TCB_OK;
 }
 
 }  // namespace
@@ -1574,8 +2124,36 @@ extern "C" int tcb_fourierrec_set_input_spectrum(tcb_fourierrec *h, int on) {
 extern "C" int tcb_fourierrec_set_gridding(tcb_fourierrec *h, int mode) {
   TCB_CHECK_ARG(h, "tcb_fourierrec_set_gridding: null handle");
   TCB_CHECK_ARG(h->grid, "tcb_fourierrec_set_gridding: handle was freed");
-  TCB_CHECK_ARG(mode == TCB_GRID_FP32 || mode == TCB_GRID_TENSOR,
+  TCB_CHECK_ARG(mode == TCB_GRID_FP32 || mode == TCB_GRID_TENSOR ||
+                    mode == TCB_GRID_TENSOR_FP32 || mode == TCB_GRID_TENSOR_STREAM,
                 "tcb_fourierrec_set_gridding: unknown mode %d", mode);
+  if (mode == TCB_GRID_TENSOR_FP32 || mode == TCB_GRID_TENSOR_STREAM) {
+    TCB_CHECK_ARG(h->precision == TCB_FLOAT32,
+                  "tcb_fourierrec_set_gridding: streamed tensor gridding needs a FLOAT32 handle");
+    TCB_CHECK_ARG(h->nproj * h->n < (size_t)INT32_MAX,
+                  "tcb_fourierrec_set_gridding: nproj * n too large for the tensor gridding");
+    const bool want_lo = mode == TCB_GRID_TENSOR_FP32;
+    if (h->sw_nn == 0 || (want_lo && !h->sw_lo)) {
+      if (h->sw_nn) {  // rebuild with lo images
+        cudaFree(h->sw_whi);
+        cudaFree(h->sw_wlo);
+        h->sw_whi = h->sw_wlo = nullptr;
+      }
+      const int st = sw_build(h, want_lo);
+      if (st != TCB_OK) return st;
+    }
+    if (!h->amax) {
+      if (cudaMalloc(&h->amax, sizeof(unsigned)) != cudaSuccess ||
+          cudaMalloc(&h->tc_err, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("tcb_fourierrec_set_gridding: out of device memory");
+        return TCB_ERR_OUT_OF_MEMORY;
+      }
+      TCB_CUDA(cudaMemset(h->tc_err, 0, sizeof(int)));
+    }
+    h->grid_mode = mode;
+    return TCB_OK;
+  }
   if (mode == TCB_GRID_TENSOR && !h->amax) {
     TCB_CHECK_ARG(h->nproj * h->n < (size_t)INT32_MAX,
                   "tcb_fourierrec_set_gridding: nproj * n too large for the tensor gridding");

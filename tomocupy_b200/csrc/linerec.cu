@@ -49,8 +49,9 @@ template <> __device__ __forceinline__ __half from_f32<__half>(float v) {
 // The reference kernel's arithmetic (kernels_linerec.cuh:23-40) with every
 // rounding written out, so that no compiler contraction can differ from the
 // reference build's: u = fma(R0, x, R1 y) + n/2,
-// v = fma(R5, z, fma(R3, x, R4 y)) + nz/2 (R3 = sin(t) cos(phi),
-// R4 = -cos(t) cos(phi)), and the bilinear sum
+// v = (fma(R3, x, R4 y) + R5 z) + nz/2 (R3 = sin(t) cos(phi),
+// R4 = -cos(t) cos(phi); R5 z = sin(phi) z does not depend on the angle and
+// is rounded on its own, as the reference's loop computes it), and the bilinear sum
 // fma(d11, w11, fma(d10, w10, fma(d00, w00, d01 w01))) added to the
 // accumulator.  Bit-identical per angle to the reference build.
 __device__ __forceinline__ float lr_u(float R0, float R1, float x, float y, float h) {
@@ -58,7 +59,7 @@ __device__ __forceinline__ float lr_u(float R0, float R1, float x, float y, floa
 }
 __device__ __forceinline__ float lr_v(float R3, float R4, float R5, float x, float y, float z,
                                       float hz) {
-  return __fadd_rn(__fmaf_rn(R5, z, __fmaf_rn(R3, x, __fmul_rn(R4, y))), hz);
+  return __fadd_rn(__fadd_rn(__fmaf_rn(R3, x, __fmul_rn(R4, y)), __fmul_rn(R5, z)), hz);
 }
 __device__ __forceinline__ float lr_interp(float d00, float d01, float d10, float d11, float u,
                                            float v) {

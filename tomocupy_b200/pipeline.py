@@ -52,7 +52,7 @@ class SinoPipeline:
     def __init__(self, n, nproj, ncz, theta, center, fbp_filter="parzen",
                  algorithm="fourierrec", minus_log=True, device="cuda", stripe=None,
                  precision="float32", out_dtype="float32", mixed_filter="fft", dezinger=None,
-                 ni=None, pad360=None):
+                 ni=None, pad360=None, gridding="auto"):
         if algorithm not in ("fourierrec", "linerec", "lprec"):
             raise NotImplementedError(f"SinoPipeline: algorithm {algorithm!r}")
         if precision not in ("float32", "mixed"):
@@ -143,8 +143,7 @@ class SinoPipeline:
         if algorithm == "fourierrec":
             self.fr = cfunc_fourierrec.cfunc_fourierrec(self.nproj, self.ncz // 2, self.n,
                                                         self.theta)
-            if precision == "mixed":  # fp16 weights/values, fp32 accumulation in TMEM
-                self.fr.set_gridding(_lib.GRID_TENSOR)
+            self.gridding = self._set_gridding(gridding, precision)
             if out_dtype == "float16":
                 self.fr.set_output(_lib.TCB_FLOAT16)
             # the fused filter hands over the projection FFT already done
@@ -168,6 +167,28 @@ class SinoPipeline:
             self.out32 = (torch.empty((self.ncz, self.n, self.n), dtype=torch.float32,
                                       device=self.device)
                           if self.out_dtype == torch.float16 else None)
+
+    def _set_gridding(self, gridding: str, precision: str) -> int:
+        """fourierrec gridding mode.  'auto': the tensor cores with streamed
+        weights (split fp16 for float32, fp16 for mixed) when their tables fit
+        in device memory, else the fp32 register gridding (float32) or the
+        tensor-core gridding that builds its weights per chunk (mixed).
+        'fp32' / 'tensor' / 'tensor_fp32' / 'tensor_stream' force a mode."""
+        modes = {"fp32": _lib.GRID_FP32, "tensor": _lib.GRID_TENSOR,
+                 "tensor_fp32": _lib.GRID_TENSOR_FP32, "tensor_stream": _lib.GRID_TENSOR_STREAM}
+        if gridding != "auto":
+            self.fr.set_gridding(modes[gridding])
+            return modes[gridding]
+        first = _lib.GRID_TENSOR_STREAM if precision == "mixed" else _lib.GRID_TENSOR_FP32
+        fallback = _lib.GRID_TENSOR if precision == "mixed" else _lib.GRID_FP32
+        try:
+            self.fr.set_gridding(first)
+            return first
+        except _lib.TcbError as e:
+            if e.status != _lib.TCB_ERR_OUT_OF_MEMORY:
+                raise
+        self.fr.set_gridding(fallback)
+        return fallback
 
     def weights(self, sht=None) -> torch.Tensor:
         """Per-slice filter spectra (cached for the zero shift)."""
@@ -401,6 +422,12 @@ def copy2d_rows(dst: torch.Tensor, src: torch.Tensor, stream=None) -> None:
     a, b, c = src.shape
     es = src.element_size()
     assert src.stride(2) == 1 and dst.stride(2) == 1
-    assert src.stride(1) == c and dst.stride(1) == c
+    if src.stride(1) != c or dst.stride(1) != c:
+        # rows narrower than their pitch (a column range of the frames, e.g.
+        # the float16 power-of-two crop): one 2D copy of b rows per a
+        for i in range(a):
+            _lib.call("tcb_copy2d", dst[i].data_ptr(), dst.stride(1) * es, src[i].data_ptr(),
+                      src.stride(1) * es, c * es, b, _lib.stream_ptr(stream))
+        return
     _lib.call("tcb_copy2d", dst.data_ptr(), dst.stride(0) * es, src.data_ptr(),
               src.stride(0) * es, b * c * es, a, _lib.stream_ptr(stream))

@@ -143,7 +143,10 @@ class Server:
         before = self._free_dev()
         pipe = SinoPipeline(n, nproj, self.ncz, req.theta, req.center, req.fbp_filter,
                             "fourierrec", device=self.device, precision=req.precision,
-                            out_dtype=req.out_dtype)
+                            out_dtype=req.out_dtype,
+                            # per-chunk weights: no per-geometry weight tables
+                            # (up to 37 GB for 4096 x 3000) in the resident set
+                            gridding="tensor" if req.precision == "mixed" else "fp32")
         tmp = [torch.empty((self.ncz, n, n), dtype=pipe.out_dtype, device=self.device)
                for _ in range(2)]
         torch.cuda.synchronize(self.device)
