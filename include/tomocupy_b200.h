@@ -215,6 +215,23 @@ int tcb_stripe_ti_apply_sino(tcb_stripe_ti *h, float *sino, size_t zstride, size
                              void *stream);
 int tcb_stripe_ti_destroy(tcb_stripe_ti *h);
 
+/* Vo's all-stripe ring removal.  Replaces remove_all_stripe with _rs_dead3,
+ * _rs_large3, _rs_sort3 and _detect_stripe_batch
+ * (src/tomocupy/processing/remove_stripe.py:311-498), called by
+ * ProcFunctions.proc_sino for remove_stripe_method 'vo-all'
+ * (src/tomocupy/processing/proc_functions.py:157-159) with vo_all_snr,
+ * vo_all_la_size, vo_all_sm_size and vo_all_dim.  create: chunk shape
+ * (nproj in [12, 8192], ni in [8, 8192]), odd median windows <= 127, dim 1
+ * (windows along the detector; dim 2 is not supported).  apply: in place on
+ * tomo[p * pstride + z * zstride + x] (nproj angles, nz rows, ni columns).
+ * Sorts along the angles are stable, as CuPy's argsort. */
+typedef struct tcb_stripe_vo tcb_stripe_vo;
+int tcb_stripe_vo_create(tcb_stripe_vo **out, size_t nproj, size_t nz, size_t ni, double snr,
+                         int la_size, int sm_size, int dim);
+int tcb_stripe_vo_apply(tcb_stripe_vo *h, float *tomo, size_t pstride, size_t zstride,
+                        void *stream);
+int tcb_stripe_vo_destroy(tcb_stripe_vo *h);
+
 /* ------------------------------------------------------------------------
  * Single-distance phase retrieval of projections.  Replaces paganin_filter
  * (methods 'paganin', 'Gpaganin') and farago_filter

@@ -98,6 +98,9 @@ SIGNATURES: dict[str, list] = {
     "tcb_stripe_ti_create": [C.POINTER(vp), sz, sz, sz, f64, f64],
     "tcb_stripe_ti_apply_sino": [vp, vp, sz, sz, vp],
     "tcb_stripe_ti_destroy": [vp],
+    "tcb_stripe_vo_create": [C.POINTER(vp), sz, sz, sz, f64, i32, i32, i32],
+    "tcb_stripe_vo_apply": [vp, vp, sz, sz, vp],
+    "tcb_stripe_vo_destroy": [vp],
     "tcb_phase_pads": [sz, sz, f64, f64, f64, i32, C.POINTER(sz), C.POINTER(sz)],
     "tcb_phase_create": [C.POINTER(vp), sz, sz, sz, i32, f64, f64, f64, f64, f64, f64, i32],
     "tcb_phase_sizes": [vp, C.POINTER(sz), C.POINTER(sz)],

@@ -39,13 +39,17 @@ DEFAULTS = {
     "flat_linear": "False",
     "dezinger": 0,
     "dezinger_threshold": 5000,
-    "remove_stripe_method": "none",         # 'none' | 'fw' | 'ti'
+    "remove_stripe_method": "none",         # 'none' | 'fw' | 'ti' | 'vo-all'
     "fw_sigma": 1.0,
     "fw_filter": "sym16",
     "fw_level": 7,
     "fw_pad": True,
     "ti_beta": 0.022,
     "ti_mask": 1.0,
+    "vo_all_snr": 3.0,
+    "vo_all_la_size": 61,
+    "vo_all_sm_size": 21,
+    "vo_all_dim": 1,
     "retrieve_phase_method": "none",        # 'none' | 'paganin' | 'Gpaganin' | 'farago'
     "energy": 20.0,                         # keV
     "propagation_distance": 0.0,            # mm

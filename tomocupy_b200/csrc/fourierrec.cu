@@ -976,10 +976,21 @@ struct SwCfg {
   static constexpr int VB = SW_K * NN * 2;                   // one V operand
   static constexpr int STAGE = WB + (SPLIT ? 2 : 1) * VB;
   static constexpr int SMEM = 2 * STAGE + 1024 + 64;
-  static constexpr uint32_t TMEM_COLS = 2 * NN;               // two M-groups
+  // two M-groups; fp32 mode: two such partial-sum buffers
+  static constexpr uint32_t TMEM_COLS = SPLIT ? 4 * NN : 2 * NN;
 };
 
-// One CTA per (16 x 16 tile, group of NN/2 slice pairs).
+// fp32 mode: chunks per TMEM partial sum.  The tensor cores add each MMA's
+// products into the fp32 accumulator without rounding to nearest, so an
+// accumulator that takes thousands of updates (the tiles near the grid
+// centre list ~25k samples at 2048 x 1500) drifts by ~1e-5 of its value;
+// partial sums of SW_F chunks (12 updates each) are added into fp32
+// registers instead, rounded to nearest, like the fp32 gridding's sums.
+constexpr int SW_F = 4;
+
+// One CTA per (16 x 16 tile, group of NN/2 slice pairs).  fp32 mode: partial
+// sums alternate between two TMEM buffers; the threads fold one into their
+// registers while the tensor cores fill the other.
 template <int NN, bool SPLIT>
 __global__ void __launch_bounds__(SW_THREADS, 1)
     grid_sw(const uint4 *__restrict__ whi, const uint4 *__restrict__ wlo,
@@ -994,7 +1005,8 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
   uint8_t *sm = swsm_raw + ((1024u - (smem_u32(swsm_raw) & 1023u)) & 1023u);
   uint64_t *wfull = reinterpret_cast<uint64_t *>(sm + 2 * Cfg::STAGE);
   uint64_t *mdone = wfull + 2;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 2);
+  uint64_t *pdone = mdone + 2;     // fp32 mode: a partial sum is complete
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(pdone + 2);
   const int twon = geo.twon;
   const int tile = tile_order[blockIdx.x];
   const int zg = zg_first + blockIdx.y;           // pair group of this launch
@@ -1011,6 +1023,8 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
     mbar_init(&wfull[1], 1);
     mbar_init(&mdone[0], 1);
     mbar_init(&mdone[1], 1);
+    mbar_init(&pdone[0], 1);
+    mbar_init(&pdone[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
@@ -1043,7 +1057,29 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
 
+  // this thread's cell (TMEM lane) and its running sums (fp32 mode)
+  const int eg = warp >> 2, eq = warp & 3;
+  float acc[SPLIT ? NN : 1];
+#pragma unroll
+  for (int j = 0; j < (SPLIT ? NN : 1); j++) acc[j] = 0.f;
   bool ok = true;
+  int flushed = 0;  // partial sums added into acc
+  auto flush = [&](int j) {  // partial sum j (buffer j & 1) into acc
+    if (tid == 0 && !mbar_wait(&pdone[j & 1], (j >> 1) & 1)) ok = false;
+    ok = __syncthreads_and(ok);
+    if (!ok) return;
+    tc_fence_after();
+#pragma unroll
+    for (int cb = 0; cb < NN; cb += 32) {
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(eq * 32) << 16) + (uint32_t)((j & 1) * 2 * NN + eg * NN + cb),
+                v);
+#pragma unroll
+      for (int i = 0; i < 32; i++) acc[(cb + i) % (SPLIT ? NN : 1)] += v[i];
+    }
+    tc_fence_before();
+    flushed = j + 1;
+  };
   int issued = 0, consumed = 0;  // chunks whose W copy was issued / arrived (thread 0)
   if (nch > 0) {
     issue(0, 0);
@@ -1076,12 +1112,15 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
         const uint32_t a_hi = smem_u32(S), a_lo = a_hi + SW_WIMG;
         const uint32_t b_hi = smem_u32(S + Cfg::WB), b_lo = b_hi + Cfg::VB;
         constexpr uint32_t idesc = idesc_f16_f32(128, NN) | (1u << 16);  // B MN-major
+        // fp32 mode: partial sum c / SW_F in buffer (c / SW_F) & 1
+        const uint32_t pbuf = SPLIT ? (uint32_t)(((c / SW_F) & 1) * 2 * NN) : 0u;
+        const bool first = SPLIT ? (c % SW_F == 0) : (c == 0);
 #pragma unroll
         for (int g = 0; g < 2; g++) {
-          const uint32_t d = tmem + (uint32_t)(g * NN);
+          const uint32_t d = tmem + pbuf + (uint32_t)(g * NN);
 #pragma unroll
           for (int kk = 0; kk < SW_K / 16; kk++) {
-            const uint32_t acc0 = (c > 0 || kk > 0) ? 1u : 0u;
+            const uint32_t acc0 = (!first || kk > 0) ? 1u : 0u;
             constexpr uint32_t lbo = NN > 64 ? 8192u : 1024u;
             const uint64_t bh = sdesc_mn(b_hi + kk * 2048, lbo);
             mma_f16(d, sdesc(a_hi + g * 16384 + kk * 32), bh, idesc, acc0);
@@ -1093,10 +1132,16 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
           }
         }
         mma_commit(&mdone[st]);
+        if (SPLIT && (c % SW_F == SW_F - 1 || c == nch - 1)) mma_commit(&pdone[(c / SW_F) & 1]);
       }
     }
     ok = __syncthreads_and(ok);
     if (!ok) break;
+    // partial c / SW_F - 1 while the tensor cores work on partial c / SW_F
+    if (SPLIT && c % SW_F == SW_F - 1 && c >= SW_F) {
+      flush(c / SW_F - 1);
+      if (!ok) break;
+    }
   }
   // all MMAs (and so all reads of shared memory) done before the epilogue
   if (nch > 0) {
@@ -1109,6 +1154,8 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
       if (consumed > 0) mbar_wait(&mdone[(consumed - 1) & 1], ((consumed - 1) >> 1) & 1);
     }
     ok = __syncthreads_and(ok);
+    if (SPLIT && ok)
+      for (int j = flushed; j <= (nch - 1) / SW_F && ok; j++) flush(j);
   }
   tc_fence_after();
   // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. of M-group w / 4.
@@ -1122,9 +1169,13 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
     const float unsc = ldexpf(1.f, ex - 14) / SW_WSCALE;
     const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
     const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
+#pragma unroll
     for (int cb = 0; cb < NN; cb += 32) {
       float v[32];
-      if (nch > 0) {
+      if (SPLIT) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) v[j] = acc[(cb + j) % (SPLIT ? NN : 1)];
+      } else if (nch > 0) {
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * NN + cb), v);
       } else {
 #pragma unroll

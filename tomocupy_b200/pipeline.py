@@ -36,6 +36,7 @@ Neither filter modifies its input.
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 import torch
@@ -126,12 +127,16 @@ class SinoPipeline:
             self.filter = cfunc_filter.cfunc_filter(self.nproj, self.ncz, self.ne)
         # optional ring removal between dark/flat and -log (ProcFunctions.proc_sino,
         # proc_functions.py:140-160): stripe is ("ti", beta, mask_size) for
-        # Titarenko's method, else (sigma, wavelet, level) for the
-        # Fourier-wavelet method; both work in place on sinograms in self.sino
+        # Titarenko's method, ("vo-all", snr, la_size, sm_size, dim) for Vo's
+        # method, else (sigma, wavelet, level) for the Fourier-wavelet method;
+        # all work in place on sinograms in self.sino
         self.fw = None
         if stripe is not None and stripe[0] == "ti":
             from .processing.remove_stripe import StripeTI
             self.fw = StripeTI(self.nproj, self.ncz, self.ni, stripe[1], stripe[2])
+        elif stripe is not None and stripe[0] == "vo-all":
+            from .processing.remove_stripe import StripeVO
+            self.fw = StripeVO(self.nproj, self.ncz, self.ni, *stripe[1:])
         elif stripe is not None:
             from .processing.remove_stripe import StripeFW
             sigma, wname, level = stripe
@@ -180,6 +185,8 @@ class SinoPipeline:
             self.fr.set_gridding(modes[gridding])
             return modes[gridding]
         first = _lib.GRID_TENSOR_STREAM if precision == "mixed" else _lib.GRID_TENSOR_FP32
+        if os.environ.get("TCB_FOURIERREC_GRIDDING") in modes:
+            first = modes[os.environ["TCB_FOURIERREC_GRIDDING"]]
         fallback = _lib.GRID_TENSOR if precision == "mixed" else _lib.GRID_FP32
         try:
             self.fr.set_gridding(first)

@@ -1,5 +1,5 @@
-"""Fourier-wavelet (``remove_stripe_fw``) and Titarenko (``remove_stripe_ti``)
-ring removal over the native operators.
+"""Fourier-wavelet (``remove_stripe_fw``), Titarenko (``remove_stripe_ti``) and
+Vo's all-stripe (``remove_all_stripe``) ring removal over the native operators.
 
 Same function signature and result layout as the reference
 (src/tomocupy/processing/remove_stripe.py:253-293): data [nproj, nz, ni]
@@ -112,3 +112,43 @@ def remove_stripe_ti(data, beta, mask_size):
     op = _ti_operator(nproj, nz, ni, float(beta), float(mask_size), data.device.index or 0)
     op.apply_sino(data.permute(1, 0, 2))   # [nz, nproj, ni] view: strides (ni, nz*ni, 1)
     return data
+
+
+# --------------------------------------------------------------------------
+# Vo's all-stripe removal (remove_stripe.py:311-498)
+# --------------------------------------------------------------------------
+class StripeVO(NativeHandle):
+    """remove_all_stripe for a fixed chunk shape, in place on sinograms
+    [nz, nproj, ni] (any slice / angle strides with contiguous rows)."""
+    _destroy = "tcb_stripe_vo_destroy"
+
+    def __init__(self, nproj, nz, ni, snr=3.0, la_size=61, sm_size=21, dim=1):
+        self._set(_lib.create("tcb_stripe_vo_create", int(nproj), int(nz), int(ni), float(snr),
+                              int(la_size), int(sm_size), int(dim)))
+        self.nproj, self.nz, self.ni = int(nproj), int(nz), int(ni)
+        # the pipeline's stripe-operator interface (no angle padding)
+        self.nproj_pad, self.poff = self.nproj, 0
+
+    def apply_sino(self, sino, stream=None):
+        """In place on sino [nz, >= nproj, ni] float32, angle rows 0..nproj-1."""
+        assert sino.dtype == torch.float32 and sino.stride(2) == 1 and sino.shape[0] == self.nz
+        _lib.call("tcb_stripe_vo_apply", self._live(), sino.data_ptr(), sino.stride(1),
+                  sino.stride(0), _lib.stream_ptr(stream))
+        return sino
+
+
+@functools.lru_cache(maxsize=8)
+def _vo_operator(nproj, nz, ni, snr, la_size, sm_size, dim, device_index):
+    return StripeVO(nproj, nz, ni, snr, la_size, sm_size, dim)
+
+
+def remove_all_stripe(tomo, snr=3, la_size=61, sm_size=21, dim=1):
+    """Remove all types of stripe artifacts (Vo's method): tomo [nproj, nz, ni]
+    float32 on the device, corrected in place and returned."""
+    nproj, nz, ni = tomo.shape
+    if tomo.dtype != torch.float32:
+        raise ValueError("remove_all_stripe: float32 data")
+    op = _vo_operator(nproj, nz, ni, float(snr), int(la_size), int(sm_size), int(dim),
+                      tomo.device.index or 0)
+    op.apply_sino(tomo.permute(1, 0, 2))   # [nz, nproj, ni] view
+    return tomo

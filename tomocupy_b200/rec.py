@@ -24,7 +24,7 @@ from .processing.proc_functions import (PHASE_METHODS, darkflat_stats, dezinger,
 
 
 def _supported():
-    if args.remove_stripe_method not in ("none", "fw", "ti"):
+    if args.remove_stripe_method not in ("none", "fw", "ti", "vo-all"):
         raise NotImplementedError(
             f"remove_stripe_method={args.remove_stripe_method!r} is not part of tomocupy_b200")
     if args.file_type not in ("standard", "double_fov"):
@@ -41,6 +41,9 @@ def _stripe_args():
         return (float(args.fw_sigma), args.fw_filter, int(args.fw_level))
     if args.remove_stripe_method == "ti":
         return ("ti", float(args.ti_beta), float(args.ti_mask))
+    if args.remove_stripe_method == "vo-all":
+        return ("vo-all", float(args.vo_all_snr), int(args.vo_all_la_size),
+                int(args.vo_all_sm_size), int(args.vo_all_dim))
     return None
 
 
@@ -287,6 +290,10 @@ class GPURec:
             elif args.remove_stripe_method == "ti":
                 from .processing.remove_stripe import remove_stripe_ti
                 remove_stripe_ti(tmp, args.ti_beta, args.ti_mask)
+            elif args.remove_stripe_method == "vo-all":
+                from .processing.remove_stripe import remove_all_stripe
+                remove_all_stripe(tmp, args.vo_all_snr, args.vo_all_la_size,
+                                  args.vo_all_sm_size, args.vo_all_dim)
             retrieve_phase(tmp)
         if _rotate() and not chunk_height:
             # a try-centre slice is rotated at its own height

@@ -60,7 +60,7 @@ class GPURecSteps:
         d0, f0, _ = darkflat_stats(dark, flat, args.bright_ratio)
         nproj, nz, n = data.shape
         out = torch.empty((nproj, nz, n), dtype=torch.float32, device=dev)
-        stripe = args.remove_stripe_method in ("fw", "ti")
+        stripe = args.remove_stripe_method in ("fw", "ti", "vo-all")
         phase = args.retrieve_phase_method in PHASE_METHODS
         rotate = float(args.rotate_proj_angle) != 0
         # -log comes last: after ring removal (proc_sino), phase retrieval and
@@ -75,6 +75,14 @@ class GPURecSteps:
             for z0 in range(0, nz, ncz):
                 part = out[:, z0:z0 + ncz].contiguous()
                 out[:, z0:z0 + ncz] = remove_stripe_ti(part, args.ti_beta, args.ti_mask)
+        elif args.remove_stripe_method == "vo-all":
+            from .processing.remove_stripe import remove_all_stripe
+            ncz = params.ncz
+            for z0 in range(0, nz, ncz):
+                part = out[:, z0:z0 + ncz].contiguous()
+                out[:, z0:z0 + ncz] = remove_all_stripe(part, args.vo_all_snr,
+                                                        args.vo_all_la_size,
+                                                        args.vo_all_sm_size, args.vo_all_dim)
         elif stripe:
             from .processing.remove_stripe import remove_stripe_fw
             ncz = params.ncz
