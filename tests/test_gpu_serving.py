@@ -77,7 +77,10 @@ def test_request_matches_gpurec(cuda):
     writer = ArrayWriter(device="cpu", pin=True)
     GPURec(ArrayReader(req.frames, req.dark, req.flat, theta=req.theta, pin=True),
            writer).recon_all()
-    assert rel_l2(req.out, writer.rec) < 1e-6
+    # the server grids with the fp32 register kernel (no per-geometry weight
+    # tables), GPURec on the tensor cores with streamed weights: the two agree
+    # within the fourierrec tolerance
+    assert rel_l2(req.out, writer.rec) < 1e-5
 
 
 @pytest.mark.gpu

@@ -16,11 +16,14 @@ import torch
 from tomocupy_b200 import _lib
 
 
+_CODES = {torch.uint16: _lib.TCB_U16, torch.uint8: _lib.TCB_U8, torch.float32: _lib.TCB_F32}
+
+
 def _noalloc(out, data, dark, flat, flags, xoff=0, width=None):
     nproj, nz, n = data.shape
     _lib.call("tcb_prep_noalloc", out.data_ptr(), data.data_ptr(), dark.data_ptr(),
               flat.data_ptr(), nproj, nz, n, dark.shape[0], flat.shape[0],
-              _lib.TCB_U16, 1.0, nproj * out.shape[-1], out.shape[-1], 0, xoff,
+              _CODES[data.dtype], 1.0, nproj * out.shape[-1], out.shape[-1], 0, xoff,
               width if width is not None else xoff + n, flags,
               torch.cuda.current_stream().cuda_stream)
 
@@ -32,9 +35,10 @@ def _allocating(out, data, dark, flat, flags, xoff=0, width=None):
     flat0 = torch.empty((nz, n), dtype=torch.float32, device=dev)
     s = torch.cuda.current_stream().cuda_stream
     _lib.call("tcb_darkflat_stats", dark0.data_ptr(), flat0.data_ptr(), 0, dark.data_ptr(),
-              flat.data_ptr(), dark.shape[0], flat.shape[0], nz, n, _lib.TCB_U16, 1.0, 0, s)
+              flat.data_ptr(), dark.shape[0], flat.shape[0], nz, n, _CODES[data.dtype], 1.0, 0,
+              s)
     _lib.call("tcb_prep_rows", out.data_ptr(), data.data_ptr(), dark0.data_ptr(),
-              flat0.data_ptr(), 0, nproj, nz, n, nz * n, n, _lib.TCB_U16,
+              flat0.data_ptr(), 0, nproj, nz, n, nz * n, n, _CODES[data.dtype],
               nproj * out.shape[-1], out.shape[-1], 0, xoff,
               width if width is not None else xoff + n, flags | _lib.PREP_DARKFLAT, s)
 
@@ -45,12 +49,23 @@ def test_noalloc_matches_allocating_path_twice():
     assert torch.cuda.is_available()
     dev = torch.device("cuda")
     cases = [
-        # (nproj, nz, n, seed, flags, xoff, width): plain -log, then edge-padded rows
-        (90, 6, 200, 21, _lib.PREP_MINUS_LOG, 0, None),
-        (60, 8, 256, 22, _lib.PREP_MINUS_LOG | _lib.PREP_EDGE_PAD, 384, 1024),
+        # (nproj, nz, n, seed, flags, xoff, width, dtype): plain -log, edge-padded
+        # rows, 8-bit and float32 frames, and the largest plane the fixed
+        # statistics hold (nz * n = TCB_NOALLOC_MAX_PLANE: both halves of the
+        # array used to the end)
+        (90, 6, 200, 21, _lib.PREP_MINUS_LOG, 0, None, torch.uint16),
+        (60, 8, 256, 22, _lib.PREP_MINUS_LOG | _lib.PREP_EDGE_PAD, 384, 1024, torch.uint16),
+        (40, 4, 128, 23, _lib.PREP_MINUS_LOG, 0, None, torch.uint8),
+        (40, 4, 128, 24, _lib.PREP_MINUS_LOG, 0, None, torch.float32),
+        (3, 512, 2048, 25, _lib.PREP_MINUS_LOG, 0, None, torch.uint16),
     ]
-    for nproj, nz, n, seed, flags, xoff, width in cases:
+    for nproj, nz, n, seed, flags, xoff, width, dt in cases:
         data, dark, flat, _, _ = synthetic.make_dataset(nproj, nz, n, seed=seed)
+        if dt == torch.uint8:   # 8-bit frames: counts scaled into [0, 255]
+            data, dark, flat = ((t.to(torch.int32) // 64).clamp(0, 255).to(torch.uint8)
+                                for t in (data, dark, flat))
+        elif dt == torch.float32:
+            data, dark, flat = (t.to(torch.float32) for t in (data, dark, flat))
         data, dark, flat = data.to(dev), dark.to(dev), flat.to(dev)
         w = width if width is not None else n
         got = torch.full((nz, nproj, w), float("nan"), device=dev)

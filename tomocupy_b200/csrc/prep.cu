@@ -393,28 +393,29 @@ extern "C" int tcb_prep_noalloc(float *out, const void *data, const void *dark,
   PrepArgs a{out, nullptr, nullptr, data, dark0, flat0, nullptr, (int)nproj, (int)nz, (int)n,
              nz * n, n, out_zstride, out_pstride, out_poff, out_xoff, out_width,
              flags | TCB_PREP_DARKFLAT};
-  unsigned rows = (unsigned)(nproj * nz);
+  const size_t rows = nproj * nz;
+  StageTimer t("prep_noalloc", s);
   switch (in_dtype) {
     case TCB_U16:
       darkflat_stats_kernel<uint16_t><<<sgrid, 256, 0, s>>>(
           dark0, flat0, nullptr, (const uint16_t *)dark, (const uint16_t *)flat, (int)ndark,
           (int)nflat, plane, bright_ratio, 0);
       TCB_LAUNCH_CHECK();
-      prep_rows_kernel<uint16_t, false><<<rows, 256, 0, s>>>(a);
+      prep_rows_kernel<uint16_t, false><<<prep_grid(rows), 256, 0, s>>>(a);
       break;
     case TCB_U8:
       darkflat_stats_kernel<uint8_t><<<sgrid, 256, 0, s>>>(
           dark0, flat0, nullptr, (const uint8_t *)dark, (const uint8_t *)flat, (int)ndark,
           (int)nflat, plane, bright_ratio, 0);
       TCB_LAUNCH_CHECK();
-      prep_rows_kernel<uint8_t, false><<<rows, 256, 0, s>>>(a);
+      prep_rows_kernel<uint8_t, false><<<prep_grid(rows), 256, 0, s>>>(a);
       break;
     default:
       darkflat_stats_kernel<float><<<sgrid, 256, 0, s>>>(
           dark0, flat0, nullptr, (const float *)dark, (const float *)flat, (int)ndark,
           (int)nflat, plane, bright_ratio, 0);
       TCB_LAUNCH_CHECK();
-      prep_rows_kernel<float, false><<<rows, 256, 0, s>>>(a);
+      prep_rows_kernel<float, false><<<prep_grid(rows), 256, 0, s>>>(a);
   }
   TCB_LAUNCH_CHECK();
   count_launch(2);

@@ -119,6 +119,7 @@ class Server:
         self.depth = int(depth)
         self.max_active = max_active
         self.copy_stream = torch.cuda.Stream(self.device)
+        self.d2h = torch.cuda.Stream(self.device)
         self.geoms: OrderedDict = OrderedDict()
         self.geom_bytes = 0
         self.req_bytes = 0
@@ -151,8 +152,11 @@ class Server:
                for _ in range(2)]
         torch.cuda.synchronize(self.device)
         nb = max(before - self._free_dev(), 2 * tmp[0].numel() * tmp[0].element_size())
-        g = _Geometry(pipe, tmp, torch.cuda.Stream(self.device), torch.cuda.Stream(self.device),
-                      nb)
+        # one copy-out stream for every geometry: results cross the host link
+        # one at a time in dispatch (oldest-request-first) order, the order
+        # that keeps the longest waits shortest on a shared link, instead of
+        # sharing its bandwidth among all requests in flight
+        g = _Geometry(pipe, tmp, torch.cuda.Stream(self.device), self.d2h, nb)
         self.geoms[key] = g
         self.geom_bytes += nb
         return g
