@@ -256,13 +256,44 @@ def _ring_removal(a):
     return dict(remove_stripe_method="fw", fw_sigma=1.0, fw_filter="sym16", fw_level=7)
 
 
+def _stated(rec):
+    """True when a stage's launches stated their algorithmic bytes."""
+    return rec.get("bytes", 0) > 0
+
+
 def _roofline(stages, a, peaks, peaks_kind, kernel=None):
     """Roofline of the dominant (or the named) native stage."""
-    own = {k: v for k, v in stages.items() if stage_bytes(k, a.n, a.nproj, a.ncz) is not None}
+    own = {k: v for k, v in stages.items()
+           if _stated(v) or stage_bytes(k, a.n, a.nproj, a.ncz) is not None}
     dom = kernel if kernel in own else (max(own, key=lambda k: own[k]["ms"]) if own else None)
     if dom is None:
         return None
     per_launch_ms = own[dom]["ms"] / own[dom]["count"]
+    if _stated(own[dom]):
+        # the stage states its bytes (and FLOPs) per launch: the streamed
+        # tensor-core gridding is bound by whichever of HBM and the tensor
+        # pipe its launch needs longer on
+        algo = own[dom]["bytes"] / own[dom]["count"]
+        flops = own[dom].get("flops", 0) / own[dom]["count"]
+        t_s = per_launch_ms / 1e3
+        hbm = {"achieved": round(algo / t_s / 1e9, 1), "peak": peaks["hbm_gbs"],
+               "unit": "GB/s", "frac": round(algo / t_s / 1e9 / peaks["hbm_gbs"], 4)}
+        out = {"bound": "hbm", "kernel": dom, **hbm,
+               "traffic": NCU_TRAFFIC.get((dom, a.n, a.nproj, a.ncz)),
+               "algorithmic_bytes_per_launch": round(algo),
+               "ms_per_launch": round(per_launch_ms, 4),
+               "peak_source": f"{peaks_kind} (MEASURED_PEAKS.json hbm_gbs)"
+               if peaks_kind == "measured" else "fallback 6.65 TB/s"}
+        if flops > 0:
+            tpeak = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
+            tfrac = flops / t_s / 1e12 / tpeak
+            out["tensor"] = {"achieved": round(flops / t_s / 1e12, 1), "peak": tpeak,
+                             "unit": "TFLOP/s", "frac": round(tfrac, 4),
+                             "flops_per_launch": round(flops)}
+            if tfrac > hbm["frac"]:  # the tensor pipe is the nearer bound
+                out.update(bound="tensor", achieved=out["tensor"]["achieved"], peak=tpeak,
+                           unit="TFLOP/s", frac=round(tfrac, 4))
+        return out
     algo = stage_bytes(dom, a.n, a.nproj, a.ncz)
     if dom == "tc_filter":  # tensor-bound: algorithmic flops, fp16 dense = bf16 dense rate
         achieved = algo / (per_launch_ms / 1e3) / 1e12
@@ -559,8 +590,10 @@ def run_methods(a, data, dark, flat, theta, dev):
             ("linerec", "linerec", min(a.nz, a.slab_rows), {})]
     for name, alg, rows, extra in legs:
         d, dk, fl = data[:, :rows], dark[:, :rows], flat[:, :rows]
+        # lprec and linerec keep 64-row chunks (their kernels gain nothing from more)
         global_vars.reset(reconstruction_algorithm=alg, fbp_filter=a.filter,
-                          nsino_per_chunk=a.ncz, **extra)
+                          nsino_per_chunk=a.ncz if alg == "fourierrec" else min(a.ncz, 64),
+                          **extra)
         rec = GPURec(ArrayReader(d, dk, fl, theta=theta), ArrayWriter(device=dev), device=dev)
         d0, f0, _ = darkflat_stats(dk, fl)
         out = torch.empty((params.nz, params.n, params.n), dtype=torch.float32, device=dev)
@@ -1069,7 +1102,7 @@ def main():
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--nproj", type=int, default=1500)
     ap.add_argument("--nz", type=int, default=2048)
-    ap.add_argument("--ncz", type=int, default=64)
+    ap.add_argument("--ncz", type=int, default=128)
     ap.add_argument("--e2e-ncz", type=int, default=32,
                     help="rows per chunk of the end-to-end (host buffer) leg")
     ap.add_argument("--algorithm", default="fourierrec", choices=["fourierrec", "lprec", "linerec"])

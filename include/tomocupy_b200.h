@@ -50,7 +50,9 @@ int tcb_version(void);
  * hooks).  tcb_profile_enable(1) clears and starts recording a CUDA event
  * pair around every native stage launch (on the stream it is launched on);
  * tcb_profile_report synchronises the recorded events and writes JSON
- * {"stage": {"count": c, "ms": total}, ...} into buf.  tcb_launch_count
+ * {"stage": {"count": c, "ms": total, "bytes": b, "flops": f}, ...} into
+ * buf, where b and f sum the algorithmic DRAM bytes and FLOPs that a stage
+ * states for its launches (0 where it states none).  tcb_launch_count
  * returns the number of native kernel launches since process start (cuFFT
  * launches are not counted). */
 int tcb_profile_enable(int on);

@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py --cpu [--ref /root/reference]
+    python tests/golden/make_golden.py --cpu --ref <reference checkout>
+    (or TOMOCUPY_REFERENCE in the environment)
         Executes the reference's own Python sources with NumPy standing in
         for CuPy (and stubs for h5py / the SWIG modules):
           * FBPFilter.calc_filter for every filter at several widths
@@ -27,6 +28,7 @@ from __future__ import annotations
 import argparse
 import importlib.util
 import json
+import os
 import sys
 import types
 from argparse import Namespace
@@ -553,7 +555,8 @@ if __name__ == "__main__":
     ap.add_argument("--pad360", action="store_true", help="only pad360.npz")
     ap.add_argument("--downsample", action="store_true", help="only downsample.npz")
     ap.add_argument("--vo", action="store_true", help="only vo_stripe.npz")
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("TOMOCUPY_REFERENCE"),
+                    required="TOMOCUPY_REFERENCE" not in os.environ)
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
     if a.cpu:

@@ -216,7 +216,9 @@ def profile_enable(on: bool = True) -> None:
 
 
 def profile_report() -> dict:
-    """{stage: {"count": c, "ms": total}} for the stages recorded since enable."""
+    """{stage: {"count": c, "ms": total, "bytes": b, "flops": f}} for the stages
+    recorded since enable (b, f: the algorithmic bytes and FLOPs the stage's
+    launches state, 0 where none is stated)."""
     import json
     buf = C.create_string_buffer(1 << 16)
     call("tcb_profile_report", buf, len(buf))

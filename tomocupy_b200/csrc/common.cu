@@ -15,15 +15,17 @@ namespace {
 struct Rec {
   std::string name;
   cudaEvent_t a, b;
+  double bytes, flops;
 };
 std::mutex g_prof_mu;
 std::atomic<bool> g_prof_on{false};
 std::vector<Rec> g_recs;
 }  // namespace
 
-StageTimer::StageTimer(const char *n, cudaStream_t s) : name(n), stream(s), slot(-1) {
+StageTimer::StageTimer(const char *n, cudaStream_t s, double bytes, double flops)
+    : name(n), stream(s), slot(-1) {
   if (!g_prof_on.load(std::memory_order_relaxed)) return;
-  Rec r{n, nullptr, nullptr};
+  Rec r{n, nullptr, nullptr, bytes, flops};
   if (cudaEventCreate(&r.a) != cudaSuccess) return;
   if (cudaEventCreate(&r.b) != cudaSuccess) {
     cudaEventDestroy(r.a);
@@ -87,21 +89,29 @@ extern "C" int tcb_profile_enable(int on) {
 extern "C" int tcb_profile_report(char *buf, size_t len) {
   TCB_CHECK_ARG(buf && len > 2, "tcb_profile_report: bad buffer");
   std::lock_guard<std::mutex> lk(tcb::g_prof_mu);
-  std::map<std::string, std::pair<long, double>> acc;
+  struct Sum {
+    long count = 0;
+    double ms = 0.0, bytes = 0.0, flops = 0.0;
+  };
+  std::map<std::string, Sum> acc;
   for (auto &r : tcb::g_recs) {
     TCB_CUDA(cudaEventSynchronize(r.b));
     float ms = 0.f;
     TCB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
     auto &e = acc[r.name];
-    e.first += 1;
-    e.second += ms;
+    e.count += 1;
+    e.ms += ms;
+    e.bytes += r.bytes;
+    e.flops += r.flops;
   }
   std::string out = "{";
   bool first = true;
-  char tmp[256];
+  char tmp[384];
   for (auto &kv : acc) {
-    snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"count\": %ld, \"ms\": %.6f}", first ? "" : ", ",
-             kv.first.c_str(), kv.second.first, kv.second.second);
+    snprintf(tmp, sizeof(tmp),
+             "%s\"%s\": {\"count\": %ld, \"ms\": %.6f, \"bytes\": %.17g, \"flops\": %.17g}",
+             first ? "" : ", ", kv.first.c_str(), kv.second.count, kv.second.ms, kv.second.bytes,
+             kv.second.flops);
     out += tmp;
     first = false;
   }

@@ -65,8 +65,10 @@ inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b
 // Launch counter and optional per-stage event timing (see tcb_profile_*).
 void count_launch(unsigned k = 1);
 struct StageTimer {
-  // Records a start event on `s` when profiling is on; stop() records the end.
-  StageTimer(const char *name, cudaStream_t s);
+  // Records a start event on `s` when profiling is on; the destructor records
+  // the end.  bytes / flops: the stage's algorithmic DRAM bytes and FLOPs of
+  // this launch (0 = not stated), summed per stage in the report.
+  StageTimer(const char *name, cudaStream_t s, double bytes = 0.0, double flops = 0.0);
   ~StageTimer();
   const char *name;
   cudaStream_t stream;

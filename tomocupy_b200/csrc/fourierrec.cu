@@ -1636,8 +1636,12 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   if (h->grid_mode == TCB_GRID_TENSOR_FP32 || h->grid_mode == TCB_GRID_TENSOR_STREAM) {
     const size_t gtot = h->nz * h->nproj * h->n;
     const size_t rows = h->nproj * h->n;
+    const double nimg = h->sw_lo ? 2.0 : 1.0;
+    // spectrum operand rows (fp16 hi, lo) of every pair group
+    const double vbytes = (double)h->sw_zgroups * rows * h->sw_nn * 2.0 * nimg;
     {
-      StageTimer st("fr_split16", s);
+      // algorithmic bytes: the spectrum read twice (maximum, split), the rows written
+      StageTimer st("fr_split16", s, 2.0 * gtot * sizeof(float2) + vbytes);
       TCB_CUDA(cudaMemsetAsync(h->amax, 0, sizeof(unsigned), s));
       absmax_kernel<<<std::min<unsigned>(ceil_div(gtot, 256), 148u * 16u), 256, 0, s>>>(
           gc, gtot, h->amax);
@@ -1654,7 +1658,14 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
       TCB_LAUNCH_CHECK();
       count_launch(1 + h->sw_zgroups);
     }
-    StageTimer st("fr_gather_sw", s);
+    // algorithmic bytes: every weight image and its sample rows streamed once,
+    // the spectrum operand read once, the grid written once; FLOPs: the
+    // products the tensor cores form (3 per term in fp32 mode)
+    const double C = (double)h->sw_chunks;
+    StageTimer st("fr_gather_sw", s,
+                  h->sw_zgroups * C * (SW_WIMG * nimg + SW_K * sizeof(int)) + vbytes +
+                      (double)h->nz * geo.twon * geo.twon * sizeof(float2),
+                  h->sw_zgroups * C * 2.0 * SW_M * h->sw_nn * SW_K * (h->sw_lo ? 3.0 : 1.0));
     const dim3 grd((unsigned)h->sw_ntiles, (unsigned)h->sw_zgroups);
 #define FR_SW(NN_, SPLIT_)                                                                 \
   grid_sw<NN_, SPLIT_><<<grd, SW_THREADS, SwCfg<NN_, SPLIT_>::SMEM, s>>>(                  \
