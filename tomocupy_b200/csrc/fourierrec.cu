@@ -793,34 +793,56 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 // The same product D[cell, comp] = sum_s W[cell, s] V[s, comp] per grid tile,
 // with every operand moved by copy engines instead of built by threads:
 //  * W depends on the geometry only.  For 16 x 16-cell tiles (M = 256 cells,
-//    two UMMA M-groups of 128) and chunks of 64 listed samples it is computed
+//    two UMMA M-groups of 128) and chunks of 32 listed samples it is computed
 //    once, with the fp32 gridding's arithmetic, scaled by 2^12 and by the
 //    sample's fftshift sign, split into fp16 hi = fp16(w) and lo = fp16(w - hi),
-//    and stored as the 32 KB shared-memory image of a K-major 128-byte-swizzled
+//    and stored as the 16 KB shared-memory image of a K-major 64-byte-swizzled
 //    operand (wimg_build).  A chunk's hi (and lo) image is one bulk copy.
 //  * V holds the spectrum values of up to 64 slice pairs (N = 128 columns:
-//    re, im per pair) of the chunk's 64 samples.  g16_split writes the
+//    re, im per pair) of the chunk's 32 samples.  g16_split writes the
 //    spectrum once per call as fp16 hi/lo rows [sample][comp] (pair-innermost,
 //    power-of-two scaled so that max |G| is in [2^13, 2^14)); each sample's
 //    256-byte row is gathered with cp.async into an MN-major 128-byte-swizzled
 //    operand, so no thread converts or transposes a value.
 //  * fp32 mode: W_hi V_hi + W_lo V_hi + W_hi V_lo (the lo x lo term, 2^-22
 //    relative, is dropped) accumulated in fp32 in TMEM; mixed mode: W_hi V_hi.
-// Two stages: the next chunk's bulk copy and gathers fly while the tensor
-// cores multiply the current one.  Waits are bounded (error flag).
+// A ring of shared-memory stages (4 in fp32 mode, 8 in mixed mode): the
+// copies of the next chunks fly while the tensor cores multiply the current
+// one, across tile boundaries.  Waits are bounded (error flag).
 constexpr int SW_TX = 16, SW_TY = 16;          // cells per tile
 constexpr int SW_M = SW_TX * SW_TY;            // 256 cells = 2 M-groups
-constexpr int SW_K = 64;                       // samples per chunk
-constexpr int SW_WIMG = SW_M * SW_K * 2;       // 32 KB: one fp16 image
+constexpr int SW_K = 32;                       // samples per chunk
+constexpr int SW_WIMG = SW_M * SW_K * 2;       // 16 KB: one fp16 image
 constexpr int SW_THREADS = 256;
 constexpr float SW_WSCALE = 4096.f;            // W is stored times 2^12
 
+// Byte offset of W element (cell row, sample k) in a K-major operand of
+// 32-sample (64-byte) rows with the 64-byte swizzle (UMMA layout type 4):
+// 8-row groups 512 bytes apart, 16-byte chunk k/8 of row r at chunk
+// position (k/8) ^ ((r/2) % 4).
+__device__ __forceinline__ uint32_t sw64_offset(int row, int k) {
+  return (uint32_t)((row >> 3) * 512 + (row & 7) * 64 + ((((k >> 3) ^ (row >> 1)) & 3) << 4) +
+                    ((k & 7) << 1));
+}
+
+// K-major, 64-byte swizzle: SBO = 512 (8 rows of 64 bytes), LBO unused.
+__device__ __forceinline__ uint64_t sdesc_k64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;
+  return d;
+}
+
 // Shared-memory byte offset of V element (sample k, comp c) in an MN-major
-// 128-byte-swizzled operand of N comps: MN atoms of 64 comps 8192 bytes
-// apart, K atoms of 8 samples 1024 bytes apart, 16-byte chunk (c % 64) / 8
-// of row k % 8 at chunk position ((c % 64) / 8) ^ (k % 8).
+// 128-byte-swizzled operand of N comps and SW_K samples: MN atoms of 64
+// comps SW_K * 128 bytes apart, K atoms of 8 samples 1024 bytes apart,
+// 16-byte chunk (c % 64) / 8 of row k % 8 at chunk position
+// ((c % 64) / 8) ^ (k % 8).
 __device__ __forceinline__ uint32_t mn_sw128_offset(int k, int c) {
-  return (uint32_t)((c >> 6) * 8192 + (k >> 3) * 1024 + (k & 7) * 128 +
+  return (uint32_t)((c >> 6) * (SW_K * 128) + (k >> 3) * 1024 + (k & 7) * 128 +
                     ((((c & 63) >> 3) ^ k) & 7) * 16 + (c & 7) * 2);
 }
 
@@ -839,7 +861,7 @@ __device__ __forceinline__ uint64_t sdesc_mn(uint32_t saddr, uint32_t lbo) {
 }
 
 // One CTA per chunk: the chunk's W images (hi, and lo when wlo != null) and
-// the spectrum row (with bit 31 clear) of each of its 64 samples (-1 = none).
+// the spectrum row (with bit 31 clear) of each of its 32 samples (-1 = none).
 __global__ void __launch_bounds__(SW_THREADS)
     wimg_build(const float2 *__restrict__ cs, const float *__restrict__ rtab,
                const float *__restrict__ etab, const long long *__restrict__ toffs,
@@ -890,7 +912,7 @@ __global__ void __launch_bounds__(SW_THREADS)
     vidx[(size_t)c * SW_K + k] = row;
   }
   __syncthreads();
-  // 64 samples x 81 footprint cells: hi (and lo) of each weight in its cell's row
+  // 32 samples x 81 footprint cells: hi (and lo) of each weight in its cell's row
   for (int e = threadIdx.x; e < SW_K * (2 * M + 1) * (2 * M + 1); e += SW_THREADS) {
     const int k = e % SW_K, d = e / SW_K;
     const int dx = d % (2 * M + 1), dy = d / (2 * M + 1);
@@ -901,7 +923,7 @@ __global__ void __launch_bounds__(SW_THREADS)
     // the product as grid_blocks forms it, then the exact power-of-two scale and sign
     const float w = (s_w[k][0][dx] * s_w[k][1][dy]) * s_sg[k];
     const __half h = __float2half_rn(w);
-    const uint32_t off = tc::sw128_offset(ly * SW_TX + lx, k);
+    const uint32_t off = sw64_offset(ly * SW_TX + lx, k);
     *reinterpret_cast<__half *>(ihi + off) = h;
     if (wlo) *reinterpret_cast<__half *>(ilo + off) = __float2half_rn(w - __half2float(h));
   }
@@ -970,61 +992,107 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
       : "memory");
 }
 
+// Warp roles of the streamed-weight gridding: 16 accumulator warps (warp w
+// reads TMEM lanes 32 (w % 4) .. of M-group (w / 4) % 2, columns half w / 8),
+// one producer warp (bulk copies of W, cp.async gathers of V) and one warp
+// whose lane 0 issues the MMAs.
+constexpr int WS_ACC_WARPS = 16;
+constexpr int WS_THREADS = (WS_ACC_WARPS + 2) * 32;
+
 template <int NN, bool SPLIT>
 struct SwCfg {
+  static constexpr int NST = SPLIT ? 4 : 8;                  // shared-memory stages
+  // a chunk's gathers are published (fenced, then arrived on its stage's
+  // mbarrier) once LAG newer chunks have been issued: the producer lanes wait
+  // for their cp.async groups LAG deep instead of one chunk at a time
+  static constexpr int LAG = NST / 2;
   static constexpr int WB = SPLIT ? 2 * SW_WIMG : SW_WIMG;   // W bytes per stage
   static constexpr int VB = SW_K * NN * 2;                   // one V operand
   static constexpr int STAGE = WB + (SPLIT ? 2 : 1) * VB;
-  static constexpr int SMEM = 2 * STAGE + 1024 + 64;
-  // two M-groups; fp32 mode: two such partial-sum buffers
-  static constexpr uint32_t TMEM_COLS = SPLIT ? 4 * NN : 2 * NN;
+  static constexpr int SMEM = NST * STAGE + 1024 + 256;
+  // two TMEM buffers (partial sums in fp32 mode, whole tiles in mixed mode)
+  // of two M-groups each
+  static constexpr uint32_t TMEM_COLS = 4 * NN;
 };
 
 // fp32 mode: chunks per TMEM partial sum.  The tensor cores add each MMA's
 // products into the fp32 accumulator without rounding to nearest, so an
 // accumulator that takes thousands of updates (the tiles near the grid
 // centre list ~25k samples at 2048 x 1500) drifts by ~1e-5 of its value;
-// partial sums of SW_F chunks (12 updates each) are added into fp32
-// registers instead, rounded to nearest, like the fp32 gridding's sums.
-constexpr int SW_F = 4;
+// partial sums of SW_F chunks (256 samples) are added into fp32 registers
+// instead, rounded to nearest, like the fp32 gridding's sums.
+constexpr int SW_F = 8;
 
-// One CTA per (16 x 16 tile, group of NN/2 slice pairs).  fp32 mode: partial
-// sums alternate between two TMEM buffers; the threads fold one into their
-// registers while the tensor cores fill the other.
+// Bounded wait by every lane of a warp; the lanes leave it together and agree
+// on the outcome (so the warp stays converged for .sync.aligned operations).
+__device__ __forceinline__ bool warp_wait(uint64_t *b, uint32_t parity) {
+  const bool w = tc::mbar_wait(b, parity);
+  return __all_sync(0xffffffffu, w);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(b)) : "memory");
+}
+
+// 16 consecutive fp32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Persistent and warp-specialised: CTA b takes the work items (tile, pair
+// group) b, b + G, ... in raster order.  The producer warp streams the
+// chunks of all its items through NST stages (W by bulk copies that complete
+// on the stage's mbarrier, V rows by cp.async whose lanes arrive on it once
+// their gathers have landed), prefetching the next chunk's row indices and
+// the next item's chunk range one step ahead; the MMA warp multiplies each
+// stage as it fills and releases it with tcgen05.commit; the accumulator
+// warps drain each finished TMEM buffer (fp32 mode: a partial sum of SW_F
+// chunks, added into registers; mixed mode: the whole tile) and release it,
+// so the tensor cores fill one buffer while the other is read and a tile's
+// grid cells are stored while the next tile streams in.  Every wait is
+// bounded: a role that gives up sets the error flag and stops, the others
+// then give up at their next wait, and the CTA lets its copies and MMAs in
+// flight finish (bounded) before it frees TMEM.
 template <int NN, bool SPLIT>
-__global__ void __launch_bounds__(SW_THREADS, 1)
+__global__ void __launch_bounds__(WS_THREADS, 1)
     grid_sw(const uint4 *__restrict__ whi, const uint4 *__restrict__ wlo,
             const int *__restrict__ vidx, const int2 *__restrict__ tile_chunks,
-            const int *__restrict__ tile_order, const __half *__restrict__ ghi,
-            const __half *__restrict__ glo, const unsigned *__restrict__ amax_bits,
-            float2 *__restrict__ grid, Geom geo, int ntx, size_t rows, int zg_first,
-            int *__restrict__ err) {
+            const int *__restrict__ tile_order, int ntiles, int nitems,
+            const __half *__restrict__ ghi, const __half *__restrict__ glo,
+            const unsigned *__restrict__ amax_bits, float2 *__restrict__ grid, Geom geo,
+            int ntx, size_t rows, int *__restrict__ err) {
   using namespace tcb::tc;
   using Cfg = SwCfg<NN, SPLIT>;
+  constexpr int NST = Cfg::NST;
   extern __shared__ uint8_t swsm_raw[];
   uint8_t *sm = swsm_raw + ((1024u - (smem_u32(swsm_raw) & 1023u)) & 1023u);
-  uint64_t *wfull = reinterpret_cast<uint64_t *>(sm + 2 * Cfg::STAGE);
-  uint64_t *mdone = wfull + 2;
-  uint64_t *pdone = mdone + 2;     // fp32 mode: a partial sum is complete
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(pdone + 2);
-  const int twon = geo.twon;
-  const int tile = tile_order[blockIdx.x];
-  const int zg = zg_first + blockIdx.y;           // pair group of this launch
-  const int z0 = zg * (NN / 2);
-  const int ix0 = (tile % ntx) * SW_TX, iy0 = (tile / ntx) * SW_TY;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + NST * Cfg::STAGE);
+  uint64_t *empty = full + NST;
+  uint64_t *pfull = empty + NST;  // TMEM buffer b holds a finished partial sum (tile)
+  uint64_t *tfree = pfull + 2;    // TMEM buffer b was read by the accumulator warps
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tfree + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int2 tc_ = tile_chunks[tile];             // (first chunk, chunks)
-  const int c0 = tc_.x, nch = tc_.y;
-  const __half *gh = ghi + (size_t)blockIdx.y * rows * NN;
-  const __half *gl = SPLIT ? glo + (size_t)blockIdx.y * rows * NN : nullptr;
+  const int G = gridDim.x;
 
   if (tid == 0) {
-    mbar_init(&wfull[0], 1);
-    mbar_init(&wfull[1], 1);
-    mbar_init(&mdone[0], 1);
-    mbar_init(&mdone[1], 1);
-    mbar_init(&pdone[0], 1);
-    mbar_init(&pdone[1], 1);
+    for (int i = 0; i < NST; i++) {
+      mbar_init(&full[i], 33);  // lane 0's expect_tx arrival + 32 gather arrivals
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&pfull[i], 1);
+      mbar_init(&tfree[i], WS_ACC_WARPS);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
@@ -1032,166 +1100,192 @@ __global__ void __launch_bounds__(SW_THREADS, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-
-  // loads of chunk cc into stage st: W by one bulk copy per image, V rows by cp.async
-  auto issue = [&](int cc, int st) {
-    uint8_t *S = sm + st * Cfg::STAGE;
-    if (tid == 0) {
-      mbar_expect_tx(&wfull[st], (uint32_t)Cfg::WB);
-      bulk_g2s(smem_u32(S), whi + (size_t)(c0 + cc) * (SW_WIMG / 16), SW_WIMG, &wfull[st]);
-      if (SPLIT)
-        bulk_g2s(smem_u32(S + SW_WIMG), wlo + (size_t)(c0 + cc) * (SW_WIMG / 16), SW_WIMG,
-                 &wfull[st]);
-    }
-    const int *vi = vidx + (size_t)(c0 + cc) * SW_K;
-    const uint32_t vb = smem_u32(S + Cfg::WB);
-    constexpr int PIECES = SW_K * (NN / 8);   // 16-byte pieces per operand
-    for (int e = tid; e < PIECES; e += SW_THREADS) {
-      const int k = e / (NN / 8), q = e % (NN / 8);
-      const int row = __ldg(vi + k);
-      const size_t so = (size_t)(row < 0 ? 0 : row) * NN + (size_t)q * 8;
-      const uint32_t d = mn_sw128_offset(k, q * 8);
-      cp_async16(vb + d, gh + so, row < 0 ? 0 : 16);
-      if (SPLIT) cp_async16(vb + Cfg::VB + d, gl + so, row < 0 ? 0 : 16);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-
-  // this thread's cell (TMEM lane) and its running sums (fp32 mode)
-  const int eg = warp >> 2, eq = warp & 3;
-  float acc[SPLIT ? NN : 1];
-#pragma unroll
-  for (int j = 0; j < (SPLIT ? NN : 1); j++) acc[j] = 0.f;
   bool ok = true;
-  int flushed = 0;  // partial sums added into acc
-  auto flush = [&](int j) {  // partial sum j (buffer j & 1) into acc
-    if (tid == 0 && !mbar_wait(&pdone[j & 1], (j >> 1) & 1)) ok = false;
-    ok = __syncthreads_and(ok);
-    if (!ok) return;
-    tc_fence_after();
+
+  if (warp == WS_ACC_WARPS) {
+    // ---------------- producer
+    long long g = 0;      // chunks issued
+    long long pub = 0;    // chunks whose gathers this lane has published
+    int it = blockIdx.x;
+    int2 cur = it < nitems ? tile_chunks[tile_order[it % ntiles]] : make_int2(0, 0);
+    int tnext = it + G < nitems ? tile_order[(it + G) % ntiles] : 0;
+    int row = cur.y > 0 ? __ldg(vidx + (size_t)cur.x * SW_K + lane) : -1;
+    bool have_row = true;
+    for (; it < nitems && ok; it += G) {
+      // one item ahead: the next item's chunk range, the tile of the one after
+      const int2 nxt = it + G < nitems ? tile_chunks[tnext] : make_int2(0, 0);
+      const int tnext2 = it + 2 * G < nitems ? tile_order[(it + 2 * G) % ntiles] : 0;
+      const int zg = it / ntiles;
+      const __half *gh = ghi + (size_t)zg * rows * NN;
+      const __half *gl = SPLIT ? glo + (size_t)zg * rows * NN : nullptr;
+      if (cur.y > 0 && !have_row) row = __ldg(vidx + (size_t)cur.x * SW_K + lane);
+      have_row = false;
+      for (int c = 0; c < cur.y; c++, g++) {
+        // the row index of the chunk after this one (possibly the next item's first)
+        int row_next = -1;
+        if (c + 1 < cur.y) {
+          row_next = __ldg(vidx + (size_t)(cur.x + c + 1) * SW_K + lane);
+        } else if (nxt.y > 0) {
+          row_next = __ldg(vidx + (size_t)nxt.x * SW_K + lane);
+          have_row = true;
+        }
+        const int s = (int)(g % NST);
+        if (g >= NST && !warp_wait(&empty[s], (uint32_t)(((g / NST) + 1) & 1))) {
+          ok = false;
+          break;
+        }
+        const size_t chunk = (size_t)(cur.x + c);
+        uint8_t *S = sm + s * Cfg::STAGE;
+        if (lane == 0) {
+          mbar_expect_tx(&full[s], (uint32_t)Cfg::WB);
+          bulk_g2s(smem_u32(S), whi + chunk * (SW_WIMG / 16), SW_WIMG, &full[s]);
+          if (SPLIT)
+            bulk_g2s(smem_u32(S + SW_WIMG), wlo + chunk * (SW_WIMG / 16), SW_WIMG, &full[s]);
+        }
+        // lane k gathers the spectrum row of the chunk's sample k (zeros when absent)
+        const uint32_t vb = smem_u32(S + Cfg::WB);
+        const size_t so = (size_t)(row < 0 ? 0 : row) * NN;
+        const int nb = row < 0 ? 0 : 16;
 #pragma unroll
-    for (int cb = 0; cb < NN; cb += 32) {
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(eq * 32) << 16) + (uint32_t)((j & 1) * 2 * NN + eg * NN + cb),
-                v);
-#pragma unroll
-      for (int i = 0; i < 32; i++) acc[(cb + i) % (SPLIT ? NN : 1)] += v[i];
-    }
-    tc_fence_before();
-    flushed = j + 1;
-  };
-  int issued = 0, consumed = 0;  // chunks whose W copy was issued / arrived (thread 0)
-  if (nch > 0) {
-    issue(0, 0);
-    issued = 1;
-  }
-  for (int c = 0; c < nch; c++) {
-    const int st = c & 1;
-    if (c + 1 < nch) {
-      // stage st^1 was read by the MMAs of chunk c - 1
-      if (c >= 1) {
-        if (tid == 0 && !mbar_wait(&mdone[st ^ 1], ((c - 1) >> 1) & 1)) ok = false;
-        ok = __syncthreads_and(ok);
-        if (!ok) break;
+        for (int q = 0; q < NN / 8; q++) {
+          const uint32_t d = mn_sw128_offset(lane, q * 8);
+          cp_async16(vb + d, gh + so + q * 8, nb);
+          if (SPLIT) cp_async16(vb + Cfg::VB + d, gl + so + q * 8, nb);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        // chunk g - LAG's gathers have landed: publish them to the async proxy
+        if (g + 1 - pub > Cfg::LAG) {
+          asm volatile("cp.async.wait_group %0;" ::"n"(Cfg::LAG) : "memory");
+          fence_proxy_async_smem();
+          mbar_arrive(&full[pub % NST]);
+          pub++;
+        }
+        row = row_next;
       }
-      issue(c + 1, st ^ 1);
-      issued = c + 2;
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      cur = nxt;
+      tnext = tnext2;
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      if (!mbar_wait(&wfull[st], (c >> 1) & 1)) {
-        ok = false;
-      } else {
-        consumed = c + 1;
+    for (; pub < g; pub++) mbar_arrive(&full[pub % NST]);
+    // the bulk copies of the last stages have landed before the CTA exits (bounded)
+    for (long long gg = g > NST ? g - NST : 0; gg < g; gg++)
+      mbar_wait(&full[gg % NST], (uint32_t)((gg / NST) & 1));
+  } else if (warp == WS_ACC_WARPS + 1) {
+    // ---------------- MMA issuer
+    long long g = 0, gp = 0;  // chunks consumed, TMEM buffers started
+    int it = blockIdx.x;
+    int nch = it < nitems ? tile_chunks[tile_order[it % ntiles]].y : 0;
+    int tnext = it + G < nitems ? tile_order[(it + G) % ntiles] : 0;
+    for (; it < nitems && ok; it += G) {
+      const int nch_next = it + G < nitems ? tile_chunks[tnext].y : 0;
+      const int tnext2 = it + 2 * G < nitems ? tile_order[(it + 2 * G) % ntiles] : 0;
+      for (int c = 0; c < nch; c++, g++) {
+        const int s = (int)(g % NST);
+        const bool pstart = SPLIT ? (c % SW_F == 0) : (c == 0);
+        const bool pend = SPLIT ? (c % SW_F == SW_F - 1 || c == nch - 1) : (c == nch - 1);
+        const uint32_t buf = (uint32_t)(gp & 1);
+        // a new partial sum (tile) goes into a buffer the accumulators have read
+        if (pstart && gp >= 2 && !warp_wait(&tfree[buf], (uint32_t)(((gp >> 1) + 1) & 1))) {
+          ok = false;
+          break;
+        }
+        if (!warp_wait(&full[s], (uint32_t)((g / NST) & 1))) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
-        uint8_t *S = sm + st * Cfg::STAGE;
-        const uint32_t a_hi = smem_u32(S), a_lo = a_hi + SW_WIMG;
-        const uint32_t b_hi = smem_u32(S + Cfg::WB), b_lo = b_hi + Cfg::VB;
-        constexpr uint32_t idesc = idesc_f16_f32(128, NN) | (1u << 16);  // B MN-major
-        // fp32 mode: partial sum c / SW_F in buffer (c / SW_F) & 1
-        const uint32_t pbuf = SPLIT ? (uint32_t)(((c / SW_F) & 1) * 2 * NN) : 0u;
-        const bool first = SPLIT ? (c % SW_F == 0) : (c == 0);
+        if (lane == 0) {
+          uint8_t *S = sm + s * Cfg::STAGE;
+          const uint32_t a_hi = smem_u32(S), a_lo = a_hi + SW_WIMG;
+          const uint32_t b_hi = smem_u32(S + Cfg::WB), b_lo = b_hi + Cfg::VB;
+          constexpr uint32_t idesc = idesc_f16_f32(128, NN) | (1u << 16);  // B MN-major
+          // MN atoms of the V operand (64 comps) are SW_K * 128 bytes apart
+          constexpr uint32_t lbo = NN > 64 ? (uint32_t)(SW_K * 128) : 1024u;
 #pragma unroll
-        for (int g = 0; g < 2; g++) {
-          const uint32_t d = tmem + pbuf + (uint32_t)(g * NN);
+          for (int gr = 0; gr < 2; gr++) {
+            const uint32_t d = tmem + buf * 2 * NN + (uint32_t)(gr * NN);
+            const uint32_t ag = (uint32_t)(gr * (SW_WIMG / 2));  // 128 rows of 64 bytes
 #pragma unroll
-          for (int kk = 0; kk < SW_K / 16; kk++) {
-            const uint32_t acc0 = (!first || kk > 0) ? 1u : 0u;
-            constexpr uint32_t lbo = NN > 64 ? 8192u : 1024u;
-            const uint64_t bh = sdesc_mn(b_hi + kk * 2048, lbo);
-            mma_f16(d, sdesc(a_hi + g * 16384 + kk * 32), bh, idesc, acc0);
-            if (SPLIT) {
-              mma_f16(d, sdesc(a_lo + g * 16384 + kk * 32), bh, idesc, 1u);
-              mma_f16(d, sdesc(a_hi + g * 16384 + kk * 32), sdesc_mn(b_lo + kk * 2048, lbo),
-                      idesc, 1u);
+            for (int kk = 0; kk < SW_K / 16; kk++) {
+              const uint32_t acc0 = (!pstart || kk > 0) ? 1u : 0u;
+              const uint64_t bh = sdesc_mn(b_hi + kk * 2048, lbo);
+              mma_f16(d, sdesc_k64(a_hi + ag + kk * 32), bh, idesc, acc0);
+              if (SPLIT) {
+                mma_f16(d, sdesc_k64(a_lo + ag + kk * 32), bh, idesc, 1u);
+                mma_f16(d, sdesc_k64(a_hi + ag + kk * 32), sdesc_mn(b_lo + kk * 2048, lbo),
+                        idesc, 1u);
+              }
             }
           }
+          mma_commit(&empty[s]);
+          if (pend) mma_commit(&pfull[buf]);
         }
-        mma_commit(&mdone[st]);
-        if (SPLIT && (c % SW_F == SW_F - 1 || c == nch - 1)) mma_commit(&pdone[(c / SW_F) & 1]);
+        __syncwarp();
+        if (pend) gp++;
       }
+      nch = nch_next;
+      tnext = tnext2;
     }
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
-    // partial c / SW_F - 1 while the tensor cores work on partial c / SW_F
-    if (SPLIT && c % SW_F == SW_F - 1 && c >= SW_F) {
-      flush(c / SW_F - 1);
-      if (!ok) break;
-    }
-  }
-  // all MMAs (and so all reads of shared memory) done before the epilogue
-  if (nch > 0) {
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    if (tid == 0 && ok && !mbar_wait(&mdone[(nch - 1) & 1], ((nch - 1) >> 1) & 1)) ok = false;
-    if (tid == 0 && !ok) {
-      // a wait gave up: let the copies still in flight land (bounded) and the
-      // last committed MMAs finish before the CTA releases its memory
-      for (int cc = consumed; cc < issued; cc++) mbar_wait(&wfull[cc & 1], (cc >> 1) & 1);
-      if (consumed > 0) mbar_wait(&mdone[(consumed - 1) & 1], ((consumed - 1) >> 1) & 1);
-    }
-    ok = __syncthreads_and(ok);
-    if (SPLIT && ok)
-      for (int j = flushed; j <= (nch - 1) / SW_F && ok; j++) flush(j);
-  }
-  tc_fence_after();
-  // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. of M-group w / 4.
-  {
-    const int g = warp >> 2, q = warp & 3;
-    const int m = g * 128 + q * 32 + lane;
-    const int cx = ix0 + (m % SW_TX), cy = iy0 + (m / SW_TX);
+    // the last MMAs have finished before the CTA frees TMEM (bounded)
+    if (g > 0) mbar_wait(&empty[(g - 1) % NST], (uint32_t)(((g - 1) / NST) & 1));
+  } else {
+    // ---------------- accumulator warps
+    constexpr int HC = NN / 2;  // columns (re, im of NN / 4 pairs) per thread
+    const int q = warp & 3, gr = (warp >> 2) & 1, hf = warp >> 3;
+    const int m = gr * 128 + q * 32 + lane;
     const float amax = __uint_as_float(*amax_bits);
     int ex = 0;
     if (amax > 0.f) frexpf(amax, &ex);
     const float unsc = ldexpf(1.f, ex - 14) / SW_WSCALE;
-    const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
-    const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
+    float acc[HC];
+    long long gp = 0;
+    int it = blockIdx.x;
+    int tile = it < nitems ? tile_order[it % ntiles] : 0;
+    for (; it < nitems && ok; it += G) {
+      const int nch = tile_chunks[tile].y;
+      const int tile_next = it + G < nitems ? tile_order[(it + G) % ntiles] : 0;
+      const int nparts = SPLIT ? (nch + SW_F - 1) / SW_F : (nch > 0 ? 1 : 0);
 #pragma unroll
-    for (int cb = 0; cb < NN; cb += 32) {
-      float v[32];
-      if (SPLIT) {
+      for (int j = 0; j < HC; j++) acc[j] = 0.f;
+      for (int p = 0; p < nparts; p++, gp++) {
+        const uint32_t buf = (uint32_t)(gp & 1);
+        if (!warp_wait(&pfull[buf], (uint32_t)((gp >> 1) & 1))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) +
+                              (uint32_t)(buf * 2 * NN + gr * NN + hf * HC);
 #pragma unroll
-        for (int j = 0; j < 32; j++) v[j] = acc[(cb + j) % (SPLIT ? NN : 1)];
-      } else if (nch > 0) {
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(g * NN + cb), v);
-      } else {
+        for (int cb = 0; cb < HC; cb += 16) {
+          float v[16];
+          tmem_ld16(base + cb, v);
 #pragma unroll
-        for (int j = 0; j < 32; j++) v[j] = 0.f;
+          for (int i = 0; i < 16; i++) acc[cb + i] += v[i];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tfree[buf]);
       }
-      if (!ok || cx >= twon || cy >= twon) continue;
+      if (!ok) break;
+      // this thread's cell, pairs z0 + hf * HC / 2 ...
+      const int ix0 = (tile % ntx) * SW_TX, iy0 = (tile / ntx) * SW_TY;
+      const int cx = ix0 + (m % SW_TX), cy = iy0 + (m / SW_TX);
+      if (cx < geo.twon && cy < geo.twon) {
+        const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
+        const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
+        const int pz0 = (it / ntiles) * (NN / 2) + hf * (HC / 2);
+        float2 *gp0 = grid + ((size_t)pz0 * geo.twon + cy) * geo.twon + cx;
+        const size_t plane = (size_t)geo.twon * geo.twon;
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int pz = z0 + cb / 2 + j;
-        if (pz < geo.nz)
-          grid[((size_t)pz * twon + cy) * twon + cx] =
-              make_float2(v[2 * j] * sgn, v[2 * j + 1] * sgn);
+        for (int j = 0; j < HC / 2; j++)
+          if (pz0 + j < geo.nz) gp0[j * plane] = make_float2(acc[2 * j] * sgn, acc[2 * j + 1] * sgn);
       }
+      tile = tile_next;
     }
   }
-  if (!ok && tid == 0) atomicOr(err, 1);
+  if (!ok && lane == 0) atomicOr(err, 1);
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -1666,11 +1760,13 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
                   h->sw_zgroups * C * (SW_WIMG * nimg + SW_K * sizeof(int)) + vbytes +
                       (double)h->nz * geo.twon * geo.twon * sizeof(float2),
                   h->sw_zgroups * C * 2.0 * SW_M * h->sw_nn * SW_K * (h->sw_lo ? 3.0 : 1.0));
-    const dim3 grd((unsigned)h->sw_ntiles, (unsigned)h->sw_zgroups);
+    // persistent: one CTA per SM (all of TMEM, ~193 KB of shared memory)
+    const int nitems = h->sw_ntiles * h->sw_zgroups;
+    const unsigned grd = (unsigned)std::min(nitems, sm_count());
 #define FR_SW(NN_, SPLIT_)                                                                 \
-  grid_sw<NN_, SPLIT_><<<grd, SW_THREADS, SwCfg<NN_, SPLIT_>::SMEM, s>>>(                  \
-      h->sw_whi, h->sw_wlo, h->sw_vidx, h->sw_tile_chunks, h->sw_order, h->sw_ghi,          \
-      h->sw_glo, h->amax, h->grid, geo, h->sw_ntx, rows, 0, h->tc_err)
+  grid_sw<NN_, SPLIT_><<<grd, WS_THREADS, SwCfg<NN_, SPLIT_>::SMEM, s>>>(                  \
+      h->sw_whi, h->sw_wlo, h->sw_vidx, h->sw_tile_chunks, h->sw_order, h->sw_ntiles,       \
+      nitems, h->sw_ghi, h->sw_glo, h->amax, h->grid, geo, h->sw_ntx, rows, h->tc_err)
     if (h->sw_nn == 128) {
       if (h->sw_lo) FR_SW(128, true); else FR_SW(128, false);
     } else {
@@ -1857,16 +1953,11 @@ int sw_build(tcb_fourierrec *h, bool with_lo) {
       cudaMalloc(&h->sw_tile_chunks, (size_t)nt * sizeof(int2)) != cudaSuccess)
     return oom("chunk table");
   TCB_CUDA(cudaMemcpy(h->sw_tile_chunks, tch.data(), nt * sizeof(int2), cudaMemcpyHostToDevice));
-  // tiles centre-first (the sample density peaks at the origin)
+  // tiles in raster order: the persistent CTAs take consecutive tiles at a
+  // time, so the grid rows they store at once (and the weight images they
+  // stream, which are laid out in tile order) are neighbours in memory
   std::vector<int> order(nt);
-  std::vector<float> dist(nt);
-  for (int t = 0; t < nt; t++) {
-    order[t] = t;
-    const float cx = (t % ntx) * SW_TX + 0.5f * SW_TX - (float)geo.n;
-    const float cy = (t / ntx) * SW_TY + 0.5f * SW_TY - (float)geo.n;
-    dist[t] = cx * cx + cy * cy;
-  }
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dist[a] < dist[b]; });
+  for (int t = 0; t < nt; t++) order[t] = t;
   if (!h->sw_order && cudaMalloc(&h->sw_order, (size_t)nt * sizeof(int)) != cudaSuccess)
     return oom("tile order");
   TCB_CUDA(cudaMemcpy(h->sw_order, order.data(), nt * sizeof(int), cudaMemcpyHostToDevice));
