@@ -586,6 +586,8 @@ def run_methods(a, data, dark, flat, theta, dev):
                                                          ti_mask=1)),
             ("fourierrec+dezinger", "fourierrec", a.nz, dict(dezinger=3,
                                                               dezinger_threshold=5000)),
+            ("fourierrec+vo-all", "fourierrec", min(a.nz, a.slab_rows),
+             dict(remove_stripe_method="vo-all")),
             ("lprec", "lprec", min(a.nz, a.slab_rows), {}),
             ("linerec", "linerec", min(a.nz, a.slab_rows), {})]
     for name, alg, rows, extra in legs:
@@ -655,11 +657,14 @@ def run_phase(a, dev, peaks, peaks_kind):
     np_tomo.retrieve_phase(x[:1].cpu().numpy(), "paganin", ps, dist, en, alpha)
     cpu_s = time.perf_counter() - t0
     alg = 8.0 * P * n * n
-    # the padded chain's least traffic per padded pixel: pad (write 4, read the
-    # image once), R2C (4 in, 4 out), multiply (8 B in + 8 out per half-spectrum
-    # entry = 8), C2R (4 + 4), crop (read and write the image): ~31 B
-    npad = float(n + 2 * op.py) * (n + 2 * op.pz)
-    chain = P * (npad * (4 + 8 + 8 + 8) + 3.0 * 4 * n * n)
+    # the three-pass chain's traffic (pairs of projections packed as one
+    # complex image): rows pass reads the two images and writes the padded
+    # row spectra (8 B per padded pixel), the columns pass reads them and
+    # writes the dy kept rows (8 B per kept-row pixel), the last rows pass
+    # reads those and writes the two images
+    Ny, Nz = n + 2 * op.py, n + 2 * op.pz
+    chain = (P / 2.0) * (2 * 4.0 * n * n + 2 * 8.0 * Ny * Nz + 2 * 8.0 * n * Nz +
+                         2 * 4.0 * n * n)
     res = {"workload": f"{P} projections {n}x{n} float32, paganin (0.65 um, 50 mm, 20 keV, "
                        f"alpha 1e-3), padded {n + 2 * op.py}x{n + 2 * op.pz}",
            "ms": round(ms, 2), "projections_per_s": round(P / (ms / 1e3), 1),
@@ -768,6 +773,10 @@ def run_ours(a, ws, rank, local):
             side["e2e_fp16_out"] = run_e2e(a, data, dark, flat, theta, dev, ws, rank,
                                            precision="mixed", out_dtype="float16")
 
+    # the e2e legs' pinned host stacks stay in torch's host cache otherwise
+    if hasattr(torch._C, "_host_emptyCache"):
+        torch._C._host_emptyCache()
+
     base = None
     if rank == 0 and ws == 1 and not a.no_cpu:
         dcpu, dkc, flc = data.cpu().numpy(), dark.cpu().numpy(), flat.cpu().numpy()
@@ -783,6 +792,8 @@ def run_ours(a, ws, rank, local):
     serving = None
     if not a.no_serve and ws == 1:
         serving = run_serving(a, dev)
+        if hasattr(torch._C, "_host_emptyCache"):
+            torch._C._host_emptyCache()
     lamino = None
     if not a.no_lamino and ws == 1:
         lamino = run_lamino(a, dev)
@@ -854,6 +865,7 @@ def _summary(line, side, methods, trycenter, serving, lamino, phase):
         "fw_ms": g(methods, "fourierrec+fw", "ms"),
         "ti_gups": g(methods, "fourierrec+ti", "value"),
         "dezinger_gups": g(methods, "fourierrec+dezinger", "value"),
+        "vo_all_gups": g(methods, "fourierrec+vo-all", "value"),
         "lprec_gups": g(methods, "lprec", "value"),
         "linerec_gups": g(methods, "linerec", "value"),
         "try_fp32_ms": g(trycenter, "float32", "ms_per_sweep"),
@@ -1103,7 +1115,7 @@ def main():
     ap.add_argument("--nproj", type=int, default=1500)
     ap.add_argument("--nz", type=int, default=2048)
     ap.add_argument("--ncz", type=int, default=128)
-    ap.add_argument("--e2e-ncz", type=int, default=32,
+    ap.add_argument("--e2e-ncz", type=int, default=64,
                     help="rows per chunk of the end-to-end (host buffer) leg")
     ap.add_argument("--algorithm", default="fourierrec", choices=["fourierrec", "lprec", "linerec"])
     ap.add_argument("--filter", default="shepp")

@@ -279,3 +279,22 @@ def test_recon_try_with_phase_and_rotation_matches_reference(cuda, ref, algorith
             ours = w.tries[(zs, float(params.save_centers[k + kk]))].cpu()
             err = rel_l2(ours, theirs[kk].cpu())
             assert err < 1e-4, (k + kk, err)
+
+
+@pytest.mark.parametrize("shape", [(4, 1024, 1024), (3, 700, 900)])
+def test_phase_own_fft_matches_cufft(cuda, monkeypatch, shape):
+    """Power-of-two padded sizes run on the library's own FFT (pairs of
+    projections packed as one complex image, padding and crop fused into
+    the row passes); the cuFFT R2C/C2R chain (TCB_PHASE_FFT set) computes
+    the same filter.  An odd projection count leaves the last pair half
+    empty."""
+    _cases()
+    from make_golden import phase_input
+    x = phase_input(*shape, seed=13)
+    args = ("paganin", 0.65e-4, 5.0, 20.0, 1e-3, 1500.0, 2e-4)
+    own = _run(torch.as_tensor(x, device=cuda), *args, batch=4)
+    monkeypatch.setenv("TCB_PHASE_FFT", "cufft")
+    lib = _run(torch.as_tensor(x, device=cuda), *args, batch=4)
+    err = rel_l2(own.cpu(), lib.cpu())
+    print(f"phase own FFT vs cuFFT {shape}: {err:.2e}")
+    assert err < 2e-6, err

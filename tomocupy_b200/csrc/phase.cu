@@ -14,14 +14,28 @@
 //    C2C pair.  cuFFT runs the 2D transforms, batched over projections.
 //  * Padding is index clamping in one kernel (the reference's four slice
 //    assignments), cropping is a second kernel.
+//  * Power-of-two padded sizes in [256, 8192] (the production case) run on
+//    the library's own FFT instead, in three passes over two projections
+//    packed as one complex image c = a + i b (Fe is real and even, so
+//    ifft2(Fe fft2(c)) = a' + i b' with a', b' the filtered projections):
+//    (1) per padded row: the padding (index clamping at load), the forward
+//    FFT along the columns (conj(ifft(conj x))), stored in groups of 8
+//    columns; (2) per column: the forward FFT along the rows, the product
+//    with Fe, the inverse FFT, only the dy rows the crop keeps stored;
+//    (3) per kept row: the inverse FFT along the columns and the crop into
+//    the two projections in place.  The padded images and spectra never
+//    exist in full: 3 passes instead of pad, R2C (2 passes), multiply, C2R
+//    (2 passes) and crop.
 //  * The filter is built once per geometry on the host with the reference's
 //    float32 operation order (_reciprocal_grid, _paganin_filter_factor,
 //    _farago_filter_factor, _paganin_filter_factorG, fftshift, / max).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
+#include "fft_pow2.cuh"
 
 struct tcb_phase {
   size_t batch, dy, dz;  // projections per transform batch, image rows x columns
@@ -31,6 +45,11 @@ struct tcb_phase {
   float *real = nullptr;   // [batch, Ny, Nz] padded images / filtered images
   float2 *spec = nullptr;  // [batch, Ny, Nz/2+1] spectra
   float *fe = nullptr;     // [Ny, Nz/2+1] even part of the normalised filter / (Ny Nz)
+  // own-FFT chain (power-of-two Ny, Nz in [256, 8192]): packed pairs of projections
+  bool own = false;
+  float2 *t1 = nullptr;    // [pairs][Nz/8][Ny][8] row spectra, columns in groups of 8
+  float2 *t2 = nullptr;    // [pairs][dy][Nz] filtered rows kept by the crop
+  float2 *twy = nullptr, *twz = nullptr;  // twiddle tables of lengths Ny and Nz
 };
 
 namespace tcb {
@@ -173,15 +192,192 @@ __global__ void phase_crop(float *__restrict__ out, const float *__restrict__ in
     if (i0 + r < dy) out[(b * dy + i0 + r) * dz + j] = v[r];
 }
 
+// ---- own-FFT chain ------------------------------------------------------------
+constexpr int PH_GW = 8;  // columns per group of the row-pass output
+
+// Pass 1: padded row i of the pair (2q, 2q + 1): forward FFT along the
+// columns of (a + i b), written to t1[q][j / 8][i][j % 8].
+template <int N>
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
+    ph_rows_fwd(const float *__restrict__ data, float2 *__restrict__ t1,
+                const float2 *__restrict__ tw, int nb, int dy, int dz, int py, int pz, int Ny) {
+  extern __shared__ float2 fsm[];
+  const int i = blockIdx.x, q = blockIdx.y;
+  const size_t img = (size_t)dy * dz;
+  const float *a = data + (size_t)(2 * q) * img + (size_t)pad_src(i, py, dy) * dz;
+  const float *b = 2 * q + 1 < nb ? a + img : nullptr;
+  float2 *dst = t1 + (size_t)q * Ny * N + (size_t)i * PH_GW;
+  // forward transform as conj(ifft(conj(x)))
+  auto in = [a, b, pz, dz](int e) {
+    const int j = pad_src(e, pz, dz);
+    return make_float2(__ldg(a + j), b ? -__ldg(b + j) : 0.f);
+  };
+  auto out = [dst, Ny](int o, float2 v) {
+    dst[(size_t)(o / PH_GW) * Ny * PH_GW + o % PH_GW] = make_float2(v.x, -v.y);
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
+}
+
+// Pass 2: cpc adjacent columns j per block: forward FFT along the rows,
+// product with the even filter Fe(k, j) (half table, Fe(k, j) = Fe(-k, -j)),
+// inverse FFT, rows [py, py + dy) to t2[q][r][j].
+template <int N>
+__global__ void __launch_bounds__(1024)
+    ph_cols(const float2 *__restrict__ t1, float2 *__restrict__ t2, const float *__restrict__ fe,
+            const float2 *__restrict__ tw, int Nz, int dy, int py, int cpc) {
+  extern __shared__ float2 fsm[];
+  constexpr int SSTR = fftk::Plan<N>::PADDED + 4;
+  const int c = threadIdx.x % cpc, tid = threadIdx.x / cpc;
+  const int ncb = Nz / cpc;
+  const int q = blockIdx.x / ncb, j = (blockIdx.x % ncb) * cpc + c;
+  const int Nc = Nz / 2 + 1;
+  const float2 *src = t1 + (size_t)q * N * Nz + (size_t)(j / PH_GW) * N * PH_GW + j % PH_GW;
+  float2 *sm = fsm + c * SSTR;
+  auto in1 = [src](int e) {
+    const float2 v = __ldg(src + (size_t)e * PH_GW);
+    return make_float2(v.x, -v.y);
+  };
+  auto out1 = [sm](int o, float2 v) { sm[fftk::pad16(o)] = make_float2(v.x, -v.y); };
+  fftk::ifft<N, true>(sm, tid, tw, in1, out1);
+  __syncthreads();
+  {
+    // times Fe(k, j) from the half table: column j, or row -k of column -j
+    const bool neg = j >= Nc;
+    const float *fcol = fe + (neg ? Nz - j : j);
+#pragma unroll 4
+    for (int k = tid; k < N; k += N / 16) {
+      const float w = __ldg(fcol + (size_t)(neg ? (N - k) & (N - 1) : k) * Nc);
+      float2 &x = sm[fftk::pad16(k)];
+      x = make_float2(x.x * w, x.y * w);
+    }
+  }
+  __syncthreads();
+  float2 *dst = t2 + (size_t)q * dy * Nz + j;
+  auto in2 = [sm](int e) { return sm[fftk::pad16(e)]; };
+  auto out2 = [dst, py, dy, Nz](int o, float2 v) {
+    const unsigned r = (unsigned)(o - py);
+    if (r < (unsigned)dy) dst[(size_t)r * Nz] = v;
+  };
+  // the second transform reads the twiddles again instead of keeping the
+  // first one's in registers (an opaque copy of the pointer)
+  const float2 *tw2;
+  asm volatile("mov.b64 %0, %1;" : "=l"(tw2) : "l"(tw));
+  fftk::ifft<N>(sm, tid, tw2, in2, out2);
+}
+
+// Pass 3: kept row r: inverse FFT along the columns, columns [pz, pz + dz)
+// written back to the two projections (real part to 2q, imaginary to 2q + 1).
+template <int N>
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
+    ph_rows_inv(const float2 *__restrict__ t2, float *__restrict__ data,
+                const float2 *__restrict__ tw, int nb, int dy, int dz, int pz) {
+  extern __shared__ float2 fsm[];
+  const int r = blockIdx.x, q = blockIdx.y;
+  const size_t img = (size_t)dy * dz;
+  const float2 *src = t2 + ((size_t)q * dy + r) * N;
+  float *a = data + (size_t)(2 * q) * img + (size_t)r * dz;
+  float *b = 2 * q + 1 < nb ? a + img : nullptr;
+  auto in = [src](int e) { return __ldg(src + e); };
+  auto out = [a, b, pz, dz](int o, float2 v) {
+    const unsigned j = (unsigned)(o - pz);
+    if (j < (unsigned)dz) {
+      a[j] = v.x;
+      if (b) b[j] = v.y;
+    }
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
+}
+
+inline int ph_cpc(int N) { return std::min(16384 / N, 16); }
+inline size_t ph_cols_smem(int N) { return (size_t)ph_cpc(N) * (N + N / 16 + 4) * sizeof(float2); }
+inline size_t ph_rows_smem(int N) { return (size_t)(N + N / 16) * sizeof(float2); }
+
+template <int N>
+cudaError_t ph_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(ph_rows_fwd<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ph_rows_smem(N));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ph_rows_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ph_rows_smem(N));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ph_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ph_cols_smem(N));
+  return e;
+}
+
+cudaError_t ph_attrs_for(int n) {
+  switch (n) {
+    case 256: return ph_attrs<256>();
+    case 512: return ph_attrs<512>();
+    case 1024: return ph_attrs<1024>();
+    case 2048: return ph_attrs<2048>();
+    case 4096: return ph_attrs<4096>();
+    default: return ph_attrs<8192>();
+  }
+}
+
+#define PH_DISPATCH(n, F)          \
+  switch (n) {                     \
+    case 256: F(256); break;       \
+    case 512: F(512); break;       \
+    case 1024: F(1024); break;     \
+    case 2048: F(2048); break;     \
+    case 4096: F(4096); break;     \
+    default: F(8192); break;       \
+  }
+
+int ph_own_apply(tcb_phase *h, float *d, size_t b, cudaStream_t s) {
+  const int Ny = (int)h->Ny, Nz = (int)h->Nz, dy = (int)h->dy, dz = (int)h->dz;
+  const int py = (int)h->py, pz = (int)h->pz, nb = (int)b;
+  const unsigned pairs = (unsigned)((b + 1) / 2);
+  {
+    StageTimer t("phase_rows_fwd", s);
+#define PH_ROWS_FWD(N)                                                                   \
+  ph_rows_fwd<N><<<dim3((unsigned)Ny, pairs), N / 16, ph_rows_smem(N), s>>>(             \
+      d, h->t1, h->twz, nb, dy, dz, py, pz, Ny)
+    PH_DISPATCH(Nz, PH_ROWS_FWD)
+#undef PH_ROWS_FWD
+    TCB_LAUNCH_CHECK();
+    count_launch();
+  }
+  {
+    StageTimer t("phase_cols", s);
+#define PH_COLS(N)                                                                       \
+  ph_cols<N><<<(unsigned)(Nz / ph_cpc(N)) * pairs, ph_cpc(N) * (N / 16), ph_cols_smem(N), \
+               s>>>(h->t1, h->t2, h->fe, h->twy, Nz, dy, py, ph_cpc(N))
+    PH_DISPATCH(Ny, PH_COLS)
+#undef PH_COLS
+    TCB_LAUNCH_CHECK();
+    count_launch();
+  }
+  {
+    StageTimer t("phase_rows_inv", s);
+#define PH_ROWS_INV(N)                                                                   \
+  ph_rows_inv<N><<<dim3((unsigned)dy, pairs), N / 16, ph_rows_smem(N), s>>>(             \
+      h->t2, d, h->twz, nb, dy, dz, pz)
+    PH_DISPATCH(Nz, PH_ROWS_INV)
+#undef PH_ROWS_INV
+    TCB_LAUNCH_CHECK();
+    count_launch();
+  }
+  return TCB_OK;
+}
+
+bool pow2_in(size_t n) { return n >= 256 && n <= 8192 && (n & (n - 1)) == 0; }
+
 void phase_release(tcb_phase *h) {
   if (h->fwd) cufftDestroy(h->fwd);
   if (h->inv) cufftDestroy(h->inv);
   cudaFree(h->real);
   cudaFree(h->spec);
   cudaFree(h->fe);
+  cudaFree(h->t1);
+  cudaFree(h->t2);
+  cudaFree(h->twy);
+  cudaFree(h->twz);
   h->fwd = h->inv = 0;
   h->real = h->fe = nullptr;
-  h->spec = nullptr;
+  h->spec = h->t1 = h->t2 = h->twy = h->twz = nullptr;
 }
 
 }  // namespace
@@ -256,17 +452,42 @@ extern "C" int tcb_phase_create(tcb_phase **out, size_t batch, size_t dy, size_t
     delete h;
     return code;
   };
-  if (cudaMalloc(&h->real, batch * Ny * Nz * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&h->spec, batch * Ny * Nc * sizeof(float2)) != cudaSuccess ||
-      cudaMalloc(&h->fe, Ny * Nc * sizeof(float)) != cudaSuccess) {
+  h->own = pow2_in(Ny) && pow2_in(Nz) && std::getenv("TCB_PHASE_FFT") == nullptr;
+  const size_t pairs = (batch + 1) / 2;
+  bool okm = cudaMalloc(&h->fe, Ny * Nc * sizeof(float)) == cudaSuccess;
+  if (okm && h->own)
+    okm = cudaMalloc(&h->t1, pairs * Ny * Nz * sizeof(float2)) == cudaSuccess &&
+          cudaMalloc(&h->t2, pairs * dy * Nz * sizeof(float2)) == cudaSuccess &&
+          cudaMalloc(&h->twy, 2 * Ny * sizeof(float2)) == cudaSuccess &&
+          cudaMalloc(&h->twz, 2 * Nz * sizeof(float2)) == cudaSuccess;
+  else if (okm)
+    okm = cudaMalloc(&h->real, batch * Ny * Nz * sizeof(float)) == cudaSuccess &&
+          cudaMalloc(&h->spec, batch * Ny * Nc * sizeof(float2)) == cudaSuccess;
+  if (!okm) {
     cudaGetLastError();
     set_error("tcb_phase_create: out of device memory (batch %zu of %zu x %zu)", batch, Ny, Nz);
     return fail(TCB_ERR_OUT_OF_MEMORY);
   }
   cudaError_t e = cudaMemcpy(h->fe, fe.data(), fe.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && h->own) {
+    const std::vector<float2> ty = fftk::twiddle_table((int)Ny), tz = fftk::twiddle_table((int)Nz);
+    if (ty.size() > 2 * Ny || tz.size() > 2 * Nz) {
+      set_error("tcb_phase_create: twiddle table larger than its buffer");
+      return fail(TCB_ERR_CUDA);
+    }
+    e = cudaMemcpy(h->twy, ty.data(), ty.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->twz, tz.data(), tz.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = ph_attrs_for((int)Ny);
+    if (e == cudaSuccess) e = ph_attrs_for((int)Nz);
+  }
   if (e != cudaSuccess) {
-    set_error("tcb_phase_create: cudaMemcpy failed: %s", cudaGetErrorString(e));
+    set_error("tcb_phase_create: setup failed: %s", cudaGetErrorString(e));
     return fail(TCB_ERR_CUDA);
+  }
+  if (h->own) {
+    *out = h;
+    return TCB_OK;
   }
   int dims[2] = {(int)Ny, (int)Nz};
   cufftResult r = cufftPlanMany(&h->fwd, 2, dims, nullptr, 1, (int)(Ny * Nz), nullptr, 1,
@@ -291,9 +512,16 @@ extern "C" int tcb_phase_sizes(tcb_phase *h, size_t *py, size_t *pz) {
 
 extern "C" int tcb_phase_apply(tcb_phase *h, float *data, size_t nproj, void *stream) {
   TCB_CHECK_ARG(h, "tcb_phase_apply: null handle");
-  TCB_CHECK_ARG(h->real, "tcb_phase_apply: handle was freed");
+  TCB_CHECK_ARG(h->real || h->t1, "tcb_phase_apply: handle was freed");
   TCB_CHECK_ARG(data || nproj == 0, "tcb_phase_apply: null data");
   cudaStream_t s = (cudaStream_t)stream;
+  if (h->own) {
+    for (size_t p0 = 0; p0 < nproj; p0 += h->batch) {
+      const int st = ph_own_apply(h, data + p0 * h->dy * h->dz, std::min(h->batch, nproj - p0), s);
+      if (st != TCB_OK) return st;
+    }
+    return TCB_OK;
+  }
   TCB_CUFFT(cufftSetStream(h->fwd, s));
   TCB_CUFFT(cufftSetStream(h->inv, s));
   const size_t Nc = h->Nz / 2 + 1, plane = h->Ny * Nc;

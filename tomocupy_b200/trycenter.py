@@ -185,10 +185,12 @@ def autotune(n, nproj, theta, center, shifts, data, dark0=None, flat0=None, *,
              cache_file=None, device="cuda"):
     """Pick (ncz, pairs_per_block) with the fastest captured sweep for this geometry.
 
-    candidates: iterable of (ncz, pairs_per_block); default chunk sizes 8..64
-    with gridding depths 4..16 pairs.  Returns {"ncz", "pairs_per_block",
-    "ms", "table"}; results are cached per geometry in-process and, when
-    cache_file is given, in that JSON file.
+    candidates: iterable of (ncz, pairs_per_block); by default chunk sizes
+    32..128 when the geometry's gridding runs on the tensor cores with
+    streamed weights (pairs_per_block does not apply there), else chunk sizes
+    8..64 with register-gridding depths 4..16 pairs.  Returns {"ncz",
+    "pairs_per_block", "ms", "table"}; results are cached per geometry
+    in-process and, when cache_file is given, in that JSON file.
     """
     key = f"{n}x{nproj}x{len(np.atleast_1d(shifts))}:{precision}:{fbp_filter}"
     if key in _TUNED:
@@ -198,12 +200,25 @@ def autotune(n, nproj, theta, center, shifts, data, dark0=None, flat0=None, *,
         if key in saved:
             _TUNED[key] = saved[key]
             return saved[key]
+    first = None
     if candidates is None:
-        candidates = [(ncz, zb) for ncz in (8, 16, 32, 64) for zb in (4, 8, 16) if zb <= ncz // 2]
+        first = TryCenterSweep(n, nproj, theta, center, shifts, fbp_filter, precision, 64, 0,
+                               device)
+        from . import _lib
+        if first.pipe.gridding in (_lib.GRID_TENSOR_FP32, _lib.GRID_TENSOR_STREAM):
+            candidates = [(64, 0), (32, 0), (128, 0)]
+        else:
+            candidates = [(ncz, zb) for ncz in (8, 16, 32, 64) for zb in (4, 8, 16)
+                          if zb <= ncz // 2]
+            first.free()
+            first = None
     table = []
     for ncz, zb in candidates:
-        sw = TryCenterSweep(n, nproj, theta, center, shifts, fbp_filter, precision, ncz, zb,
-                            device)
+        if first is not None and (ncz, zb) == (64, 0):
+            sw, first = first, None
+        else:
+            sw = TryCenterSweep(n, nproj, theta, center, shifts, fbp_filter, precision, ncz, zb,
+                                device)
         sw.load(data, dark0, flat0)
         sw.capture()
         sw.time_ms(1)
