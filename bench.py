@@ -485,6 +485,10 @@ def run_serving(a, dev):
     res["continuous_batching"] = latency_summary(mix)
     res["continuous_batching"]["peak_admitted"] = srv.peak_active
     res["continuous_batching"]["peak_resident_gb"] = round(srv.peak_bytes / 1e9, 2)
+    # same-geometry requests packed into shared chunk launches
+    res["continuous_batching"]["chunk_launches"] = srv.chunks
+    res["continuous_batching"]["chunks_one_request_each"] = int(sum(
+        -(-m.frames.shape[1] // a.serve_ncz) for m in mix))
     ratio = np.array([m.latency / s.latency for m, s in zip(mix, alone)])
     res["latency_in_mix_over_alone"] = {"p50": float(np.percentile(ratio, 50)),
                                         "p99": float(np.percentile(ratio, 99))}

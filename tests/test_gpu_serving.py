@@ -2,8 +2,9 @@
 
 The per-request computation is the fused reconstruction of GPURec; here the
 tests check what the serving layer adds: results identical alone and in a
-mix (bit for bit: every chunk depends only on its own request), agreement
-with GPURec, admission under an HBM budget, and the request generator.
+mix (bit for bit when every chunk holds one request; within 1e-6 when
+chunks pack several requests of one geometry), agreement with GPURec,
+admission under an HBM budget, and the request generator.
 """
 import numpy as np
 import pytest
@@ -52,17 +53,47 @@ SPECS = [(128, 90, 3, "float32"), (256, 180, 9, "mixed"), (128, 90, 16, "mixed")
 
 @pytest.mark.gpu
 def test_results_identical_alone_and_in_mix(cuda):
+    """Without packing every chunk holds one request's slices: bit for bit."""
     from tomocupy_b200.serving import Server
     mix = _requests(SPECS)
-    srv = Server(ncz=8)
+    srv = Server(ncz=8, pack=False)
     srv.serve(mix, realtime=False)
     assert srv.peak_active >= 2  # they really overlapped
     for r in mix:
         alone = _requests([SPECS[r.rid]], seed=r.rid)[0]
         alone.rid = r.rid
-        Server(ncz=8).serve([alone], realtime=False)
+        Server(ncz=8, pack=False).serve([alone], realtime=False)
         assert torch.equal(alone.out, r.out), r.rid
         assert np.isfinite(r.latency) and r.t_done >= r.t_admit
+
+
+@pytest.mark.gpu
+def test_packed_chunks_match_alone(cuda):
+    """Mixed-precision requests of one geometry share chunk launches (3 + 5
+    slices of 128 x 90 fill one chunk of 8, the 4 of the third one the
+    next); a slice may then be paired with another request's slice in
+    fourierrec's real/imaginary packing, whose crosstalk (the reference's
+    too) stays within the mixed-precision budget.  fp32 requests of one
+    geometry are not packed."""
+    from tomocupy_b200.serving import Server
+    specs = [(128, 90, 3, "mixed"), (256, 180, 9, "mixed"), (128, 90, 5, "mixed"),
+             (128, 90, 4, "mixed")]
+    mix = _requests(specs)
+    srv = Server(ncz=8, pack=True)
+    srv.serve(mix, realtime=False)
+    unpacked = Server(ncz=8, pack=False)
+    unpacked.serve(_requests(specs), realtime=False)
+    assert (srv.chunks, unpacked.chunks) == (4, 5), (srv.chunks, unpacked.chunks)
+    for r in mix:
+        alone = _requests([specs[r.rid]], seed=r.rid)[0]
+        Server(ncz=8).serve([alone], realtime=False)
+        err = rel_l2(r.out, alone.out)
+        print(f"request {r.rid}: packed vs alone {err:.2e}")
+        assert err < 1e-3, (r.rid, err)
+    fp32 = [(128, 90, 3, "float32"), (128, 90, 5, "float32")]
+    srv32 = Server(ncz=8, pack=True)
+    srv32.serve(_requests(fp32), realtime=False)
+    assert srv32.chunks == 2
 
 
 @pytest.mark.gpu

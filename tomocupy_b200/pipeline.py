@@ -210,12 +210,25 @@ class SinoPipeline:
         return torch.view_as_real(
             phase_weights(self.wfilter, self.t, self.center, sht, self.n)).contiguous()
 
-    def load_rows(self, data, dark0=None, flat0=None, z_lo=0, stream=None, flat1=None):
+    def load_rows(self, data, dark0=None, flat0=None, z_lo=0, stream=None, flat1=None,
+                  row0=0):
         """Fill the padded filter rows from a [nproj, nz, n] frame (or float) stack view.
         flat1: the second flat mean of flat_linear (the per-angle blend of
-        proc_functions.py:62-66), or None."""
+        proc_functions.py:62-66), or None.  row0: first filter row to fill
+        (several stacks packed into one chunk; plain fused pipelines only)."""
         nz = data.shape[1]
-        assert nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.ni
+        assert row0 + nz <= self.ncz and data.shape[0] == self.nproj and data.shape[2] == self.ni
+        if row0:
+            if (self.dezinger is not None or self.fw is not None or self.tensor_filter
+                    or not self.fused or self.pad360 is not None):
+                raise NotImplementedError("rows packed at an offset: plain fused pipelines only")
+            prep_rows(self.rows[row0:], data, None if dark0 is None else dark0[z_lo:z_lo + nz],
+                      None if flat0 is None else flat0[z_lo:z_lo + nz],
+                      None if flat1 is None else flat1[z_lo:z_lo + nz],
+                      darkflat=dark0 is not None, minus_log=self.minus_log,
+                      flat_linear=flat1 is not None, out_zstride=self.nproj * self.n,
+                      out_pstride=self.n, stream=stream)
+            return
         if self.pad360 is not None and not self.fused:
             raise NotImplementedError("double-FOV padding: fused fp32 filter only")
         if self.dezinger is not None:

@@ -9,17 +9,29 @@ and per-request dark/flat statistics, and runs a continuous-batching loop:
 * admission: a request that has arrived is admitted when its device bytes
   (frames, darks, flats, statistics) plus the resident geometries fit the HBM
   budget; its frames go to the device on a copy stream;
-* dispatch: the request's rows are cut into chunks of ``ncz`` slices; every
-  worker stream ("slot") that has finished its previous chunk takes the next
-  chunk of the oldest admitted request, so requests of different widths,
-  angle counts and slice counts run concurrently on the device and a request
-  that arrives while others run starts as soon as a slot frees up;
+* dispatch: every geometry stream with room takes the next ``ncz`` slices of
+  its oldest admitted request and, for mixed-precision requests, when that
+  request has fewer left, fills the rest of the chunk with the next slices
+  of the other admitted requests of the same geometry (their frames are
+  normalised into the chunk's rows side by side, then one filter, gridding
+  and inverse-FFT launch serves them all); requests of different widths,
+  angle counts and slice counts run concurrently on their own streams, and
+  a request that arrives while others run starts as soon as a stream has
+  room;
 * completion: each chunk's slices are copied back to the request's pinned
   host output on the slot's stream; a request is done when its last chunk's
   copy is.
 
-Chunks of a request depend only on that request's data (partial chunks are
-zero-filled), so its result is bit-identical alone and in any mix.
+Partial chunks are zero-filled.  fourierrec packs slice k of a chunk with
+slice k + ncz/2 as the real and imaginary parts of one complex sinogram
+(the reference's FourierRec does the same), and the polar samples are not
+symmetric about the origin (radii -n/2 .. n/2 - 1), so a slice's result
+carries ~1e-4 (relative) of its partner's: a slice paired with another
+request's slice differs from the same slice paired with zeros by that much.
+fp32 requests are therefore never packed with others (every chunk holds one
+request's slices: bit-identical alone and in any mix, and paired as
+GPURec pairs them); mixed-precision requests, whose budget is 1e-3, are
+(tested within 1e-3 of alone).
 
 The reference has no serving layer; the per-request computation is the same
 as GPURec.recon_all (src/tomocupy/rec.py:113-208).
@@ -97,10 +109,14 @@ class _Active:
     dark0: torch.Tensor
     flat0: torch.Tensor
     ready: torch.cuda.Event
-    chunks: list
+    nz: int
     nbytes: int
-    next: int = 0
+    z_next: int = 0        # first slice not yet dispatched
     events: list = field(default_factory=list)
+
+    @property
+    def pending(self) -> bool:
+        return self.z_next < self.nz
 
 
 class Server:
@@ -109,15 +125,20 @@ class Server:
     hbm_budget: bytes of device memory the server may hold (resident
     geometries + admitted requests).  ncz: slices per chunk.  depth: chunks
     queued ahead per geometry stream.  max_active: admitted requests at most
-    (None = memory-bound only; 1 gives one-at-a-time serving).
+    (None = memory-bound only; 1 gives one-at-a-time serving).  pack: fill
+    a chunk with the slices of several mixed-precision requests of one
+    geometry.
     """
 
-    def __init__(self, device="cuda", hbm_budget=150e9, ncz=8, depth=2, max_active=None):
+    def __init__(self, device="cuda", hbm_budget=150e9, ncz=8, depth=2, max_active=None,
+                 pack=True):
         self.device = torch.device(device)
         self.budget = float(hbm_budget)
         self.ncz = int(ncz)
         self.depth = int(depth)
         self.max_active = max_active
+        self.pack = bool(pack)
+        self.chunks = 0           # chunk launches (last serve call)
         self.copy_stream = torch.cuda.Stream(self.device)
         self.d2h = torch.cuda.Stream(self.device)
         self.geoms: OrderedDict = OrderedDict()
@@ -219,11 +240,10 @@ class Server:
             req.out = torch.empty((nz, n, n), pin_memory=True,
                                   dtype=torch.float16 if req.out_dtype == "float16"
                                   else torch.float32)
-        chunks = [(z0, min(self.ncz, nz - z0)) for z0 in range(0, nz, self.ncz)]
         self.req_bytes += need
         g.users += 1
         req.t_admit = now
-        return _Active(req, key, frames, dark0, flat0, ready, chunks, need)
+        return _Active(req, key, frames, dark0, flat0, ready, nz, need)
 
     def _to_device(self, t: torch.Tensor, stream) -> torch.Tensor:
         d = torch.empty(tuple(t.shape), dtype=t.dtype, device=self.device)
@@ -233,31 +253,49 @@ class Server:
             d.copy_(t, non_blocking=True)
         return d
 
-    def _dispatch(self, a: _Active) -> None:
+    def _dispatch(self, a: _Active, active: list) -> None:
+        """One chunk on a's geometry stream: a's next slices, then (packing)
+        the next slices of the other admitted requests of that geometry."""
         g = self.geoms[a.key]
-        z0, lz = a.chunks[a.next]
-        a.next += 1
+        segs, row = [], 0
+        packs = self.pack and a.req.precision == "mixed"
+        for b in [a] + ([x for x in active if x is not a and x.key == a.key] if packs
+                        else []):
+            if row == self.ncz:
+                break
+            if not b.pending:
+                continue
+            lz = min(self.ncz - row, b.nz - b.z_next)
+            segs.append((b, b.z_next, lz, row))
+            b.z_next += lz
+            row += lz
         s = g.stream
         i = g.flip
         g.flip ^= 1
         tmp = g.tmp[i]
-        s.wait_event(a.ready)
+        for b, _, _, _ in segs:
+            s.wait_event(b.ready)
         if g.tmp_free[i] is not None:
             s.wait_event(g.tmp_free[i])  # the previous copy-out of this buffer
         with torch.cuda.stream(s):
-            g.pipe.clear_rows(lz, s)
-            g.pipe.reconstruct(tmp, a.frames[:, z0:z0 + lz], a.dark0, a.flat0, z_lo=z0,
-                               stream=s)
+            g.pipe.clear_rows(row, s)
+            for b, z0, lz, r0 in segs:
+                g.pipe.load_rows(b.frames[:, z0:z0 + lz], b.dark0, b.flat0, z_lo=z0, stream=s,
+                                 row0=r0)
+            g.pipe.filter_and_backproject(tmp, stream=s)
             done = torch.cuda.Event()
             done.record(s)
+        self.chunks += 1
         g.d2h.wait_event(done)
         with torch.cuda.stream(g.d2h):
-            a.req.out[z0:z0 + lz].copy_(tmp[:lz], non_blocking=True)
+            for b, z0, lz, r0 in segs:
+                b.req.out[z0:z0 + lz].copy_(tmp[r0:r0 + lz], non_blocking=True)
             copied = torch.cuda.Event()
             copied.record(g.d2h)
         g.tmp_free[i] = copied
         g.inflight.append(done)
-        a.events.append(copied)
+        for b, _, _, _ in segs:
+            b.events.append(copied)
 
     def _finish(self, a: _Active, now: float) -> None:
         a.req.t_done = now
@@ -276,6 +314,7 @@ class Server:
         active: list[_Active] = []
         self.peak_active = 0
         self.peak_bytes = 0
+        self.chunks = 0
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
@@ -301,12 +340,12 @@ class Server:
             # fill their own streams, so everything admitted runs concurrently
             for a in active:
                 g = self.geoms[a.key]
-                while a.next < len(a.chunks) and len(g.inflight) < self.depth:
-                    self._dispatch(a)
+                while a.pending and len(g.inflight) < self.depth:
+                    self._dispatch(a, active)
                     progressed = True
             # completion
             for a in list(active):
-                if a.next == len(a.chunks) and all(e.query() for e in a.events):
+                if not a.pending and all(e.query() for e in a.events):
                     self._finish(a, time.perf_counter() - t0)
                     active.remove(a)
                     progressed = True
