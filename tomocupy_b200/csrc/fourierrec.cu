@@ -1142,15 +1142,23 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
           if (SPLIT)
             bulk_g2s(smem_u32(S + SW_WIMG), wlo + chunk * (SW_WIMG / 16), SW_WIMG, &full[s]);
         }
-        // lane k gathers the spectrum row of the chunk's sample k (zeros when absent)
+        // the chunk's spectrum rows (zeros for absent samples): lane k holds the
+        // row index of sample k; each step the warp copies LPR lanes' worth of
+        // 16-byte pieces per row, whole rows side by side, so every warp
+        // access reads full 128-byte lines
         const uint32_t vb = smem_u32(S + Cfg::WB);
-        const size_t so = (size_t)(row < 0 ? 0 : row) * NN;
-        const int nb = row < 0 ? 0 : 16;
+        constexpr int LPR = NN / 8;         // lanes per row (16-byte pieces of a row)
+        constexpr int RPS = 32 / LPR;       // rows per step
+        const int q = lane % LPR;
 #pragma unroll
-        for (int q = 0; q < NN / 8; q++) {
-          const uint32_t d = mn_sw128_offset(lane, q * 8);
-          cp_async16(vb + d, gh + so + q * 8, nb);
-          if (SPLIT) cp_async16(vb + Cfg::VB + d, gl + so + q * 8, nb);
+        for (int k0 = 0; k0 < SW_K; k0 += RPS) {
+          const int k = k0 + lane / LPR;
+          const int rk = __shfl_sync(0xffffffffu, row, k);
+          const size_t so = (size_t)(rk < 0 ? 0 : rk) * NN + (size_t)q * 8;
+          const int nb = rk < 0 ? 0 : 16;
+          const uint32_t d = mn_sw128_offset(k, q * 8);
+          cp_async16(vb + d, gh + so, nb);
+          if (SPLIT) cp_async16(vb + Cfg::VB + d, gl + so, nb);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
         // chunk g - LAG's gathers have landed: publish them to the async proxy
