@@ -36,11 +36,22 @@ def test_fw_matches_reference_fixture(cuda, i):
     assert err < 1e-5, (i, err)
 
 
+@pytest.fixture
+def cufft_damping(monkeypatch):
+    """fw operators built with the band damping on cuFFT (TCB_FW_DAMP)."""
+    from tomocupy_b200.processing import remove_stripe
+    monkeypatch.setenv("TCB_FW_DAMP", "cufft")
+    remove_stripe._operator.cache_clear()
+    yield
+    remove_stripe._operator.cache_clear()
+
+
 @pytest.mark.parametrize("i", range(5))
-def test_fw_filter_banks_reproduce_regression_fixture(cuda, i):
+def test_fw_filter_banks_reproduce_regression_fixture(cuda, cufft_damping, i):
     """Bit-for-bit against outputs recorded with the one-output-per-thread
-    filter-bank kernels (tests/golden/make_fw_b200.py): the register-blocked
-    kernels keep every output's multiply-then-add tap order."""
+    filter-bank kernels and the cuFFT band damping
+    (tests/golden/make_fw_b200.py): the register-blocked kernels keep every
+    output's multiply-then-add tap order."""
     import sys
     sys.path.insert(0, str(ROOT / "tests" / "golden"))
     from make_fw_b200 import CASES
@@ -54,6 +65,29 @@ def test_fw_filter_banks_reproduce_regression_fixture(cuda, i):
     assert got.shape == want.shape
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), \
         (i, float(np.abs(got - want).max()))
+
+
+@pytest.mark.parametrize("nproj,nz,n,level,sigma", [
+    (1500, 2, 2048, 7, 1.0),     # production sizes: bands of 859 (odd) ... rows
+    (720, 3, 1024, 5, 2.0),
+    (181, 2, 256, 3, 3.0),       # wide Gaussian: 32 modes, short bands on cuFFT
+])
+def test_fw_mode_damping_matches_cufft(cuda, monkeypatch, nproj, nz, n, level, sigma):
+    """The band damping by projection onto the Gaussian's few Fourier modes
+    equals the rfft -> multiply -> irfft damping (cuFFT) to float rounding."""
+    from tomocupy_b200.processing import remove_stripe
+    from tomocupy_b200 import synthetic
+    data, dark, flat, _, _ = synthetic.make_dataset(nproj, nz, n, seed=4, stripes=12)
+    x = (data.to(torch.float32) / 1000.0).to(cuda)
+    remove_stripe._operator.cache_clear()
+    modes = remove_stripe.remove_stripe_fw(x, sigma, "sym16", level)
+    monkeypatch.setenv("TCB_FW_DAMP", "cufft")
+    remove_stripe._operator.cache_clear()
+    fft = remove_stripe.remove_stripe_fw(x, sigma, "sym16", level)
+    remove_stripe._operator.cache_clear()
+    err = rel_l2(modes.cpu(), fft.cpu())
+    print(f"fw mode damping vs cuFFT {nproj}x{n} level {level} sigma {sigma}: {err:.2e}")
+    assert err < 1e-6, err
 
 
 def test_fw_removes_stripes(cuda):

@@ -18,11 +18,19 @@
 // stages reproduce its float32 arithmetic; the band FFTs use cuFFT.
 // B200 design: one kernel per filter pass over all slices of the chunk,
 // both output channels of a pass from one read of the input window, the
-// pyramid kept in HBM, the damped band transposed so the angle FFTs are
-// contiguous batched transforms, 1/N of the inverse FFT folded into the
-// damping factors.
+// pyramid kept in HBM.  The damping y = irfft(rfft(x) (1 - g)) along the
+// angles equals x - (1/H) sum_k g_k X_k e^{2 pi i k q / H}, and the
+// Gaussian g_k = exp(-v_k^2 / (2 sigma^2)) (v_k = k, or k + 1/2 for even H,
+// as the reference's ifftshifted grid gives) is below 1e-12 beyond a few
+// modes (k <= 7 for sigma = 1): the band is damped in place by projecting
+// each column onto those modes (sums of x cos, x sin) and subtracting the
+// low-pass, one read and one write of the band, no transposes, no FFTs.
+// Levels whose band is too short for the modes, or sigmas that need more
+// than 32 (TCB_FW_DAMP=cufft forces it), transpose the band and use cuFFT
+// R2C / C2R with 1/N folded into the damping factors.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -477,6 +485,69 @@ __global__ void damp_kernel(float2 *__restrict__ spec, const float *__restrict__
   spec[i] = make_float2(v.x * d, v.y * d);
 }
 
+// Damping by the low Fourier modes, in place on band [B][H][W] (slice
+// stride bstride): a block takes 32 adjacent columns (threadIdx.x) of one
+// slice, 8 row phases (threadIdx.y).  cs[k * H + q] = (cos, sin)(2 pi k q / H)
+// and gw[k] = g_k / H (k = 0) or 2 g_k / H (k >= 1, the mode and its mirror
+// H - k).  Pass 1 sums A_k = sum_q x_q cos, S_k = sum_q x_q sin per column;
+// pass 2 writes x_q - sum_k gw_k (A_k cos + S_k sin).
+constexpr int DM_R = 8;
+
+template <int V1>
+__global__ void __launch_bounds__(32 * DM_R)
+    damp_modes(float *__restrict__ band, long long bstride, int H, int W,
+               const float2 *__restrict__ cs, const float *__restrict__ gw) {
+  __shared__ float red[DM_R][V1][32];
+  const int w = blockIdx.x * 32 + threadIdx.x, r = threadIdx.y;
+  float *col = band + (long long)blockIdx.y * bstride + w;
+  const bool on = w < W;
+  float A[V1], S[V1];
+#pragma unroll
+  for (int k = 0; k < V1; k++) A[k] = S[k] = 0.f;
+  if (on)
+    for (int q = r; q < H; q += DM_R) {
+      const float x = col[(long long)q * W];
+#pragma unroll
+      for (int k = 0; k < V1; k++) {
+        const float2 t = __ldg(cs + k * H + q);
+        A[k] = fmaf(x, t.x, A[k]);
+        S[k] = fmaf(x, t.y, S[k]);
+      }
+    }
+  // the 8 row phases' partial sums, cosine then sine terms through one buffer
+#pragma unroll
+  for (int k = 0; k < V1; k++) red[r][k][threadIdx.x] = A[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < V1; k++) {
+    float a = 0.f;
+#pragma unroll
+    for (int j = 0; j < DM_R; j++) a += red[j][k][threadIdx.x];
+    A[k] = a * __ldg(gw + k);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < V1; k++) red[r][k][threadIdx.x] = S[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < V1; k++) {
+    float b = 0.f;
+#pragma unroll
+    for (int j = 0; j < DM_R; j++) b += red[j][k][threadIdx.x];
+    S[k] = b * __ldg(gw + k);
+  }
+  if (!on) return;
+  for (int q = r; q < H; q += DM_R) {
+    float lp = 0.f;
+#pragma unroll
+    for (int k = 0; k < V1; k++) {
+      const float2 t = __ldg(cs + k * H + q);
+      lp = fmaf(A[k], t.x, fmaf(S[k], t.y, lp));
+    }
+    col[(long long)q * W] -= lp;
+  }
+}
+
 }  // namespace sw
 }  // namespace tcb
 
@@ -489,6 +560,9 @@ struct tcb_stripe_fw {
   std::vector<float *> Y; // per level [nz][4][H[k+1]][W[k+1]]
   std::vector<float *> damp;  // per level damping factors (with 1/H)
   std::vector<cufftHandle> r2c, c2r;
+  std::vector<int> modes;     // per level: modes of the direct damping (0 = cuFFT)
+  std::vector<float2 *> mcs;  // per level [modes][H] (cos, sin)(2 pi k q / H)
+  std::vector<float *> mgw;   // per level [modes] weights
   float *tmp = nullptr;    // [nz][2][H][W] scratch
   float *bt = nullptr;     // transposed band scratch
   float2 *spec = nullptr;  // band spectrum scratch
@@ -542,6 +616,11 @@ static void fw_release(tcb_stripe_fw *h) {
   for (auto p : h->damp) cudaFree(p);
   for (auto p : h->r2c) if (p) cufftDestroy(p);
   for (auto p : h->c2r) if (p) cufftDestroy(p);
+  for (auto p : h->mcs) cudaFree(p);
+  for (auto p : h->mgw) cudaFree(p);
+  h->mcs.clear();
+  h->mgw.clear();
+  h->modes.clear();
   h->Y.clear();
   h->damp.clear();
   h->r2c.clear();
@@ -635,6 +714,50 @@ extern "C" int tcb_stripe_fw_create(tcb_stripe_fw **out, size_t nproj, size_t nz
       return fail(TCB_ERR_CUFFT, "cufftPlanMany failed");
     h->r2c.push_back(p1);
     h->c2r.push_back(p2);
+    // the direct damping: modes k with g_k above 1e-12, padded to 8, 16 or 32
+    // (the extra ones carry their exact, negligible weights); the mode and its
+    // mirror H - k must be distinct
+    int need = 0;
+    while (need < Ho) {
+      const double v = (Ho % 2) ? (double)need : need + 0.5;
+      if (std::exp(-v * v / (2.0 * (double)sigma * sigma)) < 1e-12) break;
+      need++;
+    }
+    int V1 = need <= 8 ? 8 : need <= 16 ? 16 : need <= 32 ? 32 : 0;
+    if (2 * V1 >= Ho || std::getenv("TCB_FW_DAMP") != nullptr) V1 = 0;
+    float2 *mc = nullptr;
+    float *mg = nullptr;
+    if (V1) {
+      std::vector<float2> tab((size_t)V1 * Ho);
+      std::vector<float> wt(V1);
+      for (int k = 0; k < V1; k++) {
+        for (int q = 0; q < Ho; q++) {
+          // 2 pi k q / H reduced exactly: (k q mod H) / H
+          const double a = 2.0 * M_PI * (double)(((long long)k * q) % Ho) / (double)Ho;
+          tab[(size_t)k * Ho + q] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        const double v = (Ho % 2) ? (double)k : k + 0.5;
+        const double g = std::exp(-v * v / (2.0 * (double)sigma * sigma)) / Ho;
+        // bin 0 is its own mirror; bin k >= 1 comes with bin H - k, whose
+        // factor the half-spectrum inverse takes from bin k
+        wt[k] = (float)(k == 0 ? g : 2.0 * g);
+      }
+      if (cudaMalloc(&mc, tab.size() * sizeof(float2)) != cudaSuccess ||
+          cudaMalloc(&mg, V1 * sizeof(float)) != cudaSuccess) {
+        cudaFree(mc);
+        return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+      }
+      if (cudaMemcpy(mc, tab.data(), tab.size() * sizeof(float2), cudaMemcpyHostToDevice) !=
+              cudaSuccess ||
+          cudaMemcpy(mg, wt.data(), V1 * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(mc);
+        cudaFree(mg);
+        return fail(TCB_ERR_CUDA, "cudaMemcpy failed");
+      }
+    }
+    h->modes.push_back(V1);
+    h->mcs.push_back(mc);
+    h->mgw.push_back(mg);
     maxband = std::max(maxband, (size_t)nz * Ho * Wo);
     maxtmp = std::max(maxtmp, (size_t)nz * 2 * h->H[k] * Wo);          // afb rows output
     maxtmp = std::max(maxtmp, (size_t)nz * 2 * (2 * Ho - L + 2) * Wo);  // sfb cols output
@@ -704,6 +827,17 @@ extern "C" int tcb_stripe_fw_apply_sino(tcb_stripe_fw *h, float *sino, size_t ss
     StageTimer std_("fw_damp", s);
     // damp band 1 (index 2 of the level: high-pass along the detector, low-pass along angles)
     float *band = h->Y[k] + 2LL * Ho * Wo;
+    if (h->modes[k]) {
+      const dim3 gd(ceil_div(Wo, 32), B), bd(32, DM_R);
+      switch (h->modes[k]) {
+        case 8: damp_modes<8><<<gd, bd, 0, s>>>(band, 4LL * Ho * Wo, Ho, Wo, h->mcs[k], h->mgw[k]); break;
+        case 16: damp_modes<16><<<gd, bd, 0, s>>>(band, 4LL * Ho * Wo, Ho, Wo, h->mcs[k], h->mgw[k]); break;
+        default: damp_modes<32><<<gd, bd, 0, s>>>(band, 4LL * Ho * Wo, Ho, Wo, h->mcs[k], h->mgw[k]);
+      }
+      TCB_LAUNCH_CHECK();
+      count_launch();
+      continue;
+    }
     dim3 tb(32, 8);
     dim3 g1(ceil_div(Wo, 32), ceil_div(Ho, 32), B);
     transpose_bands<<<g1, tb, 0, s>>>(band, 4LL * Ho * Wo, h->bt, (long long)Ho * Wo, Ho, Wo);
