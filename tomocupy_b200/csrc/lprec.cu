@@ -16,13 +16,25 @@
 //    with coalesced row loads;
 //  * the 2/(nrho*ntheta) normalisation is folded into an internal copy of fZ
 //    (one pass fewer per span);
-//  * interpolation kernels use flat 1D grids over the point lists.
+//  * interpolation kernels use flat 1D grids over the point lists;
+//  * for power-of-two nrho and ntheta in [256, 8192] the FFT convolution runs
+//    on the library's own FFT: two log-polar slices packed as one complex
+//    image (the kernel's Hermitian extension H maps each real slice to a real
+//    result), rows forward, then per column forward, times H, inverse, then
+//    rows inverse with the real and imaginary parts written back to the two
+//    slices.  cuFFT's C2R takes the zero-frequency column of the product
+//    through its Hermitian part, so H's column 0 is (fZ(k, 0) +
+//    conj(fZ(-k, 0))) / 2.
 // Texture objects and layered CUDA arrays are used exactly as the reference
 // uses them, because its parity depends on the texture unit's 8-bit
 // fixed-point filtering weights.
 #include <cuda_fp16.h>
 
+#include <cstdlib>
+#include <vector>
+
 #include "common.cuh"
+#include "fft_pow2.cuh"
 
 struct tcb_lprec {
   int nproj, nz, n, ntheta, nrho, precision;
@@ -41,6 +53,12 @@ struct tcb_lprec {
   cudaArray_t ga = nullptr, fla = nullptr;
   cudaTextureObject_t texg = 0, texfl = 0;
   cufftHandle fwd = 0, inv = 0;
+  // own-FFT convolution
+  bool own = false;
+  float2 *t1 = nullptr;   // [pairs][ntheta/8][nrho][8] row spectra
+  float2 *t2 = nullptr;   // [pairs][nrho][ntheta] filtered, rows not yet inverted
+  float2 *h0 = nullptr;   // [nrho] Hermitian part of column 0 of fzs
+  float2 *twr = nullptr, *twt = nullptr;  // twiddles of lengths nrho, ntheta
 };
 
 namespace tcb {
@@ -222,6 +240,163 @@ __global__ void f2h(__half *__restrict__ d, const float *__restrict__ s, size_t 
   if (i < total) d[i] = __float2half_rn(s[i]);
 }
 
+// ---- own-FFT convolution ------------------------------------------------------
+constexpr int LC_GW = 8;
+
+// column 0 of the filter, Hermitian part: h0[k] = (f[k][0] + conj(f[-k][0])) / 2
+__global__ void lc_h0(float2 *__restrict__ h0, const float2 *__restrict__ fzs, int nrho, int nc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nrho) return;
+  const float2 a = fzs[(size_t)k * nc], b = fzs[(size_t)((nrho - k) % nrho) * nc];
+  h0[k] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+}
+
+// Pass 1: row r of the pair (2q, 2q + 1): forward FFT along theta of a + i b.
+template <int N>
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
+    lc_rows_fwd(const float *__restrict__ fl, float2 *__restrict__ t1,
+                const float2 *__restrict__ tw, int nb, int nrho) {
+  extern __shared__ float2 fsm[];
+  const int r = blockIdx.x, q = blockIdx.y;
+  const size_t img = (size_t)nrho * N;
+  const float *a = fl + (size_t)(2 * q) * img + (size_t)r * N;
+  const float *b = 2 * q + 1 < nb ? a + img : nullptr;
+  float2 *dst = t1 + (size_t)q * nrho * N + (size_t)r * LC_GW;
+  auto in = [a, b](int e) { return make_float2(__ldg(a + e), b ? -__ldg(b + e) : 0.f); };
+  auto out = [dst, nrho](int o, float2 v) {
+    dst[(size_t)(o / LC_GW) * nrho * LC_GW + o % LC_GW] = make_float2(v.x, -v.y);
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
+}
+
+// Pass 2: cpc adjacent columns k2 per block: forward FFT along rho, times
+// H(k1, k2) (column 0: h0; k2 <= ntheta/2: fzs; beyond: conj(fzs(-k1, -k2))),
+// inverse FFT along rho, to t2[q][k1][k2].
+template <int N>
+__global__ void __launch_bounds__(1024)
+    lc_cols(const float2 *__restrict__ t1, float2 *__restrict__ t2,
+            const float2 *__restrict__ fzs, const float2 *__restrict__ h0,
+            const float2 *__restrict__ tw, int ntheta, int cpc) {
+  extern __shared__ float2 fsm[];
+  constexpr int SSTR = fftk::Plan<N>::PADDED + 4;
+  const int c = threadIdx.x % cpc, tid = threadIdx.x / cpc;
+  const int ncb = ntheta / cpc;
+  const int q = blockIdx.x / ncb, j = (blockIdx.x % ncb) * cpc + c;
+  const int nc = ntheta / 2 + 1;
+  const float2 *src = t1 + (size_t)q * N * ntheta + (size_t)(j / LC_GW) * N * LC_GW + j % LC_GW;
+  float2 *sm = fsm + c * SSTR;
+  auto in1 = [src](int e) {
+    const float2 v = __ldg(src + (size_t)e * LC_GW);
+    return make_float2(v.x, -v.y);
+  };
+  auto out1 = [sm](int o, float2 v) { sm[fftk::pad16(o)] = make_float2(v.x, -v.y); };
+  fftk::ifft<N, true>(sm, tid, tw, in1, out1);
+  __syncthreads();
+  {
+    const bool neg = j >= nc;
+    for (int k = tid; k < N; k += N / 16) {
+      float2 hv;
+      if (j == 0) {
+        hv = __ldg(h0 + k);
+      } else if (!neg) {
+        hv = __ldg(fzs + (size_t)k * nc + j);
+      } else {
+        const float2 t = __ldg(fzs + (size_t)((N - k) & (N - 1)) * nc + (ntheta - j));
+        hv = make_float2(t.x, -t.y);
+      }
+      float2 &x = sm[fftk::pad16(k)];
+      x = make_float2(x.x * hv.x - x.y * hv.y, x.x * hv.y + x.y * hv.x);
+    }
+  }
+  __syncthreads();
+  float2 *dst = t2 + (size_t)q * N * ntheta + j;
+  auto in2 = [sm](int e) { return sm[fftk::pad16(e)]; };
+  auto out2 = [dst, ntheta](int o, float2 v) { dst[(size_t)o * ntheta] = v; };
+  const float2 *tw2;  // the second transform reloads its twiddles
+  asm volatile("mov.b64 %0, %1;" : "=l"(tw2) : "l"(tw));
+  fftk::ifft<N>(sm, tid, tw2, in2, out2);
+}
+
+// Pass 3: row r: inverse FFT along theta, real part to slice 2q, imaginary
+// part to slice 2q + 1.
+template <int N>
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
+    lc_rows_inv(const float2 *__restrict__ t2, float *__restrict__ fl,
+                const float2 *__restrict__ tw, int nb, int nrho) {
+  extern __shared__ float2 fsm[];
+  const int r = blockIdx.x, q = blockIdx.y;
+  const size_t img = (size_t)nrho * N;
+  const float2 *src = t2 + ((size_t)q * nrho + r) * N;
+  float *a = fl + (size_t)(2 * q) * img + (size_t)r * N;
+  float *b = 2 * q + 1 < nb ? a + img : nullptr;
+  auto in = [src](int e) { return __ldg(src + e); };
+  auto out = [a, b](int o, float2 v) {
+    a[o] = v.x;
+    if (b) b[o] = v.y;
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
+}
+
+inline int lc_cpc(int N) { return std::min(16384 / N, 16); }
+inline size_t lc_cols_smem(int N) { return (size_t)lc_cpc(N) * (N + N / 16 + 4) * sizeof(float2); }
+inline size_t lc_rows_smem(int N) { return (size_t)(N + N / 16) * sizeof(float2); }
+
+#define LC_DISPATCH(n, F)      \
+  switch (n) {                 \
+    case 256: F(256); break;   \
+    case 512: F(512); break;   \
+    case 1024: F(1024); break; \
+    case 2048: F(2048); break; \
+    case 4096: F(4096); break; \
+    default: F(8192); break;   \
+  }
+
+cudaError_t lc_attrs(int nrho, int ntheta) {
+  cudaError_t e = cudaSuccess;
+#define LC_ROWS_ATTR(N)                                                                 \
+  e = cudaFuncSetAttribute(lc_rows_fwd<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                           (int)lc_rows_smem(N));                                       \
+  if (e == cudaSuccess)                                                                 \
+    e = cudaFuncSetAttribute(lc_rows_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             (int)lc_rows_smem(N));
+#define LC_COLS_ATTR(N)                                                                 \
+  e = cudaFuncSetAttribute(lc_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                           (int)lc_cols_smem(N));
+  LC_DISPATCH(ntheta, LC_ROWS_ATTR)
+  if (e != cudaSuccess) return e;
+  LC_DISPATCH(nrho, LC_COLS_ATTR)
+#undef LC_ROWS_ATTR
+#undef LC_COLS_ATTR
+  return e;
+}
+
+int lc_apply(tcb_lprec *h, cudaStream_t s) {
+  const int nrho = h->nrho, ntheta = h->ntheta, nb = h->nz;
+  const unsigned pairs = (unsigned)((nb + 1) / 2);
+#define LC_FWD(N)                                                                      \
+  lc_rows_fwd<N><<<dim3((unsigned)nrho, pairs), N / 16, lc_rows_smem(N), s>>>(h->fl, h->t1, \
+                                                                            h->twt, nb, nrho)
+  LC_DISPATCH(ntheta, LC_FWD)
+#undef LC_FWD
+  TCB_LAUNCH_CHECK();
+#define LC_COLS(N)                                                                     \
+  lc_cols<N><<<(unsigned)(ntheta / lc_cpc(N)) * pairs, lc_cpc(N) * (N / 16), lc_cols_smem(N), \
+               s>>>(h->t1, h->t2, h->fzs, h->h0, h->twr, ntheta, lc_cpc(N))
+  LC_DISPATCH(nrho, LC_COLS)
+#undef LC_COLS
+  TCB_LAUNCH_CHECK();
+#define LC_INV(N)                                                                      \
+  lc_rows_inv<N><<<dim3((unsigned)nrho, pairs), N / 16, lc_rows_smem(N), s>>>(h->t2, h->fl, \
+                                                                            h->twt, nb, nrho)
+  LC_DISPATCH(ntheta, LC_INV)
+#undef LC_INV
+  TCB_LAUNCH_CHECK();
+  count_launch(3);
+  return TCB_OK;
+}
+
+bool lc_pow2(int n) { return n >= 256 && n <= 8192 && (n & (n - 1)) == 0; }
+
 int copy_to_array(cudaArray_t arr, const float *src, int w, int h, int d, cudaStream_t s) {
   cudaMemcpy3DParms p = {};
   p.srcPtr = make_cudaPitchedPtr((void *)src, w * sizeof(float), w, h);
@@ -244,6 +419,12 @@ void release(tcb_lprec *h) {
   cudaFree(h->flc);
   cudaFree(h->g32);
   cudaFree(h->f32);
+  cudaFree(h->t1);
+  cudaFree(h->t2);
+  cudaFree(h->h0);
+  cudaFree(h->twr);
+  cudaFree(h->twt);
+  h->t1 = h->t2 = h->h0 = h->twr = h->twt = nullptr;
   h->fwd = h->inv = 0;
   h->texg = h->texfl = 0;
   h->ga = h->fla = nullptr;
@@ -319,6 +500,23 @@ extern "C" int tcb_lprec_create(tcb_lprec **out, size_t nproj, size_t nz, size_t
       cufftPlanMany(&h->inv, 2, dims, cemb, 1, (int)(nrho * nc), dims, 1,
                     (int)(nrho * ntheta), CUFFT_C2R, (int)nz) != CUFFT_SUCCESS)
     return fail(TCB_ERR_CUFFT, "cufftPlanMany failed");
+  h->own = lc_pow2((int)nrho) && lc_pow2((int)ntheta) && std::getenv("TCB_LPREC_FFT") == nullptr;
+  if (h->own) {
+    const size_t pairs = (nz + 1) / 2;
+    const std::vector<float2> tr = fftk::twiddle_table((int)nrho), tt = fftk::twiddle_table((int)ntheta);
+    if (cudaMalloc(&h->t1, pairs * nrho * ntheta * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&h->t2, pairs * nrho * ntheta * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&h->h0, nrho * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&h->twr, tr.size() * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&h->twt, tt.size() * sizeof(float2)) != cudaSuccess)
+      return fail(TCB_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    if (cudaMemcpy(h->twr, tr.data(), tr.size() * sizeof(float2), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(h->twt, tt.data(), tt.size() * sizeof(float2), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        lc_attrs((int)nrho, (int)ntheta) != cudaSuccess)
+      return fail(TCB_ERR_CUDA, "own-FFT setup failed");
+  }
   *out = h;
   return TCB_OK;
 }
@@ -351,6 +549,10 @@ extern "C" int tcb_lprec_setgrids(tcb_lprec *h, const void *fz, const float *lp2
   scale_fz<<<ceil_div(total, 256), 256>>>(h->fzs, h->fz, 2 / (float)(h->nrho * h->ntheta),
                                           total);
   TCB_LAUNCH_CHECK();
+  if (h->own) {
+    lc_h0<<<ceil_div(h->nrho, 256), 256>>>(h->h0, h->fzs, h->nrho, h->ntheta / 2 + 1);
+    TCB_LAUNCH_CHECK();
+  }
   TCB_CUDA(cudaDeviceSynchronize());
   return TCB_OK;
 }
@@ -407,7 +609,11 @@ extern "C" int tcb_lprec_backprojection(tcb_lprec *h, void *f, void *g, void *st
         count_launch();
       }
     }
-    {
+    if (h->own) {
+      StageTimer st("lprec_fft", s);
+      const int rc = lc_apply(h, s);
+      if (rc != TCB_OK) return rc;
+    } else {
       StageTimer st("lprec_fft", s);
       TCB_CUFFT(cufftExecR2C(h->fwd, h->fl, (cufftComplex *)h->flc));
       mul_fz<<<ceil_div(nc * nz, 256), 256, 0, s>>>(h->flc, h->fzs, nc, nc * nz);

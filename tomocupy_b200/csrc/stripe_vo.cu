@@ -440,30 +440,54 @@ extern "C" int tcb_stripe_vo_apply(tcb_stripe_vo *h, float *tomo, size_t pstride
   };
   StageTimer t("stripe_vo", s);
   // 1. dead stripes
-  vo_dead_diff<<<cgrid, 128, 0, s>>>(tomo, pstride, zstride, np, nz, ni, h->l1);
-  median(h->l1, h->l2, 1, h->la);
-  vo_detect<<<nz, 256, dsm, s>>>(h->l1, h->l2, ni, n2, h->snr, 1, h->fact, h->mask, h->nbr);
-  vo_dead_interp<<<pgrid, 128, 0, s>>>(tomo, pstride, zstride, np, ni, h->mask, h->nbr);
-  TCB_LAUNCH_CHECK();
+  {
+    StageTimer st("stripe_vo_dead", s);
+    vo_dead_diff<<<cgrid, 128, 0, s>>>(tomo, pstride, zstride, np, nz, ni, h->l1);
+    median(h->l1, h->l2, 1, h->la);
+    vo_detect<<<nz, 256, dsm, s>>>(h->l1, h->l2, ni, n2, h->snr, 1, h->fact, h->mask, h->nbr);
+    vo_dead_interp<<<pgrid, 128, 0, s>>>(tomo, pstride, zstride, np, ni, h->mask, h->nbr);
+    TCB_LAUNCH_CHECK();
+  }
   // 2. large stripes
-  vo_sort_cols<<<dim3(ni, nz), 512, (size_t)p2 * 8, s>>>(tomo, pstride, zstride, np, ni, p2,
-                                                        h->srt, h->ids);
-  median(h->srt, h->smooth, np, h->la);
-  vo_rank_means<<<ceil_div(h->nz * h->ni * 32, 256), 256, 0, s>>>(h->srt, h->smooth, np,
-                                                                  nz * ni, nd, h->l1, h->l2);
-  vo_detect<<<nz, 256, dsm, s>>>(h->l1, h->l2, ni, n2, h->snr, 0, h->fact, h->mask, h->nbr);
-  vo_divide<<<pgrid, 128, 0, s>>>(tomo, pstride, zstride, np, nz, ni, h->fact);
-  vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(tomo, pstride, zstride, np,
-                                                                  ni, h->smooth, h->ids,
-                                                                  h->mask);
+  {
+    StageTimer st("stripe_vo_sort", s);
+    vo_sort_cols<<<dim3(ni, nz), 512, (size_t)p2 * 8, s>>>(tomo, pstride, zstride, np, ni, p2,
+                                                          h->srt, h->ids);
+  }
+  {
+    StageTimer st("stripe_vo_median", s);
+    median(h->srt, h->smooth, np, h->la);
+  }
+  {
+    StageTimer st("stripe_vo_large", s);
+    vo_rank_means<<<ceil_div(h->nz * h->ni * 32, 256), 256, 0, s>>>(h->srt, h->smooth, np,
+                                                                    nz * ni, nd, h->l1, h->l2);
+    vo_detect<<<nz, 256, dsm, s>>>(h->l1, h->l2, ni, n2, h->snr, 0, h->fact, h->mask, h->nbr);
+    vo_divide<<<pgrid, 128, 0, s>>>(tomo, pstride, zstride, np, nz, ni, h->fact);
+  }
+  {
+    StageTimer st("stripe_vo_unsort", s);
+    vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(tomo, pstride, zstride, np,
+                                                                    ni, h->smooth, h->ids,
+                                                                    h->mask);
+  }
   TCB_LAUNCH_CHECK();
   // 3. small and medium stripes
-  vo_sort_cols<<<dim3(ni, nz), 512, (size_t)p2 * 8, s>>>(tomo, pstride, zstride, np, ni, p2,
-                                                        h->srt, h->ids);
-  median(h->srt, h->smooth, np, h->sm);
-  vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(tomo, pstride, zstride, np,
-                                                                  ni, h->smooth, h->ids,
-                                                                  nullptr);
+  {
+    StageTimer st("stripe_vo_sort", s);
+    vo_sort_cols<<<dim3(ni, nz), 512, (size_t)p2 * 8, s>>>(tomo, pstride, zstride, np, ni, p2,
+                                                          h->srt, h->ids);
+  }
+  {
+    StageTimer st("stripe_vo_median", s);
+    median(h->srt, h->smooth, np, h->sm);
+  }
+  {
+    StageTimer st("stripe_vo_unsort", s);
+    vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(tomo, pstride, zstride, np,
+                                                                    ni, h->smooth, h->ids,
+                                                                    nullptr);
+  }
   TCB_LAUNCH_CHECK();
   count_launch(13);
   return TCB_OK;
