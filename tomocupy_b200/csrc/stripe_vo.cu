@@ -23,6 +23,7 @@
 // per-row statistics (stripe detection) are one CTA per row.  Float32
 // reductions add in another order than the reference's, so results agree
 // to float rounding; the sorts, medians and interpolation weights are exact.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -31,6 +32,7 @@ struct tcb_stripe_vo {
   size_t nproj, nz, ni;
   float snr;
   int la, sm;
+  float *tt = nullptr;       // [nz][ni][nproj] the chunk with contiguous columns
   float *srt = nullptr;      // [nz][ni][nproj] values sorted along the angles
   int *ids = nullptr;        // [nz][ni][nproj] angle of each sorted value
   float *smooth = nullptr;   // [nz][ni][nproj]
@@ -61,43 +63,94 @@ __device__ __forceinline__ uint32_t fkey(float f) {
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
+__device__ __forceinline__ float fdecode(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+// Compare-exchange of key a (index i) with its partner b: the lower index
+// keeps the smaller key in an ascending run (i & k == 0), the larger in a
+// descending one.
+__device__ __forceinline__ unsigned long long bitonic_keep(unsigned long long a,
+                                                           unsigned long long b, int i, int j,
+                                                           int k) {
+  const bool up = (i & k) == 0, lower = (i & j) == 0;
+  return (lower == up) ? (a < b ? a : b) : (a < b ? b : a);
+}
+
+// The exchanges at distance J < E among a thread's own keys.
+template <int E, int J>
+__device__ __forceinline__ void in_thread(unsigned long long (&v)[E], int t, int k) {
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if ((e & J) == 0) {
+      const int i = t * E + e;
+      const unsigned long long a = v[e], b = v[e | J];
+      const bool up = (i & k) == 0;
+      v[e] = (a < b) == up ? a : b;
+      v[e | J] = (a < b) == up ? b : a;
+    }
+  }
+}
+
 // One CTA per column (z, x): the nproj values sorted ascending, ties in
-// angle order; srt/ids [(z * ni + x) * nproj + r].
+// angle order; srt/ids [(z * ni + x) * nproj + r].  Bitonic sort of p2 =
+// E * blockDim 64-bit keys (order bits of the value, angle): thread t holds
+// keys t*E .. t*E + E - 1 in registers; exchanges at distance j < E stay in
+// the thread, E <= j < 32 E go through warp shuffles, only the longer ones
+// through shared memory.  The sorted values are decoded from the keys.
+template <int E>
 __global__ void vo_sort_cols(const float *__restrict__ tomo, size_t pstride, size_t zstride,
-                             int nproj, int ni, int p2, float *__restrict__ srt,
+                             size_t xstride, int nproj, int ni, int p2, float *__restrict__ srt,
                              int *__restrict__ ids) {
   extern __shared__ unsigned long long key[];
-  const int x = blockIdx.x, z = blockIdx.y;
-  const float *col = tomo + (size_t)z * zstride + x;
-  for (int r = threadIdx.x; r < p2; r += blockDim.x) {
+  const int x = blockIdx.x, z = blockIdx.y, t = threadIdx.x;
+  const float *col = tomo + (size_t)z * zstride + (size_t)x * xstride;
+  unsigned long long v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int r = t * E + e;
     const uint32_t k = r < nproj ? fkey(col[(size_t)r * pstride]) : 0xFFFFFFFFu;
-    key[r] = ((unsigned long long)k << 32) | (unsigned)r;
+    v[e] = ((unsigned long long)k << 32) | (unsigned)r;
   }
-  __syncthreads();
   for (int k = 2; k <= p2; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < p2; i += blockDim.x) {
-        const int l = i ^ j;
-        if (l > i) {
-          const unsigned long long a = key[i], b = key[l];
-          const bool up = (i & k) == 0;
-          if ((a > b) == up) {
-            key[i] = b;
-            key[l] = a;
-          }
+      if (j < E) {
+        if (j == 1) in_thread<E, 1>(v, t, k);
+        else if (j == 2) in_thread<E, 2>(v, t, k);
+        else if (E > 4) in_thread<E, (E > 4 ? 4 : 1)>(v, t, k);
+      } else if (j < 32 * E) {
+        const int lm = j / E;  // partner lane
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const unsigned long long b = __shfl_xor_sync(0xffffffffu, v[e], lm);
+          v[e] = bitonic_keep(v[e], b, t * E + e, j, k);
         }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; e++) key[t * E + e] = v[e];
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const int i = t * E + e;
+          v[e] = bitonic_keep(v[e], key[i ^ j], i, j, k);
+        }
+        __syncthreads();
       }
-      __syncthreads();
     }
   float *so = srt + ((size_t)z * ni + x) * nproj;
   int *io = ids + ((size_t)z * ni + x) * nproj;
-  for (int r = threadIdx.x; r < nproj; r += blockDim.x) {
-    const unsigned long long kk = key[r];
-    const int p = (int)(kk & 0xFFFFFFFFu);
-    so[r] = col[(size_t)p * pstride];
-    io[r] = p;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int r = t * E + e;
+    if (r < nproj) {
+      so[r] = fdecode((uint32_t)(v[e] >> 32));
+      io[r] = (int)(v[e] & 0xFFFFFFFFu);
+    }
   }
 }
+
+// keys per thread and threads for a column of p2 (power of two) keys
+inline int sort_e(int p2) { return p2 <= 4096 ? 4 : 8; }
 
 // Median over w (odd) columns, reflect mode, of in[(z * ni + x) * R + r] for
 // every (z, x, r): each thread slides a sorted window along a run of VO_RUN
@@ -319,28 +372,61 @@ __global__ void vo_dead_interp(float *__restrict__ tomo, size_t pstride, size_t 
   }
 }
 
-__global__ void vo_divide(float *__restrict__ tomo, size_t pstride, size_t zstride, int nproj,
-                          int nz, int ni, const float *__restrict__ fact) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
-  if (x >= ni) return;
-  const float f = fact[(size_t)z * ni + x];
-  float *col = tomo + (size_t)z * zstride + x;
-  for (int p = blockIdx.z; p < nproj; p += gridDim.z) col[(size_t)p * pstride] /= f;
-}
-
-// tomo[ids[r]][z][x] = vals[z][x][r] for the columns whose mask is set (or all).
-__global__ void vo_unsort(float *__restrict__ tomo, size_t pstride, size_t zstride, int nproj,
-                          int ni, const float *__restrict__ vals, const int *__restrict__ ids,
+// tt[z][x][ids[r]] = vals[z][x][r] for the columns whose mask is set (or all).
+__global__ void vo_unsort(float *__restrict__ tt, int nproj, int ni,
+                          const float *__restrict__ vals, const int *__restrict__ ids,
                           const float *__restrict__ mask) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int x = blockIdx.y, z = blockIdx.z;
   if (r >= nproj) return;
   if (mask && mask[(size_t)z * ni + x] <= 0.f) return;
-  const size_t c = ((size_t)z * ni + x) * nproj + r;
-  tomo[(size_t)ids[c] * pstride + (size_t)z * zstride + x] = vals[c];
+  const size_t c = ((size_t)z * ni + x) * nproj;
+  tt[c + ids[c + r]] = vals[c + r];
+}
+
+// tt[z][x][p] /= fact[z][x]
+__global__ void vo_divide_t(float *__restrict__ tt, int nproj, size_t total,
+                            const float *__restrict__ fact) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  tt[i] /= fact[i / nproj];
+}
+
+// [z][p][x] (strides pstride, zstride; x contiguous) <-> [z][x][p], 32 x 32
+// shared-memory tiles; to_t: towards the column-contiguous layout.
+__global__ void vo_transpose(float *__restrict__ tomo, size_t pstride, size_t zstride,
+                             float *__restrict__ tt, int nproj, int ni, int to_t) {
+  __shared__ float tile[32][33];
+  const int z = blockIdx.z;
+  const int p0 = blockIdx.y * 32, x0 = blockIdx.x * 32;
+  float *row = tomo + (size_t)z * zstride;
+  float *colt = tt + (size_t)z * ni * nproj;
+  if (to_t) {
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+      const int p = p0 + k, x = x0 + threadIdx.x;
+      if (p < nproj && x < ni) tile[k][threadIdx.x] = row[(size_t)p * pstride + x];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+      const int x = x0 + k, p = p0 + threadIdx.x;
+      if (p < nproj && x < ni) colt[(size_t)x * nproj + p] = tile[threadIdx.x][k];
+    }
+  } else {
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+      const int x = x0 + k, p = p0 + threadIdx.x;
+      if (p < nproj && x < ni) tile[threadIdx.x][k] = colt[(size_t)x * nproj + p];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+      const int p = p0 + k, x = x0 + threadIdx.x;
+      if (p < nproj && x < ni) row[(size_t)p * pstride + x] = tile[k][threadIdx.x];
+    }
+  }
 }
 
 void vo_release(tcb_stripe_vo *h) {
+  cudaFree(h->tt);
+  h->tt = nullptr;
   cudaFree(h->srt);
   cudaFree(h->ids);
   cudaFree(h->smooth);
@@ -387,7 +473,8 @@ extern "C" int tcb_stripe_vo_create(tcb_stripe_vo **out, size_t nproj, size_t nz
   h->la = la_size;
   h->sm = sm_size;
   const size_t cols = nz * ni, vals = cols * nproj;
-  if (cudaMalloc(&h->srt, vals * sizeof(float)) != cudaSuccess ||
+  if (cudaMalloc(&h->tt, vals * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->srt, vals * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&h->ids, vals * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&h->smooth, vals * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&h->l1, cols * sizeof(float)) != cudaSuccess ||
@@ -401,9 +488,11 @@ extern "C" int tcb_stripe_vo_create(tcb_stripe_vo **out, size_t nproj, size_t nz
     set_error("tcb_stripe_vo_create: out of device memory");
     return TCB_ERR_OUT_OF_MEMORY;
   }
-  const int sort_smem = pow2_at_least((int)nproj) * 8;
+  const int sort_smem = std::max(pow2_at_least((int)nproj), 128) * 8;
   const int med_smem = VO_MAXW * VO_MED_T * 4;
-  if (cudaFuncSetAttribute(vo_sort_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(vo_sort_cols<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           sort_smem) != cudaSuccess ||
+      cudaFuncSetAttribute(vo_sort_cols<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            sort_smem) != cudaSuccess ||
       cudaFuncSetAttribute(vo_median_x, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            med_smem) != cudaSuccess ||
@@ -428,10 +517,22 @@ extern "C" int tcb_stripe_vo_apply(tcb_stripe_vo *h, float *tomo, size_t pstride
                 "tcb_stripe_vo_apply: strides make rows overlap");
   cudaStream_t s = (cudaStream_t)stream;
   const int np = (int)h->nproj, nz = (int)h->nz, ni = (int)h->ni;
-  const int p2 = pow2_at_least(np), n2 = pow2_at_least(ni);
+  // at least a full warp of threads (the shuffle stages)
+  const int p2 = std::max(pow2_at_least(np), 128), n2 = pow2_at_least(ni);
   const dim3 cgrid(ceil_div(h->ni, 128), nz), pgrid(ceil_div(h->ni, 128), nz, 16);
   const int nd = (int)(0.5 * 0.1 * np);  // drop_ratio 0.1
   const int dsm = (int)(2 * h->ni * 4 + n2 * 4);
+  // sorts read the column-contiguous copy tt
+  auto sort_cols = [&]() {
+    const size_t zs = (size_t)ni * np;
+    if (sort_e(p2) == 4)
+      vo_sort_cols<4><<<dim3(ni, nz), p2 / 4, (size_t)p2 * 8, s>>>(h->tt, 1, zs, np, np, ni, p2,
+                                                                   h->srt, h->ids);
+    else
+      vo_sort_cols<8><<<dim3(ni, nz), p2 / 8, (size_t)p2 * 8, s>>>(h->tt, 1, zs, np, np, ni, p2,
+                                                                   h->srt, h->ids);
+  };
+  const dim3 tgrid(ceil_div(h->ni, 32), ceil_div(h->nproj, 32), nz), tblk(32, 8);
   auto median = [&](const float *in, float *outp, int R, int w) {
     const int nrun = (ni + VO_RUN - 1) / VO_RUN;
     const long long thr = (long long)nz * nrun * R;
@@ -448,35 +549,34 @@ extern "C" int tcb_stripe_vo_apply(tcb_stripe_vo *h, float *tomo, size_t pstride
     vo_dead_interp<<<pgrid, 128, 0, s>>>(tomo, pstride, zstride, np, ni, h->mask, h->nbr);
     TCB_LAUNCH_CHECK();
   }
-  // 2. large stripes
+  // 2. large stripes (on the column-contiguous copy)
   {
     StageTimer st("stripe_vo_sort", s);
-    vo_sort_cols<<<dim3(ni, nz), 512, (size_t)p2 * 8, s>>>(tomo, pstride, zstride, np, ni, p2,
-                                                          h->srt, h->ids);
+    vo_transpose<<<tgrid, tblk, 0, s>>>(tomo, pstride, zstride, h->tt, np, ni, 1);
+    sort_cols();
   }
   {
     StageTimer st("stripe_vo_median", s);
     median(h->srt, h->smooth, np, h->la);
   }
+  const size_t vals = (size_t)nz * ni * np;
   {
     StageTimer st("stripe_vo_large", s);
     vo_rank_means<<<ceil_div(h->nz * h->ni * 32, 256), 256, 0, s>>>(h->srt, h->smooth, np,
                                                                     nz * ni, nd, h->l1, h->l2);
     vo_detect<<<nz, 256, dsm, s>>>(h->l1, h->l2, ni, n2, h->snr, 0, h->fact, h->mask, h->nbr);
-    vo_divide<<<pgrid, 128, 0, s>>>(tomo, pstride, zstride, np, nz, ni, h->fact);
+    vo_divide_t<<<ceil_div(vals, 256), 256, 0, s>>>(h->tt, np, vals, h->fact);
   }
   {
     StageTimer st("stripe_vo_unsort", s);
-    vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(tomo, pstride, zstride, np,
-                                                                    ni, h->smooth, h->ids,
-                                                                    h->mask);
+    vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(h->tt, np, ni, h->smooth,
+                                                                    h->ids, h->mask);
   }
   TCB_LAUNCH_CHECK();
   // 3. small and medium stripes
   {
     StageTimer st("stripe_vo_sort", s);
-    vo_sort_cols<<<dim3(ni, nz), 512, (size_t)p2 * 8, s>>>(tomo, pstride, zstride, np, ni, p2,
-                                                          h->srt, h->ids);
+    sort_cols();
   }
   {
     StageTimer st("stripe_vo_median", s);
@@ -484,12 +584,12 @@ extern "C" int tcb_stripe_vo_apply(tcb_stripe_vo *h, float *tomo, size_t pstride
   }
   {
     StageTimer st("stripe_vo_unsort", s);
-    vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(tomo, pstride, zstride, np,
-                                                                    ni, h->smooth, h->ids,
-                                                                    nullptr);
+    vo_unsort<<<dim3(ceil_div(h->nproj, 128), ni, nz), 128, 0, s>>>(h->tt, np, ni, h->smooth,
+                                                                    h->ids, nullptr);
+    vo_transpose<<<tgrid, tblk, 0, s>>>(tomo, pstride, zstride, h->tt, np, ni, 0);
   }
   TCB_LAUNCH_CHECK();
-  count_launch(13);
+  count_launch(15);
   return TCB_OK;
 }
 
