@@ -1070,7 +1070,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
             const int *__restrict__ tile_order, int ntiles, int nitems,
             const __half *__restrict__ ghi, const __half *__restrict__ glo,
             const unsigned *__restrict__ amax_bits, float2 *__restrict__ grid, Geom geo,
-            int ntx, size_t rows, int *__restrict__ err) {
+            int ntx, size_t rows, int skip_empty, int *__restrict__ err) {
   using namespace tcb::tc;
   using Cfg = SwCfg<NN, SPLIT>;
   constexpr int NST = Cfg::NST;
@@ -1277,10 +1277,11 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         if (lane == 0) mbar_arrive(&tfree[buf]);
       }
       if (!ok) break;
-      // this thread's cell, pairs z0 + hf * HC / 2 ...
+      // this thread's cell, pairs z0 + hf * HC / 2 ... (a tile no sample
+      // reaches keeps the zeros the grid holds there when skip_empty is set)
       const int ix0 = (tile % ntx) * SW_TX, iy0 = (tile / ntx) * SW_TY;
       const int cx = ix0 + (m % SW_TX), cy = iy0 + (m / SW_TX);
-      if (cx < geo.twon && cy < geo.twon) {
+      if (cx < geo.twon && cy < geo.twon && !(skip_empty && nch == 0)) {
         const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
         const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
         const int pz0 = (it / ntiles) * (NN / 2) + hf * (HC / 2);
@@ -1630,6 +1631,10 @@ struct tcb_fourierrec {
   int sw_nn = 0;                   // comps per CTA (64 or 128); 0 = not built
   int sw_ntx = 0, sw_ntiles = 0, sw_zgroups = 0;
   long long sw_chunks = 0;
+  int sw_nonempty = 0;     // tiles with at least one listed sample
+  // the grid cells outside every sample footprint hold zeros (set once; only
+  // the gridding writes the grid when the inverse FFT is the library's own)
+  bool grid_zeroed = false;
   bool sw_lo = false;              // lo images present (fp32 mode)
   long long *sw_toffs = nullptr;
   int *sw_tlist = nullptr;
@@ -1760,13 +1765,23 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
       TCB_LAUNCH_CHECK();
       count_launch(1 + h->sw_zgroups);
     }
+    // with the library's own inverse FFT (which reads the grid, never writes
+    // it) the cells no sample reaches are zeroed once and never rewritten
+    const bool skip = h->own_n != 0;
+    if (skip && !h->grid_zeroed) {
+      TCB_CUDA(cudaMemsetAsync(h->grid, 0, h->nz * (size_t)geo.twon * geo.twon * sizeof(float2), s));
+      h->grid_zeroed = true;
+    }
     // algorithmic bytes: every weight image and its sample rows streamed once,
-    // the spectrum operand read once, the grid written once; FLOPs: the
-    // products the tensor cores form (3 per term in fp32 mode)
+    // the spectrum operand read once, the grid cells of the tiles written
+    // (all tiles, or those samples reach); FLOPs: the products the tensor
+    // cores form (3 per term in fp32 mode)
     const double C = (double)h->sw_chunks;
+    const double gcells = skip ? (double)h->sw_nonempty * SW_M
+                               : (double)geo.twon * geo.twon;
     StageTimer st("fr_gather_sw", s,
                   h->sw_zgroups * C * (SW_WIMG * nimg + SW_K * sizeof(int)) + vbytes +
-                      (double)h->nz * geo.twon * geo.twon * sizeof(float2),
+                      (double)h->nz * gcells * sizeof(float2),
                   h->sw_zgroups * C * 2.0 * SW_M * h->sw_nn * SW_K * (h->sw_lo ? 3.0 : 1.0));
     // persistent: one CTA per SM (all of TMEM, ~193 KB of shared memory)
     const int nitems = h->sw_ntiles * h->sw_zgroups;
@@ -1774,7 +1789,8 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
 #define FR_SW(NN_, SPLIT_)                                                                 \
   grid_sw<NN_, SPLIT_><<<grd, WS_THREADS, SwCfg<NN_, SPLIT_>::SMEM, s>>>(                  \
       h->sw_whi, h->sw_wlo, h->sw_vidx, h->sw_tile_chunks, h->sw_order, h->sw_ntiles,       \
-      nitems, h->sw_ghi, h->sw_glo, h->amax, h->grid, geo, h->sw_ntx, rows, h->tc_err)
+      nitems, h->sw_ghi, h->sw_glo, h->amax, h->grid, geo, h->sw_ntx, rows, skip ? 1 : 0,   \
+      h->tc_err)
     if (h->sw_nn == 128) {
       if (h->sw_lo) FR_SW(128, true); else FR_SW(128, false);
     } else {
@@ -2018,6 +2034,8 @@ int sw_build(tcb_fourierrec *h, bool with_lo) {
   h->sw_ntiles = nt;
   h->sw_zgroups = zgroups;
   h->sw_chunks = C;
+  h->sw_nonempty = 0;
+  for (int t = 0; t < nt; t++) h->sw_nonempty += tch[t].y > 0;
   h->sw_lo = with_lo;
   return TCB_OK;
 }
