@@ -1,5 +1,9 @@
 """GPU parity of projection rotation (tcb_rotate_proj) with the oracle's
-restatement of scipy.ndimage's geometric transform (bit for bit), and of
+restatement of scipy.ndimage's geometric transform (bit for bit against
+scipy's rotate; the reference calls cupyx's rotate, a separate NVRTC-compiled
+implementation that may fuse multiply-adds and is not installed here, so
+agreement with the reference's own call is bounded by the 1e-5
+reconstruction parity below, not shown bit for bit), and of
 reconstructions with rotate_proj_angle set: the step driver (whole
 projections) and GPURec.recon_all (each sinogram chunk, as the reference's
 recon_all runs proc_proj) against the oracle's pre-processing fed to the
