@@ -385,7 +385,7 @@ def run_try(a, dev):
     outs = {}
     for prec in ("float32", "mixed"):
         tune = autotune(n, P, theta, center, shifts, data, d0, f0, fbp_filter="parzen",
-                        precision=prec, candidates=[(32, 8), (32, 16), (64, 16)], reps=1)
+                        precision=prec, candidates=[(32, 16), (64, 16), (128, 16)], reps=1)
         sw = TryCenterSweep(n, P, theta, center, shifts, "parzen", prec, tune["ncz"],
                             tune["pairs_per_block"], dev)
         sw.load(data, d0, f0)
