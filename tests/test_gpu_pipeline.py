@@ -331,9 +331,11 @@ def test_recon_try_mixed_matches_fp32(cuda, c1):
         GPURec(ArrayReader(data, dark, flat, theta=theta), writer).recon_try()
         res[dtype] = {k: v.cpu() for k, v in writer.tries.items()}
     assert res["float32"].keys() == res["mixed"].keys() and len(res["mixed"]) == 8
+    # mixed precision grids with fp16 operands and keeps the oversampled grid
+    # in fp16 (per-tile scales): within half the 1e-3 mixed budget of fp32
     for k in res["mixed"]:
         err = rel_l2(res["mixed"][k], res["float32"][k])
-        assert err < 1e-4, (k, err)
+        assert err < 5e-4, (k, err)
 
 
 def test_c1_mixed_fp16_output_vs_fp64_oracle(cuda, c1):

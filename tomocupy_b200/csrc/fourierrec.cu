@@ -1070,17 +1070,22 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
             const int *__restrict__ tile_order, int ntiles, int nitems,
             const __half *__restrict__ ghi, const __half *__restrict__ glo,
             const unsigned *__restrict__ amax_bits, float2 *__restrict__ grid, Geom geo,
-            int ntx, size_t rows, int skip_empty, int *__restrict__ err) {
+            int ntx, size_t rows, int skip_empty, float *__restrict__ tscale,
+            int *__restrict__ err) {
   using namespace tcb::tc;
   using Cfg = SwCfg<NN, SPLIT>;
   constexpr int NST = Cfg::NST;
+  // fp16 grid (tscale != null): per-warp maxima of each pair over a tile, two
+  // item parities x two column halves x 8 warps
+  __shared__ float s_red[2][2][8][32];
   extern __shared__ uint8_t swsm_raw[];
   uint8_t *sm = swsm_raw + ((1024u - (smem_u32(swsm_raw) & 1023u)) & 1023u);
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + NST * Cfg::STAGE);
   uint64_t *empty = full + NST;
   uint64_t *pfull = empty + NST;  // TMEM buffer b holds a finished partial sum (tile)
   uint64_t *tfree = pfull + 2;    // TMEM buffer b was read by the accumulator warps
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tfree + 2);
+  uint64_t *tred = tfree + 2;     // fp16 grid: the 8 warps of column half h posted maxima
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tred + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int G = gridDim.x;
 
@@ -1092,6 +1097,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     for (int i = 0; i < 2; i++) {
       mbar_init(&pfull[i], 1);
       mbar_init(&tfree[i], WS_ACC_WARPS);
+      mbar_init(&tred[i], WS_ACC_WARPS / 2);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -1248,6 +1254,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     const float unsc = ldexpf(1.f, ex - 14) / SW_WSCALE;
     float acc[HC];
     long long gp = 0;
+    long long rc = 0;  // fp16 grid: tiles whose maxima this half reduced
     int it = blockIdx.x;
     int tile = it < nitems ? tile_order[it % ntiles] : 0;
     for (; it < nitems && ok; it += G) {
@@ -1281,12 +1288,49 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       // reaches keeps the zeros the grid holds there when skip_empty is set)
       const int ix0 = (tile % ntx) * SW_TX, iy0 = (tile / ntx) * SW_TY;
       const int cx = ix0 + (m % SW_TX), cy = iy0 + (m / SW_TX);
-      if (cx < geo.twon && cy < geo.twon && !(skip_empty && nch == 0)) {
-        const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
-        const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
-        const int pz0 = (it / ntiles) * (NN / 2) + hf * (HC / 2);
+      const bool store = !(skip_empty && nch == 0);
+      const int sx = 1 - 2 * ((cx + M + 1) % 2), sy = 1 - 2 * ((cy + M + 1) % 2);
+      const float sgn = (float)(sx * sy) * geo.coeff0 * (geo.scale * unsc);
+      const int pz0 = (it / ntiles) * (NN / 2) + hf * (HC / 2);
+      const size_t plane = (size_t)geo.twon * geo.twon;
+      if (tscale != nullptr) {
+        // fp16 grid (every tile lies inside the grid): each pair's values of
+        // the tile scaled by a power of two that puts their maximum |value|
+        // in [2^13, 2^14); the inverse scale goes to tscale[pair][tile]
+        if (store) {
+          const int par = (int)(rc & 1);
+          float mine = 0.f;  // lane j: this warp's maximum of pair j
+#pragma unroll
+          for (int j = 0; j < HC / 2; j++) {
+            const float a = fmaxf(fabsf(acc[2 * j]), fabsf(acc[2 * j + 1])) * fabsf(sgn);
+            const unsigned r = __reduce_max_sync(0xffffffffu, __float_as_uint(a));
+            if (lane == j) mine = __uint_as_float(r);
+          }
+          s_red[par][hf][warp & 7][lane] = mine;
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tred[hf]);
+          if (!warp_wait(&tred[hf], (uint32_t)(rc & 1))) {
+            ok = false;
+            break;
+          }
+          float mx = 0.f;
+#pragma unroll
+          for (int w = 0; w < 8; w++) mx = fmaxf(mx, s_red[par][hf][w][lane]);
+          int e = 0;
+          if (mx > 0.f) frexpf(mx, &e);
+          const float sc = mx > 0.f ? ldexpf(1.f, 14 - e) : 1.f;  // lane j: pair j
+          if ((warp & 7) == 0 && lane < HC / 2 && pz0 + lane < geo.nz)
+            tscale[(size_t)(pz0 + lane) * ntiles + tile] = mx > 0.f ? ldexpf(1.f, e - 14) : 0.f;
+          __half2 *hp0 = reinterpret_cast<__half2 *>(grid) + ((size_t)pz0 * geo.twon + cy) * geo.twon + cx;
+#pragma unroll
+          for (int j = 0; j < HC / 2; j++) {
+            const float f = sgn * __shfl_sync(0xffffffffu, sc, j);
+            if (pz0 + j < geo.nz) hp0[j * plane] = __floats2half2_rn(acc[2 * j] * f, acc[2 * j + 1] * f);
+          }
+          rc++;
+        }
+      } else if (cx < geo.twon && cy < geo.twon && store) {
         float2 *gp0 = grid + ((size_t)pz0 * geo.twon + cy) * geo.twon + cx;
-        const size_t plane = (size_t)geo.twon * geo.twon;
 #pragma unroll
         for (int j = 0; j < HC / 2; j++)
           if (pz0 + j < geo.nz) gp0[j * plane] = make_float2(acc[2 * j] * sgn, acc[2 * j + 1] * sgn);
@@ -1450,6 +1494,38 @@ __global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
   fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
 }
 
+// Pass 1 on an fp16 grid (mixed precision): cell (x, y) of pair z holds
+// value / tscale[z][tile(x, y)], tiles of 16 x 16 cells; the row is scaled
+// back to fp32 as it is read.
+template <int N, int GW = T1_GW>
+__global__ void __launch_bounds__(N / 16, (16384 / N < 16 ? 16384 / N : 16))
+    ifft_rows_first_h(const __half2 *__restrict__ hgrid, const float *__restrict__ tscale,
+                      float2 *__restrict__ t1, const float2 *__restrict__ tw) {
+  extern __shared__ float2 fsm[];
+  constexpr int n = N / 2;
+  constexpr int NTX = N / 16;
+  const size_t row = blockIdx.x;  // pair * N + y
+  const int y = (int)(row % N);
+  const size_t pair = row / N;
+  const __half2 *src = hgrid + row * N;
+  const float *srow = tscale + pair * (size_t)NTX * NTX + (size_t)(y / 16) * NTX;
+  float2 *dst = t1 + (row - y) * n + (size_t)y * GW;
+  // the row's NTX tile scales, staged once (N / 16 threads: one each)
+  __shared__ float s_sc[NTX];
+  s_sc[threadIdx.x] = __ldg(srow + threadIdx.x);
+  __syncthreads();
+  auto in = [src](int e) {
+    const float2 v = __half22float2(src[e]);
+    const float c = s_sc[e / 16];
+    return make_float2(v.x * c, v.y * c);
+  };
+  auto out = [dst](int o, float2 v) {
+    const unsigned x = (unsigned)(o - N / 4);
+    if (x < (unsigned)n) dst[(size_t)(x / GW) * N * GW + x % GW] = v;
+  };
+  fftk::ifft<N>(fsm, threadIdx.x, tw, in, out);
+}
+
 // Pass 2 (columns): CPC adjacent columns tx of t1 per block; the inverse
 // FFT along y keeps y' in [n/2 + 1, 3n/2 + 1) and applies deapodization and
 // the output layout (ty = y' - n/2 - 1).
@@ -1489,6 +1565,9 @@ cudaError_t rows_first_attrs(int csm) {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)rows_smem(N));
   if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ifft_rows_first_h<N, GW>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_smem(N));
+  if (e == cudaSuccess)
     e = cudaFuncSetAttribute(ifft_cols_deapod<N, float, GW>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
   if (e == cudaSuccess)
@@ -1501,10 +1580,14 @@ cudaError_t rows_first_attrs(int csm) {
 template <int N, int GW>
 void rows_first_launch(const float2 *grid, float2 *t1, const float2 *tw, const float4 *dtab,
                        void *f, bool half, const Geom &geo, int unpack, size_t nz, int cpc,
-                       cudaStream_t s) {
+                       const float *tscale, cudaStream_t s) {
   {
     StageTimer st("fr_ifft_rows", s);
-    ifft_rows_first<N, GW><<<(unsigned)(N * nz), N / 16, rows_smem(N), s>>>(grid, t1, tw);
+    if (tscale)
+      ifft_rows_first_h<N, GW><<<(unsigned)(N * nz), N / 16, rows_smem(N), s>>>(
+          reinterpret_cast<const __half2 *>(grid), tscale, t1, tw);
+    else
+      ifft_rows_first<N, GW><<<(unsigned)(N * nz), N / 16, rows_smem(N), s>>>(grid, t1, tw);
     count_launch();
   }
   StageTimer st("fr_ifft_cols_deapod", s);
@@ -1539,14 +1622,14 @@ cudaError_t own_fft_attrs() {
 template <int N>
 void own_fft_launch(const float2 *grid, float2 *t1, const float2 *tw, const float4 *dtab,
                     void *f, bool half, const Geom &geo, int unpack, size_t nz, int cpc,
-                    bool rows_first, int gw, cudaStream_t s) {
+                    bool rows_first, int gw, const float *tscale, cudaStream_t s) {
   if (rows_first) {
     if (gw == 4)
-      rows_first_launch<N, 4>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, s);
+      rows_first_launch<N, 4>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, tscale, s);
     else if (gw == 16)
-      rows_first_launch<N, 16>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, s);
+      rows_first_launch<N, 16>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, tscale, s);
     else
-      rows_first_launch<N, 8>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, s);
+      rows_first_launch<N, 8>(grid, t1, tw, dtab, f, half, geo, unpack, nz, cpc, tscale, s);
     return;
   }
   {
@@ -1632,9 +1715,12 @@ struct tcb_fourierrec {
   int sw_ntx = 0, sw_ntiles = 0, sw_zgroups = 0;
   long long sw_chunks = 0;
   int sw_nonempty = 0;     // tiles with at least one listed sample
-  // the grid cells outside every sample footprint hold zeros (set once; only
-  // the gridding writes the grid when the inverse FFT is the library's own)
-  bool grid_zeroed = false;
+  float *sw_tscale = nullptr;  // mixed: [pairs][tiles] inverse scales of the fp16 grid
+  // the format in which the grid cells outside every sample footprint hold
+  // zeros (0: not known, 1: fp32 grid, 2: fp16 grid); set once, then kept,
+  // because only the gridding writes the grid when the inverse FFT is the
+  // library's own
+  int grid_zero_fmt = 0;
   bool sw_lo = false;              // lo images present (fp32 mode)
   long long *sw_toffs = nullptr;
   int *sw_tlist = nullptr;
@@ -1682,6 +1768,8 @@ void fr_release(tcb_fourierrec *h) {
   cudaFree(h->sw_vidx);
   cudaFree(h->sw_ghi);
   cudaFree(h->sw_glo);
+  cudaFree(h->sw_tscale);
+  h->sw_tscale = nullptr;
   h->sw_toffs = nullptr;
   h->sw_tlist = nullptr;
   h->sw_tile_chunks = nullptr;
@@ -1740,6 +1828,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     StageTimer st("fr_fft1d", s);
     TCB_CUFFT(cufftExecC2C(h->plan1d, (cufftComplex *)gc, (cufftComplex *)gc, CUFFT_FORWARD));
   }
+  bool grid_h = false;  // the gridding writes an fp16 grid with per-tile scales
   if (h->grid_mode == TCB_GRID_TENSOR_FP32 || h->grid_mode == TCB_GRID_TENSOR_STREAM) {
     const size_t gtot = h->nz * h->nproj * h->n;
     const size_t rows = h->nproj * h->n;
@@ -1768,10 +1857,18 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     // with the library's own inverse FFT (which reads the grid, never writes
     // it) the cells no sample reaches are zeroed once and never rewritten
     const bool skip = h->own_n != 0;
-    if (skip && !h->grid_zeroed) {
+    // mixed precision read by the own rows-first FFT: the grid is stored in
+    // fp16, each pair of each tile scaled by its own power of two
+    grid_h = !h->sw_lo && skip && h->own_rows_first && h->sw_tscale != nullptr &&
+             geo.twon % SW_TX == 0;
+    const int fmt = grid_h ? 2 : 1;
+    if (skip && h->grid_zero_fmt != fmt) {
       TCB_CUDA(cudaMemsetAsync(h->grid, 0, h->nz * (size_t)geo.twon * geo.twon * sizeof(float2), s));
-      h->grid_zeroed = true;
+      if (grid_h)
+        TCB_CUDA(cudaMemsetAsync(h->sw_tscale, 0, h->nz * (size_t)h->sw_ntiles * sizeof(float), s));
+      h->grid_zero_fmt = fmt;
     }
+    if (!skip) h->grid_zero_fmt = 0;
     // algorithmic bytes: every weight image and its sample rows streamed once,
     // the spectrum operand read once, the grid cells of the tiles written
     // (all tiles, or those samples reach); FLOPs: the products the tensor
@@ -1781,7 +1878,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
                                : (double)geo.twon * geo.twon;
     StageTimer st("fr_gather_sw", s,
                   h->sw_zgroups * C * (SW_WIMG * nimg + SW_K * sizeof(int)) + vbytes +
-                      (double)h->nz * gcells * sizeof(float2),
+                      (double)h->nz * gcells * (grid_h ? sizeof(__half2) : sizeof(float2)),
                   h->sw_zgroups * C * 2.0 * SW_M * h->sw_nn * SW_K * (h->sw_lo ? 3.0 : 1.0));
     // persistent: one CTA per SM (all of TMEM, ~193 KB of shared memory)
     const int nitems = h->sw_ntiles * h->sw_zgroups;
@@ -1790,7 +1887,7 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
   grid_sw<NN_, SPLIT_><<<grd, WS_THREADS, SwCfg<NN_, SPLIT_>::SMEM, s>>>(                  \
       h->sw_whi, h->sw_wlo, h->sw_vidx, h->sw_tile_chunks, h->sw_order, h->sw_ntiles,       \
       nitems, h->sw_ghi, h->sw_glo, h->amax, h->grid, geo, h->sw_ntx, rows, skip ? 1 : 0,   \
-      h->tc_err)
+      grid_h ? h->sw_tscale : nullptr, h->tc_err)
     if (h->sw_nn == 128) {
       if (h->sw_lo) FR_SW(128, true); else FR_SW(128, false);
     } else {
@@ -1810,10 +1907,12 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
         gc, h->grid, h->tile_order, h->toffs, h->trec, h->amax, geo, h->tc_err);
     TCB_LAUNCH_CHECK();
     count_launch(2);
+    h->grid_zero_fmt = h->own_n ? 1 : 0;  // every cell written, fp32
   } else {
     StageTimer st("fr_gather", s);
     int rc;
     const size_t zb = h->zblock ? (size_t)h->zblock : 16;
+    h->grid_zero_fmt = h->own_n ? 1 : 0;  // every cell written, fp32
     if (h->nz >= 16 && zb >= 16) rc = launch_grid<16>(h, gc, s);
     else if (h->nz >= 8 && zb >= 8) rc = launch_grid<8>(h, gc, s);
     else if (h->nz >= 4 && zb >= 4) rc = launch_grid<4>(h, gc, s);
@@ -1826,13 +1925,14 @@ int fr_run(tcb_fourierrec *h, void *f, void *g, void *stream, int unpack) {
     const int cpc = h->own_cpc;
     const bool rf = h->own_rows_first;
     const int gw = h->t1_gw;
+    const float *ts = grid_h ? h->sw_tscale : nullptr;  // the gridding wrote an fp16 grid
     switch (h->own_n) {
-      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
-      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
-      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
-      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
-      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
-      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, s); break;
+      case 256: own_fft_launch<256>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, ts, s); break;
+      case 512: own_fft_launch<512>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, ts, s); break;
+      case 1024: own_fft_launch<1024>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, ts, s); break;
+      case 2048: own_fft_launch<2048>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, ts, s); break;
+      case 4096: own_fft_launch<4096>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, ts, s); break;
+      default: own_fft_launch<8192>(h->grid, h->t1, h->tw, h->dtab, f, half, geo, unpack, h->nz, cpc, rf, gw, ts, s); break;
     }
     TCB_LAUNCH_CHECK();
     return TCB_OK;
@@ -1999,6 +2099,9 @@ int sw_build(tcb_fourierrec *h, bool with_lo) {
     const size_t gb = (size_t)zgroups * rows * nn * sizeof(__half);
     if (cudaMalloc(&h->sw_ghi, gb) != cudaSuccess) return oom("fp16 spectrum");
   }
+  if (!with_lo && !h->sw_tscale &&
+      cudaMalloc(&h->sw_tscale, h->nz * (size_t)nt * sizeof(float)) != cudaSuccess)
+    return oom("fp16 grid scales");
   if (with_lo && !h->sw_glo) {
     const size_t gb = (size_t)zgroups * rows * nn * sizeof(__half);
     if (cudaMalloc(&h->sw_glo, gb) != cudaSuccess) return oom("fp16 spectrum");
